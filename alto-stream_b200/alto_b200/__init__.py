@@ -1,0 +1,371 @@
+"""alto_b200 -- Python host side of the B200 ALTO library.
+
+Mirrors the reference's operator interface for the hot path
+(jeewhanchoi/ALTO-stream, include/alto.hpp, include/cpd.hpp,
+src/streaming_cpd.cpp) over the C ABI in ``include/alto_b200.h``:
+
+* ``create_alto`` / ``init_salto`` + ``update_salto`` / ``destroy_alto``
+  (include/alto.hpp:151-604) -> :class:`AltoTensor`;
+* ``mttkrp_alto_par`` (include/alto.hpp:902) -> :func:`mttkrp_alto_par`
+  (accumulates into ``factors[target_mode]`` like the reference);
+* ``cpd_alto`` (include/cpd.hpp:47) -> :func:`cpd_alto`;
+* ``cpstream`` (src/streaming_cpd.cpp:26) -> :class:`CPStream`.
+
+The library is the CUDA build ``libalto_b200.so`` next to this file.  There
+is no CPU fallback: importing works anywhere, but every call that needs the
+library raises :class:`AltoError` when it is missing or no GPU is usable.
+Device buffers are torch CUDA tensors (torch is plumbing here: memory and
+streams); host buffers are numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, byref, c_char_p, c_double, c_int, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libalto_b200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_SPD, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
+F32, BF16, F64 = 0, 1, 2
+AUTO, ATOMIC, STAGED, STREAM, SORTED = range(5)
+UNCONSTRAINED, NONNEG, LASSO = range(3)
+FIT_REFERENCE, FIT_EXACT = 0, 1
+
+EXPORTED = [
+    "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
+    "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
+    "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
+    "alto_mttkrp_choose", "alto_mttkrp_host", "alto_cpd_als", "alto_stream_open",
+    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
+]
+
+
+class AltoError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"alto status {status}: {msg}")
+        self.status = status
+
+
+class alto_coo(ctypes.Structure):
+    _fields_ = [("nmodes", c_int), ("dims", POINTER(c_uint64)), ("nnz", c_uint64),
+                ("cidx", POINTER(c_void_p)), ("index_bytes", c_int), ("vals", c_void_p),
+                ("val_dtype", c_int), ("on_device", c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AltoError(ERR_CUDA, f"{LIB_PATH} is not built (run `make -C alto-stream_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.alto_status_string.restype = c_char_p
+        L.alto_last_error.restype = c_char_p
+        L.alto_kernel_launches.restype = c_uint64
+        for name in EXPORTED:
+            if name not in ("alto_status_string", "alto_last_error", "alto_kernel_launches", "alto_version"):
+                getattr(L, name).restype = c_int
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != OK:
+        L = lib()
+        raise AltoError(status, f"{L.alto_status_string(status).decode()}: {L.alto_last_error().decode()}")
+
+
+def kernel_launches():
+    return int(lib().alto_kernel_launches())
+
+
+def _stream_handle(stream):
+    if stream is None:
+        try:
+            import torch
+
+            if torch.cuda.is_available():
+                return c_void_p(torch.cuda.current_stream().cuda_stream)
+        except ImportError:
+            pass
+        return c_void_p(0)
+    if isinstance(stream, int):
+        return c_void_p(stream)
+    return c_void_p(stream.cuda_stream)
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+class _Coo:
+    """Holds an alto_coo and keeps its buffers alive."""
+
+    def __init__(self, dims, cidx, vals):
+        self.dims = np.ascontiguousarray(dims, dtype=np.uint64)
+        N = len(self.dims)
+        keep = []
+        ptrs = (c_void_p * N)()
+        if _is_torch(cidx) or (isinstance(cidx, (list, tuple)) and len(cidx) and _is_torch(cidx[0])):
+            cols = [cidx[m] for m in range(N)]
+            ib = cols[0].element_size()
+            for m, c in enumerate(cols):
+                c = c.contiguous()
+                keep.append(c)
+                ptrs[m] = c.data_ptr()
+            on_dev = 1
+            nnz = cols[0].numel()
+            v = vals.contiguous()
+            keep.append(v)
+            vptr = v.data_ptr()
+            vdt = F64 if v.element_size() == 8 else F32
+        else:
+            cidx = np.ascontiguousarray(cidx)
+            if cidx.dtype not in (np.uint64, np.int64, np.uint32, np.int32):
+                cidx = cidx.astype(np.uint64)
+            ib = cidx.dtype.itemsize
+            nnz = cidx.shape[1] if cidx.ndim == 2 else 0
+            for m in range(N):
+                row = np.ascontiguousarray(cidx[m])
+                keep.append(row)
+                ptrs[m] = row.ctypes.data
+            v = np.ascontiguousarray(vals)
+            if v.dtype not in (np.float64, np.float32):
+                v = v.astype(np.float64)
+            keep.append(v)
+            vptr = v.ctypes.data
+            vdt = F64 if v.dtype == np.float64 else F32
+            on_dev = 0
+        self.keep = keep
+        self.ptrs = ptrs
+        self.c = alto_coo(N, self.dims.ctypes.data_as(POINTER(c_uint64)), nnz,
+                          ctypes.cast(ptrs, POINTER(c_void_p)), ib, c_void_p(vptr), vdt, on_dev)
+        self.nnz = nnz
+
+
+def compute_masks(dims, key_bits=128):
+    """setup_packed_alto on the host (no GPU needed): (masks [N, 2], alto_mask [2], bits)."""
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    N = len(dims)
+    masks = np.zeros(2 * N, np.uint64)
+    am = np.zeros(2, np.uint64)
+    bits = c_int()
+    check(lib().alto_compute_masks(c_int(N), dims.ctypes.data_as(c_void_p), c_int(key_bits),
+                                   masks.ctypes.data_as(c_void_p), am.ctypes.data_as(c_void_p), byref(bits)))
+    return masks.reshape(N, 2), am, bits.value
+
+
+class AltoTensor:
+    """A device-resident ALTO tensor (the reference's AltoTensor<LIT>).
+
+    dims: mode lengths; cidx: [nmodes, nnz] 0-based indices (numpy host array
+    or torch CUDA tensor); vals: nnz values.  nprtn is the reference's
+    partition count (used for exported prtn_ptr / prtn_intervals);
+    stream_mode >= 0 marks the streaming mode (init_salto)."""
+
+    def __init__(self, dims, cidx, vals, nprtn=1, stream_mode=-1, key_bits=0, stream=None):
+        L = lib()
+        coo = _Coo(dims, cidx, vals)
+        h = c_void_p()
+        check(L.alto_tensor_create(byref(coo.c), c_int(key_bits), c_int(nprtn), c_int(stream_mode),
+                                   _stream_handle(stream), byref(h)))
+        self.h = h
+        self._refresh()
+
+    def _refresh(self):
+        L = lib()
+        n = c_int()
+        dims = (c_uint64 * 8)()
+        nnz = c_uint64()
+        kb, ab, np_, sm = c_int(), c_int(), c_int(), c_int()
+        check(L.alto_tensor_info(self.h, byref(n), dims, byref(nnz), byref(kb), byref(ab), byref(np_), byref(sm)))
+        self.nmodes = n.value
+        self.dims = np.array(dims[: n.value], np.uint64)
+        self.nnz = nnz.value
+        self.key_bits = kb.value
+        self.alto_bits = ab.value
+        self.nprtn = np_.value
+        self.stream_mode = sm.value
+
+    def update(self, dims, cidx, vals, nprtn=1, stream=None):
+        """update_salto: re-encode a new slice into this tensor."""
+        coo = _Coo(dims, cidx, vals)
+        check(lib().alto_tensor_update(self.h, byref(coo.c), c_int(nprtn), _stream_handle(stream)))
+        self._refresh()
+
+    def export(self):
+        N, nnz, P = self.nmodes, self.nnz, self.nprtn
+        masks = np.zeros(2 * N, np.uint64)
+        am = np.zeros(2, np.uint64)
+        idx = np.zeros(2 * max(nnz, 1), np.uint64)
+        vals = np.zeros(max(nnz, 1), np.float64)
+        perm = np.zeros(max(nnz, 1), np.uint64)
+        pp = np.zeros(P + 1, np.uint64)
+        iv = np.zeros(2 * P * N, np.uint64)
+        p = lambda a: a.ctypes.data_as(c_void_p)
+        check(lib().alto_tensor_export(self.h, p(masks), p(am), p(idx), p(vals), p(perm), p(pp), p(iv)))
+        return dict(masks=masks.reshape(N, 2), alto_mask=am, idx=idx[: 2 * nnz].reshape(nnz, 2),
+                    vals=vals[:nnz], perm=perm[:nnz], prtn_ptr=pp, intervals=iv.reshape(P, N, 2))
+
+    def device_bytes(self):
+        b = c_uint64()
+        check(lib().alto_tensor_device_bytes(self.h, byref(b)))
+        return b.value
+
+    def mttkrp(self, mode, factors, rank, out=None, accumulate=False, variant=AUTO, stream=None):
+        """MTTKRP of `mode` into `out` (float32 torch CUDA tensor, allocated if None)."""
+        import torch
+
+        N = self.nmodes
+        if out is None:
+            ref = next(f for i, f in enumerate(factors) if i != mode)
+            out = torch.empty((int(self.dims[mode]), rank), dtype=torch.float32, device=ref.device)
+            accumulate = False
+        dt = None
+        ptrs = (c_void_p * N)()
+        for m in range(N):
+            if m == mode:
+                ptrs[m] = None
+                continue
+            f = factors[m]
+            if not f.is_contiguous():
+                raise ValueError("factor matrices must be contiguous")
+            fdt = BF16 if f.dtype == torch.bfloat16 else F32
+            if f.dtype not in (torch.float32, torch.bfloat16):
+                raise ValueError("factors must be float32 or bfloat16")
+            if dt is not None and fdt != dt:
+                raise ValueError("all factors must share one dtype")
+            dt = fdt
+            ptrs[m] = f.data_ptr()
+        if out.dtype != torch.float32 or not out.is_contiguous():
+            raise ValueError("out must be a contiguous float32 tensor")
+        check(lib().alto_mttkrp_variant_run(self.h, c_int(mode), ptrs, c_int(dt), c_int(rank),
+                                            c_void_p(out.data_ptr()), c_int(1 if accumulate else 0),
+                                            c_int(variant), _stream_handle(stream)))
+        return out
+
+    def choose_variant(self, mode, rank, fdtype=F32):
+        v = c_int()
+        check(lib().alto_mttkrp_choose(self.h, c_int(mode), c_int(rank), c_int(fdtype), byref(v)))
+        return v.value
+
+    def mttkrp_host(self, mode, factors, rank, stream=None):
+        """The reference calling convention on host float64 arrays:
+        factors[mode] is accumulated into, in place."""
+        arrs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+        for a, f in zip(arrs, factors):
+            if a is not f:
+                raise ValueError("host factors must be C-contiguous float64 arrays")
+        ptrs = (POINTER(c_double) * self.nmodes)(*[a.ctypes.data_as(POINTER(c_double)) for a in arrs])
+        check(lib().alto_mttkrp_host(self.h, c_int(mode), ptrs, c_int(rank), _stream_handle(stream)))
+        return factors
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().alto_tensor_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------- reference-named mirrors
+
+def create_alto(dims, cidx, vals, nprtn=1, key_bits=0, stream=None):
+    """create_alto (include/alto.hpp:436): build the ALTO tensor."""
+    return AltoTensor(dims, cidx, vals, nprtn=nprtn, stream_mode=-1, key_bits=key_bits, stream=stream)
+
+
+def init_salto(dims, cidx, vals, max_nprtn, stream_mode, key_bits=0, stream=None):
+    """init_salto + the first update_salto (include/alto.hpp:151-299)."""
+    return AltoTensor(dims, cidx, vals, nprtn=max_nprtn, stream_mode=stream_mode, key_bits=key_bits,
+                      stream=stream)
+
+
+def update_salto(dims, cidx, vals, at, nprtn=1, stream=None):
+    at.update(dims, cidx, vals, nprtn=nprtn, stream=stream)
+    return at
+
+
+def destroy_alto(at):
+    at.close()
+
+
+def mttkrp_alto_par(target_mode, factors, rank, at, stream=None):
+    """mttkrp_alto_par (include/alto.hpp:902): accumulates the MTTKRP of
+    target_mode into factors[target_mode] (torch float32 CUDA tensors)."""
+    at.mttkrp(target_mode, factors, rank, out=factors[target_mode], accumulate=True, stream=stream)
+    return factors[target_mode]
+
+
+def cpd_alto(at, U, lam, rank, max_iters, epsilon, fit_mode=FIT_REFERENCE, storage=F32, stream=None):
+    """cpd_alto (include/cpd.hpp:47): CP-ALS on the device.
+
+    U: list of host float64 arrays (dims[n] x rank), lam: host float64
+    (rank); both hold the initial model and are returned updated (copies).
+    Returns (U, lam, fits, iterations)."""
+    Us = [np.array(u, dtype=np.float64, copy=True, order="C") for u in U]
+    lam = np.array(lam, dtype=np.float64, copy=True)
+    fits = np.zeros(max(max_iters, 1), np.float64)
+    it = c_int()
+    ptrs = (POINTER(c_double) * len(Us))(*[u.ctypes.data_as(POINTER(c_double)) for u in Us])
+    check(lib().alto_cpd_als(at.h, c_int(rank), ptrs, lam.ctypes.data_as(POINTER(c_double)),
+                             c_int(max_iters), c_double(epsilon), c_int(fit_mode), c_int(storage),
+                             fits.ctypes.data_as(POINTER(c_double)), byref(it), _stream_handle(stream)))
+    return Us, lam, fits[: it.value], it.value
+
+
+class CPStream:
+    """A CP-stream session (cpstream, src/streaming_cpd.cpp:26) whose model,
+    Grams and ADMM state stay on the device between time batches."""
+
+    def __init__(self, nmodes, stream_mode, rank, constraint=UNCONSTRAINED, forgetting=0.99,
+                 max_inner=10, epsilon=1e-5, stream=None):
+        h = c_void_p()
+        check(lib().alto_stream_open(c_int(nmodes), c_int(stream_mode), c_int(rank), c_int(constraint),
+                                     c_double(forgetting), c_int(max_inner), c_double(epsilon),
+                                     _stream_handle(stream), byref(h)))
+        self.h = h
+        self.nmodes = nmodes
+        self.stream_mode = stream_mode
+        self.rank = rank
+
+    def push(self, dims, cidx, vals, init_vals=None):
+        """Process one time batch; init_vals feeds the rows the model gains."""
+        coo = _Coo(dims, cidx, vals)
+        iv = np.ascontiguousarray(init_vals if init_vals is not None else np.zeros(0), dtype=np.float64)
+        inner = c_int()
+        check(lib().alto_stream_push(self.h, byref(coo.c), iv.ctypes.data_as(c_void_p), c_uint64(len(iv)),
+                                     byref(inner)))
+        return inner.value
+
+    def factor(self, mode, max_rows):
+        out = np.zeros((max(max_rows, 1), self.rank), np.float64)
+        rows = c_uint64()
+        check(lib().alto_stream_factor(self.h, c_int(mode), out.ctypes.data_as(c_void_p), byref(rows)))
+        return out[: rows.value]
+
+    def lam(self):
+        out = np.zeros(self.rank, np.float64)
+        check(lib().alto_stream_lambda(self.h, out.ctypes.data_as(c_void_p)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().alto_stream_close(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,660 @@
+// ALTO encoding on the device: linearisation, radix sort, line layout and
+// partition intervals.
+//
+// Reference behaviour (jeewhanchoi/ALTO-stream):
+//   setup_packed_alto(LSB_FIRST, SHORT_FIRST)  include/alto.hpp:955-1057
+//   linearisation (PDEP per mode)              include/alto.hpp:513-533, 239-252
+//   sort_alto (std::sort by key)               include/alto.hpp:1066-1090
+//   ALT_PEXT re-encoding                       include/alto.hpp:541-573
+//   prtn_alto (partitions, intervals)          include/alto.hpp:1128-1226
+//
+// The device pipeline: (1) every nonzero's bit-interleaved key is built by
+// depositing each mode index into its mask bits; (2) an LSD radix sort
+// (8-bit digits, stable, over only the bits the masks use) orders keys with
+// the input position as payload -- keys are unique for unique coordinates,
+// so the order equals std::sort's; (3) one pass extracts each mode's index
+// from the sorted key, packs it into the mode-contiguous line key and
+// gathers the value; (4) per-tile and per-partition interval reductions.
+#include <algorithm>
+#include <cstring>
+
+#include "alto_internal.cuh"
+
+namespace alto {
+
+// ------------------------------------------------------- host mask setup
+
+static int bits_for(uint64_t dim) {
+  if (dim <= 1) return 0;  // clz(0) = 64 on LZCNT hardware: a length-1 mode takes no bits
+  return 64 - __builtin_clzll(dim - 1);
+}
+
+// setup_packed_alto, include/alto.hpp:955-1057: modes ordered by bit count
+// (stable), bits dealt LSB first round-robin over the modes still active at
+// each level.  Returns the total bits or -1 when they exceed max_bits.
+int setup_masks(int nmodes, const uint64_t* dims, int max_bits, Key2* masks, Key2* alto_mask,
+                int* bits) {
+  int order[ALTO_MAX_MODES];
+  int total = 0;
+  for (int n = 0; n < nmodes; ++n) {
+    bits[n] = bits_for(dims[n]);
+    order[n] = n;
+    total += bits[n];
+    masks[n] = {0, 0};
+  }
+  if (total > max_bits) return -1;
+  std::stable_sort(order, order + nmodes, [&](int a, int b) { return bits[a] < bits[b]; });
+  int shift = 0;
+  for (int level = 0;; ++level) {
+    bool any = false;
+    for (int k = 0; k < nmodes; ++k) {
+      int n = order[k];
+      if (level < bits[n]) {
+        if (shift < 64)
+          masks[n].lo |= 1ull << shift;
+        else
+          masks[n].hi |= 1ull << (shift - 64);
+        ++shift;
+        any = true;
+      }
+    }
+    if (!any) break;
+  }
+  *alto_mask = {0, 0};
+  for (int n = 0; n < nmodes; ++n) {
+    alto_mask->lo |= masks[n].lo;
+    alto_mask->hi |= masks[n].hi;
+  }
+  return total;
+}
+
+// ------------------------------------------------------------- kernels
+
+struct MaskSet {
+  int nmodes;
+  uint64_t lo[ALTO_MAX_MODES];
+  uint64_t hi[ALTO_MAX_MODES];
+};
+
+// PDEP: scatter the low bits of x into the set bits of (mlo, mhi).
+__device__ __forceinline__ void deposit(uint64_t x, uint64_t mlo, uint64_t mhi, uint64_t& klo,
+                                        uint64_t& khi) {
+  while (mlo) {
+    int b = __ffsll((long long)mlo) - 1;
+    klo |= (x & 1ull) << b;
+    x >>= 1;
+    mlo &= mlo - 1;
+  }
+  while (mhi) {
+    int b = __ffsll((long long)mhi) - 1;
+    khi |= (x & 1ull) << b;
+    x >>= 1;
+    mhi &= mhi - 1;
+  }
+}
+
+// PEXT: gather the bits of (klo, khi) selected by (mlo, mhi) into the low bits.
+__device__ __forceinline__ uint64_t extract(uint64_t klo, uint64_t khi, uint64_t mlo,
+                                            uint64_t mhi) {
+  uint64_t r = 0;
+  int k = 0;
+  while (mlo) {
+    int b = __ffsll((long long)mlo) - 1;
+    r |= ((klo >> b) & 1ull) << k;
+    ++k;
+    mlo &= mlo - 1;
+  }
+  while (mhi) {
+    int b = __ffsll((long long)mhi) - 1;
+    r |= ((khi >> b) & 1ull) << k;
+    ++k;
+    mhi &= mhi - 1;
+  }
+  return r;
+}
+
+struct CooPtrs {
+  const void* cidx[ALTO_MAX_MODES];
+};
+
+// Key of nonzero i = OR over modes of PDEP(cidx[m][i], mask[m]).
+template <int IB>
+__global__ void linearize_kernel(CooPtrs coo, MaskSet ms, uint32_t nnz, uint64_t* __restrict__ klo,
+                                 uint64_t* __restrict__ khi, uint32_t* __restrict__ perm) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = 0;
+#pragma unroll
+    for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+      if (m < ms.nmodes) {
+        uint64_t x = IB == 8 ? ((const uint64_t*)coo.cidx[m])[i]
+                             : (uint64_t)((const uint32_t*)coo.cidx[m])[i];
+        deposit(x, ms.lo[m], ms.hi[m], lo, hi);
+      }
+    }
+    klo[i] = lo;
+    if (khi) khi[i] = hi;
+    perm[i] = i;
+  }
+}
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+__device__ __forceinline__ uint32_t digit_of(const uint64_t* klo, const uint64_t* khi, uint32_t i,
+                                             int shift) {
+  uint64_t w = shift >= 64 ? khi[i] : klo[i];
+  return (uint32_t)(w >> (shift & 63)) & (kRadix - 1);
+}
+
+// Per-tile digit histogram, written digit-major: counts[d * ntiles + tile].
+__global__ void __launch_bounds__(kSortThreads)
+    radix_hist_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
+                      uint32_t n, int shift, uint32_t ntiles, uint32_t* __restrict__ counts) {
+  __shared__ uint32_t hist[kRadix];
+  for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0;
+  __syncthreads();
+  uint32_t base = blockIdx.x * kSortTile;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    uint32_t i = base + r * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&hist[digit_of(klo, khi, i, shift)], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+    counts[(size_t)d * ntiles + blockIdx.x] = hist[d];
+}
+
+// Stable scatter of one tile: elements are ranked in index order, round by
+// round (round r holds elements base + r*256 + thread), with per-warp
+// digit counts combined in warp order and a running per-digit count.
+__global__ void __launch_bounds__(kSortThreads)
+    radix_scatter_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
+                         const uint32_t* __restrict__ pin, uint32_t n, int shift,
+                         uint32_t ntiles, const uint32_t* __restrict__ offsets,
+                         uint64_t* __restrict__ olo, uint64_t* __restrict__ ohi,
+                         uint32_t* __restrict__ pout) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t warp_cnt[kWarps][kRadix];
+  __shared__ uint32_t running[kRadix];
+  __shared__ uint32_t gbase[kRadix];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int d = tid; d < kRadix; d += kSortThreads) {
+    running[d] = 0;
+    gbase[d] = offsets[(size_t)d * ntiles + blockIdx.x];
+  }
+  uint32_t base = blockIdx.x * kSortTile;
+  for (int r = 0; r < kSortItems; ++r) {
+    for (int d = tid; d < kRadix; d += kSortThreads)
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) warp_cnt[w][d] = 0;
+    __syncthreads();
+    uint32_t i = base + r * kSortThreads + tid;
+    bool valid = i < n;
+    uint32_t d = 0, lane_rank = 0;
+    uint64_t vlo = 0, vhi = 0;
+    uint32_t vp = 0;
+    unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      vlo = klo[i];
+      vhi = khi ? khi[i] : 0;
+      vp = pin[i];
+      d = (uint32_t)((shift >= 64 ? vhi : vlo) >> (shift & 63)) & (kRadix - 1);
+      unsigned peers = __match_any_sync(vmask, d);
+      lane_rank = __popc(peers & ((1u << lane) - 1));
+      if (lane_rank == 0) warp_cnt[warp][d] = __popc(peers);
+    }
+    __syncthreads();
+    for (int dd = tid; dd < kRadix; dd += kSortThreads) {
+      uint32_t run = running[dd];
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        uint32_t c = warp_cnt[w][dd];
+        warp_cnt[w][dd] = run;
+        run += c;
+      }
+      running[dd] = run;
+    }
+    __syncthreads();
+    if (valid) {
+      uint32_t dst = gbase[d] + warp_cnt[warp][d] + lane_rank;
+      olo[dst] = vlo;
+      if (ohi) ohi[dst] = vhi;
+      pout[dst] = vp;
+    }
+    __syncthreads();
+  }
+}
+
+// Sorted interleaved keys -> mode-contiguous line keys, values gathered by
+// input position (float64 or float32 input, stored float32).
+template <typename VT>
+__global__ void layout_kernel(const uint64_t* __restrict__ slo, const uint64_t* __restrict__ shi,
+                              const uint32_t* __restrict__ sperm, const VT* __restrict__ vin,
+                              MaskSet ms, LineDecode dec, uint32_t nnz, uint64_t* __restrict__ llo,
+                              void* __restrict__ lhi, float* __restrict__ vout,
+                              uint32_t* __restrict__ perm_out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    uint64_t klo = slo[i], khi = shi ? shi[i] : 0;
+    uint64_t lo = 0, hi = 0;
+#pragma unroll
+    for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+      if (m < ms.nmodes) {
+        uint64_t x = extract(klo, khi, ms.lo[m], ms.hi[m]);
+        int p = dec.pos[m];
+        if (p >= 64) {
+          hi |= x << (p - 64);
+        } else {
+          lo |= x << p;
+          if (p > 0) hi |= x >> (64 - p);
+        }
+      }
+    }
+    llo[i] = lo;
+    if (dec.hi_words == 1) ((uint32_t*)lhi)[i] = (uint32_t)hi;
+    if (dec.hi_words == 2) ((uint64_t*)lhi)[i] = hi;
+    uint32_t p = sperm[i];
+    vout[i] = (float)vin[p];
+    perm_out[i] = p;
+  }
+}
+
+__device__ __forceinline__ uint64_t load_hi(const void* khi, int hi_words, uint32_t i) {
+  if (hi_words == 1) return ((const uint32_t*)khi)[i];
+  if (hi_words == 2) return ((const uint64_t*)khi)[i];
+  return 0;
+}
+
+// Per tile and mode: [min, max] row of the tile's nonzeros, stored as
+// (first row, row count).
+__global__ void __launch_bounds__(256)
+    tile_interval_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
+                         LineDecode dec, uint32_t nnz, uint32_t tile_nnz,
+                         uint32_t* __restrict__ tile_iv) {
+  __shared__ uint32_t smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
+  uint32_t lo_r[ALTO_MAX_MODES], hi_r[ALTO_MAX_MODES];
+#pragma unroll
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    lo_r[m] = 0xffffffffu;
+    hi_r[m] = 0;
+  }
+  uint32_t s = blockIdx.x * tile_nnz;
+  uint32_t e = min(s + tile_nnz, nnz);
+  for (uint32_t i = s + threadIdx.x; i < e; i += blockDim.x) {
+    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, i);
+#pragma unroll
+    for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+      if (m < dec.nmodes) {
+        uint32_t v = (uint32_t)line_field(lo, hi, dec.pos[m], dec.mask[m]);
+        lo_r[m] = min(lo_r[m], v);
+        hi_r[m] = max(hi_r[m], v);
+      }
+    }
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    if (m >= dec.nmodes) continue;
+    uint32_t a = lo_r[m], b = hi_r[m];
+    for (int o = 16; o; o >>= 1) {
+      a = min(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if (lane == 0) {
+      smin[m][warp] = a;
+      smax[m][warp] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < (unsigned)dec.nmodes) {
+    int m = threadIdx.x;
+    uint32_t a = 0xffffffffu, b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a = min(a, smin[m][w]);
+      b = max(b, smax[m][w]);
+    }
+    if (a > b) a = b;  // empty tile
+    tile_iv[((size_t)blockIdx.x * dec.nmodes + m) * 2] = a;
+    tile_iv[((size_t)blockIdx.x * dec.nmodes + m) * 2 + 1] = b - a + 1;
+  }
+}
+
+// prtn_alto's intervals (include/alto.hpp:1199-1226): one block per
+// partition; start = dims, stop = 0 sentinels, start clamped to stop when
+// the partition is empty.
+__global__ void __launch_bounds__(256)
+    prtn_interval_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
+                         LineDecode dec, const uint64_t* __restrict__ prtn_ptr,
+                         const uint64_t* __restrict__ dims, uint64_t* __restrict__ iv) {
+  __shared__ uint64_t smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
+  int p = blockIdx.x;
+  uint64_t s = prtn_ptr[p], e = prtn_ptr[p + 1];
+  uint64_t lo_r[ALTO_MAX_MODES], hi_r[ALTO_MAX_MODES];
+#pragma unroll
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    lo_r[m] = m < dec.nmodes ? dims[m] : 0;
+    hi_r[m] = 0;
+  }
+  for (uint64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
+    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, (uint32_t)i);
+#pragma unroll
+    for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+      if (m < dec.nmodes) {
+        uint64_t v = line_field(lo, hi, dec.pos[m], dec.mask[m]);
+        lo_r[m] = min(lo_r[m], v);
+        hi_r[m] = max(hi_r[m], v);
+      }
+    }
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    if (m >= dec.nmodes) continue;
+    uint64_t a = lo_r[m], b = hi_r[m];
+    for (int o = 16; o; o >>= 1) {
+      a = min(a, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)a, o));
+      b = max(b, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)b, o));
+    }
+    if (lane == 0) {
+      smin[m][warp] = a;
+      smax[m][warp] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < (unsigned)dec.nmodes) {
+    int m = threadIdx.x;
+    uint64_t a = dims[m], b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a = min(a, smin[m][w]);
+      b = max(b, smax[m][w]);
+    }
+    if (a > b) a = b;
+    iv[((size_t)p * dec.nmodes + m) * 2] = a;
+    iv[((size_t)p * dec.nmodes + m) * 2 + 1] = b;
+  }
+}
+
+// ------------------------------------------------------------ scan utility
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t wsum[kScanThreads / 32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  uint32_t wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    uint32_t c = wsum[w];
+    if (w < warp) wpre += c;
+    tot += c;
+  }
+  __syncthreads();
+  if (total) *total = tot;
+  return wpre + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_reduce_kernel(const uint32_t* __restrict__ data, size_t n, uint32_t* __restrict__ part) {
+  size_t base = (size_t)blockIdx.x * kScanTile;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    size_t i = base + (size_t)k * kScanThreads + threadIdx.x;
+    if (i < n) s += data[i];
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ uint32_t ws[kScanThreads / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) t += ws[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_apply_kernel(uint32_t* __restrict__ data, size_t n, const uint32_t* __restrict__ part) {
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < n ? data[base + k] : 0;
+    s += v[k];
+  }
+  uint32_t pre = block_exclusive_scan(s, nullptr) + (part ? part[blockIdx.x] : 0);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) data[base + k] = pre;
+    pre += v[k];
+  }
+}
+
+static alto_status scan_level(uint32_t* data, size_t n, uint32_t* scratch, cudaStream_t st) {
+  if (n <= (size_t)kScanTile) {
+    scan_apply_kernel<<<1, kScanThreads, 0, st>>>(data, n, nullptr);
+    ALTO_LAUNCHED();
+    return ALTO_OK;
+  }
+  size_t nb = (n + kScanTile - 1) / kScanTile;
+  uint32_t* part = scratch;
+  scan_reduce_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(data, n, part);
+  ALTO_LAUNCHED();
+  ALTO_TRY(scan_level(part, nb, scratch + nb, st));
+  scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(data, n, part);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+alto_status exclusive_scan_u32(uint32_t* data, size_t n, DevBuf& scratch, cudaStream_t st) {
+  if (n == 0) return ALTO_OK;
+  size_t need = 0, m = n;
+  while (m > (size_t)kScanTile) {
+    m = (m + kScanTile - 1) / kScanTile;
+    need += m;
+  }
+  ALTO_TRY(scratch.ensure((need + 1) * sizeof(uint32_t)));
+  return scan_level(data, n, scratch.as<uint32_t>(), st);
+}
+
+// -------------------------------------------------------------- pipeline
+
+static unsigned grid_for(uint64_t n, int threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b > 148ull * 64) b = 148ull * 64;
+  return (unsigned)(b ? b : 1);
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st) {
+  const int N = coo->nmodes;
+  const uint64_t nnz = coo->nnz;
+  t->nmodes = N;
+  t->nnz = nnz;
+  t->nprtn = nprtn;
+  for (int m = 0; m < N; ++m) t->dims[m] = coo->dims[m];
+  int total = setup_masks(N, t->dims, t->key_bits, t->masks, &t->alto_mask, t->mode_bits);
+  if (total < 0) {
+    set_error("index bits of the modes exceed the %d-bit key", t->key_bits);
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  t->alto_bits = total;
+
+  // line layout: fields in natural mode order (ALT_PEXT mode_pos)
+  LineDecode& dec = t->dec;
+  dec.nmodes = N;
+  int pos = 0;
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    dec.pos[m] = 0;
+    dec.mask[m] = 0;
+  }
+  for (int m = 0; m < N; ++m) {
+    dec.pos[m] = pos;
+    dec.mask[m] = t->mode_bits[m] >= 64 ? ~0ull : ((1ull << t->mode_bits[m]) - 1);
+    pos += t->mode_bits[m];
+  }
+  dec.hi_words = total <= 64 ? 0 : (total <= 96 ? 1 : 2);
+
+  // capacity of the per-nonzero arrays
+  uint64_t cap = std::max<uint64_t>(nnz, 1);
+  if (cap > t->cap || !t->klo.p) {
+    ALTO_TRY(t->klo.ensure(cap * 8));
+    ALTO_TRY(t->vals.ensure(cap * 4));
+    ALTO_TRY(t->perm.ensure(cap * 4));
+    t->cap = cap;
+  }
+  if (dec.hi_words) ALTO_TRY(t->khi.ensure(cap * (dec.hi_words == 1 ? 4 : 8)));
+
+  // construction scratch: two key/payload buffers, staged COO, counts
+  const bool two_words = total > 64;
+  const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
+  const int vbytes = coo->val_dtype == ALTO_F64 ? 8 : 4;
+  size_t off = 0;
+  size_t o_lo0 = off; off = align_up(off + cap * 8, 256);
+  size_t o_lo1 = off; off = align_up(off + cap * 8, 256);
+  size_t o_hi0 = off; off = align_up(off + (two_words ? cap * 8 : 0), 256);
+  size_t o_hi1 = off; off = align_up(off + (two_words ? cap * 8 : 0), 256);
+  size_t o_p0 = off; off = align_up(off + cap * 4, 256);
+  size_t o_p1 = off; off = align_up(off + cap * 4, 256);
+  size_t o_cnt = off; off = align_up(off + (size_t)kRadix * std::max<size_t>(tiles_sort, 1) * 4, 256);
+  size_t o_vals = off; off = align_up(off + (coo->on_device ? 0 : cap * vbytes), 256);
+  size_t o_cidx = off; off = align_up(off + (coo->on_device ? 0 : cap * coo->index_bytes * N), 256);
+  ALTO_TRY(t->scratch.ensure(off));
+  char* sb = t->scratch.as<char>();
+  uint64_t* klo[2] = {(uint64_t*)(sb + o_lo0), (uint64_t*)(sb + o_lo1)};
+  uint64_t* khi[2] = {two_words ? (uint64_t*)(sb + o_hi0) : nullptr,
+                      two_words ? (uint64_t*)(sb + o_hi1) : nullptr};
+  uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
+  uint32_t* counts = (uint32_t*)(sb + o_cnt);
+
+  CooPtrs cp{};
+  const void* vin = coo->vals;
+  if (coo->on_device) {
+    for (int m = 0; m < N; ++m) cp.cidx[m] = coo->cidx[m];
+  } else {
+    for (int m = 0; m < N; ++m) {
+      void* dst = sb + o_cidx + (size_t)m * cap * coo->index_bytes;
+      if (nnz)
+        ALTO_TRY_CUDA(cudaMemcpyAsync(dst, coo->cidx[m], nnz * coo->index_bytes,
+                                      cudaMemcpyHostToDevice, st));
+      cp.cidx[m] = dst;
+    }
+    if (nnz)
+      ALTO_TRY_CUDA(cudaMemcpyAsync(sb + o_vals, coo->vals, nnz * vbytes, cudaMemcpyHostToDevice, st));
+    vin = sb + o_vals;
+  }
+
+  MaskSet ms{};
+  ms.nmodes = N;
+  for (int m = 0; m < N; ++m) {
+    ms.lo[m] = t->masks[m].lo;
+    ms.hi[m] = t->masks[m].hi;
+  }
+
+  const uint32_t n32 = (uint32_t)nnz;
+  if (nnz) {
+    if (coo->index_bytes == 8)
+      linearize_kernel<8><<<grid_for(nnz, 256), 256, 0, st>>>(cp, ms, n32, klo[0], khi[0], pm[0]);
+    else
+      linearize_kernel<4><<<grid_for(nnz, 256), 256, 0, st>>>(cp, ms, n32, klo[0], khi[0], pm[0]);
+    ALTO_LAUNCHED();
+
+    // LSD radix sort over the used bits
+    int cur = 0;
+    const uint32_t ntiles = (uint32_t)tiles_sort;
+    for (int shift = 0; shift < total; shift += kRadixBits) {
+      radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], n32, shift, ntiles,
+                                                         counts);
+      ALTO_LAUNCHED();
+      ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, t->scan_scratch, st));
+      radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], pm[cur], n32, shift,
+                                                            ntiles, counts, klo[cur ^ 1],
+                                                            khi[cur ^ 1], pm[cur ^ 1]);
+      ALTO_LAUNCHED();
+      cur ^= 1;
+    }
+
+    if (coo->val_dtype == ALTO_F64)
+      layout_kernel<double><<<grid_for(nnz, 256), 256, 0, st>>>(
+          klo[cur], khi[cur], pm[cur], (const double*)vin, ms, dec, n32, t->klo.as<uint64_t>(),
+          t->khi.p, t->vals.as<float>(), t->perm.as<uint32_t>());
+    else
+      layout_kernel<float><<<grid_for(nnz, 256), 256, 0, st>>>(
+          klo[cur], khi[cur], pm[cur], (const float*)vin, ms, dec, n32, t->klo.as<uint64_t>(),
+          t->khi.p, t->vals.as<float>(), t->perm.as<uint32_t>());
+    ALTO_LAUNCHED();
+  }
+
+  // MTTKRP tiles and their intervals
+  t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
+  ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
+  if (t->ntiles) {
+    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, dec, n32,
+                                                    t->tile_nnz, t->tile_iv.as<uint32_t>());
+    ALTO_LAUNCHED();
+  }
+
+  // the reference's partitions
+  t->prtn_ptr.assign(nprtn + 1, 0);
+  uint64_t per = (nnz + nprtn - 1) / nprtn;
+  for (int p = 0; p < nprtn; ++p) {
+    uint64_t e = std::min<uint64_t>((uint64_t)(p + 1) * per, nnz);
+    t->prtn_ptr[p + 1] = e;
+  }
+  ALTO_TRY(t->prtn_iv.ensure((size_t)nprtn * N * 2 * 8 + (size_t)(nprtn + 1) * 8 + N * 8));
+  uint64_t* d_iv = t->prtn_iv.as<uint64_t>();
+  uint64_t* d_ptr = d_iv + (size_t)nprtn * N * 2;
+  uint64_t* d_dims = d_ptr + nprtn + 1;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(d_ptr, t->prtn_ptr.data(), (nprtn + 1) * 8, cudaMemcpyHostToDevice, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(d_dims, t->dims, N * 8, cudaMemcpyHostToDevice, st));
+  prtn_interval_kernel<<<nprtn, 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, dec, d_ptr, d_dims,
+                                              d_iv);
+  ALTO_LAUNCHED();
+  if (!coo->on_device) ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // host COO must outlive the copies
+  return ALTO_OK;
+}
+
+// Re-derive the reference's interleaved key from the line key (export).
+__global__ void export_key_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
+                                  LineDecode dec, MaskSet ms, uint32_t nnz,
+                                  uint64_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, i);
+    uint64_t klo = 0, khi = 0;
+#pragma unroll
+    for (int m = 0; m < ALTO_MAX_MODES; ++m)
+      if (m < dec.nmodes) deposit(line_field(lo, hi, dec.pos[m], dec.mask[m]), ms.lo[m], ms.hi[m], klo, khi);
+    out[2 * (size_t)i] = klo;
+    out[2 * (size_t)i + 1] = khi;
+  }
+}
+
+alto_status export_keys(const alto_tensor* t, uint64_t* d_out, cudaStream_t st) {
+  MaskSet ms{};
+  ms.nmodes = t->nmodes;
+  for (int m = 0; m < t->nmodes; ++m) {
+    ms.lo[m] = t->masks[m].lo;
+    ms.hi[m] = t->masks[m].hi;
+  }
+  if (!t->nnz) return ALTO_OK;
+  export_key_kernel<<<grid_for(t->nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, t->dec,
+                                                           ms, (uint32_t)t->nnz, d_out);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+}  // namespace alto

@@ -1,0 +1,166 @@
+// Internal declarations shared by the CUDA translation units of libalto_b200.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/alto_b200.h"
+
+namespace alto {
+
+// ------------------------------------------------------------------ errors
+
+void set_error(const char* fmt, ...);
+extern std::atomic<uint64_t> g_kernel_launches;
+
+inline alto_status cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+  if (e == cudaSuccess) return ALTO_OK;
+  set_error("%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  return e == cudaErrorMemoryAllocation ? ALTO_ERR_NOMEM : ALTO_ERR_CUDA;
+}
+
+#define ALTO_TRY_CUDA(call)                                                   \
+  do {                                                                        \
+    alto_status s_ = ::alto::cuda_status((call), #call, __FILE__, __LINE__);  \
+    if (s_ != ALTO_OK) return s_;                                             \
+  } while (0)
+
+#define ALTO_TRY(call)               \
+  do {                               \
+    alto_status s_ = (call);         \
+    if (s_ != ALTO_OK) return s_;    \
+  } while (0)
+
+// Count and check a kernel launch.
+#define ALTO_LAUNCHED()                                                        \
+  do {                                                                         \
+    ::alto::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);         \
+    ALTO_TRY_CUDA(cudaGetLastError());                                         \
+  } while (0)
+
+// ------------------------------------------------------------ device memory
+
+// A growable device allocation owned by a handle.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Ensure at least n bytes; contents are not preserved on growth.
+  alto_status ensure(size_t n) {
+    if (n <= bytes && p) return ALTO_OK;
+    release();
+    size_t want = n < 256 ? 256 : n;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_status(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    bytes = want;
+    return ALTO_OK;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// ------------------------------------------------------------- ALTO keys
+
+struct Key2 {
+  uint64_t lo, hi;
+};
+
+// Per-mode bit fields of the mode-contiguous ("line") key: mode m occupies
+// bits [pos[m], pos[m] + bits[m]) of a 128-bit word stored as a 64-bit low
+// part plus, when the fields need more than 64 bits, a 32- or 64-bit high
+// part.  This is the reference's ALT_PEXT layout (include/alto.hpp:541-573,
+// mode_pos at :982-988) split into separately streamed words.
+struct LineDecode {
+  int nmodes;
+  int hi_words;    // 0: no high part; 1: uint32 high part; 2: uint64 high part
+  int pos[ALTO_MAX_MODES];
+  uint64_t mask[ALTO_MAX_MODES];  // (1 << bits) - 1
+};
+
+// Field of mode-contiguous key (lo, hi) at bit pos with the given mask; hi is
+// 0 when the key has no high part.
+__device__ __forceinline__ uint64_t line_field(uint64_t lo, uint64_t hi, int pos, uint64_t mask) {
+  if (pos >= 64) return (hi >> (pos - 64)) & mask;
+  uint64_t v = lo >> pos;
+  if (pos > 0) v |= hi << (64 - pos);
+  return v & mask;
+}
+
+// --------------------------------------------------------------- scans
+
+// Exclusive prefix sum of n uint32 counts in place (device), stream-ordered.
+alto_status exclusive_scan_u32(uint32_t* data, size_t n, DevBuf& scratch, cudaStream_t st);
+
+}  // namespace alto
+
+// ------------------------------------------------------------- the handle
+
+struct alto_tensor {
+  int nmodes = 0;
+  int nprtn = 1;
+  int stream_mode = -1;
+  int key_bits = 64;   // width of the reference key type (64 or 128)
+  int alto_bits = 0;   // bits the masks use
+  uint64_t nnz = 0;
+  uint64_t cap = 0;    // capacity of the per-nonzero device arrays
+  uint64_t dims[ALTO_MAX_MODES] = {0};
+  alto::Key2 masks[ALTO_MAX_MODES] = {};
+  alto::Key2 alto_mask = {0, 0};
+  int mode_bits[ALTO_MAX_MODES] = {0};
+  alto::LineDecode dec = {};
+
+  // The line: per nonzero, the mode-contiguous key and the value, in ALTO
+  // (bit-interleaved key) order.
+  alto::DevBuf klo;    // uint64 [cap]
+  alto::DevBuf khi;    // uint32 or uint64 [cap] (only when alto_bits > 64)
+  alto::DevBuf vals;   // float   [cap]
+  alto::DevBuf perm;   // uint32  [cap]: input position of each line entry
+
+  // Tiles of the line used by the MTTKRP kernels: tile t covers
+  // [t * tile_nnz, min((t+1) * tile_nnz, nnz)); tile_iv holds, per tile and
+  // mode, the first row and the row count of its interval.
+  uint32_t tile_nnz = 4096;
+  uint32_t ntiles = 0;
+  alto::DevBuf tile_iv;  // uint32 [ntiles * nmodes * 2]
+
+  // The reference's partitions (prtn_ptr / prtn_intervals).
+  std::vector<uint64_t> prtn_ptr;
+  alto::DevBuf prtn_iv;  // uint64 [nprtn * nmodes * 2]
+
+  // Construction scratch (sort buffers, scan partials).
+  alto::DevBuf scratch;
+  alto::DevBuf scan_scratch;
+  cudaStream_t stream = nullptr;
+};
+
+namespace alto {
+// Encode (linearise, sort, lay out, partition) a COO tensor into t.
+alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st);
+// Host-side mask setup (setup_packed_alto).
+int setup_masks(int nmodes, const uint64_t* dims, int max_bits, Key2* masks, Key2* alto_mask,
+                int* bits);
+// MTTKRP dispatcher.
+alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
+                       int rank, float* out, int accumulate, alto_mttkrp_variant variant,
+                       cudaStream_t st);
+alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype);
+}  // namespace alto

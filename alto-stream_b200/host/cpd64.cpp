@@ -1,0 +1,374 @@
+// cpd64 -- the reference's command-line driver (src/main.cpp), rebuilt on the
+// C ABI of libalto_b200 so that every MTTKRP, CP-ALS and CP-stream step runs
+// on the GPU.  Flags follow src/main.cpp:68-93:
+//
+//   -i FILE   .tns text tensor (1-based unless -u)      -b FILE  binary tensor
+//   -r R      rank (16)                                 -m K     max iterations (10)
+//   -x SEED   seed for the initial model (srand/rand)   -t MODE  target mode (-1: all)
+//   -e EPS    epsilon (5e-2)                            -u       zero-based indices
+//   -p        MTTKRP benchmark (BenchmarkAlto)          -c       check MTTKRP against COO
+//   -l MODEL  als | cpstream_alto                       -z CON   nonneg | lasso
+//   -a MODE   streaming mode                            -g L     time slices per batch (1)
+//   -k T      nonzero threshold per batch               -f F     forgetting factor (0.99)
+//   -h / -v   help / version
+//
+// The initial model uses the C library's rand() after srand(seed), drawing
+// values in [-3, 3] with a random sign as the reference does
+// (src/util.cpp:28-43, src/main.cpp:188), so both drivers start from the
+// same model on the same C library.  -c computes its float64 COO ground
+// truth on the host: it is a verification mode, as in the reference.
+#include <getopt.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "alto_b200.h"
+
+namespace {
+
+struct Coo {
+  int nmodes = 0;
+  std::vector<uint64_t> dims;
+  std::vector<std::vector<uint64_t>> cidx;
+  std::vector<double> vals;
+  uint64_t nnz() const { return vals.size(); }
+};
+
+[[noreturn]] void die(const char* what, alto_status s) {
+  fprintf(stderr, "cpd64: %s failed: %s (%s)\n", what, alto_status_string(s), alto_last_error());
+  exit(1);
+}
+
+#define CHECK(call)                   \
+  do {                                \
+    alto_status s_ = (call);          \
+    if (s_ != ALTO_OK) die(#call, s_); \
+  } while (0)
+
+// Text format (src/sptensor.cpp:74-158): whitespace-separated indices then a
+// value per line, '#' comments, dims = max index.
+bool read_tns(const char* path, bool zero_based, Coo& X) {
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  char* line = nullptr;
+  size_t cap = 0;
+  ssize_t n;
+  while ((n = getline(&line, &cap, f)) != -1) {
+    if (n <= 1 || line[0] == '#') continue;
+    std::vector<double> tok;
+    char* p = line;
+    char* end;
+    while (true) {
+      double v = strtod(p, &end);
+      if (end == p) break;
+      tok.push_back(v);
+      p = end;
+    }
+    if (tok.size() < 2) continue;
+    if (X.nmodes == 0) {
+      X.nmodes = (int)tok.size() - 1;
+      X.cidx.assign(X.nmodes, {});
+      X.dims.assign(X.nmodes, 0);
+    }
+    for (int m = 0; m < X.nmodes; ++m) {
+      uint64_t ix = (uint64_t)tok[m] - (zero_based ? 0 : 1);
+      X.cidx[m].push_back(ix);
+      X.dims[m] = std::max(X.dims[m], ix + 1);
+    }
+    X.vals.push_back(tok[X.nmodes]);
+  }
+  free(line);
+  fclose(f);
+  return X.nmodes > 0;
+}
+
+// Binary format (src/sptensor.cpp:206-242): u64 nmodes, u64 dims[n], u64 nnz,
+// u64 cidx[n][nnz] (0-based), f64 vals[nnz].
+bool read_bin(const char* path, Coo& X) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  uint64_t nm = 0, nnz = 0;
+  bool ok = fread(&nm, 8, 1, f) == 1 && nm >= 1 && nm <= ALTO_MAX_MODES;
+  if (ok) {
+    X.nmodes = (int)nm;
+    X.dims.resize(nm);
+    ok = fread(X.dims.data(), 8, nm, f) == nm && fread(&nnz, 8, 1, f) == 1;
+  }
+  if (ok) {
+    X.cidx.assign(nm, std::vector<uint64_t>(nnz));
+    for (uint64_t m = 0; m < nm && ok; ++m) ok = fread(X.cidx[m].data(), 8, nnz, f) == nnz;
+    X.vals.resize(nnz);
+    ok = ok && fread(X.vals.data(), 8, nnz, f) == nnz;
+  }
+  fclose(f);
+  return ok;
+}
+
+alto_coo view(const Coo& X, std::vector<const void*>& ptrs) {
+  ptrs.resize(X.nmodes);
+  for (int m = 0; m < X.nmodes; ++m) ptrs[m] = X.cidx[m].data();
+  alto_coo c;
+  c.nmodes = X.nmodes;
+  c.dims = X.dims.data();
+  c.nnz = X.nnz();
+  c.cidx = ptrs.data();
+  c.index_bytes = 8;
+  c.vals = X.vals.data();
+  c.val_dtype = ALTO_F64;
+  c.on_device = 0;
+  return c;
+}
+
+// rand_val of the reference (src/util.cpp:28-35).
+double rand_val() {
+  double v = 3.0 * ((double)rand() / (double)RAND_MAX);
+  if (rand() % 2 == 0) v *= -1;
+  return v;
+}
+
+std::vector<std::vector<double>> random_model(const std::vector<uint64_t>& dims, int R) {
+  std::vector<std::vector<double>> U(dims.size());
+  for (size_t m = 0; m < dims.size(); ++m) {
+    U[m].resize(dims[m] * R);
+    for (auto& x : U[m]) x = rand_val();
+  }
+  return U;
+}
+
+double now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void usage(const char* argv0) {
+  fprintf(stderr,
+          "usage: %s (-i FILE | -b FILE) [-r R] [-m K] [-x SEED] [-t MODE] [-e EPS] [-u]\n"
+          "          [-p | -c | -l als|cpstream_alto] [-z nonneg|lasso] [-a MODE] [-g L] [-k T] [-f F]\n",
+          argv0);
+}
+
+int run_bench(alto_tensor* t, const Coo& X, int R, int target, int iters) {
+  auto U = random_model(X.dims, R);
+  std::vector<double*> ptrs(X.nmodes);
+  for (int m = 0; m < X.nmodes; ++m) ptrs[m] = U[m].data();
+  int m0 = target < 0 ? 0 : target, m1 = target < 0 ? X.nmodes : target + 1;
+  for (int m = m0; m < m1; ++m) CHECK(alto_mttkrp_host(t, m, ptrs.data(), R, nullptr));
+  double t0 = now();
+  for (int i = 0; i < iters; ++i)
+    for (int m = m0; m < m1; ++m) CHECK(alto_mttkrp_host(t, m, ptrs.data(), R, nullptr));
+  printf("ALTO runtime:   %f\n", now() - t0);
+  return 0;
+}
+
+int run_check(alto_tensor* t, const Coo& X, int R, int target) {
+  auto U = random_model(X.dims, R);
+  int m0 = target < 0 ? 0 : target, m1 = target < 0 ? X.nmodes : target + 1;
+  int bad_modes = 0;
+  for (int mode = m0; mode < m1; ++mode) {
+    std::vector<std::vector<double>> F = U;
+    std::fill(F[mode].begin(), F[mode].end(), 0.0);
+    std::vector<double> truth(X.dims[mode] * R, 0.0), row(R);
+    for (uint64_t i = 0; i < X.nnz(); ++i) {  // COO ground truth (src/mttkrp.cpp:122-156)
+      for (int r = 0; r < R; ++r) row[r] = X.vals[i];
+      for (int m = 0; m < X.nmodes; ++m)
+        if (m != mode)
+          for (int r = 0; r < R; ++r) row[r] *= F[m][X.cidx[m][i] * R + r];
+      for (int r = 0; r < R; ++r) truth[X.cidx[mode][i] * R + r] += row[r];
+    }
+    std::vector<double*> ptrs(X.nmodes);
+    for (int m = 0; m < X.nmodes; ++m) ptrs[m] = F[m].data();
+    CHECK(alto_mttkrp_host(t, mode, ptrs.data(), R, nullptr));
+    double maxabs = 0, maxerr = 0;
+    for (size_t q = 0; q < truth.size(); ++q) {
+      maxabs = std::max(maxabs, std::fabs(truth[q]));
+      maxerr = std::max(maxerr, std::fabs(truth[q] - F[mode][q]));
+    }
+    const double rel = maxabs > 0 ? maxerr / maxabs : maxerr;
+    printf("mode %d: normwise error %.3e %s\n", mode, rel, rel <= 1e-5 ? "correct" : "INCORRECT");
+    bad_modes += rel > 1e-5;
+  }
+  return bad_modes ? 1 : 0;
+}
+
+int run_als(alto_tensor* t, const Coo& X, int R, int iters, double eps) {
+  auto U = random_model(X.dims, R);
+  std::vector<double> lambda(R, 1.0), fits(std::max(iters, 1));
+  std::vector<double*> ptrs(X.nmodes);
+  for (int m = 0; m < X.nmodes; ++m) ptrs[m] = U[m].data();
+  printf("Running ALTO CP-ALS with %d max iterations and %.2e epsilon\n", iters, eps);
+  int done = 0;
+  double t0 = now();
+  CHECK(alto_cpd_als(t, R, ptrs.data(), lambda.data(), iters, eps, ALTO_FIT_REFERENCE, ALTO_F32,
+                     fits.data(), &done, nullptr));
+  double el = now() - t0;
+  for (int i = 0; i < done; ++i)
+    printf("it: %d\t fit: %g\t fit-delta: %g\n", i, fits[i], i ? std::fabs(fits[i] - fits[i - 1]) : fits[i]);
+  printf("CPD (ALTO) time: %f s (%d iterations)\n", el, done);
+  return 0;
+}
+
+// StreamingSparseTensor (src/streaming_sptensor.cpp:69-264): sort by the
+// stream mode then the following modes cyclically, relabel the non-stream
+// indices in first-seen order, and cut batches of timeslice_limit time steps
+// (or until nnz_threshold).
+int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_constraint con,
+                 uint64_t nnz_threshold, uint64_t limit, double forgetting) {
+  Coo X = X0;
+  const int N = X.nmodes;
+  std::vector<uint64_t> order(X.nnz());
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
+    for (int k = 0; k < N; ++k) {
+      int m = (tmode + k) % N;
+      if (X.cidx[m][a] != X.cidx[m][b]) return X.cidx[m][a] < X.cidx[m][b];
+    }
+    return false;
+  });
+  Coo S = X;
+  for (int m = 0; m < N; ++m)
+    for (uint64_t i = 0; i < X.nnz(); ++i) S.cidx[m][i] = X.cidx[m][order[i]];
+  for (uint64_t i = 0; i < X.nnz(); ++i) S.vals[i] = X.vals[order[i]];
+  for (int m = 0; m < N; ++m) {
+    if (m == tmode) continue;
+    std::vector<uint64_t> perm(S.dims[m], UINT64_MAX);
+    uint64_t seen = 0;
+    for (auto& ix : S.cidx[m]) {
+      if (perm[ix] == UINT64_MAX) perm[ix] = seen++;
+      ix = perm[ix];
+    }
+  }
+  alto_stream_session* s = nullptr;
+  CHECK(alto_stream_open(N, tmode, R, con, forgetting, iters, eps, nullptr, &s));
+  std::vector<uint64_t> prev(N, 0);
+  uint64_t ptr = 0, batch_num = 0;
+  int nb = 0;
+  double t0 = now();
+  while (ptr < S.nnz()) {
+    uint64_t start = ptr, end = ptr, first_batch = batch_num;
+    while (end - start < nnz_threshold && end < S.nnz()) {
+      while (end < S.nnz() && S.cidx[tmode][end] < batch_num + 1) ++end;
+      ++batch_num;
+      if (batch_num - first_batch >= limit) break;
+    }
+    Coo B;
+    B.nmodes = N;
+    B.dims.assign(N, 0);
+    B.cidx.assign(N, {});
+    B.vals.assign(S.vals.begin() + start, S.vals.begin() + end);
+    for (int m = 0; m < N; ++m) {
+      B.cidx[m].assign(S.cidx[m].begin() + start, S.cidx[m].begin() + end);
+      if (m == tmode) {
+        for (auto& ix : B.cidx[m]) ix -= first_batch;
+        B.dims[m] = batch_num - first_batch;
+      } else {
+        uint64_t mx = 0;
+        for (auto ix : B.cidx[m]) mx = std::max(mx, ix);
+        B.dims[m] = std::max(mx + 1, prev[m]);
+        prev[m] = B.dims[m];
+      }
+    }
+    ptr = end;
+    if (B.nnz() == 0) continue;
+    std::vector<double> init;
+    static std::vector<uint64_t> have(ALTO_MAX_MODES, 0);
+    for (int m = 0; m < N; ++m) {
+      uint64_t d = std::max(have[m], B.dims[m]);
+      for (uint64_t q = have[m] * R; q < d * R; ++q) init.push_back(rand_val());
+      have[m] = d;
+    }
+    std::vector<const void*> ptrs;
+    alto_coo c = view(B, ptrs);
+    int inner = 0;
+    CHECK(alto_stream_push(s, &c, init.data(), init.size(), &inner));
+    ++nb;
+    fprintf(stderr, "batch %d: %llu nnz, %d inner iterations\n", nb, (unsigned long long)B.nnz(), inner);
+  }
+  double el = now() - t0;
+  printf("CPSTREAM (ALTO) on the GPU: %d batches in %f s (%f s/batch)\n", nb, el, nb ? el / nb : 0.0);
+  alto_stream_close(s);
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  static const option long_opt[] = {
+      {"help", 0, nullptr, 'h'}, {"version", 0, nullptr, 'v'}, {"input", 1, nullptr, 'i'},
+      {"bin", 1, nullptr, 'b'}, {"model", 1, nullptr, 'l'}, {"constraint", 1, nullptr, 'z'},
+      {"rank", 1, nullptr, 'r'}, {"max-iter", 1, nullptr, 'm'}, {"seed", 1, nullptr, 'x'},
+      {"target-mode", 1, nullptr, 't'}, {"epsilon", 1, nullptr, 'e'}, {"zero-based", 0, nullptr, 'u'},
+      {"check", 0, nullptr, 'c'}, {"bench", 0, nullptr, 'p'}, {"streaming-mode", 1, nullptr, 'a'},
+      {"timeslice-limit", 1, nullptr, 'g'}, {"nnz-threshold", 1, nullptr, 'k'},
+      {"forgetting", 1, nullptr, 'f'}, {nullptr, 0, nullptr, 0}};
+  std::string text, bin, model = "als";
+  int R = 16, iters = 10, target = -1, tmode = -1;
+  double eps = 5e-2, forgetting = 0.99;
+  bool zero = false, check = false, bench = false;
+  alto_constraint con = ALTO_UNCONSTRAINED;
+  uint64_t nnz_threshold = UINT64_MAX, limit = 1;
+  srand((unsigned)time(nullptr));
+  int c;
+  while ((c = getopt_long(argc, argv, "hvi:b:l:z:r:m:x:t:e:ucpa:g:k:f:", long_opt, nullptr)) != -1) {
+    switch (c) {
+      case 'h': usage(argv[0]); return 0;
+      case 'v': printf("cpd64 (B200) %d\n", alto_version()); return 0;
+      case 'i': text = optarg; break;
+      case 'b': bin = optarg; break;
+      case 'l': model = optarg; break;
+      case 'z':
+        if (!strcmp(optarg, "nonneg")) con = ALTO_NONNEG;
+        else if (!strcmp(optarg, "lasso")) con = ALTO_LASSO;
+        break;
+      case 'r': R = atoi(optarg); break;
+      case 'm': iters = atoi(optarg); break;
+      case 'x': srand((unsigned)atoi(optarg)); break;
+      case 't': target = atoi(optarg); break;
+      case 'e': eps = atof(optarg); break;
+      case 'u': zero = true; break;
+      case 'c': check = true; break;
+      case 'p': bench = true; break;
+      case 'a': tmode = atoi(optarg); break;
+      case 'g': limit = strtoull(optarg, nullptr, 10); break;
+      case 'k': nnz_threshold = strtoull(optarg, nullptr, 10); break;
+      case 'f': forgetting = atof(optarg); break;
+      default: usage(argv[0]); return 1;
+    }
+  }
+  Coo X;
+  if (!bin.empty()) {
+    if (!read_bin(bin.c_str(), X)) { fprintf(stderr, "cannot read %s\n", bin.c_str()); return 1; }
+  } else if (!text.empty()) {
+    if (!read_tns(text.c_str(), zero, X)) { fprintf(stderr, "cannot read %s\n", text.c_str()); return 1; }
+  } else {
+    usage(argv[0]);
+    return 1;
+  }
+  if (R < 1 || target >= X.nmodes) { usage(argv[0]); return 1; }
+  printf("tensor: %d modes, %llu nonzeros, rank %d\n", X.nmodes, (unsigned long long)X.nnz(), R);
+  if (model == "cpstream_alto" || model == "CPSTREAM_ALTO") {
+    if (tmode < 0 || tmode >= X.nmodes) { fprintf(stderr, "need -a streaming mode\n"); return 1; }
+    return run_cpstream(X, R, iters, eps, tmode, con, nnz_threshold, limit ? limit : 1, forgetting);
+  }
+  if (model == "spcpstream_alto" || model == "SPCPSTREAM_ALTO") {
+    fprintf(stderr, "spcpstream_alto is not available in this build\n");
+    return 2;
+  }
+  std::vector<const void*> ptrs;
+  alto_coo coo = view(X, ptrs);
+  alto_tensor* t = nullptr;
+  double t0 = now();
+  CHECK(alto_tensor_create(&coo, 0, 1, -1, nullptr, &t));
+  printf("ALTO creation time:   %f\n", now() - t0);
+  int rc = 0;
+  if (check) rc = run_check(t, X, R, target);
+  else if (bench) rc = run_bench(t, X, R, target, iters);
+  else rc = run_als(t, X, R, iters, eps);
+  alto_tensor_destroy(t);
+  return rc;
+}

@@ -1,0 +1,202 @@
+/*
+ * alto_b200.h -- C ABI of the B200 implementation of ALTO's hot path.
+ *
+ * The reference (jeewhanchoi/ALTO-stream) is a header-only C++ library used
+ * in-process; it has no C ABI or FFI.  Each entry point below replaces one
+ * reference interface, cited as file:line within the reference project.
+ * Conventions that replace the reference's assert()/exit():
+ *   - every call returns an alto_status; alto_last_error() describes the
+ *     last failure on the calling thread;
+ *   - all device work is ordered on the caller's CUDA stream (NULL = the
+ *     legacy default stream); calls marked "synchronous" wait for it;
+ *   - handles are not thread safe: use one handle from one host thread at
+ *     a time;
+ *   - index and size arguments are 64-bit; nonzero counts must be below 2^32;
+ *     at most ALTO_MAX_MODES modes; ALTO keys are 64 or 128 bits wide.
+ * There is no CPU fallback: without a usable CUDA device every call that
+ * does device work returns ALTO_ERR_CUDA.
+ */
+#ifndef ALTO_B200_H_
+#define ALTO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALTO_MAX_MODES 8
+#define ALTO_VERSION 100
+
+typedef enum {
+  ALTO_OK = 0,
+  ALTO_ERR_INVALID = 1,     /* bad argument (the reference asserts)                  */
+  ALTO_ERR_CUDA = 2,        /* a CUDA runtime call failed or no device is usable     */
+  ALTO_ERR_NOMEM = 3,       /* device allocation failed                             */
+  ALTO_ERR_NOT_SPD = 4,     /* Cholesky of a normal-equation matrix failed          */
+  ALTO_ERR_UNSUPPORTED = 5, /* configuration outside the supported range            */
+  ALTO_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up                   */
+} alto_status;
+
+typedef enum { ALTO_F32 = 0, ALTO_BF16 = 1, ALTO_F64 = 2 } alto_dtype;
+
+/* MTTKRP kernel variants (the reference's variants, include/alto.hpp:1349-1801,
+ * re-designed for the GPU).  ALTO_MTTKRP_AUTO applies the reference's
+ * selection rule (include/alto.hpp:826-848) and then the tuned choice. */
+typedef enum {
+  ALTO_MTTKRP_AUTO = 0,
+  ALTO_MTTKRP_ATOMIC = 1,   /* vector atomics per nonzero, consecutive equal rows merged in the warp */
+  ALTO_MTTKRP_STAGED = 2,   /* partition-local output rows staged in shared memory (da_mem_pull)    */
+  ALTO_MTTKRP_STREAM = 3,   /* single or few output rows held in registers (mttkrp_alto_stream)     */
+  ALTO_MTTKRP_SORTED = 4    /* nonzeros visited in output-row order, run reduction (op_sched)       */
+} alto_mttkrp_variant;
+
+/* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
+ * reference projects LASSO onto the non-negative orthant too). */
+typedef enum { ALTO_UNCONSTRAINED = 0, ALTO_NONNEG = 1, ALTO_LASSO = 2 } alto_constraint;
+
+/* CP-ALS fit: the reference's value keeps only the diagonal of the Gram
+ * Hadamard product (its Gram lower triangles are never written,
+ * include/cpd.hpp:228-256); EXACT uses the full product. */
+typedef enum { ALTO_FIT_REFERENCE = 0, ALTO_FIT_EXACT = 1 } alto_fit_mode;
+
+/* A coordinate-format sparse tensor (the reference's SparseTensor,
+ * include/sptensor.hpp:8-26): cidx[m] holds the nnz 0-based indices of mode
+ * m, vals the nnz values.  Host or device memory. */
+typedef struct {
+  int nmodes;
+  const uint64_t* dims;        /* host array [nmodes]                        */
+  uint64_t nnz;
+  const void* const* cidx;     /* host array of nmodes pointers              */
+  int index_bytes;             /* 8 (uint64_t, the reference's IType) or 4   */
+  const void* vals;
+  alto_dtype val_dtype;        /* ALTO_F64 (the reference's FType) or F32    */
+  int on_device;               /* 0: cidx/vals are host memory; 1: device    */
+} alto_coo;
+
+typedef struct alto_tensor alto_tensor;
+typedef struct alto_stream_session alto_stream_session;
+typedef void* alto_cuda_stream; /* a cudaStream_t */
+
+/* ------------------------------------------------------------- library */
+
+const char* alto_status_string(alto_status s);
+const char* alto_last_error(void);
+int alto_version(void);
+/* Number of kernels this library launched since load (for launch audits). */
+uint64_t alto_kernel_launches(void);
+
+/* ------------------------------------------------------ the ALTO tensor */
+
+/* The linearisation masks for a tensor shape, host only (no device work):
+ * setup_packed_alto(LSB_FIRST, SHORT_FIRST), include/alto.hpp:955-1057.
+ * masks: 2*nmodes words (low, high); alto_mask: 2 words; *alto_bits the
+ * total.  Returns ALTO_ERR_UNSUPPORTED when the bits exceed key_bits. */
+alto_status alto_compute_masks(int nmodes, const uint64_t* dims, int key_bits, uint64_t* masks,
+                               uint64_t* alto_mask, int* alto_bits);
+
+/* Linearise, sort and partition a COO tensor on the device.
+ * Replaces create_alto (include/alto.hpp:436-582) when stream_mode < 0 and
+ * init_salto + update_salto (include/alto.hpp:151-299) otherwise.
+ * key_bits: 0 picks 64 when the index bits fit, else 128; 64 or 128 forces.
+ * nprtn: the reference's partition count (prtn_ptr / prtn_intervals,
+ * include/alto.hpp:1128-1226), kept for export and the staged variant. */
+alto_status alto_tensor_create(const alto_coo* coo, int key_bits, int nprtn, int stream_mode,
+                               alto_cuda_stream stream, alto_tensor** out);
+
+/* Re-encode a new slice into an existing tensor, reusing its device
+ * capacity (update_salto, include/alto.hpp:195-299). */
+alto_status alto_tensor_update(alto_tensor* t, const alto_coo* coo, int nprtn,
+                               alto_cuda_stream stream);
+
+/* Copy the encoding to host memory, synchronous; any pointer may be NULL.
+ * masks: 2*nmodes words (low, high 64 bits of each mode mask,
+ * AltoTensor::mode_masks); alto_mask: 2 words; idx: 2*nnz words (the
+ * reference's bit-interleaved LIT key, include/alto.hpp:513-533); vals: nnz
+ * (float32 as stored, widened); perm: nnz input positions in line order;
+ * prtn_ptr: nprtn+1; intervals: 2*nprtn*nmodes (start, stop), partition-major. */
+alto_status alto_tensor_export(const alto_tensor* t, uint64_t* masks, uint64_t* alto_mask,
+                               uint64_t* idx, double* vals, uint64_t* perm, uint64_t* prtn_ptr,
+                               uint64_t* intervals);
+
+/* Shape and encoding parameters (host outputs, any may be NULL). */
+alto_status alto_tensor_info(const alto_tensor* t, int* nmodes, uint64_t* dims, uint64_t* nnz,
+                             int* key_bits, int* alto_bits, int* nprtn, int* stream_mode);
+
+/* Bytes of device memory the tensor holds. */
+alto_status alto_tensor_device_bytes(const alto_tensor* t, uint64_t* bytes);
+
+alto_status alto_tensor_destroy(alto_tensor* t); /* destroy_alto, include/alto.hpp:584-604 */
+
+/* --------------------------------------------------------------- MTTKRP */
+
+/* out (rows dims[mode] x rank, row-major float32, device) receives the
+ * mode-`mode` MTTKRP of the tensor with the factor matrices factors[m]
+ * (device, dims[m] x rank row-major, dtype fdtype = ALTO_F32 or ALTO_BF16;
+ * factors[mode] is not read).  accumulate != 0 adds to out as the reference
+ * does (it accumulates into factors[target_mode]); 0 overwrites.
+ * Replaces mttkrp_alto_par (include/alto.hpp:902-908). */
+alto_status alto_mttkrp(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
+                        int rank, float* out, int accumulate, alto_cuda_stream stream);
+
+/* As alto_mttkrp with an explicit kernel variant (for tests and tuning). */
+alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const* factors,
+                                    alto_dtype fdtype, int rank, float* out, int accumulate,
+                                    alto_mttkrp_variant variant, alto_cuda_stream stream);
+
+/* The variant ALTO_MTTKRP_AUTO resolves to for this tensor, mode and rank. */
+alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dtype fdtype,
+                               alto_mttkrp_variant* variant);
+
+/* Host-buffer MTTKRP, the drop-in for mttkrp_alto_par's calling convention:
+ * factors_host[m] are dims[m] x rank float64 host arrays and
+ * factors_host[mode] is accumulated into, as in the reference.  Copies in,
+ * computes in float32 on the device, copies out; synchronous. */
+alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const* factors_host, int rank,
+                             alto_cuda_stream stream);
+
+/* --------------------------------------------------------------- CP-ALS */
+
+/* CP-ALS on the device (cpd_alto, include/cpd.hpp:47-191).  U_host[n]
+ * (dims[n] x rank float64) and lambda_host (rank) hold the initial model on
+ * entry and the result on exit.  Factors are stored on the device as
+ * storage (ALTO_F32 or ALTO_BF16); MTTKRP accumulates in float32; Grams,
+ * Cholesky, solves and fit are float64.  fits (max_iters, may be NULL)
+ * receives the per-iteration residual; *iters the iterations run.
+ * Synchronous. */
+alto_status alto_cpd_als(alto_tensor* t, int rank, double* const* U_host, double* lambda_host,
+                         int max_iters, double epsilon, alto_fit_mode fit_mode,
+                         alto_dtype storage, double* fits, int* iters, alto_cuda_stream stream);
+
+/* ------------------------------------------------------------ CP-stream */
+
+/* A CP-stream session keeps the model, previous model, Grams and ADMM state
+ * resident on the device between time batches (cpstream,
+ * src/streaming_cpd.cpp:26-366 with cpstream_alto_iter :1198-1519).
+ * forgetting: the temporal Gram decay (the reference hard-codes 0.99,
+ * src/streaming_cpd.cpp:18). */
+alto_status alto_stream_open(int nmodes, int stream_mode, int rank, alto_constraint constraint,
+                             double forgetting, int max_inner_iters, double epsilon,
+                             alto_cuda_stream stream, alto_stream_session** out);
+
+/* Process one time batch.  Rows the model gains take their initial values
+ * from init_vals (host, n_init values consumed in order: mode 0's new rows,
+ * then mode 1's, ...; the reference draws them from rand(),
+ * src/kruskal_model.cpp:101-178); missing values are zero.  *inner_iters
+ * (may be NULL) receives the inner iterations run.  Synchronous. */
+alto_status alto_stream_push(alto_stream_session* s, const alto_coo* batch,
+                             const double* init_vals, uint64_t n_init, int* inner_iters);
+
+/* Copy mode m of the current model (dims[m] x rank float64) to host memory;
+ * for the stream mode this is the concatenated time factor (every batch's
+ * time rows).  rows receives the row count.  Synchronous. */
+alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_out,
+                               uint64_t* rows);
+alto_status alto_stream_lambda(alto_stream_session* s, double* host_out);
+alto_status alto_stream_close(alto_stream_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALTO_B200_H_ */

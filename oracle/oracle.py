@@ -1,0 +1,299 @@
+"""ctypes wrappers for the ALTO oracle (test infrastructure only).
+
+Two checkers live here:
+
+* ``liboracle.so`` -- the single-threaded FP64 C restatement of the reference
+  algorithm (``oracle/alto_oracle.c``), the checker the CUDA path's parity
+  tests compare against;
+* ``_ref/libaltoref{64,128}.so`` -- the reference implementation itself,
+  compiled from its own sources by ``oracle/ref/Makefile`` and driven by
+  ``oracle/ref/ref_harness.cpp``; it pins the restatement and is the timed
+  CPU baseline of ``bench.py``.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its CPU
+baseline and reference arm) import this module.  The product library never
+does: it has no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = {}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+def _dptrs(arrs):
+    """double** over a list of contiguous float64 arrays."""
+    arr = (POINTER(c_double) * len(arrs))()
+    for i, a in enumerate(arrs):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        arr[i] = a.ctypes.data_as(POINTER(c_double))
+    return arr
+
+
+def lib():
+    """Load (building if needed) the C restatement."""
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            import subprocess
+
+            subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True,
+                           stdout=subprocess.DEVNULL)
+        L = ctypes.CDLL(path)
+        L.ora_setup_masks.restype = c_int
+        L.ora_alto_build.restype = c_int
+        L.ora_cpd_als.restype = c_int
+        L.ora_cpstream.restype = c_int
+        _LIB = L
+    return _LIB
+
+
+def ref_available(bits=64):
+    return os.path.exists(os.path.join(HERE, "_ref", f"libaltoref{bits}.so"))
+
+
+def ref_lib(bits=64):
+    """Load the compiled reference (64- or 128-bit ALTO keys)."""
+    if bits not in _REF:
+        path = os.path.join(HERE, "_ref", f"libaltoref{bits}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference sources exist")
+        L = ctypes.CDLL(path)
+        L.ref_alto_create.restype = c_void_p
+        L.ref_alto_destroy.argtypes = [c_void_p]
+        L.ref_alto_export.argtypes = [c_void_p] + [c_void_p] * 6
+        L.ref_alto_nprtn.argtypes = [c_void_p]
+        L.ref_mttkrp.argtypes = [c_void_p, c_int, c_void_p, c_int]
+        L.ref_coo_mttkrp.argtypes = [c_void_p, c_int, c_void_p, c_int]
+        L.ref_mttkrp_time.argtypes = [c_void_p, c_int, c_void_p, c_int, c_int]
+        L.ref_mttkrp_time.restype = c_double
+        L.ref_cpd_als.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_void_p]
+        L.ref_cpd_als.restype = c_int
+        L.ref_cpstream.restype = c_int
+        L.ref_get_num_ptrn.argtypes = [c_uint64]
+        L.ref_get_num_ptrn.restype = c_int
+        L.ref_max_threads.restype = c_int
+        L.ref_set_threads.argtypes = [c_int]
+        _REF[bits] = L
+    return _REF[bits]
+
+
+def join128(lohi):
+    """(n, 2) uint64 lo/hi pairs -> list of Python ints."""
+    lohi = np.asarray(lohi, dtype=np.uint64).reshape(-1, 2)
+    return [int(lo) | (int(hi) << 64) for lo, hi in lohi]
+
+
+def mode_bits(dim):
+    return 0 if dim <= 1 else int(dim - 1).bit_length()
+
+
+# ------------------------------------------------------------ restatement
+
+def setup_masks(dims, max_bits=128):
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    N = len(dims)
+    masks = np.zeros(2 * N, np.uint64)
+    am = np.zeros(2, np.uint64)
+    pos = np.zeros(N, np.int32)
+    bits = lib().ora_setup_masks(c_int(N), _ptr(dims), c_int(max_bits), _ptr(masks), _ptr(am), _ptr(pos))
+    if bits < 0:
+        raise ValueError("index bits exceed key width")
+    return dict(masks=masks.reshape(N, 2), alto_mask=am, mode_pos=pos, alto_bits=bits)
+
+
+def build(dims, cidx, vals, nprtn=1, max_bits=128):
+    """Encode, sort and partition a COO tensor the way create_alto does."""
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    N, nnz = cidx.shape
+    masks = np.zeros(2 * N, np.uint64)
+    am = np.zeros(2, np.uint64)
+    idx = np.zeros(2 * max(nnz, 1), np.uint64)
+    sv = np.zeros(max(nnz, 1), np.float64)
+    perm = np.zeros(max(nnz, 1), np.uint64)
+    pp = np.zeros(nprtn + 1, np.uint64)
+    iv = np.zeros(2 * nprtn * N, np.uint64)
+    bits = lib().ora_alto_build(c_int(N), _ptr(dims), c_uint64(nnz), _ptr(cidx), _ptr(vals),
+                                c_int(max_bits), c_int(nprtn), _ptr(masks), _ptr(am), _ptr(idx),
+                                _ptr(sv), _ptr(perm), _ptr(pp), _ptr(iv))
+    if bits < 0:
+        raise ValueError("index bits exceed key width")
+    return dict(dims=dims, nmodes=N, nnz=nnz, masks=masks.reshape(N, 2), alto_mask=am,
+                idx=idx[: 2 * nnz].reshape(nnz, 2), vals=sv[:nnz], perm=perm[:nnz],
+                prtn_ptr=pp, intervals=iv.reshape(nprtn, N, 2), alto_bits=bits)
+
+
+def partition(enc, nprtn):
+    N, nnz = enc["nmodes"], enc["nnz"]
+    pp = np.zeros(nprtn + 1, np.uint64)
+    iv = np.zeros(2 * nprtn * N, np.uint64)
+    lib().ora_partition(c_int(N), _ptr(enc["dims"]), c_uint64(nnz), _ptr(np.ascontiguousarray(enc["idx"])),
+                        _ptr(np.ascontiguousarray(enc["masks"])), c_int(nprtn), _ptr(pp), _ptr(iv))
+    return pp, iv.reshape(nprtn, N, 2)
+
+
+def decode(enc):
+    N, nnz = enc["nmodes"], enc["nnz"]
+    out = np.zeros((N, max(nnz, 1)), np.uint64)
+    lib().ora_decode(c_int(N), c_uint64(nnz), _ptr(np.ascontiguousarray(enc["idx"])),
+                     _ptr(np.ascontiguousarray(enc["masks"])), _ptr(out))
+    return out[:, :nnz]
+
+
+def mttkrp(enc, mode, factors, rank):
+    """Accumulate the ALTO MTTKRP of `mode` into factors[mode] (FP64)."""
+    fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    lib().ora_mttkrp(c_int(enc["nmodes"]), c_uint64(enc["nnz"]), _ptr(np.ascontiguousarray(enc["idx"])),
+                     _ptr(np.ascontiguousarray(enc["vals"], dtype=np.float64)),
+                     _ptr(np.ascontiguousarray(enc["masks"])), c_int(mode), _dptrs(fs), c_int(rank))
+    return fs
+
+
+def coo_mttkrp(cidx, vals, mode, factors, rank):
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    lib().ora_coo_mttkrp(c_int(cidx.shape[0]), c_uint64(cidx.shape[1]), _ptr(cidx), _ptr(vals),
+                         c_int(mode), _dptrs(fs), c_int(rank))
+    return fs
+
+
+def cpd_als(enc, U, lam, rank, max_iters, eps, fit_exact=False):
+    Us = [np.array(u, dtype=np.float64, copy=True, order="C") for u in U]
+    lam = np.array(lam, dtype=np.float64, copy=True)
+    fits = np.zeros(max(max_iters, 1), np.float64)
+    it = lib().ora_cpd_als(c_int(enc["nmodes"]), _ptr(enc["dims"]), c_uint64(enc["nnz"]),
+                           _ptr(np.ascontiguousarray(enc["idx"])), _ptr(np.ascontiguousarray(enc["vals"])),
+                           _ptr(np.ascontiguousarray(enc["masks"])), _dptrs(Us), _ptr(lam), c_int(rank),
+                           c_int(max_iters), c_double(eps), c_int(1 if fit_exact else 0), _ptr(fits))
+    return Us, lam, fits[: abs(it)], it
+
+
+def _stream_args(batches):
+    dims = np.ascontiguousarray(np.concatenate([np.asarray(b["dims"], np.uint64) for b in batches]))
+    nnz = np.ascontiguousarray([b["cidx"].shape[1] for b in batches], dtype=np.uint64)
+    cidx = np.ascontiguousarray(np.concatenate([np.asarray(b["cidx"], np.uint64).ravel() for b in batches]))
+    vals = np.ascontiguousarray(np.concatenate([np.asarray(b["vals"], np.float64) for b in batches]))
+    return dims, nnz, cidx, vals
+
+
+def _stream_outputs(batches, stream_mode, rank):
+    last = batches[-1]["dims"]
+    total_t = int(sum(int(b["dims"][stream_mode]) for b in batches))
+    outs = []
+    for m, d in enumerate(last):
+        n = total_t if m == stream_mode else int(d)
+        outs.append(np.zeros((max(n, 1), rank), np.float64))
+    return outs
+
+
+def cpstream(batches, stream_mode, rank, max_iters, eps, nonneg, init_vals, forgetting=0.99):
+    """CP-stream over a list of batches {dims, cidx (N x nnz), vals}."""
+    N = len(batches[0]["dims"])
+    dims, nnz, cidx, vals = _stream_args(batches)
+    init_vals = np.ascontiguousarray(init_vals, dtype=np.float64)
+    outs = _stream_outputs(batches, stream_mode, rank)
+    lam = np.zeros(rank, np.float64)
+    inner = np.zeros(len(batches), np.int32)
+    tt = lib().ora_cpstream(c_int(N), c_int(stream_mode), c_int(len(batches)), _ptr(dims), _ptr(nnz),
+                            _ptr(cidx), _ptr(vals), c_int(rank), c_int(max_iters), c_double(eps),
+                            c_int(1 if nonneg else 0), c_double(forgetting), _ptr(init_vals),
+                            c_uint64(len(init_vals)), _dptrs(outs), _ptr(lam), _ptr(inner))
+    if tt < 0:
+        raise RuntimeError("oracle CP-stream: factorisation failed")
+    return outs, lam, inner
+
+
+# ------------------------------------------------------ compiled reference
+
+class RefTensor:
+    """The reference's AltoTensor, built by create_alto (or init/update_salto)."""
+
+    def __init__(self, dims, cidx, vals, nprtn, stream_mode=-1, bits=None):
+        dims = np.ascontiguousarray(dims, dtype=np.uint64)
+        self.cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+        self.vals_in = np.ascontiguousarray(vals, dtype=np.float64)
+        if bits is None:
+            bits = 64 if sum(mode_bits(int(d)) for d in dims) <= 64 else 128
+        self.bits = bits
+        self.L = ref_lib(bits)
+        self.dims = dims
+        self.N = len(dims)
+        self.nnz = self.cidx.shape[1]
+        self.h = self.L.ref_alto_create(c_int(self.N), _ptr(dims), c_uint64(self.nnz), _ptr(self.cidx),
+                                        _ptr(self.vals_in), c_int(nprtn), c_int(stream_mode))
+        self.nprtn = self.L.ref_alto_nprtn(self.h)
+
+    def export(self):
+        N, nnz, P = self.N, self.nnz, self.nprtn
+        masks = np.zeros(2 * N, np.uint64)
+        am = np.zeros(2, np.uint64)
+        idx = np.zeros(2 * max(nnz, 1), np.uint64)
+        vals = np.zeros(max(nnz, 1), np.float64)
+        pp = np.zeros(P + 1, np.uint64)
+        iv = np.zeros(2 * P * N, np.uint64)
+        self.L.ref_alto_export(self.h, _ptr(masks), _ptr(am), _ptr(idx), _ptr(vals), _ptr(pp), _ptr(iv))
+        return dict(masks=masks.reshape(N, 2), alto_mask=am, idx=idx[: 2 * nnz].reshape(nnz, 2),
+                    vals=vals[:nnz], prtn_ptr=pp, intervals=iv.reshape(P, N, 2))
+
+    def mttkrp(self, mode, factors, rank):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+        self.L.ref_mttkrp(self.h, mode, ctypes.cast(_dptrs(fs), c_void_p), rank)
+        return fs
+
+    def coo_mttkrp(self, mode, factors, rank):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+        self.L.ref_coo_mttkrp(self.h, mode, ctypes.cast(_dptrs(fs), c_void_p), rank)
+        return fs
+
+    def mttkrp_time(self, mode, factors, rank, reps):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+        return self.L.ref_mttkrp_time(self.h, mode, ctypes.cast(_dptrs(fs), c_void_p), rank, reps)
+
+    def cpd_als(self, U, lam, rank, max_iters, eps):
+        Us = [np.array(u, dtype=np.float64, copy=True, order="C") for u in U]
+        lam = np.array(lam, dtype=np.float64, copy=True)
+        fits = np.zeros(max(max_iters, 1), np.float64)
+        it = self.L.ref_cpd_als(self.h, ctypes.cast(_dptrs(Us), c_void_p), _ptr(lam), rank, max_iters,
+                                eps, _ptr(fits))
+        return Us, lam, fits[:it], it
+
+    def close(self):
+        if self.h:
+            self.L.ref_alto_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_cpstream(batches, stream_mode, rank, max_iters, eps, nonneg, init_vals, bits=64):
+    """The reference's CP-stream (ALTO) over the same batches (forgetting 0.99)."""
+    L = ref_lib(bits)
+    N = len(batches[0]["dims"])
+    dims, nnz, cidx, vals = _stream_args(batches)
+    init_vals = np.ascontiguousarray(init_vals, dtype=np.float64)
+    outs = _stream_outputs(batches, stream_mode, rank)
+    lam = np.zeros(rank, np.float64)
+    secs = np.zeros(len(batches), np.float64)
+    tt = L.ref_cpstream(c_int(N), c_int(stream_mode), c_int(len(batches)), _ptr(dims), _ptr(nnz),
+                        _ptr(cidx), _ptr(vals), c_int(rank), c_int(max_iters), c_double(eps),
+                        c_int(1 if nonneg else 0), _ptr(init_vals), c_uint64(len(init_vals)),
+                        _dptrs(outs), _ptr(lam), _ptr(secs))
+    return outs, lam, secs

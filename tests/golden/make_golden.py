@@ -1,0 +1,134 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Run here, where the reference sources exist (the GPU box has no copy):
+
+    make -C oracle ref         # oracle/_ref/libaltoref{64,128}.so
+    python tests/golden/make_golden.py [path-to-reference]
+
+Inputs are the reference's own fixture tensors (tests/tensors/*.tns in the
+reference project, 1-based text format, src/sptensor.cpp:74-158) plus seeded
+synthetic cases.  Every output below comes from the compiled reference
+(oracle/ref/ref_harness.cpp driving the reference's functions), so the
+fixtures pin both the C restatement in oracle/ and the CUDA path:
+
+* per tensor: the inputs (0-based cidx, values) as compressed arrays; the
+  mode masks and alto_mask; SHA-256 digests of the sorted key array, the
+  sorted values, prtn_ptr and prtn_intervals at P = 1, 3 and 8;
+* MTTKRP (rank 8, factors from a seeded numpy generator) per mode: the full
+  output for tensors under 1000 rows, else column sums, Frobenius norm and
+  16 sampled rows;
+* CP-ALS: fits of 8 iterations on med.tns at rank 8;
+* CP-stream: final factor norms of a small seeded stream, unconstrained and
+  non-negative.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "alto-stream_b200"))
+
+import oracle as O  # noqa: E402
+from alto_b200 import synth  # noqa: E402
+
+FIXTURES = ["small.tns", "small4.tns", "small4_zeroidx.tns", "med.tns", "med4.tns", "med5.tns"]
+RANK = 8
+
+
+def load_tns(path, zero_based=False):
+    rows = [ln.split() for ln in open(path) if ln.strip() and not ln.startswith("#")]
+    a = np.array(rows, dtype=np.float64)
+    idx = a[:, :-1].astype(np.int64)
+    if not zero_based:
+        idx -= 1
+    return np.ascontiguousarray(idx.T.astype(np.uint64)), a[:, -1].copy()
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def factors_for(dims, seed=11):
+    rng = np.random.default_rng(seed)
+    return [rng.uniform(-1.0, 1.0, (int(d), RANK)) for d in dims]
+
+
+def mttkrp_summary(out):
+    if out.shape[0] < 1000:
+        return {"full": out.tolist()}
+    rows = np.linspace(0, out.shape[0] - 1, 16).astype(int)
+    return {"colsum": out.sum(0).tolist(), "fro": float(np.linalg.norm(out)),
+            "rows": rows.tolist(), "sample": out[rows].tolist()}
+
+
+def main(ref_root):
+    out_json = {}
+    for fn in FIXTURES:
+        zero = "zeroidx" in fn
+        cidx, vals = load_tns(os.path.join(ref_root, "tests", "tensors", fn), zero_based=zero)
+        dims = (cidx.max(1) + 1).astype(np.uint64)
+        name = fn[:-4]
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), cidx=cidx.astype(np.uint32), vals=vals, dims=dims)
+        rec = {"dims": dims.tolist(), "nnz": int(cidx.shape[1])}
+        for P in (1, 3, 8):
+            t = O.RefTensor(dims, cidx, vals, P)
+            e = t.export()
+            rec[f"P{P}"] = {"idx": digest(e["idx"]), "vals": digest(e["vals"]),
+                            "prtn_ptr": e["prtn_ptr"].tolist(), "intervals": digest(e["intervals"])}
+            if P == 1:
+                rec["bits"] = t.bits
+                rec["masks"] = [[int(a), int(b)] for a, b in e["masks"]]
+                rec["alto_mask"] = [int(x) for x in e["alto_mask"]]
+                F = factors_for(dims)
+                rec["mttkrp"] = []
+                for m in range(len(dims)):
+                    fs = [f.copy() for f in F]
+                    fs[m][:] = 0
+                    res = t.mttkrp(m, fs, RANK)
+                    rec["mttkrp"].append(mttkrp_summary(res[m]))
+            t.close()
+        out_json[name] = rec
+        print(fn, "done", file=sys.stderr)
+
+    # CP-ALS on med.tns
+    d = np.load(os.path.join(HERE, "med.npz"))
+    dims = d["dims"]
+    init = synth.init_values(int(dims.sum()) * RANK, seed=3)
+    U0, off = [], 0
+    for n in dims:
+        U0.append(init[off:off + int(n) * RANK].reshape(int(n), RANK))
+        off += int(n) * RANK
+    t = O.RefTensor(dims, d["cidx"], d["vals"], 4)
+    _, lam, fits, it = t.cpd_als(U0, np.ones(RANK), RANK, 8, 1e-12)
+    out_json["cpd_als_med"] = {"rank": RANK, "iters": it, "fits": fits.tolist(), "init_seed": 3,
+                               "lambda": lam.tolist()}
+    t.close()
+
+    # CP-stream on a small seeded stream
+    b = synth.stream_batches([200, 300, 50], 6, lambda rng, s: 400 + 50 * s, [1.1, 1.1, None], seed=5)
+    np.savez_compressed(os.path.join(HERE, "stream_small.npz"),
+                        **{f"dims{s}": x["dims"] for s, x in enumerate(b)},
+                        **{f"cidx{s}": x["cidx"] for s, x in enumerate(b)},
+                        **{f"vals{s}": x["vals"] for s, x in enumerate(b)})
+    ntot = sum(int(x) for x in b[-1]["dims"]) * RANK + 1000
+    iv = synth.init_values(ntot, seed=7)
+    for nonneg in (0, 1):
+        outs, lam, _ = O.ref_cpstream(b, 0, RANK, 20, 1e-5, nonneg, iv)
+        out_json[f"cpstream_small_nonneg{nonneg}"] = {
+            "rank": RANK, "max_iters": 20, "eps": 1e-5, "init_seed": 7, "n_init": ntot,
+            "norms": [float(np.linalg.norm(o)) for o in outs],
+            "colsums": [o.sum(0).tolist() for o in outs]}
+
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(out_json, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,150 @@
+"""GPU MTTKRP against the FP64 oracle.
+
+The oracle receives the factor values the GPU reads (float32, or bfloat16
+for the BF16 path, widened to float64), so the comparison isolates the
+float32 accumulation.  Bound: max |gpu - oracle| / max |oracle| <= 1e-5
+(normwise) for every mode, rank and variant."""
+import numpy as np
+import pytest
+
+import alto_b200 as A
+import oracle as O
+from alto_b200 import synth
+from conftest import FIXTURE_NAMES, load_fixture
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def to_dev(F, dtype):
+    import torch
+
+    return [torch.tensor(f, dtype=torch.float32, device="cuda").to(dtype).contiguous() for f in F]
+
+
+def seen_by_gpu(Fd):
+    return [f.float().cpu().numpy().astype(np.float64) for f in Fd]
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def check_modes(dims, cidx, vals, R, variants=(A.AUTO,), dtype=None, seed=0):
+    import torch
+
+    dtype = dtype or torch.float32
+    rng = np.random.default_rng(seed)
+    F = [rng.uniform(-1.0, 1.0, (int(d), R)) for d in dims]
+    Fd = to_dev(F, dtype)
+    Fo = seen_by_gpu(Fd)
+    t = A.create_alto(dims, cidx, vals)
+    vals32 = vals.astype(np.float32).astype(np.float64)
+    enc = O.build(dims, cidx, vals32)
+    for m in range(len(dims)):
+        fs = [f.copy() for f in Fo]
+        fs[m][:] = 0
+        ref = O.mttkrp(enc, m, fs, R)[m]
+        for v in variants:
+            out = t.mttkrp(m, Fd, R, variant=v).cpu().numpy()
+            assert rel_err(out, ref) <= TOL, (m, v, rel_err(out, ref))
+
+
+@pytest.mark.parametrize("name", FIXTURE_NAMES)
+def test_fixtures_rank8(name):
+    dims, cidx, vals = load_fixture(name)
+    check_modes(dims, cidx, vals, 8, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+
+
+@pytest.mark.parametrize("R", [4, 8, 16, 32, 64, 128, 10, 33])
+def test_uniform_ranks(R):
+    dims = np.array([1000, 1000, 1000], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 150000, seed=R)
+    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.STAGED), seed=R)
+
+
+@pytest.mark.parametrize("R", [8, 16, 32, 64])
+def test_bf16_factor_storage(R):
+    import torch
+
+    dims = np.array([800, 700, 900], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 100000, seed=R + 1)
+    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC), dtype=torch.bfloat16, seed=R)
+
+
+def test_power_law_128bit_keys():
+    """Zipf-1.2 coordinates with scattered labels and a 65-bit key."""
+    dims = np.array([4800000, 1800000, 1800000], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 200000, [1.2, 1.2, 1.2], seed=3, values="lognormal")
+    check_modes(dims, cidx, vals, 32, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+
+
+def test_five_modes_rank64():
+    dims = np.array([100000, 100000, 10000, 1000, 100], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 150000, [1.1, 1.1, None, None, None], seed=4)
+    check_modes(dims, cidx, vals, 64, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+
+
+def test_stream_mode_single_row():
+    dims = np.array([1, 3000, 4000, 500], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 100000, seed=6)
+    import torch
+
+    R = 16
+    rng = np.random.default_rng(1)
+    F = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+    Fd = to_dev(F, torch.float32)
+    t = A.init_salto(dims, cidx, vals, 1, stream_mode=0)
+    assert t.choose_variant(0, R) == A.STREAM
+    enc = O.build(dims, cidx, vals.astype(np.float32).astype(np.float64))
+    fs = seen_by_gpu(Fd)
+    fs[0][:] = 0
+    ref = O.mttkrp(enc, 0, fs, R)[0]
+    out = t.mttkrp(0, Fd, R).cpu().numpy()
+    assert rel_err(out, ref) <= TOL
+
+
+def test_accumulate_semantics():
+    import torch
+
+    dims = np.array([300, 200, 100], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 30000, seed=8)
+    R = 16
+    rng = np.random.default_rng(2)
+    F = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+    Fd = to_dev(F, torch.float32)
+    t = A.create_alto(dims, cidx, vals)
+    base = Fd[1].clone()
+    A.mttkrp_alto_par(1, Fd, R, t)  # accumulates into Fd[1]
+    fresh = t.mttkrp(1, Fd, R).cpu().numpy()
+    np.testing.assert_allclose(Fd[1].cpu().numpy(), base.cpu().numpy() + fresh, rtol=1e-5, atol=1e-5)
+
+
+def test_host_buffer_entry_point():
+    dims = np.array([400, 500, 600], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 50000, seed=10)
+    R = 16
+    rng = np.random.default_rng(3)
+    F = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+    t = A.create_alto(dims, cidx, vals)
+    for m in range(3):
+        fs = [f.copy() for f in F]
+        start = fs[m].copy()
+        t.mttkrp_host(m, fs, R)
+        fo = [f.astype(np.float32).astype(np.float64) for f in F]
+        fo[m][:] = 0
+        ref = O.mttkrp(O.build(dims, cidx, vals.astype(np.float32).astype(np.float64)), m, fo, R)[m]
+        assert rel_err(fs[m] - start, ref) <= TOL
+
+
+def test_launch_counter_advances():
+    import torch
+
+    dims = np.array([50, 60, 70], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 1000, seed=1)
+    t = A.create_alto(dims, cidx, vals)
+    Fd = to_dev([np.ones((int(d), 8)) for d in dims], torch.float32)
+    n0 = A.kernel_launches()
+    t.mttkrp(0, Fd, 8)
+    torch.cuda.synchronize()
+    assert A.kernel_launches() > n0

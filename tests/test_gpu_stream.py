@@ -1,0 +1,64 @@
+"""GPU CP-stream (unconstrained and non-negative ADMM) against the oracle
+and the reference's recorded factor norms.  Bound: final factors within
+1e-4 normwise of the FP64 oracle fed the same batches and initial values."""
+import numpy as np
+import pytest
+
+import alto_b200 as A
+import oracle as O
+from alto_b200 import synth
+from conftest import load_stream_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(batches, R, max_iters, eps, nonneg, iv, forgetting=0.99):
+    N = len(batches[0]["dims"])
+    s = A.CPStream(N, 0, R, constraint=A.NONNEG if nonneg else A.UNCONSTRAINED, forgetting=forgetting,
+                   max_inner=max_iters, epsilon=eps)
+    used = 0
+    prev = np.zeros(N, np.int64)
+    inner = []
+    for b in batches:
+        d = b["dims"].astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * R
+        inner.append(s.push(b["dims"], b["cidx"], b["vals"], iv[used:used + need]))
+        used += need
+        prev = np.maximum(prev, d)
+    outs = []
+    for m in range(N):
+        rows = int(sum(int(b["dims"][0]) for b in batches)) if m == 0 else int(batches[-1]["dims"][m])
+        outs.append(s.factor(m, rows))
+    return outs, s.lam(), inner
+
+
+def normwise(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("nonneg", [0, 1])
+def test_small_stream_matches_oracle_and_reference(nonneg, golden):
+    g = golden[f"cpstream_small_nonneg{nonneg}"]
+    b = load_stream_fixture()
+    iv = synth.init_values(g["n_init"], seed=g["init_seed"])
+    R = g["rank"]
+    outs, lam, inner = run_gpu(b, R, g["max_iters"], g["eps"], nonneg, iv)
+    ivo = iv.astype(np.float32).astype(np.float64)
+    bo = [dict(dims=x["dims"], cidx=x["cidx"], vals=x["vals"].astype(np.float32).astype(np.float64)) for x in b]
+    oo, lo, inner_o = O.cpstream(bo, 0, R, g["max_iters"], g["eps"], nonneg, ivo)
+    for a, c in zip(outs, oo):
+        assert normwise(a, c) <= 1e-4, normwise(a, c)
+    np.testing.assert_allclose([np.linalg.norm(o) for o in outs], g["norms"], rtol=1e-4)
+    if nonneg:
+        assert all(np.all(o >= 0) for m, o in enumerate(outs) if m != 0)
+
+
+def test_forgetting_factor_is_a_parameter():
+    b = load_stream_fixture()[:3]
+    R = 8
+    iv = synth.init_values(20000, seed=1)
+    o1, _, _ = run_gpu(b, R, 10, 1e-5, 0, iv, forgetting=0.95)
+    bo = [dict(dims=x["dims"], cidx=x["cidx"], vals=x["vals"].astype(np.float32).astype(np.float64)) for x in b]
+    oo, _, _ = O.cpstream(bo, 0, R, 10, 1e-5, 0, iv.astype(np.float32).astype(np.float64), forgetting=0.95)
+    for a, c in zip(o1, oo):
+        assert normwise(a, c) <= 1e-4
