@@ -38,7 +38,7 @@ EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
     "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
-    "alto_mttkrp_choose", "alto_mttkrp_host", "alto_cpd_als", "alto_stream_open",
+    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
 ]
 
@@ -254,6 +254,18 @@ class AltoTensor:
         v = c_int()
         check(lib().alto_mttkrp_choose(self.h, c_int(mode), c_int(rank), c_int(fdtype), byref(v)))
         return v.value
+
+    def autotune(self, factors, rank, stream=None):
+        """Time the MTTKRP variants per mode and make AUTO use the fastest.
+        Returns the chosen variant per mode."""
+        import torch
+
+        N = self.nmodes
+        ptrs = (c_void_p * N)(*[f.data_ptr() for f in factors])
+        dt = BF16 if factors[0].dtype == torch.bfloat16 else F32
+        out = (c_int * N)()
+        check(lib().alto_mttkrp_autotune(self.h, ptrs, c_int(dt), c_int(rank), _stream_handle(stream), out))
+        return list(out)
 
     def mttkrp_host(self, mode, factors, rank, stream=None):
         """The reference calling convention on host float64 arrays:

@@ -322,6 +322,20 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
                     (cudaStream_t)stream);
 }
 
+alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,
+                                 int rank, alto_cuda_stream stream, alto_mttkrp_variant* variants) {
+  if (!t || !factors || rank < 1 || (fdtype != ALTO_F32 && fdtype != ALTO_BF16)) {
+    set_error("bad arguments");
+    return ALTO_ERR_INVALID;
+  }
+  for (int m = 0; m < t->nmodes; ++m)
+    if (!factors[m]) {
+      set_error("factors[%d] is NULL", m);
+      return ALTO_ERR_INVALID;
+    }
+  return autotune(t, factors, fdtype, rank, (cudaStream_t)stream, variants);
+}
+
 alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dtype fdtype,
                                alto_mttkrp_variant* variant) {
   if (!t || !variant || mode < 0 || mode >= t->nmodes) {

@@ -321,58 +321,82 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// prtn_alto's intervals (include/alto.hpp:1199-1226): one block per
-// partition; start = dims, stop = 0 sentinels, start clamped to stop when
-// the partition is empty.
+// prtn_alto's intervals (include/alto.hpp:1199-1226), computed over the
+// whole grid: block b reduces its chunk of the line separately for every
+// partition the chunk overlaps and merges the result with 64-bit atomic
+// min / max.  iv starts at the reference's sentinels (start = dims, stop = 0);
+// prtn_interval_fix_kernel clamps start to stop for empty partitions.
+constexpr uint32_t kPrtnChunk = 4096;
+
+__global__ void prtn_interval_init_kernel(const uint64_t* __restrict__ dims, int nmodes, int nprtn,
+                                          unsigned long long* __restrict__ iv) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nprtn * nmodes; q += gridDim.x * blockDim.x) {
+    iv[2 * q] = dims[q % nmodes];
+    iv[2 * q + 1] = 0;
+  }
+}
+
+__global__ void prtn_interval_fix_kernel(int n, unsigned long long* __restrict__ iv) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    if (iv[2 * q] > iv[2 * q + 1]) iv[2 * q] = iv[2 * q + 1];
+}
+
 __global__ void __launch_bounds__(256)
     prtn_interval_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                         LineDecode dec, const uint64_t* __restrict__ prtn_ptr,
-                         const uint64_t* __restrict__ dims, uint64_t* __restrict__ iv) {
-  __shared__ uint64_t smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
-  int p = blockIdx.x;
-  uint64_t s = prtn_ptr[p], e = prtn_ptr[p + 1];
-  uint64_t lo_r[ALTO_MAX_MODES], hi_r[ALTO_MAX_MODES];
-#pragma unroll
-  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
-    lo_r[m] = m < dec.nmodes ? dims[m] : 0;
-    hi_r[m] = 0;
-  }
-  for (uint64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
-    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, (uint32_t)i);
+                         LineDecode dec, uint64_t nnz, uint64_t per,
+                         unsigned long long* __restrict__ iv) {
+  __shared__ unsigned long long smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
+  const uint64_t cs = (uint64_t)blockIdx.x * kPrtnChunk;
+  const uint64_t ce = min(cs + kPrtnChunk, nnz);
+  if (cs >= ce) return;
+  const uint64_t p0 = cs / per, p1 = (ce - 1) / per;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint64_t p = p0; p <= p1; ++p) {
+    const uint64_t s = max(cs, p * per), e = min(ce, (p + 1) * per);
+    unsigned long long lo_r[ALTO_MAX_MODES], hi_r[ALTO_MAX_MODES];
 #pragma unroll
     for (int m = 0; m < ALTO_MAX_MODES; ++m) {
-      if (m < dec.nmodes) {
-        uint64_t v = line_field(lo, hi, dec.pos[m], dec.mask[m]);
-        lo_r[m] = min(lo_r[m], v);
-        hi_r[m] = max(hi_r[m], v);
+      lo_r[m] = ~0ull;
+      hi_r[m] = 0;
+    }
+    for (uint64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
+      const uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, (uint32_t)i);
+#pragma unroll
+      for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+        if (m < dec.nmodes) {
+          const unsigned long long v = line_field(lo, hi, dec.pos[m], dec.mask[m]);
+          lo_r[m] = v < lo_r[m] ? v : lo_r[m];
+          hi_r[m] = v > hi_r[m] ? v : hi_r[m];
+        }
       }
     }
-  }
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
-    if (m >= dec.nmodes) continue;
-    uint64_t a = lo_r[m], b = hi_r[m];
-    for (int o = 16; o; o >>= 1) {
-      a = min(a, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)a, o));
-      b = max(b, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)b, o));
+    for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+      if (m >= dec.nmodes) continue;
+      unsigned long long a = lo_r[m], b = hi_r[m];
+      for (int o = 16; o; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, a, o);
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, b, o);
+        a = x < a ? x : a;
+        b = y > b ? y : b;
+      }
+      if (lane == 0) {
+        smin[m][warp] = a;
+        smax[m][warp] = b;
+      }
     }
-    if (lane == 0) {
-      smin[m][warp] = a;
-      smax[m][warp] = b;
+    __syncthreads();
+    if (threadIdx.x < (unsigned)dec.nmodes) {
+      const int m = threadIdx.x;
+      unsigned long long a = ~0ull, b = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        a = smin[m][w] < a ? smin[m][w] : a;
+        b = smax[m][w] > b ? smax[m][w] : b;
+      }
+      atomicMin(&iv[(p * dec.nmodes + m) * 2], a);
+      atomicMax(&iv[(p * dec.nmodes + m) * 2 + 1], b);
     }
-  }
-  __syncthreads();
-  if (threadIdx.x < (unsigned)dec.nmodes) {
-    int m = threadIdx.x;
-    uint64_t a = dims[m], b = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      a = min(a, smin[m][w]);
-      b = max(b, smax[m][w]);
-    }
-    if (a > b) a = b;
-    iv[((size_t)p * dec.nmodes + m) * 2] = a;
-    iv[((size_t)p * dec.nmodes + m) * 2 + 1] = b;
+    __syncthreads();
   }
 }
 
@@ -602,10 +626,24 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   // MTTKRP tiles and their intervals
   t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
   ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    t->sorted[m].ready = false;
+    t->tile_len_sorted[m].clear();
+  }
+  t->tuned.clear();
   if (t->ntiles) {
     tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, dec, n32,
                                                     t->tile_nnz, t->tile_iv.as<uint32_t>());
     ALTO_LAUNCHED();
+    std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
+    ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+    for (int m = 0; m < N; ++m) {
+      auto& v = t->tile_len_sorted[m];
+      v.resize(t->ntiles);
+      for (uint32_t k = 0; k < t->ntiles; ++k) v[k] = iv[((size_t)k * N + m) * 2 + 1];
+      std::sort(v.begin(), v.end());
+    }
   }
 
   // the reference's partitions
@@ -621,10 +659,103 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   uint64_t* d_dims = d_ptr + nprtn + 1;
   ALTO_TRY_CUDA(cudaMemcpyAsync(d_ptr, t->prtn_ptr.data(), (nprtn + 1) * 8, cudaMemcpyHostToDevice, st));
   ALTO_TRY_CUDA(cudaMemcpyAsync(d_dims, t->dims, N * 8, cudaMemcpyHostToDevice, st));
-  prtn_interval_kernel<<<nprtn, 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, dec, d_ptr, d_dims,
-                                              d_iv);
+unsigned long long* d_ivu = reinterpret_cast<unsigned long long*>(d_iv);
+  prtn_interval_init_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(d_dims, N, nprtn, d_ivu);
+  ALTO_LAUNCHED();
+  if (nnz) {
+    prtn_interval_kernel<<<(unsigned)((nnz + kPrtnChunk - 1) / kPrtnChunk), 256, 0, st>>>(
+        t->klo.as<uint64_t>(), t->khi.p, dec, nnz, per, d_ivu);
+    ALTO_LAUNCHED();
+  }
+  prtn_interval_fix_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(nprtn * N, d_ivu);
   ALTO_LAUNCHED();
   if (!coo->on_device) ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // host COO must outlive the copies
+  return ALTO_OK;
+}
+
+// ------------------------------------------------ per-mode row-sorted lines
+
+// Row index of every line entry for one mode, and the identity payload.
+__global__ void mode_rows_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
+                                 LineDecode dec, int mode, uint32_t nnz, uint64_t* __restrict__ rows,
+                                 uint32_t* __restrict__ pos) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    rows[i] = line_field(llo[i], load_hi(lhi, dec.hi_words, i), dec.pos[mode], dec.mask[mode]);
+    pos[i] = i;
+  }
+}
+
+// Gather the line in the given order (key words and value).
+__global__ void gather_line_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
+                                   const float* __restrict__ vals, int hi_words,
+                                   const uint32_t* __restrict__ order, uint32_t nnz,
+                                   uint64_t* __restrict__ olo, void* __restrict__ ohi,
+                                   float* __restrict__ ovals) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    const uint32_t p = order[i];
+    olo[i] = llo[p];
+    if (hi_words == 1) ((uint32_t*)ohi)[i] = ((const uint32_t*)lhi)[p];
+    if (hi_words == 2) ((uint64_t*)ohi)[i] = ((const uint64_t*)lhi)[p];
+    ovals[i] = vals[p];
+  }
+}
+
+// A copy of the line ordered by the row of `mode`, ALTO order kept among
+// equal rows (stable LSD sort over the mode's bits).  This is the device
+// form of the reference's op_sched traversal (include/alto.hpp:1708-1801,
+// oidx from sort_alto_rowsparse :1100-1126): runs of one output row become
+// contiguous, so they reduce in registers and need one update per run.
+alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
+  SortedLine& s = t->sorted[mode];
+  const uint64_t nnz = t->nnz;
+  const int hw = t->dec.hi_words;
+  ALTO_TRY(s.klo.ensure(std::max<uint64_t>(nnz, 1) * 8));
+  if (hw) ALTO_TRY(s.khi.ensure(std::max<uint64_t>(nnz, 1) * (hw == 1 ? 4 : 8)));
+  ALTO_TRY(s.vals.ensure(std::max<uint64_t>(nnz, 1) * 4));
+  const size_t cap = std::max<uint64_t>(nnz, 1);
+  const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
+  size_t off = 0;
+  size_t o_r0 = off; off = align_up(off + cap * 8, 256);
+  size_t o_r1 = off; off = align_up(off + cap * 8, 256);
+  size_t o_p0 = off; off = align_up(off + cap * 4, 256);
+  size_t o_p1 = off; off = align_up(off + cap * 4, 256);
+  size_t o_cnt = off; off = align_up(off + (size_t)kRadix * std::max<size_t>(tiles_sort, 1) * 4, 256);
+  ALTO_TRY(t->scratch.ensure(off));
+  char* sb = t->scratch.as<char>();
+  uint64_t* rk[2] = {(uint64_t*)(sb + o_r0), (uint64_t*)(sb + o_r1)};
+  uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
+  uint32_t* counts = (uint32_t*)(sb + o_cnt);
+  const uint32_t n32 = (uint32_t)nnz;
+  if (nnz) {
+    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, t->dec, mode,
+                                                         n32, rk[0], pm[0]);
+    ALTO_LAUNCHED();
+    int cur = 0;
+    const uint32_t ntiles = (uint32_t)tiles_sort;
+    for (int shift = 0; shift < t->mode_bits[mode]; shift += kRadixBits) {
+      radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(rk[cur], nullptr, n32, shift, ntiles, counts);
+      ALTO_LAUNCHED();
+      ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, t->scan_scratch, st));
+      radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(rk[cur], nullptr, pm[cur], n32, shift, ntiles,
+                                                            counts, rk[cur ^ 1], nullptr, pm[cur ^ 1]);
+      ALTO_LAUNCHED();
+      cur ^= 1;
+    }
+    gather_line_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p,
+                                                           t->vals.as<float>(), hw, pm[cur], n32,
+                                                           s.klo.as<uint64_t>(), s.khi.p,
+                                                           s.vals.as<float>());
+    ALTO_LAUNCHED();
+  }
+  s.ntiles = t->ntiles;
+  ALTO_TRY(s.tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * t->nmodes * 2 * 4));
+  if (t->ntiles) {
+    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(s.klo.as<uint64_t>(), s.khi.p, t->dec, n32,
+                                                    t->tile_nnz, s.tile_iv.as<uint32_t>());
+    ALTO_LAUNCHED();
+  }
+  s.ready = true;
+  s.for_nnz = nnz;
   return ALTO_OK;
 }
 

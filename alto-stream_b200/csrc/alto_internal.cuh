@@ -114,6 +114,22 @@ alto_status exclusive_scan_u32(uint32_t* data, size_t n, DevBuf& scratch, cudaSt
 
 // ------------------------------------------------------------- the handle
 
+namespace alto {
+// A copy of the line ordered by one mode's row (see build_sorted_line).
+struct SortedLine {
+  DevBuf klo, khi, vals, tile_iv;
+  uint32_t ntiles = 0;
+  uint64_t for_nnz = 0;
+  bool ready = false;
+};
+
+// Tuned MTTKRP choice per (mode, rank, factor dtype).
+struct TuneEntry {
+  int mode, rank, fdtype;
+  alto_mttkrp_variant variant;
+};
+}  // namespace alto
+
 struct alto_tensor {
   int nmodes = 0;
   int nprtn = 1;
@@ -146,6 +162,14 @@ struct alto_tensor {
   std::vector<uint64_t> prtn_ptr;
   alto::DevBuf prtn_iv;  // uint64 [nprtn * nmodes * 2]
 
+  // Row-sorted copies of the line, built on first use per mode.
+  alto::SortedLine sorted[ALTO_MAX_MODES];
+  // Per mode, the tiles' interval lengths in ascending order (host copy),
+  // used to decide whether per-tile shared-memory staging can pay off.
+  std::vector<uint32_t> tile_len_sorted[ALTO_MAX_MODES];
+  // Variants chosen by alto_mttkrp_autotune, per (mode, rank, dtype).
+  std::vector<alto::TuneEntry> tuned;
+
   // Construction scratch (sort buffers, scan partials).
   alto::DevBuf scratch;
   alto::DevBuf scan_scratch;
@@ -163,4 +187,9 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
                        int rank, float* out, int accumulate, alto_mttkrp_variant variant,
                        cudaStream_t st);
 alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype);
+// Build the per-mode row-sorted copy of the line.
+alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st);
+// Measure the variants per mode and record the fastest (synchronous).
+alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype, int rank,
+                     cudaStream_t st, alto_mttkrp_variant* chosen);
 }  // namespace alto

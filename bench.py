@@ -250,6 +250,8 @@ def ours(args):
     factors = [(torch.rand((d, R), generator=g, device=dev) * 2 - 1).contiguous() for d in DIMS]
     outs = [torch.empty((d, R), device=dev, dtype=torch.float32) for d in DIMS]
     stream = torch.cuda.current_stream()
+    variants = t.autotune(factors, R)  # project autotuner: fastest kernel variant per mode
+    vnames = {A.ATOMIC: "atomic", A.STAGED: "staged", A.STREAM: "stream", A.SORTED: "sorted"}
 
     def step(ev=None):
         for m in range(N):
@@ -351,7 +353,9 @@ def ours(args):
                        "values": "lognormal(0,1)", "key_bits": t.key_bits, "alto_bits": alto_bits,
                        "factor_dtype": "f32", "parallelism": f"independent tensor per GPU x{world}",
                        "l2": "inputs larger than L2 (line + factors > 3 GB); no flush",
-                       "line_bytes_per_nnz": line_bytes_per_nnz(alto_bits)},
+                       "line_bytes_per_nnz": line_bytes_per_nnz(alto_bits),
+                       "variants": [vnames.get(v, str(v)) for v in variants],
+                       "device_bytes": t.device_bytes()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic.get("bytes_per_launch") if traffic else None,

@@ -49,7 +49,7 @@ typedef enum {
   ALTO_MTTKRP_ATOMIC = 1,   /* vector atomics per nonzero, consecutive equal rows merged in the warp */
   ALTO_MTTKRP_STAGED = 2,   /* partition-local output rows staged in shared memory (da_mem_pull)    */
   ALTO_MTTKRP_STREAM = 3,   /* single or few output rows held in registers (mttkrp_alto_stream)     */
-  ALTO_MTTKRP_SORTED = 4    /* nonzeros visited in output-row order, run reduction (op_sched)       */
+  ALTO_MTTKRP_SORTED = 4    /* a row-sorted copy of the line, runs reduced in registers (op_sched)  */
 } alto_mttkrp_variant;
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
@@ -144,6 +144,14 @@ alto_status alto_mttkrp(alto_tensor* t, int mode, const void* const* factors, al
 alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const* factors,
                                     alto_dtype fdtype, int rank, float* out, int accumulate,
                                     alto_mttkrp_variant variant, alto_cuda_stream stream);
+
+/* Project autotuner: time every applicable variant once per mode with these
+ * factors (rank, fdtype) and make ALTO_MTTKRP_AUTO use the fastest.
+ * variants (may be NULL) receives the choice per mode.  Synchronous; call
+ * it outside stream capture.  The reference fixes its choice at compile
+ * time (rank/mode specialisation, include/alto.hpp:826-900). */
+alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,
+                                 int rank, alto_cuda_stream stream, alto_mttkrp_variant* variants);
 
 /* The variant ALTO_MTTKRP_AUTO resolves to for this tensor, mode and rank. */
 alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dtype fdtype,

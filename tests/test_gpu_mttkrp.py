@@ -53,14 +53,14 @@ def check_modes(dims, cidx, vals, R, variants=(A.AUTO,), dtype=None, seed=0):
 @pytest.mark.parametrize("name", FIXTURE_NAMES)
 def test_fixtures_rank8(name):
     dims, cidx, vals = load_fixture(name)
-    check_modes(dims, cidx, vals, 8, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+    check_modes(dims, cidx, vals, 8, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
 
 
 @pytest.mark.parametrize("R", [4, 8, 16, 32, 64, 128, 10, 33])
 def test_uniform_ranks(R):
     dims = np.array([1000, 1000, 1000], np.uint64)
     cidx, vals = synth.uniform_coo(dims, 150000, seed=R)
-    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.STAGED), seed=R)
+    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED), seed=R)
 
 
 @pytest.mark.parametrize("R", [8, 16, 32, 64])
@@ -69,20 +69,20 @@ def test_bf16_factor_storage(R):
 
     dims = np.array([800, 700, 900], np.uint64)
     cidx, vals = synth.uniform_coo(dims, 100000, seed=R + 1)
-    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC), dtype=torch.bfloat16, seed=R)
+    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.SORTED), dtype=torch.bfloat16, seed=R)
 
 
 def test_power_law_128bit_keys():
     """Zipf-1.2 coordinates with scattered labels and a 65-bit key."""
     dims = np.array([4800000, 1800000, 1800000], np.uint64)
     cidx, vals = synth.powerlaw_coo(dims, 200000, [1.2, 1.2, 1.2], seed=3, values="lognormal")
-    check_modes(dims, cidx, vals, 32, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+    check_modes(dims, cidx, vals, 32, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
 
 
 def test_five_modes_rank64():
     dims = np.array([100000, 100000, 10000, 1000, 100], np.uint64)
     cidx, vals = synth.powerlaw_coo(dims, 150000, [1.1, 1.1, None, None, None], seed=4)
-    check_modes(dims, cidx, vals, 64, variants=(A.AUTO, A.ATOMIC, A.STAGED))
+    check_modes(dims, cidx, vals, 64, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
 
 
 def test_stream_mode_single_row():
@@ -148,3 +148,25 @@ def test_launch_counter_advances():
     t.mttkrp(0, Fd, 8)
     torch.cuda.synchronize()
     assert A.kernel_launches() > n0
+
+
+def test_autotune_records_a_choice_per_mode():
+    import torch
+
+    dims = np.array([4800000, 1800000, 1800000], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 300000, [1.2, 1.2, 1.2], seed=5, values="lognormal")
+    R = 32
+    rng = np.random.default_rng(4)
+    Fd = to_dev([rng.uniform(-1, 1, (int(d), R)) for d in dims], torch.float32)
+    t = A.create_alto(dims, cidx, vals)
+    chosen = t.autotune(Fd, R)
+    assert len(chosen) == 3 and all(c in (A.ATOMIC, A.STAGED, A.SORTED) for c in chosen)
+    for m in range(3):
+        assert t.choose_variant(m, R) == chosen[m]
+    Fo = seen_by_gpu(Fd)
+    enc = O.build(dims, cidx, vals.astype(np.float32).astype(np.float64))
+    for m in range(3):
+        fs = [f.copy() for f in Fo]
+        fs[m][:] = 0
+        ref = O.mttkrp(enc, m, fs, R)[m]
+        assert rel_err(t.mttkrp(m, Fd, R).cpu().numpy(), ref) <= TOL
