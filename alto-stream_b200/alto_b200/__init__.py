@@ -38,7 +38,7 @@ EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
     "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
-    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_cpd_als", "alto_stream_open",
+    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
 ]
 
@@ -288,6 +288,20 @@ class AltoTensor:
             self.close()
         except Exception:
             pass
+
+
+def gram(U, out=None, stream=None):
+    """update_gram: G = U^T U (float64, full symmetric) of a float32 CUDA tensor."""
+    import torch
+
+    if U.dtype != torch.float32 or not U.is_contiguous() or U.dim() != 2:
+        raise ValueError("U must be a contiguous 2-D float32 tensor")
+    rows, rank = U.shape
+    if out is None:
+        out = torch.empty((rank, rank), dtype=torch.float64, device=U.device)
+    check(lib().alto_gram(c_void_p(U.data_ptr()), c_uint64(rows), c_int(rank), c_void_p(out.data_ptr()),
+                          _stream_handle(stream)))
+    return out
 
 
 # ------------------------------------------------- reference-named mirrors

@@ -571,3 +571,17 @@ alto_status rank_update(double* G, const double* S, uint64_t rows, int R, cudaSt
 }
 
 }  // namespace alto
+
+extern "C" alto_status alto_gram(const float* U, uint64_t rows, int rank, double* G,
+                                 alto_cuda_stream stream) {
+  if (!G || (rows && !U)) {
+    alto::set_error("U or G is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  if (rank < 1 || rank > 128) {
+    alto::set_error("rank %d outside 1..128", rank);
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  static thread_local alto::DevBuf* partials = new alto::DevBuf();
+  return alto::gram(U, rows, rank, G, *partials, (cudaStream_t)stream);
+}

@@ -164,6 +164,16 @@ alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dt
 alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const* factors_host, int rank,
                              alto_cuda_stream stream);
 
+/* ------------------------------------------------------ dense helpers */
+
+/* G = U^T U in float64 (rank x rank, full symmetric, row-major, device) of a
+ * float32 factor U (rows x rank, row-major, device): update_gram / mat_aTa
+ * (src/gram.cpp:29-41, src/matrix.cpp:252-267; the reference's dsyrk fills
+ * only the upper triangle, here both are written).  rank <= 128.  The
+ * per-block partial sums live in device memory the library allocates and
+ * keeps for later calls. */
+alto_status alto_gram(const float* U, uint64_t rows, int rank, double* G, alto_cuda_stream stream);
+
 /* --------------------------------------------------------------- CP-ALS */
 
 /* CP-ALS on the device (cpd_alto, include/cpd.hpp:47-191).  U_host[n]
