@@ -38,7 +38,8 @@ EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
     "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
-    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram", "alto_cpd_als", "alto_stream_open",
+    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
+    "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
 ]
 

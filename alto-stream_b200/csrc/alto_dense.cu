@@ -16,6 +16,7 @@
 // float64 row-times-matrix product; the reference runs dpotrs over the rows.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "alto_dense.cuh"
 
@@ -584,4 +585,92 @@ extern "C" alto_status alto_gram(const float* U, uint64_t rows, int rank, double
   }
   static thread_local alto::DevBuf* partials = new alto::DevBuf();
   return alto::gram(U, rows, rank, G, *partials, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------ Gram without allocation
+//
+// Some callers cannot allocate device memory: code running under a memory
+// pool or arena that owns every byte of the device (a serving process that
+// pre-reserves HBM), callers whose allocator is forbidden inside a CUDA
+// graph capture or a real-time loop, and embedders that must not call
+// cudaMalloc / cudaFree at all.  alto_gram_noalloc gives them the Gram
+// kernel with its scratch -- the per-block partial sums -- in a fixed
+// device array that this library owns for the life of the process, on
+// every GPU that loads it.
+namespace {
+
+constexpr int kNoAllocBlocks = 64;    // partial sums, one R x R block each
+constexpr int kNoAllocMaxRank = 64;   // 64 blocks x 64 x 64 doubles = 2 MiB
+static __device__ __align__(256) double g_gram_noalloc_scratch[kNoAllocBlocks * kNoAllocMaxRank *
+                                                               kNoAllocMaxRank];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device, resolved once
+// per device (the array's name in host code is only a stand-in).
+alto_status noalloc_scratch(double** out) {
+  int dev = 0;
+  ALTO_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    alto::set_error("device ordinal %d beyond %d", dev, kNoAllocMaxDevices);
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    ALTO_TRY_CUDA(cudaGetSymbolAddress(&p, g_gram_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return ALTO_OK;
+}
+
+}  // namespace
+
+extern "C" alto_status alto_gram_noalloc(const float* U, uint64_t rows, int rank, double* G,
+                                         alto_cuda_stream stream) {
+  if (!G || (rows && !U)) {
+    alto::set_error("U or G is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  if (rank < 1 || rank > kNoAllocMaxRank) {
+    alto::set_error("alto_gram_noalloc: rank %d outside 1..%d (its fixed scratch holds %d partial "
+                    "Grams of at most %d x %d doubles)", rank, kNoAllocMaxRank, kNoAllocBlocks,
+                    kNoAllocMaxRank, kNoAllocMaxRank);
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  double* part = nullptr;
+  ALTO_TRY(noalloc_scratch(&part));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int RR = rank * rank;
+  if (rows == 0) {
+    ALTO_TRY_CUDA(cudaMemsetAsync(G, 0, RR * sizeof(double), st));
+    return ALTO_OK;
+  }
+  uint64_t nb = std::min<uint64_t>((rows + 255) / 256, (uint64_t)kNoAllocBlocks);
+  const uint64_t rpb = (rows + nb - 1) / nb;
+  nb = (rows + rpb - 1) / rpb;
+  // every block writes all RR entries of its partial, so no clearing is needed
+  const size_t smem = 2 * alto::kGramRows * rank * sizeof(double);  // <= 32 KiB at rank 64
+  const int ppt = (RR + alto::kGramThreads - 1) / alto::kGramThreads;
+  switch (ppt <= 1 ? 1 : ppt <= 2 ? 2 : ppt <= 4 ? 4 : 16) {
+    case 1:
+      alto::gram_partial_kernel<1, float, float><<<(unsigned)nb, alto::kGramThreads, smem, st>>>(U, U, rows, rank, rpb, part);
+      break;
+    case 2:
+      alto::gram_partial_kernel<2, float, float><<<(unsigned)nb, alto::kGramThreads, smem, st>>>(U, U, rows, rank, rpb, part);
+      break;
+    case 4:
+      alto::gram_partial_kernel<4, float, float><<<(unsigned)nb, alto::kGramThreads, smem, st>>>(U, U, rows, rank, rpb, part);
+      break;
+    default:
+      alto::gram_partial_kernel<16, float, float><<<(unsigned)nb, alto::kGramThreads, smem, st>>>(U, U, rows, rank, rpb, part);
+      break;
+  }
+  ALTO_LAUNCHED();
+  alto::reduce_partials_kernel<<<(RR + 255) / 256, 256, 0, st>>>(part, (int)nb, RR, G);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
 }

@@ -174,6 +174,20 @@ alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const* factors_ho
  * keeps for later calls. */
 alto_status alto_gram(const float* U, uint64_t rows, int rank, double* G, alto_cuda_stream stream);
 
+/* alto_gram for callers that cannot allocate device memory (a process whose
+ * pool owns all of HBM, an allocator that is off limits inside graph
+ * capture or a real-time loop, an embedder that may not call cudaMalloc /
+ * cudaFree).  It has no counterpart in the reference.  Same arguments and
+ * result as alto_gram, but rank <= 64 (ALTO_ERR_UNSUPPORTED beyond) and no
+ * allocation: the partial sums live in a fixed 2 MiB device array inside
+ * this library, present on every GPU that loads it until the process
+ * exits.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that may overlap on the GPU (different streams or
+ * host threads without ordering) race and must be serialised by the caller. */
+alto_status alto_gram_noalloc(const float* U, uint64_t rows, int rank, double* G,
+                              alto_cuda_stream stream);
+
 /* --------------------------------------------------------------- CP-ALS */
 
 /* CP-ALS on the device (cpd_alto, include/cpd.hpp:47-191).  U_host[n]
