@@ -31,6 +31,7 @@ LIB_PATH = os.path.join(HERE, "libalto_b200.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_SPD, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
 F32, BF16, F64 = 0, 1, 2
 AUTO, ATOMIC, STAGED, STREAM, SORTED = range(5)
+FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
 UNCONSTRAINED, NONNEG, LASSO = range(3)
 FIT_REFERENCE, FIT_EXACT = 0, 1
 

@@ -19,7 +19,7 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
-alto_status export_keys(const alto_tensor* t, uint64_t* d_out, cudaStream_t st);
+alto_status export_keys(const alto_tensor* t, uint64_t* d_out, float* d_vals, cudaStream_t st);
 
 static alto_status check_coo(const alto_coo* coo) {
   if (!coo) {
@@ -221,16 +221,14 @@ alto_status alto_tensor_export(const alto_tensor* t, uint64_t* masks, uint64_t* 
     ALTO_TRY_CUDA(cudaMemcpyAsync(intervals, t->prtn_iv.p, (size_t)t->nprtn * N * 2 * 8,
                                   cudaMemcpyDeviceToHost, st));
   if (nnz && (idx || vals || perm)) {
-    DevBuf tmp;
+    DevBuf tmp, tmpv;
     ALTO_TRY(tmp.ensure(nnz * 16));
-    if (idx) {
-      ALTO_TRY(export_keys(t, tmp.as<uint64_t>(), st));
-      ALTO_TRY_CUDA(cudaMemcpyAsync(idx, tmp.p, nnz * 16, cudaMemcpyDeviceToHost, st));
-      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-    }
+    ALTO_TRY(tmpv.ensure(nnz * 4));
+    ALTO_TRY(export_keys(t, idx ? tmp.as<uint64_t>() : nullptr, tmpv.as<float>(), st));
+    if (idx) ALTO_TRY_CUDA(cudaMemcpyAsync(idx, tmp.p, nnz * 16, cudaMemcpyDeviceToHost, st));
     if (vals) {
       std::vector<float> v(nnz);
-      ALTO_TRY_CUDA(cudaMemcpyAsync(v.data(), t->vals.p, nnz * 4, cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaMemcpyAsync(v.data(), tmpv.p, nnz * 4, cudaMemcpyDeviceToHost, st));
       ALTO_TRY_CUDA(cudaStreamSynchronize(st));
       for (uint64_t i = 0; i < nnz; ++i) vals[i] = v[i];
     }
@@ -267,8 +265,10 @@ alto_status alto_tensor_device_bytes(const alto_tensor* t, uint64_t* bytes) {
     set_error("tensor or bytes is NULL");
     return ALTO_ERR_INVALID;
   }
-  *bytes = t->klo.bytes + t->khi.bytes + t->vals.bytes + t->perm.bytes + t->tile_iv.bytes +
-           t->prtn_iv.bytes + t->scratch.bytes + t->scan_scratch.bytes;
+  uint64_t b = t->line.bytes + t->perm.bytes + t->tile_iv.bytes + t->prtn_iv.bytes + t->scratch.bytes +
+               t->scan_scratch.bytes + t->err.bytes;
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) b += t->sorted[m].line.bytes + t->sorted[m].tile_iv.bytes;
+  *bytes = b;
   return ALTO_OK;
 }
 
@@ -314,12 +314,15 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
                                     alto_dtype fdtype, int rank, float* out, int accumulate,
                                     alto_mttkrp_variant variant, alto_cuda_stream stream) {
   ALTO_TRY(check_mttkrp(t, mode, factors, fdtype, rank, out));
-  if (variant < ALTO_MTTKRP_AUTO || variant > ALTO_MTTKRP_SORTED) {
+  const int bulk = ((int)variant & ALTO_MTTKRP_FEED_BULK) ? 1 : 0;
+  const alto_mttkrp_variant v = (alto_mttkrp_variant)((int)variant & ~ALTO_MTTKRP_FEED_BULK);
+  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_SORTED ||
+      (bulk && v != ALTO_MTTKRP_ATOMIC && v != ALTO_MTTKRP_SORTED)) {
     set_error("unknown variant %d", (int)variant);
     return ALTO_ERR_INVALID;
   }
-  return run_mttkrp(t, mode, factors, fdtype, rank, out, accumulate, variant,
-                    (cudaStream_t)stream);
+  return run_mttkrp_feed(t, mode, factors, fdtype, rank, out, accumulate, v,
+                         v == ALTO_MTTKRP_AUTO ? -1 : bulk, (cudaStream_t)stream);
 }
 
 alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,

@@ -42,6 +42,8 @@ static unsigned ew_grid(uint64_t n) {
   return (unsigned)(b ? b : 1);
 }
 
+alto_status export_keys(const alto_tensor* t, uint64_t* d_out, float* d_vals, cudaStream_t st);
+
 alto_status convert_f64_to_f32(const double* a, uint64_t n, float* b, cudaStream_t st) {
   if (!n) return ALTO_OK;
   f64_to_f32_kernel<<<ew_grid(n), 256, 0, st>>>(a, n, b);
@@ -154,7 +156,13 @@ extern "C" alto_status alto_cpd_als(alto_tensor* t, int rank, double* const* U_h
   }
   ALTO_TRY_CUDA(cudaMemcpyAsync(lam.p, lambda_host, R * 8, cudaMemcpyHostToDevice, st));
   double* d_scal = scal.as<double>();  // [0] normX, [1..3] dot stats, [4] normU
-  ALTO_TRY(sum_squares(t->vals.as<float>(), t->nnz, d_scal + 0, dscr, st));
+  {  // ||X||^2 over the stored (float32) values
+    DevBuf v;
+    ALTO_TRY(v.ensure(std::max<uint64_t>(t->nnz, 1) * 4));
+    ALTO_TRY(export_keys(t, nullptr, v.as<float>(), st));
+    ALTO_TRY(sum_squares(v.as<float>(), t->nnz, d_scal + 0, dscr, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  }
 
   const void* fac[ALTO_MAX_MODES];
   for (int m = 0; m < N; ++m) fac[m] = bf16 ? Ub[m].p : U[m].p;

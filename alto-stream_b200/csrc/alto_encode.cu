@@ -228,13 +228,12 @@ __global__ void __launch_bounds__(kSortThreads)
   }
 }
 
-// Sorted interleaved keys -> mode-contiguous line keys, values gathered by
-// input position (float64 or float32 input, stored float32).
+// Sorted interleaved keys -> line records (mode-contiguous key + value), the
+// value gathered by input position (float64 or float32 input, stored float32).
 template <typename VT>
 __global__ void layout_kernel(const uint64_t* __restrict__ slo, const uint64_t* __restrict__ shi,
                               const uint32_t* __restrict__ sperm, const VT* __restrict__ vin,
-                              MaskSet ms, LineDecode dec, uint32_t nnz, uint64_t* __restrict__ llo,
-                              void* __restrict__ lhi, float* __restrict__ vout,
+                              MaskSet ms, LineDecode dec, uint32_t nnz, void* __restrict__ line,
                               uint32_t* __restrict__ perm_out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
     uint64_t klo = slo[i], khi = shi ? shi[i] : 0;
@@ -252,27 +251,17 @@ __global__ void layout_kernel(const uint64_t* __restrict__ slo, const uint64_t* 
         }
       }
     }
-    llo[i] = lo;
-    if (dec.hi_words == 1) ((uint32_t*)lhi)[i] = (uint32_t)hi;
-    if (dec.hi_words == 2) ((uint64_t*)lhi)[i] = hi;
-    uint32_t p = sperm[i];
-    vout[i] = (float)vin[p];
+    const uint32_t p = sperm[i];
+    rec_write(line, dec.hi_words, i, lo, hi, (float)vin[p]);
     perm_out[i] = p;
   }
-}
-
-__device__ __forceinline__ uint64_t load_hi(const void* khi, int hi_words, uint32_t i) {
-  if (hi_words == 1) return ((const uint32_t*)khi)[i];
-  if (hi_words == 2) return ((const uint64_t*)khi)[i];
-  return 0;
 }
 
 // Per tile and mode: [min, max] row of the tile's nonzeros, stored as
 // (first row, row count).
 __global__ void __launch_bounds__(256)
-    tile_interval_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                         LineDecode dec, uint32_t nnz, uint32_t tile_nnz,
-                         uint32_t* __restrict__ tile_iv) {
+    tile_interval_kernel(const void* __restrict__ line, LineDecode dec, uint32_t nnz,
+                         uint32_t tile_nnz, uint32_t* __restrict__ tile_iv) {
   __shared__ uint32_t smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
   uint32_t lo_r[ALTO_MAX_MODES], hi_r[ALTO_MAX_MODES];
 #pragma unroll
@@ -283,7 +272,9 @@ __global__ void __launch_bounds__(256)
   uint32_t s = blockIdx.x * tile_nnz;
   uint32_t e = min(s + tile_nnz, nnz);
   for (uint32_t i = s + threadIdx.x; i < e; i += blockDim.x) {
-    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, i);
+    uint64_t lo, hi;
+    float val;
+    rec_read(line, dec.hi_words, i, lo, hi, val);
 #pragma unroll
     for (int m = 0; m < ALTO_MAX_MODES; ++m) {
       if (m < dec.nmodes) {
@@ -342,8 +333,7 @@ __global__ void prtn_interval_fix_kernel(int n, unsigned long long* __restrict__
 }
 
 __global__ void __launch_bounds__(256)
-    prtn_interval_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                         LineDecode dec, uint64_t nnz, uint64_t per,
+    prtn_interval_kernel(const void* __restrict__ line, LineDecode dec, uint64_t nnz, uint64_t per,
                          unsigned long long* __restrict__ iv) {
   __shared__ unsigned long long smin[ALTO_MAX_MODES][8], smax[ALTO_MAX_MODES][8];
   const uint64_t cs = (uint64_t)blockIdx.x * kPrtnChunk;
@@ -360,7 +350,9 @@ __global__ void __launch_bounds__(256)
       hi_r[m] = 0;
     }
     for (uint64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
-      const uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, (uint32_t)i);
+      uint64_t lo, hi;
+      float val;
+      rec_read(line, dec.hi_words, i, lo, hi, val);
 #pragma unroll
       for (int m = 0; m < ALTO_MAX_MODES; ++m) {
         if (m < dec.nmodes) {
@@ -535,13 +527,11 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
   // capacity of the per-nonzero arrays
   uint64_t cap = std::max<uint64_t>(nnz, 1);
-  if (cap > t->cap || !t->klo.p) {
-    ALTO_TRY(t->klo.ensure(cap * 8));
-    ALTO_TRY(t->vals.ensure(cap * 4));
+  ALTO_TRY(t->line.ensure((cap + kLinePad) * rec_bytes(dec.hi_words)));
+  if (cap > t->cap || !t->perm.p) {
     ALTO_TRY(t->perm.ensure(cap * 4));
     t->cap = cap;
   }
-  if (dec.hi_words) ALTO_TRY(t->khi.ensure(cap * (dec.hi_words == 1 ? 4 : 8)));
 
   // construction scratch: two key/payload buffers, staged COO, counts
   const bool two_words = total > 64;
@@ -614,12 +604,10 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
     if (coo->val_dtype == ALTO_F64)
       layout_kernel<double><<<grid_for(nnz, 256), 256, 0, st>>>(
-          klo[cur], khi[cur], pm[cur], (const double*)vin, ms, dec, n32, t->klo.as<uint64_t>(),
-          t->khi.p, t->vals.as<float>(), t->perm.as<uint32_t>());
+          klo[cur], khi[cur], pm[cur], (const double*)vin, ms, dec, n32, t->line.p, t->perm.as<uint32_t>());
     else
       layout_kernel<float><<<grid_for(nnz, 256), 256, 0, st>>>(
-          klo[cur], khi[cur], pm[cur], (const float*)vin, ms, dec, n32, t->klo.as<uint64_t>(),
-          t->khi.p, t->vals.as<float>(), t->perm.as<uint32_t>());
+          klo[cur], khi[cur], pm[cur], (const float*)vin, ms, dec, n32, t->line.p, t->perm.as<uint32_t>());
     ALTO_LAUNCHED();
   }
 
@@ -632,8 +620,8 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   }
   t->tuned.clear();
   if (t->ntiles) {
-    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, dec, n32,
-                                                    t->tile_nnz, t->tile_iv.as<uint32_t>());
+    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->line.p, dec, n32, t->tile_nnz,
+                                                    t->tile_iv.as<uint32_t>());
     ALTO_LAUNCHED();
     std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
     ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -664,7 +652,7 @@ unsigned long long* d_ivu = reinterpret_cast<unsigned long long*>(d_iv);
   ALTO_LAUNCHED();
   if (nnz) {
     prtn_interval_kernel<<<(unsigned)((nnz + kPrtnChunk - 1) / kPrtnChunk), 256, 0, st>>>(
-        t->klo.as<uint64_t>(), t->khi.p, dec, nnz, per, d_ivu);
+        t->line.p, dec, nnz, per, d_ivu);
     ALTO_LAUNCHED();
   }
   prtn_interval_fix_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(nprtn * N, d_ivu);
@@ -676,27 +664,24 @@ unsigned long long* d_ivu = reinterpret_cast<unsigned long long*>(d_iv);
 // ------------------------------------------------ per-mode row-sorted lines
 
 // Row index of every line entry for one mode, and the identity payload.
-__global__ void mode_rows_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                                 LineDecode dec, int mode, uint32_t nnz, uint64_t* __restrict__ rows,
-                                 uint32_t* __restrict__ pos) {
+__global__ void mode_rows_kernel(const void* __restrict__ line, LineDecode dec, int mode, uint32_t nnz,
+                                 uint64_t* __restrict__ rows, uint32_t* __restrict__ pos) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
-    rows[i] = line_field(llo[i], load_hi(lhi, dec.hi_words, i), dec.pos[mode], dec.mask[mode]);
+    uint64_t lo, hi;
+    float v;
+    rec_read(line, dec.hi_words, i, lo, hi, v);
+    rows[i] = line_field(lo, hi, dec.pos[mode], dec.mask[mode]);
     pos[i] = i;
   }
 }
 
-// Gather the line in the given order (key words and value).
-__global__ void gather_line_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                                   const float* __restrict__ vals, int hi_words,
+// Gather line records (`words` 16-byte words each) in the given order.
+__global__ void gather_line_kernel(const uint4* __restrict__ line, int words,
                                    const uint32_t* __restrict__ order, uint32_t nnz,
-                                   uint64_t* __restrict__ olo, void* __restrict__ ohi,
-                                   float* __restrict__ ovals) {
+                                   uint4* __restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
     const uint32_t p = order[i];
-    olo[i] = llo[p];
-    if (hi_words == 1) ((uint32_t*)ohi)[i] = ((const uint32_t*)lhi)[p];
-    if (hi_words == 2) ((uint64_t*)ohi)[i] = ((const uint64_t*)lhi)[p];
-    ovals[i] = vals[p];
+    for (int w = 0; w < words; ++w) out[(size_t)i * words + w] = line[(size_t)p * words + w];
   }
 }
 
@@ -709,9 +694,7 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   SortedLine& s = t->sorted[mode];
   const uint64_t nnz = t->nnz;
   const int hw = t->dec.hi_words;
-  ALTO_TRY(s.klo.ensure(std::max<uint64_t>(nnz, 1) * 8));
-  if (hw) ALTO_TRY(s.khi.ensure(std::max<uint64_t>(nnz, 1) * (hw == 1 ? 4 : 8)));
-  ALTO_TRY(s.vals.ensure(std::max<uint64_t>(nnz, 1) * 4));
+  ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
   const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
   size_t off = 0;
@@ -727,8 +710,7 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   uint32_t* counts = (uint32_t*)(sb + o_cnt);
   const uint32_t n32 = (uint32_t)nnz;
   if (nnz) {
-    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, t->dec, mode,
-                                                         n32, rk[0], pm[0]);
+    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, mode, n32, rk[0], pm[0]);
     ALTO_LAUNCHED();
     int cur = 0;
     const uint32_t ntiles = (uint32_t)tiles_sort;
@@ -741,17 +723,15 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
       ALTO_LAUNCHED();
       cur ^= 1;
     }
-    gather_line_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p,
-                                                           t->vals.as<float>(), hw, pm[cur], n32,
-                                                           s.klo.as<uint64_t>(), s.khi.p,
-                                                           s.vals.as<float>());
+    gather_line_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.as<uint4>(), rec_bytes(hw) / 16,
+                                                           pm[cur], n32, s.line.as<uint4>());
     ALTO_LAUNCHED();
   }
   s.ntiles = t->ntiles;
   ALTO_TRY(s.tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * t->nmodes * 2 * 4));
   if (t->ntiles) {
-    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(s.klo.as<uint64_t>(), s.khi.p, t->dec, n32,
-                                                    t->tile_nnz, s.tile_iv.as<uint32_t>());
+    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(s.line.p, t->dec, n32, t->tile_nnz,
+                                                    s.tile_iv.as<uint32_t>());
     ALTO_LAUNCHED();
   }
   s.ready = true;
@@ -760,11 +740,14 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
 }
 
 // Re-derive the reference's interleaved key from the line key (export).
-__global__ void export_key_kernel(const uint64_t* __restrict__ llo, const void* __restrict__ lhi,
-                                  LineDecode dec, MaskSet ms, uint32_t nnz,
-                                  uint64_t* __restrict__ out) {
+__global__ void export_key_kernel(const void* __restrict__ line, LineDecode dec, MaskSet ms, uint32_t nnz,
+                                  uint64_t* __restrict__ out, float* __restrict__ vals) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
-    uint64_t lo = llo[i], hi = load_hi(lhi, dec.hi_words, i);
+    uint64_t lo, hi;
+    float v;
+    rec_read(line, dec.hi_words, i, lo, hi, v);
+    if (vals) vals[i] = v;
+    if (!out) continue;
     uint64_t klo = 0, khi = 0;
 #pragma unroll
     for (int m = 0; m < ALTO_MAX_MODES; ++m)
@@ -774,7 +757,9 @@ __global__ void export_key_kernel(const uint64_t* __restrict__ llo, const void* 
   }
 }
 
-alto_status export_keys(const alto_tensor* t, uint64_t* d_out, cudaStream_t st) {
+// Re-derive the interleaved keys (d_out, 2 words per nonzero, may be NULL)
+// and the values (d_vals, may be NULL) of the line.
+alto_status export_keys(const alto_tensor* t, uint64_t* d_out, float* d_vals, cudaStream_t st) {
   MaskSet ms{};
   ms.nmodes = t->nmodes;
   for (int m = 0; m < t->nmodes; ++m) {
@@ -782,8 +767,8 @@ alto_status export_keys(const alto_tensor* t, uint64_t* d_out, cudaStream_t st) 
     ms.hi[m] = t->masks[m].hi;
   }
   if (!t->nnz) return ALTO_OK;
-  export_key_kernel<<<grid_for(t->nnz, 256), 256, 0, st>>>(t->klo.as<uint64_t>(), t->khi.p, t->dec,
-                                                           ms, (uint32_t)t->nnz, d_out);
+  export_key_kernel<<<grid_for(t->nnz, 256), 256, 0, st>>>(t->line.p, t->dec, ms, (uint32_t)t->nnz, d_out,
+                                                           d_vals);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }

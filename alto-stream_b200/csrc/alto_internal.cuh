@@ -96,6 +96,60 @@ struct LineDecode {
   uint64_t mask[ALTO_MAX_MODES];  // (1 << bits) - 1
 };
 
+// Entries of padding after every line array, so that bulk copies rounded
+// up to 16 bytes stay inside the allocation.
+constexpr uint64_t kLinePad = 16;
+
+// One line record per nonzero: the mode-contiguous key and the value, read
+// with one 16-byte load when the key fits 96 bits (hi_words <= 1):
+//   {key bits 0..63, key bits 64..95, value}
+// and with two when it needs up to 128 bits (hi_words == 2):
+//   {key bits 0..63, key bits 64..127, value, 12 bytes of padding}.
+struct __align__(16) LineRec16 {
+  uint64_t lo;
+  uint32_t hi;
+  float v;
+};
+struct __align__(16) LineRec32 {
+  uint64_t lo;
+  uint64_t hi;
+  float v;
+  uint32_t pad[3];
+};
+
+__host__ __device__ __forceinline__ int rec_bytes(int hi_words) { return hi_words == 2 ? 32 : 16; }
+
+// Read record i of a line with any key width.
+__device__ __forceinline__ void rec_read(const void* line, int hi_words, uint64_t i, uint64_t& lo,
+                                         uint64_t& hi, float& v) {
+  if (hi_words == 2) {
+    const LineRec32 r = static_cast<const LineRec32*>(line)[i];
+    lo = r.lo;
+    hi = r.hi;
+    v = r.v;
+  } else {
+    const uint4 q = static_cast<const uint4*>(line)[i];
+    lo = (uint64_t)q.x | ((uint64_t)q.y << 32);
+    hi = q.z;
+    v = __uint_as_float(q.w);
+  }
+}
+
+__device__ __forceinline__ void rec_write(void* line, int hi_words, uint64_t i, uint64_t lo, uint64_t hi,
+                                          float v) {
+  if (hi_words == 2) {
+    LineRec32 r;
+    r.lo = lo;
+    r.hi = hi;
+    r.v = v;
+    r.pad[0] = r.pad[1] = r.pad[2] = 0;
+    static_cast<LineRec32*>(line)[i] = r;
+  } else {
+    static_cast<uint4*>(line)[i] =
+        make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, __float_as_uint(v));
+  }
+}
+
 // Field of mode-contiguous key (lo, hi) at bit pos with the given mask; hi is
 // 0 when the key has no high part.
 __device__ __forceinline__ uint64_t line_field(uint64_t lo, uint64_t hi, int pos, uint64_t mask) {
@@ -117,7 +171,7 @@ alto_status exclusive_scan_u32(uint32_t* data, size_t n, DevBuf& scratch, cudaSt
 namespace alto {
 // A copy of the line ordered by one mode's row (see build_sorted_line).
 struct SortedLine {
-  DevBuf klo, khi, vals, tile_iv;
+  DevBuf line, tile_iv;
   uint32_t ntiles = 0;
   uint64_t for_nnz = 0;
   bool ready = false;
@@ -127,6 +181,7 @@ struct SortedLine {
 struct TuneEntry {
   int mode, rank, fdtype;
   alto_mttkrp_variant variant;
+  bool bulk_feed;  // line streamed through shared memory by bulk copy
 };
 }  // namespace alto
 
@@ -144,11 +199,9 @@ struct alto_tensor {
   int mode_bits[ALTO_MAX_MODES] = {0};
   alto::LineDecode dec = {};
 
-  // The line: per nonzero, the mode-contiguous key and the value, in ALTO
-  // (bit-interleaved key) order.
-  alto::DevBuf klo;    // uint64 [cap]
-  alto::DevBuf khi;    // uint32 or uint64 [cap] (only when alto_bits > 64)
-  alto::DevBuf vals;   // float   [cap]
+  // The line: per nonzero, one record (mode-contiguous key and value, see
+  // LineRec16 / LineRec32) in ALTO (bit-interleaved key) order.
+  alto::DevBuf line;   // records [cap + kLinePad]
   alto::DevBuf perm;   // uint32  [cap]: input position of each line entry
 
   // Tiles of the line used by the MTTKRP kernels: tile t covers
@@ -170,6 +223,9 @@ struct alto_tensor {
   // Variants chosen by alto_mttkrp_autotune, per (mode, rank, dtype).
   std::vector<alto::TuneEntry> tuned;
 
+  // Device error word of the kernels' bounded waits (0 = none).
+  alto::DevBuf err;
+
   // Construction scratch (sort buffers, scan partials).
   alto::DevBuf scratch;
   alto::DevBuf scan_scratch;
@@ -186,6 +242,9 @@ int setup_masks(int nmodes, const uint64_t* dims, int max_bits, Key2* masks, Key
 alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                        int rank, float* out, int accumulate, alto_mttkrp_variant variant,
                        cudaStream_t st);
+alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
+                            int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
+                            cudaStream_t st);
 alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype);
 // Build the per-mode row-sorted copy of the line.
 alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st);

@@ -44,9 +44,7 @@ struct FactorSet {
 };
 
 struct MttkrpArgs {
-  const uint64_t* klo;
-  const void* khi;
-  const float* vals;
+  const void* line;  // line records (LineRec16 / LineRec32)
   const uint32_t* tile_iv;
   uint32_t nnz;
   uint32_t tile_nnz;
@@ -77,12 +75,6 @@ __device__ __forceinline__ float4 load4<__nv_bfloat16>(const void* base, size_t 
   return r;
 }
 
-template <int HW>
-__device__ __forceinline__ uint64_t hi_word(const void* khi, uint32_t i) {
-  if (HW == 1) return __ldg(static_cast<const uint32_t*>(khi) + i);
-  if (HW == 2) return __ldg(static_cast<const uint64_t*>(khi) + i);
-  return 0;
-}
 
 // Decode one mode's field from the line key held as 32-bit words
 // w0..w3 (w0 lowest): a funnel shift of the two words the field starts in.
@@ -100,12 +92,14 @@ __device__ __forceinline__ uint32_t field32(uint32_t w0, uint32_t w1, uint32_t w
   return v & mask;
 }
 
-// V consecutive floats of a factor row (V = 4 or 8 or 16).
-template <typename FT, int V>
-__device__ __forceinline__ void load_row(const void* base, size_t off, float (&x)[V]) {
+// This lane's V floats of a factor row: V/4 float4 pieces at columns
+// q*4G + 4*sub (q = 0..V/4-1), so that one load instruction of the G lanes of
+// a group reads 4G contiguous floats (whole 32-byte sectors).
+template <typename FT, int V, int G>
+__device__ __forceinline__ void load_row(const void* base, size_t row_off, int sub, float (&x)[V]) {
 #pragma unroll
   for (int q = 0; q < V / 4; ++q) {
-    const float4 f = load4<FT>(base, off + q * 4);
+    const float4 f = load4<FT>(base, row_off + q * 4 * G + sub * 4);
     x[q * 4 + 0] = f.x;
     x[q * 4 + 1] = f.y;
     x[q * 4 + 2] = f.z;
@@ -113,47 +107,89 @@ __device__ __forceinline__ void load_row(const void* base, size_t off, float (&x
   }
 }
 
-// One update of output row `row` with this lane's V floats (at column c0).
-template <int R, int V>
+// One update of output row `row` with this lane's V floats.
+template <int R, int V, int G>
 __device__ __forceinline__ void flush_row(bool staged, float* smem, uint32_t iv_start, float* out,
-                                          uint32_t row, int c0, const float (&acc)[V]) {
+                                          uint32_t row, int sub, const float (&acc)[V]) {
   if (staged) {
-    float* s = smem + (size_t)(row - iv_start) * R + c0;
-#pragma unroll
-    for (int q = 0; q < V; ++q) atomicAdd(s + q, acc[q]);
-  } else {
-    float* o = out + (size_t)row * R + c0;
+    float* s = smem + (size_t)(row - iv_start) * R + sub * 4;
 #pragma unroll
     for (int q = 0; q < V / 4; ++q)
-      atomicAdd(reinterpret_cast<float4*>(o + q * 4),
+#pragma unroll
+      for (int k = 0; k < 4; ++k) atomicAdd(s + q * 4 * G + k, acc[q * 4 + k]);
+  } else {
+    float* o = out + (size_t)row * R + sub * 4;
+#pragma unroll
+    for (int q = 0; q < V / 4; ++q)
+      atomicAdd(reinterpret_cast<float4*>(o + q * 4 * G),
                 make_float4(acc[q * 4], acc[q * 4 + 1], acc[q * 4 + 2], acc[q * 4 + 3]));
   }
 }
 
-// Floats per lane for rank R: 8 where the rank allows (R >= 8), else R.
+// Floats per lane for rank R: 4, so the G = R/4 lanes of a group read one
+// factor row with one 16-byte load each -- whole 128-byte lines at R = 32,
+// which keeps the L1 data pipe at one wavefront per row.
 template <int R>
 struct LaneWidth {
-  static constexpr int V = R >= 8 ? 8 : R;
+  static constexpr int V = 4;
   static constexpr int G = R / V;     // lanes per nonzero
   static constexpr int NPW = 32 / G;  // groups (nonzeros in flight) per warp
 };
 
+// Keys and values of U consecutive line records, from global memory or
+// from the line tile staged in shared memory (SMEM): one 16-byte load per
+// record (two when the key needs more than 96 bits, HW == 2).
+template <int HW, int U, bool SMEM>
+__device__ __forceinline__ void load_keys(const void* line, uint32_t i0, uint32_t ge,
+                                          uint32_t (&w)[U][4], float (&v)[U], bool (&valid)[U]) {
+  const uint4* q = static_cast<const uint4*>(line);
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const uint32_t i = i0 + u;
+    valid[u] = i < ge;
+    uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
+    if (valid[u]) {
+      if (HW == 2) {
+        a = SMEM ? q[2 * i] : __ldg(q + 2 * i);
+        b = SMEM ? q[2 * i + 1] : __ldg(q + 2 * i + 1);
+      } else {
+        a = SMEM ? q[i] : __ldg(q + i);
+      }
+    }
+    w[u][0] = a.x;
+    w[u][1] = a.y;
+    if (HW == 2) {
+      w[u][2] = a.z;
+      w[u][3] = a.w;
+      v[u] = __uint_as_float(b.x);
+    } else {
+      w[u][2] = a.z;
+      w[u][3] = 0;
+      v[u] = __uint_as_float(a.w);
+    }
+  }
+}
+
 // Walk line range [ws, we) with one warp: the range is split into NPW
 // contiguous sub-ranges, one per lane group; a group walks its sub-range in
-// order, two nonzeros per iteration (loads of both issued first), keeps the
-// running sum of the current output row in registers and updates the output
-// once per run of equal rows.  NM is the mode count (3, 4, 5 specialised as
-// in the reference's ALTO_MODES_SPECIALIZED, 8 for the rest).
-template <int R, typename FT, int HW, int NM>
-__device__ __forceinline__ void warp_range(const MttkrpArgs& a, uint32_t ws, uint32_t we,
+// order, U nonzeros per iteration (two for 3 modes, one for more, to stay in
+// registers), with the next iteration's keys loaded while this iteration's
+// factor rows are in flight; it keeps the running sum of the current output
+// row in registers and updates the output once per run of equal rows.  NM is
+// the mode count (3, 4, 5 specialised as in the reference's
+// ALTO_MODES_SPECIALIZED, 8 for the rest).
+template <int R, typename FT, int HW, int NM, bool SMEM>
+__device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
                                            bool staged, float* smem, uint32_t iv_start) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
-  constexpr int U = NM <= 3 ? 2 : 1;  // nonzeros per group per iteration
+  constexpr int U = NM <= 3 ? 2 : 1;
   const int lane = threadIdx.x & 31;
   const int grp = lane / G, sub = lane % G;
-  const int c0 = sub * V;
-  const uint32_t sublen = (we - ws + NPW - 1) / NPW;
+  // groups' sub-ranges; odd lengths when reading shared memory, so the
+  // groups' records fall in different banks
+  uint32_t sublen = (we - ws + NPW - 1) / NPW;
+  if (SMEM) sublen |= 1u;
   const uint32_t gs = min(ws + grp * sublen, we);
   const uint32_t ge = min(gs + sublen, we);
   float acc[V];
@@ -161,22 +197,11 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, uint32_t ws, uin
   for (int q = 0; q < V; ++q) acc[q] = 0.f;
   uint32_t cur = kNoRow;
 
+  uint32_t w[U][4];
+  float v[U];
+  bool valid[U];
+  load_keys<HW, U, SMEM>(line, gs, ge, w, v, valid);
   for (uint32_t k = 0; k < sublen; k += U) {
-    uint32_t w[U][4];
-    float v[U];
-    bool valid[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const uint32_t i = gs + k + u;
-      valid[u] = i < ge;
-      const uint64_t lo = valid[u] ? __ldg(a.klo + i) : 0;
-      const uint64_t hi = valid[u] ? hi_word<HW>(a.khi, i) : 0;
-      v[u] = valid[u] ? __ldg(a.vals + i) : 0.f;
-      w[u][0] = (uint32_t)lo;
-      w[u][1] = (uint32_t)(lo >> 32);
-      w[u][2] = (uint32_t)hi;
-      w[u][3] = (uint32_t)(hi >> 32);
-    }
     // factor rows of the NM-1 input modes (j-th input mode m = j, or j+1
     // past the target)
     float f[U][NM - 1][V];
@@ -187,26 +212,34 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, uint32_t ws, uin
         const int m = j < a.target ? j : j + 1;
         if (m < a.dec.nmodes && valid[u]) {
           const uint32_t r = field32(w[u][0], w[u][1], w[u][2], w[u][3], a.dec.pos[m], (uint32_t)a.dec.mask[m]);
-          load_row<FT, V>(a.fac.f[m], (size_t)r * R + c0, f[u][j]);
+          load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
         }
       }
     }
+    uint32_t rows[U];
+    float vals[U];
+    bool ok[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      if (!valid[u]) continue;
+      rows[u] = field32(w[u][0], w[u][1], w[u][2], w[u][3], a.dec.pos[a.target], (uint32_t)a.dec.mask[a.target]);
+      vals[u] = v[u];
+      ok[u] = valid[u];
+    }
+    load_keys<HW, U, SMEM>(line, gs + k + U, ge, w, v, valid);  // next iteration's keys
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u]) continue;
       float p[V];
 #pragma unroll
-      for (int q = 0; q < V; ++q) p[q] = v[u];
+      for (int q = 0; q < V; ++q) p[q] = vals[u];
 #pragma unroll
       for (int j = 0; j < NM - 1; ++j)
         if ((j < a.target ? j : j + 1) < a.dec.nmodes)
 #pragma unroll
           for (int q = 0; q < V; ++q) p[q] *= f[u][j][q];
-      const uint32_t row =
-          field32(w[u][0], w[u][1], w[u][2], w[u][3], a.dec.pos[a.target], (uint32_t)a.dec.mask[a.target]);
-      if (row != cur) {
-        if (cur != kNoRow) flush_row<R, V>(staged, smem, iv_start, a.out, cur, c0, acc);
-        cur = row;
+      if (rows[u] != cur) {
+        if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+        cur = rows[u];
 #pragma unroll
         for (int q = 0; q < V; ++q) acc[q] = p[q];
       } else {
@@ -215,7 +248,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, uint32_t ws, uin
       }
     }
   }
-  if (cur != kNoRow) flush_row<R, V>(staged, smem, iv_start, a.out, cur, c0, acc);
+  if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
 }
 
 template <int R, typename FT, int HW, bool STAGE, int NM>
@@ -243,7 +276,7 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
     const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
     const uint32_t ws = min(ts + warp * chunk, te);
     const uint32_t we = min(ws + chunk, te);
-    warp_range<R, FT, HW, NM>(a, ws, we, staged, smem, iv_start);
+    warp_range<R, FT, HW, NM, false>(a, a.line, ws, we, staged, smem, iv_start);
     if (STAGE && staged) {
       __syncthreads();
       const uint32_t iv_len = a.tile_iv[((size_t)tile * N + a.target) * 2 + 1];
@@ -259,6 +292,115 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
   }
 }
 
+// ------------------------------------------- line tiles staged by bulk copy
+//
+// The non-staged variants (ATOMIC, SORTED) stream the line through shared
+// memory: per CTA, tiles of kLineTile entries are copied global -> shared by
+// the bulk-copy engine (cp.async.bulk, completion on an mbarrier), double
+// buffered, so the next tile is in flight while this one is walked.  The
+// keys then come from shared memory (broadcast reads) and the LSU pipe
+// carries only the factor-row gathers.  Waits are bounded: a wait that runs
+// out sets *err and the whole block leaves after a second bounded wait for
+// its copies in flight.
+
+constexpr uint32_t kLineTile = 1024;
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+  for (uint32_t spin = 0; spin < kSpinLimit; ++spin)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+
+template <int R, typename FT, int HW, int NM>
+__global__ void __launch_bounds__(kMttkrpThreads, 3)
+    mttkrp_tma_kernel(const MttkrpArgs a, int* __restrict__ err) {
+  constexpr uint32_t kRec = HW == 2 ? 32 : 16;  // record bytes
+  constexpr uint32_t kBuf = kLineTile * kRec;
+  extern __shared__ __align__(128) unsigned char sline[];
+  __shared__ __align__(8) uint64_t bars[2];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t ntiles = (a.nnz + kLineTile - 1) / kLineTile;
+
+  auto buf = [&](int b) { return static_cast<void*>(sline + b * kBuf); };
+  auto issue = [&](uint32_t tile, int b) {
+    const uint32_t s0 = tile * kLineTile;
+    const uint32_t n = min(kLineTile, a.nnz - s0);
+    mbar_expect_tx(&bars[b], n * kRec);
+    bulk_g2s(buf(b), static_cast<const unsigned char*>(a.line) + (size_t)s0 * kRec, n * kRec, &bars[b]);
+  };
+
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  uint32_t it = 0;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int b = it & 1;
+    const uint32_t phase = (it >> 1) & 1;
+    const bool ok = mbar_wait_bounded(&bars[b], phase);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        // the other buffer may still have a copy in flight: give it a bounded wait
+        mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1);
+      }
+      return;
+    }
+    const uint32_t s0 = tile * kLineTile;
+    const uint32_t n = min(kLineTile, a.nnz - s0);
+    const uint32_t chunk = (n + kMttkrpWarps - 1) / kMttkrpWarps;
+    const uint32_t ws = min(warp * chunk, n);
+    const uint32_t we = min(ws + chunk, n);
+    warp_range<R, FT, HW, NM, true>(a, buf(b), ws, we, false, nullptr, 0);
+    __syncthreads();  // every warp is done with buffer b
+    if (tid == 0) {
+      const uint32_t nt = tile + 2 * gridDim.x;
+      if (nt < ntiles) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(nt, b);
+      }
+    }
+  }
+}
+
 // Any rank: one warp per nonzero, lanes stride the rank, scalar atomics.
 template <typename FT, int HW>
 __global__ void __launch_bounds__(kMttkrpThreads)
@@ -267,9 +409,9 @@ __global__ void __launch_bounds__(kMttkrpThreads)
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t i = gw; i < a.nnz; i += nw) {
-    const uint64_t lo = __ldg(a.klo + i);
-    const uint64_t hi = hi_word<HW>(a.khi, i);
-    const float v = __ldg(a.vals + i);
+    uint64_t lo, hi;
+    float v;
+    rec_read(a.line, HW, i, lo, hi, v);
     uint32_t rows[ALTO_MAX_MODES];
 #pragma unroll
     for (int m = 0; m < ALTO_MAX_MODES; ++m)
@@ -324,11 +466,32 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   return ALTO_OK;
 }
 
+template <int R, typename FT, int HW, int NM>
+static alto_status launch_tma(const MttkrpArgs& a, int* err, cudaStream_t st) {
+  const size_t smem = 2 * (size_t)kLineTile * (HW == 2 ? 32 : 16);
+  static int blocks_per_sm = 0;
+  if (!blocks_per_sm) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tma_kernel<R, FT, HW, NM>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks_per_sm, mttkrp_tma_kernel<R, FT, HW, NM>, kMttkrpThreads, smem));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const unsigned ntiles = (a.nnz + kLineTile - 1) / kLineTile;
+  const unsigned grid = std::min<unsigned>(ntiles, (unsigned)(num_sms() * blocks_per_sm));
+  if (!grid) return ALTO_OK;
+  mttkrp_tma_kernel<R, FT, HW, NM><<<grid, kMttkrpThreads, smem, st>>>(a, err);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
 template <int R, typename FT, int HW>
-static alto_status launch_modes(const MttkrpArgs& a, bool stage, cudaStream_t st) {
-#define NM_CASE(NN)                                                                        \
-  case NN:                                                                                 \
-    return stage ? launch_tile<R, FT, HW, true, NN>(a, st) : launch_tile<R, FT, HW, false, NN>(a, st);
+static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
+                                cudaStream_t st) {
+#define NM_CASE(NN)                                                                   \
+  case NN:                                                                            \
+    if (stage) return launch_tile<R, FT, HW, true, NN>(a, st);                        \
+    return bulk_feed ? launch_tma<R, FT, HW, NN>(a, err, st) : launch_tile<R, FT, HW, false, NN>(a, st);
   switch (a.dec.nmodes) {
     NM_CASE(3)
     NM_CASE(4)
@@ -341,12 +504,12 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, cudaStream_t st
 }
 
 template <typename FT, int HW>
-static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool aligned,
-                               cudaStream_t st) {
+static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool aligned,
+                               int* err, cudaStream_t st) {
   if (aligned) {
 #define RANK_CASE(RR) \
   case RR:            \
-    return launch_modes<RR, FT, HW>(a, stage, st);
+    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, err, st);
     switch (rank) {
       RANK_CASE(8)
       RANK_CASE(16)
@@ -374,9 +537,14 @@ static double stageable_fraction(const alto_tensor* t, int mode, int rank) {
   return (double)n / (double)v.size();
 }
 
-alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype) {
+static const TuneEntry* tuned_entry(const alto_tensor* t, int mode, int rank, alto_dtype fdtype) {
   for (const auto& e : t->tuned)
-    if (e.mode == mode && e.rank == rank && e.fdtype == (int)fdtype) return e.variant;
+    if (e.mode == mode && e.rank == rank && e.fdtype == (int)fdtype) return &e;
+  return nullptr;
+}
+
+alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype) {
+  if (const TuneEntry* e = tuned_entry(t, mode, rank, fdtype)) return e->variant;
   // The reference's rule (include/alto.hpp:835-846) picks atomics for long
   // low-reuse modes, the stream kernel for the stream mode and da_mem
   // otherwise.  On the device: stage where the tiles' intervals fit, walk a
@@ -393,23 +561,31 @@ alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alt
 alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                        int rank, float* out, int accumulate, alto_mttkrp_variant variant,
                        cudaStream_t st) {
+  return run_mttkrp_feed(t, mode, factors, fdtype, rank, out, accumulate, variant, -1, st);
+}
+
+// feed: 1 streams the line through shared memory by bulk copy, 0 loads it
+// directly, -1 uses the autotuned choice (direct when untuned).
+alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
+                            int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
+                            cudaStream_t st) {
+  if (feed < 0) {
+    const TuneEntry* e = variant == ALTO_MTTKRP_AUTO ? tuned_entry(t, mode, rank, fdtype) : nullptr;
+    feed = e ? (e->bulk_feed ? 1 : 0) : 0;
+  }
   if (variant == ALTO_MTTKRP_AUTO) variant = choose_variant(t, mode, rank, fdtype);
   if (!accumulate)
     ALTO_TRY_CUDA(cudaMemsetAsync(out, 0, (size_t)t->dims[mode] * rank * sizeof(float), st));
   if (!t->nnz) return ALTO_OK;
   MttkrpArgs a{};
-  a.klo = t->klo.as<uint64_t>();
-  a.khi = t->khi.p;
-  a.vals = t->vals.as<float>();
+  a.line = t->line.p;
   a.tile_iv = t->tile_iv.as<uint32_t>();
   a.ntiles = t->ntiles;
   if (variant == ALTO_MTTKRP_SORTED) {
     if (!t->sorted[mode].ready || t->sorted[mode].for_nnz != t->nnz)
       ALTO_TRY(build_sorted_line(t, mode, st));
     const SortedLine& s = t->sorted[mode];
-    a.klo = s.klo.as<uint64_t>();
-    a.khi = s.khi.p;
-    a.vals = s.vals.as<float>();
+    a.line = s.line.p;
     a.tile_iv = s.tile_iv.as<uint32_t>();
     a.ntiles = s.ntiles;
   }
@@ -426,14 +602,20 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
   }
   const bool stage = variant == ALTO_MTTKRP_STAGED || variant == ALTO_MTTKRP_STREAM;
   const int hw = t->dec.hi_words;
-  if (fdtype == ALTO_BF16) {
-    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, aligned, st);
-    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, aligned, st);
-    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, aligned, st);
+  if (!t->err.p) {
+    ALTO_TRY(t->err.ensure(16));
+    ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
-  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, aligned, st);
-  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, aligned, st);
-  return launch_rank<float, 2>(a, rank, stage, aligned, st);
+  int* err = t->err.as<int>();
+  const bool bulk = feed == 1;
+  if (fdtype == ALTO_BF16) {
+    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, aligned, err, st);
+    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, aligned, err, st);
+  }
+  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
+  return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
 }
 
 // Time every applicable variant once per mode (after one warm run) into a
@@ -454,16 +636,23 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
   t->tuned = keep;
   alto_status status = ALTO_OK;
   for (int m = 0; m < t->nmodes && status == ALTO_OK; ++m) {
-    const alto_mttkrp_variant cands[] = {ALTO_MTTKRP_ATOMIC, ALTO_MTTKRP_STAGED, ALTO_MTTKRP_SORTED};
+    struct Cand {
+      alto_mttkrp_variant v;
+      int feed;
+    };
+    const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
+    int best_feed = 0;
     float best_ms = 1e30f;
-    for (auto v : cands) {
+    for (const Cand& c : cands) {
+      const alto_mttkrp_variant v = c.v;
       if (v == ALTO_MTTKRP_STAGED && stageable_fraction(t, m, rank) == 0.0) continue;
       if (v == ALTO_MTTKRP_SORTED && t->nnz / std::max<uint64_t>(t->dims[m], 1) < 2) continue;
-      status = run_mttkrp(t, m, factors, fdtype, rank, out.as<float>(), 0, v, st);  // warm / build
+      status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);  // warm / build
       if (status != ALTO_OK) break;
       cudaEventRecord(e0, st);
-      status = run_mttkrp(t, m, factors, fdtype, rank, out.as<float>(), 0, v, st);
+      status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);
       cudaEventRecord(e1, st);
       if (status != ALTO_OK) break;
       if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -475,9 +664,10 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       if (ms < best_ms) {
         best_ms = ms;
         best = v;
+        best_feed = c.feed;
       }
     }
-    t->tuned.push_back({m, rank, (int)fdtype, best});
+    t->tuned.push_back({m, rank, (int)fdtype, best, best_feed == 1});
     if (chosen) chosen[m] = best;
   }
   cudaEventDestroy(e0);

@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--factor-dtype", choices=["f32", "bf16"], default="f32",
+                    help="factor storage (bf16 halves gather bytes; accumulation stays f32)")
     ap.add_argument("--profile-small", action="store_true",
                     help="small tensor (for ncu captures): 20M nonzeros, 1 step")
     return ap.parse_args()
@@ -247,7 +249,8 @@ def ours(args):
     torch.cuda.empty_cache()
     g = torch.Generator(device=dev)
     g.manual_seed(99 + rank)
-    factors = [(torch.rand((d, R), generator=g, device=dev) * 2 - 1).contiguous() for d in DIMS]
+    fdt = torch.bfloat16 if args.factor_dtype == "bf16" else torch.float32
+    factors = [(torch.rand((d, R), generator=g, device=dev) * 2 - 1).to(fdt).contiguous() for d in DIMS]
     outs = [torch.empty((d, R), device=dev, dtype=torch.float32) for d in DIMS]
     stream = torch.cuda.current_stream()
     variants = t.autotune(factors, R)  # project autotuner: fastest kernel variant per mode
@@ -299,7 +302,7 @@ def ours(args):
     per_mode = []
     for m in range(N):
         dt = statistics.mean(events[k][m][0].elapsed_time(events[k][m][1]) / 1e3 for k in range(steps))
-        b = mttkrp_bytes(DIMS, nnz, R, m, alto_bits)
+        b = mttkrp_bytes(DIMS, nnz, R, m, alto_bits, fbytes=2 if args.factor_dtype == "bf16" else 4)
         per_mode.append((m, dt, b))
     bytes_launch = sum(b for _, _, b in per_mode) / N
     dt_launch = sum(dt for _, dt, _ in per_mode) / N
@@ -312,7 +315,7 @@ def ours(args):
     if not args.no_e2e:
         hostF = [torch.empty((d, R), dtype=torch.float64, pin_memory=True) for d in DIMS]
         for h, f in zip(hostF, factors):
-            h.copy_(f.double().cpu())
+            h.copy_(f.float().double().cpu())
         hostN = [h.numpy() for h in hostF]
         t.mttkrp_host(0, hostN, R)  # warm
         torch.cuda.synchronize()
@@ -351,7 +354,7 @@ def ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "dims": DIMS, "nnz": nnz, "rank": R, "zipf": 1.2,
                        "values": "lognormal(0,1)", "key_bits": t.key_bits, "alto_bits": alto_bits,
-                       "factor_dtype": "f32", "parallelism": f"independent tensor per GPU x{world}",
+                       "factor_dtype": args.factor_dtype, "parallelism": f"independent tensor per GPU x{world}",
                        "l2": "inputs larger than L2 (line + factors > 3 GB); no flush",
                        "line_bytes_per_nnz": line_bytes_per_nnz(alto_bits),
                        "variants": [vnames.get(v, str(v)) for v in variants],

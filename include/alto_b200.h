@@ -52,6 +52,11 @@ typedef enum {
   ALTO_MTTKRP_SORTED = 4    /* a row-sorted copy of the line, runs reduced in registers (op_sched)  */
 } alto_mttkrp_variant;
 
+/* OR-ed into the variant given to alto_mttkrp_variant_run (ATOMIC or
+ * SORTED): stream the line through shared memory with bulk copies
+ * (cp.async.bulk, double buffered) instead of loading it directly. */
+#define ALTO_MTTKRP_FEED_BULK 0x100
+
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */
 typedef enum { ALTO_UNCONSTRAINED = 0, ALTO_NONNEG = 1, ALTO_LASSO = 2 } alto_constraint;

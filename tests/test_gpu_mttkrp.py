@@ -14,6 +14,7 @@ from conftest import FIXTURE_NAMES, load_fixture
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
+ALL_VARIANTS = (A.AUTO, A.ATOMIC, A.STAGED, A.SORTED, A.ATOMIC | A.FEED_BULK, A.SORTED | A.FEED_BULK)
 
 
 def to_dev(F, dtype):
@@ -53,14 +54,14 @@ def check_modes(dims, cidx, vals, R, variants=(A.AUTO,), dtype=None, seed=0):
 @pytest.mark.parametrize("name", FIXTURE_NAMES)
 def test_fixtures_rank8(name):
     dims, cidx, vals = load_fixture(name)
-    check_modes(dims, cidx, vals, 8, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
+    check_modes(dims, cidx, vals, 8, variants=ALL_VARIANTS)
 
 
 @pytest.mark.parametrize("R", [4, 8, 16, 32, 64, 128, 10, 33])
 def test_uniform_ranks(R):
     dims = np.array([1000, 1000, 1000], np.uint64)
     cidx, vals = synth.uniform_coo(dims, 150000, seed=R)
-    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED), seed=R)
+    check_modes(dims, cidx, vals, R, variants=ALL_VARIANTS, seed=R)
 
 
 @pytest.mark.parametrize("R", [8, 16, 32, 64])
@@ -69,20 +70,20 @@ def test_bf16_factor_storage(R):
 
     dims = np.array([800, 700, 900], np.uint64)
     cidx, vals = synth.uniform_coo(dims, 100000, seed=R + 1)
-    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.SORTED), dtype=torch.bfloat16, seed=R)
+    check_modes(dims, cidx, vals, R, variants=(A.AUTO, A.ATOMIC, A.SORTED, A.SORTED | A.FEED_BULK), dtype=torch.bfloat16, seed=R)
 
 
 def test_power_law_128bit_keys():
     """Zipf-1.2 coordinates with scattered labels and a 65-bit key."""
     dims = np.array([4800000, 1800000, 1800000], np.uint64)
     cidx, vals = synth.powerlaw_coo(dims, 200000, [1.2, 1.2, 1.2], seed=3, values="lognormal")
-    check_modes(dims, cidx, vals, 32, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
+    check_modes(dims, cidx, vals, 32, variants=ALL_VARIANTS)
 
 
 def test_five_modes_rank64():
     dims = np.array([100000, 100000, 10000, 1000, 100], np.uint64)
     cidx, vals = synth.powerlaw_coo(dims, 150000, [1.1, 1.1, None, None, None], seed=4)
-    check_modes(dims, cidx, vals, 64, variants=(A.AUTO, A.ATOMIC, A.STAGED, A.SORTED))
+    check_modes(dims, cidx, vals, 64, variants=ALL_VARIANTS)
 
 
 def test_stream_mode_single_row():
