@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(HERE, "libalto_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_SPD, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
 F32, BF16, F64 = 0, 1, 2
-AUTO, ATOMIC, STAGED, STREAM, SORTED = range(5)
+AUTO, ATOMIC, STAGED, STREAM, SORTED, DETERMINISTIC = range(6)
 FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
 UNCONSTRAINED, NONNEG, LASSO = range(3)
 FIT_REFERENCE, FIT_EXACT = 0, 1
@@ -42,6 +42,8 @@ EXPORTED = [
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
+    "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
+    "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
 
 
@@ -395,5 +397,82 @@ class CPStream:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving
+
+class alto_stream_config(ctypes.Structure):
+    _fields_ = [("nmodes", c_int), ("stream_mode", c_int), ("rank", c_int), ("constraint", c_int),
+                ("forgetting", c_double), ("max_inner_iters", c_int), ("epsilon", c_double)]
+
+
+class alto_serving_stats(ctypes.Structure):
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("p50_ms", c_double), ("p99_ms", c_double),
+                ("max_ms", c_double), ("slices_per_s", c_double), ("reserved_bytes", c_uint64),
+                ("admitted_streams", c_int), ("pending_streams", c_int)]
+
+
+class Server:
+    """Many CP-stream tensors served concurrently (alto_server_*): slices are
+    queued per stream and processed by `workers` threads on their own CUDA
+    streams; streams are admitted under an HBM budget."""
+
+    def __init__(self, hbm_budget_bytes, workers=8):
+        h = c_void_p()
+        check(lib().alto_server_create(c_uint64(int(hbm_budget_bytes)), c_int(workers), byref(h)))
+        self.h = h
+        self.rank = {}
+
+    def open(self, nmodes, stream_mode, rank, max_dims, max_slice_nnz, constraint=UNCONSTRAINED,
+             forgetting=0.99, max_inner=10, epsilon=1e-5):
+        cfg = alto_stream_config(nmodes, stream_mode, rank, constraint, forgetting, max_inner, epsilon)
+        md = np.ascontiguousarray(max_dims, dtype=np.uint64)
+        sid = c_int()
+        check(lib().alto_server_open(self.h, byref(cfg), md.ctypes.data_as(c_void_p), c_uint64(int(max_slice_nnz)),
+                                     byref(sid)))
+        self.rank[sid.value] = rank
+        return sid.value
+
+    def submit(self, sid, dims, cidx, vals, init_vals=None):
+        coo = _Coo(dims, cidx, vals)
+        iv = np.ascontiguousarray(init_vals if init_vals is not None else np.zeros(0), dtype=np.float64)
+        t = c_uint64()
+        check(lib().alto_server_submit(self.h, c_int(sid), byref(coo.c), iv.ctypes.data_as(c_void_p),
+                                       c_uint64(len(iv)), byref(t)))
+        return t.value
+
+    def wait(self, ticket):
+        inner, lat = c_int(), c_double()
+        check(lib().alto_server_wait(self.h, c_uint64(ticket), byref(inner), byref(lat)))
+        return inner.value, lat.value
+
+    def drain(self):
+        check(lib().alto_server_drain(self.h))
+
+    def stats(self):
+        st = alto_serving_stats()
+        check(lib().alto_server_stats(self.h, byref(st)))
+        return {f: getattr(st, f) for f, _ in alto_serving_stats._fields_}
+
+    def factor(self, sid, mode):
+        rows = c_uint64()
+        check(lib().alto_server_factor(self.h, c_int(sid), c_int(mode), None, byref(rows)))
+        out = np.zeros((max(rows.value, 1), self.rank[sid]), np.float64)
+        check(lib().alto_server_factor(self.h, c_int(sid), c_int(mode), out.ctypes.data_as(c_void_p), byref(rows)))
+        return out[: rows.value]
+
+    def close(self, sid):
+        check(lib().alto_server_close(self.h, c_int(sid)))
+
+    def destroy(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().alto_server_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
         except Exception:
             pass

@@ -47,20 +47,28 @@ def uniform_coo(dims, nnz, seed=0, values="uniform"):
     return cidx, vals
 
 
+class ZipfSampler:
+    """Draws from a Zipf(s) law truncated to ranks 1..dim, as 0-based indices
+    whose labels are randomly permuted once (so hot rows are scattered, and
+    stay the same rows across calls)."""
+
+    def __init__(self, rng, dim, s, permute=True):
+        ranks = np.arange(1, dim + 1, dtype=np.float64)
+        cdf = np.cumsum(ranks ** (-float(s)))
+        self.cdf = cdf / cdf[-1]
+        self.dim = dim
+        self.labels = rng.permutation(dim).astype(np.uint64) if permute else None
+
+    def sample(self, rng, n):
+        r = np.searchsorted(self.cdf, rng.random(n), side="right").astype(np.uint64)
+        r = np.minimum(r, self.dim - 1)
+        return self.labels[r] if self.labels is not None else r
+
+
 def zipf_indices(rng, dim, s, n, permute=True):
-    """n draws from a Zipf(s) law truncated to ranks 1..dim, as 0-based indices
-    whose labels are randomly permuted (so hot rows are scattered)."""
-    ranks = np.arange(1, dim + 1, dtype=np.float64)
-    w = ranks ** (-float(s))
-    cdf = np.cumsum(w)
-    cdf /= cdf[-1]
-    u = rng.random(n)
-    r = np.searchsorted(cdf, u, side="right").astype(np.uint64)
-    r = np.minimum(r, dim - 1)
-    if permute:
-        labels = rng.permutation(dim).astype(np.uint64)
-        r = labels[r]
-    return r
+    """n draws from a Zipf(s) law truncated to ranks 1..dim (one label
+    permutation per call; use ZipfSampler to keep labels across calls)."""
+    return ZipfSampler(rng, dim, s, permute).sample(rng, n)
 
 
 def _values(rng, n, kind):
@@ -105,39 +113,44 @@ def stream_batches(space_dims, nslices, nnz_fn, exponents, seed=0, values="poiss
 
     Every batch is {dims, cidx, vals} as the reference's
     StreamingSparseTensor.next_dynamic_batch hands it over
-    (src/streaming_sptensor.cpp:196-264): the time mode has extent 1 and
-    index 0, the other modes carry first-seen relabelled indices and their
-    extents grow monotonically (max index + 1, never shrinking).
-    nnz_fn(rng, s) gives the number of coordinate draws for slice s.
+    (src/streaming_sptensor.cpp:69-264): the batch's nonzeros are in the
+    slicer's sorted order (lexicographic over the modes that follow the time
+    mode), the time mode has extent 1 and index 0, the other modes carry
+    first-seen relabelled indices (first seen in that order, over the whole
+    stream) and their extents grow monotonically (max index + 1, never
+    shrinking).  nnz_fn(rng, s) gives the number of coordinate draws for
+    slice s; zero values are dropped.
     """
     rng = np.random.default_rng(seed)
     nsp = len(space_dims)
     nmodes = nsp + 1
-    seen = [dict() for _ in range(nsp)]
+    samplers = [ZipfSampler(rng, int(d), e) if e is not None else None for d, e in zip(space_dims, exponents)]
+    maps = [np.full(int(d), -1, np.int64) for d in space_dims]
+    nxt = [0] * nsp
     prev = [0] * nmodes
     batches = []
     for s in range(nslices):
         n = int(nnz_fn(rng, s))
         cols = []
-        for d, e in zip(space_dims, exponents):
-            cols.append(zipf_indices(rng, int(d), e, n) if e is not None
-                        else rng.integers(0, int(d), n, dtype=np.uint64))
+        for d, zs in zip(space_dims, samplers):
+            cols.append(zs.sample(rng, n) if zs is not None else rng.integers(0, int(d), n, dtype=np.uint64))
         c = _dedup_shuffle(np.stack(cols), rng, n)
         v = _values(rng, c.shape[1], values)
         keep = v != 0
         c, v = c[:, keep], v[keep]
+        order = np.lexsort(c[::-1])  # sorted by (mode 1, mode 2, ...) as the slicer's tt_sort
+        c, v = np.ascontiguousarray(c[:, order]), v[order]
         if relabel:
             for m in range(nsp):
-                mp = seen[m]
-                col = c[m]
-                out = np.empty_like(col)
-                for i, x in enumerate(col.tolist()):
-                    y = mp.get(x)
-                    if y is None:
-                        y = len(mp)
-                        mp[x] = y
-                    out[i] = y
-                c[m] = out
+                col = c[m].astype(np.int64)
+                mp = maps[m]
+                unseen = mp[col] < 0
+                if unseen.any():
+                    u, first = np.unique(col[unseen], return_index=True)
+                    newv = u[np.argsort(first)]
+                    mp[newv] = np.arange(nxt[m], nxt[m] + len(newv))
+                    nxt[m] += len(newv)
+                c[m] = mp[col].astype(np.uint64)
         full = np.zeros((nmodes, c.shape[1]), np.uint64)
         dims = [0] * nmodes
         k = 0

@@ -10,6 +10,7 @@
 namespace alto {
 
 std::atomic<uint64_t> g_kernel_launches{0};
+thread_local cudaStream_t tls_alloc_stream = nullptr;
 static thread_local char g_err[512] = "";
 
 void set_error(const char* fmt, ...) {
@@ -316,7 +317,7 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
   ALTO_TRY(check_mttkrp(t, mode, factors, fdtype, rank, out));
   const int bulk = ((int)variant & ALTO_MTTKRP_FEED_BULK) ? 1 : 0;
   const alto_mttkrp_variant v = (alto_mttkrp_variant)((int)variant & ~ALTO_MTTKRP_FEED_BULK);
-  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_SORTED ||
+  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_DETERMINISTIC ||
       (bulk && v != ALTO_MTTKRP_ATOMIC && v != ALTO_MTTKRP_SORTED)) {
     set_error("unknown variant %d", (int)variant);
     return ALTO_ERR_INVALID;

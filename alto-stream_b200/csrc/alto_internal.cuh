@@ -46,6 +46,13 @@ inline alto_status cuda_status(cudaError_t e, const char* what, const char* file
 
 // ------------------------------------------------------------ device memory
 
+// The stream on which this host thread allocates and frees device memory.
+// Null (the default) means cudaMalloc / cudaFree; a stream means the
+// stream-ordered allocator (cudaMallocAsync / cudaFreeAsync), which does not
+// synchronise the device, so threads that work on their own streams (the
+// serving workers) do not stall one another when buffers grow.
+extern thread_local cudaStream_t tls_alloc_stream;
+
 // A growable device allocation owned by a handle.
 struct DevBuf {
   void* p = nullptr;
@@ -55,7 +62,12 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (tls_alloc_stream)
+        cudaFreeAsync(p, tls_alloc_stream);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
   }
@@ -64,7 +76,7 @@ struct DevBuf {
     if (n <= bytes && p) return ALTO_OK;
     release();
     size_t want = n < 256 ? 256 : n;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = tls_alloc_stream ? cudaMallocAsync(&p, want, tls_alloc_stream) : cudaMalloc(&p, want);
     if (e != cudaSuccess) {
       p = nullptr;
       return cuda_status(e, "cudaMalloc", __FILE__, __LINE__);
@@ -226,6 +238,10 @@ struct alto_tensor {
   // Device error word of the kernels' bounded waits (0 = none).
   alto::DevBuf err;
 
+  // Deterministic MTTKRP: sub-range boundary slots (rows, partial sums) and
+  // the list of long chains with its count.
+  alto::DevBuf det_rows, det_vals, det_long;
+
   // Construction scratch (sort buffers, scan partials).
   alto::DevBuf scratch;
   alto::DevBuf scan_scratch;
@@ -246,6 +262,8 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st);
 alto_mttkrp_variant choose_variant(const alto_tensor* t, int mode, int rank, alto_dtype fdtype);
+// Whether ALTO_MTTKRP_DETERMINISTIC runs for this rank and factor type.
+bool deterministic_supported(int rank, alto_dtype fdtype);
 // Build the per-mode row-sorted copy of the line.
 alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st);
 // Measure the variants per mode and record the fastest (synchronous).

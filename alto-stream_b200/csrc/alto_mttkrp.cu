@@ -45,6 +45,10 @@ struct FactorSet {
 
 struct MttkrpArgs {
   const void* line;  // line records (LineRec16 / LineRec32)
+  // DETERMINISTIC: per lane-group sub-range, its first and last run (slots
+  // 2s and 2s+1: output row and R partial sums)
+  uint32_t* det_rows;
+  float* det_vals;
   const uint32_t* tile_iv;
   uint32_t nnz;
   uint32_t tile_nnz;
@@ -178,9 +182,39 @@ __device__ __forceinline__ void load_keys(const void* line, uint32_t i0, uint32_
 // row in registers and updates the output once per run of equal rows.  NM is
 // the mode count (3, 4, 5 specialised as in the reference's
 // ALTO_MODES_SPECIALIZED, 8 for the rest).
-template <int R, typename FT, int HW, int NM, bool SMEM>
+// Deterministic mode (DET): the line is ordered by the target row, so a run
+// that is neither the first nor the last of its sub-range holds every
+// nonzero of its row and is added to the output without atomics; the first
+// and last runs go to the sub-range's two slots (sub-range `sr`) and are
+// summed in slot order by det_fix_*.
+template <int R, int V, int G>
+__device__ __forceinline__ void det_slot(const MttkrpArgs& a, uint32_t slot, uint32_t row, int sub,
+                                         const float (&acc)[V], bool zero) {
+  if (sub == 0) a.det_rows[slot] = row;
+#pragma unroll
+  for (int q = 0; q < V / 4; ++q)
+    *reinterpret_cast<float4*>(a.det_vals + (size_t)slot * R + q * 4 * G + sub * 4) =
+        zero ? make_float4(0.f, 0.f, 0.f, 0.f)
+             : make_float4(acc[q * 4], acc[q * 4 + 1], acc[q * 4 + 2], acc[q * 4 + 3]);
+}
+
+template <int R, int V, int G>
+__device__ __forceinline__ void det_plain(float* out, uint32_t row, int sub, const float (&acc)[V]) {
+#pragma unroll
+  for (int q = 0; q < V / 4; ++q) {
+    float4* o = reinterpret_cast<float4*>(out + (size_t)row * R + q * 4 * G + sub * 4);
+    float4 x = *o;
+    x.x += acc[q * 4];
+    x.y += acc[q * 4 + 1];
+    x.z += acc[q * 4 + 2];
+    x.w += acc[q * 4 + 3];
+    *o = x;
+  }
+}
+
+template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false>
 __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
-                                           bool staged, float* smem, uint32_t iv_start) {
+                                           bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
   constexpr int U = NM <= 3 ? 2 : 1;
@@ -196,6 +230,8 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
 #pragma unroll
   for (int q = 0; q < V; ++q) acc[q] = 0.f;
   uint32_t cur = kNoRow;
+  uint32_t nrun = 0;  // runs emitted (DET)
+  const uint32_t slot0 = 2 * (sr_base + grp);
 
   uint32_t w[U][4];
   float v[U];
@@ -238,7 +274,14 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
 #pragma unroll
           for (int q = 0; q < V; ++q) p[q] *= f[u][j][q];
       if (rows[u] != cur) {
-        if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+        if (cur != kNoRow) {
+          if (!DET)
+            flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+          else if (nrun++ == 0)
+            det_slot<R, V, G>(a, slot0, cur, sub, acc, false);
+          else
+            det_plain<R, V, G>(a.out, cur, sub, acc);
+        }
         cur = rows[u];
 #pragma unroll
         for (int q = 0; q < V; ++q) acc[q] = p[q];
@@ -248,10 +291,29 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
       }
     }
   }
-  if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+  if (!DET) {
+    if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+  } else if (cur == kNoRow) {
+    // empty sub-range: both slots carry the row of the entry before it (the
+    // last run of an earlier sub-range) with zeros, keeping slot rows sorted
+    uint32_t w0[1][4];
+    float v0[1];
+    bool ok0[1];
+    const uint32_t at = gs > 0 ? gs - 1 : 0;
+    load_keys<HW, 1, SMEM>(line, at, at + 1, w0, v0, ok0);
+    const uint32_t r0 = field32(w0[0][0], w0[0][1], w0[0][2], w0[0][3], a.dec.pos[a.target],
+                                (uint32_t)a.dec.mask[a.target]);
+    det_slot<R, V, G>(a, slot0, r0, sub, acc, true);
+    det_slot<R, V, G>(a, slot0 + 1, r0, sub, acc, true);
+  } else if (nrun == 0) {
+    det_slot<R, V, G>(a, slot0, cur, sub, acc, false);
+    det_slot<R, V, G>(a, slot0 + 1, cur, sub, acc, true);
+  } else {
+    det_slot<R, V, G>(a, slot0 + 1, cur, sub, acc, false);
+  }
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM>
+template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false>
 __global__ void __launch_bounds__(kMttkrpThreads, 3)
     mttkrp_tile_kernel(const MttkrpArgs a) {
   extern __shared__ float4 smem4[];
@@ -276,7 +338,8 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
     const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
     const uint32_t ws = min(ts + warp * chunk, te);
     const uint32_t we = min(ws + chunk, te);
-    warp_range<R, FT, HW, NM, false>(a, a.line, ws, we, staged, smem, iv_start);
+    warp_range<R, FT, HW, NM, false, DET>(a, a.line, ws, we, staged, smem, iv_start,
+                                          (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW);
     if (STAGE && staged) {
       __syncthreads();
       const uint32_t iv_len = a.tile_iv[((size_t)tile * N + a.target) * 2 + 1];
@@ -289,6 +352,96 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
       }
       __syncthreads();
     }
+  }
+}
+
+// ------------------------------------------------ deterministic fix-up
+//
+// The slots of DET hold, in line order, the first and last run of every
+// sub-range; their rows are non-decreasing, and a row appears in the slots
+// only if it is in none of the interior runs.  A chain (maximal stretch of
+// slots with one row) is summed in slot order, by one warp when it is short
+// and by one block with a fixed split and a fixed tree when it is long (a
+// hot row, or the single row of the stream mode).  The summation order is a
+// function of nnz, the rank and the line alone, so results repeat bit for
+// bit from run to run and whatever else runs on the device.
+
+constexpr uint32_t kShortChain = 64;
+
+__global__ void __launch_bounds__(256)
+    det_fix_short_kernel(const uint32_t* __restrict__ rows, const float* __restrict__ vals, uint32_t nslots,
+                         int R, float* __restrict__ out, uint2* __restrict__ longs, uint32_t* __restrict__ nlong) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < nslots; i += nw) {
+    const uint32_t row = rows[i];
+    if (i > 0 && rows[i - 1] == row) continue;  // not the head of its chain
+    uint32_t lo = i + 1, hi = nslots;           // chain end: first slot with a larger row
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (rows[mid] == row)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo - i > kShortChain) {
+      if (lane == 0) longs[atomicAdd(nlong, 1u)] = make_uint2(i, lo);
+      continue;
+    }
+    for (int r = lane; r < R; r += 32) {
+      float x = 0.f;
+      for (uint32_t k = i; k < lo; ++k) x += vals[(size_t)k * R + r];
+      out[(size_t)row * R + r] += x;
+    }
+  }
+}
+
+// One block per long chain: thread (s, q) sums slots first+s, first+s+S, ...
+// of rank quad q (S = 256 / (R/4)), then a fixed tree over s.
+__global__ void __launch_bounds__(256)
+    det_fix_long_kernel(const uint32_t* __restrict__ rows, const float* __restrict__ vals, int R,
+                        float* __restrict__ out, const uint2* __restrict__ longs,
+                        const uint32_t* __restrict__ nlong) {
+  __shared__ float4 part[256];
+  const int Q = R / 4, S = 256 / Q;
+  const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
+  const uint32_t n = *nlong;
+  for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
+    const uint2 ch = longs[c];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sidx < S)
+      for (uint32_t k = ch.x + sidx; k < ch.y; k += S) {
+        const float4 v = *reinterpret_cast<const float4*>(vals + (size_t)k * R + q * 4);
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
+      }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int stride = S / 2; stride >= 1; stride >>= 1) {
+      if (sidx < stride) {
+        const float4 o = part[(sidx + stride) * Q + q];
+        float4& m = part[sidx * Q + q];
+        m.x += o.x;
+        m.y += o.y;
+        m.z += o.z;
+        m.w += o.w;
+      }
+      __syncthreads();
+    }
+    if (sidx == 0) {
+      float4* o = reinterpret_cast<float4*>(out + (size_t)rows[ch.x] * R + q * 4);
+      float4 x = *o;
+      const float4 p = part[q];
+      x.x += p.x;
+      x.y += p.y;
+      x.z += p.z;
+      x.w += p.w;
+      *o = x;
+    }
+    __syncthreads();
   }
 }
 
@@ -485,6 +638,59 @@ static alto_status launch_tma(const MttkrpArgs& a, int* err, cudaStream_t st) {
   return ALTO_OK;
 }
 
+// Deterministic MTTKRP: the tile kernel in DET mode (float32 factors, the
+// specialised ranks) followed by the two fix-up kernels.
+template <int R, int HW, int NM>
+static alto_status launch_det_nm(const MttkrpArgs& a, uint2* longs, uint32_t* nlong, cudaStream_t st) {
+  static int blocks_per_sm = 0;
+  if (!blocks_per_sm) {
+    ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks_per_sm, mttkrp_tile_kernel<R, float, HW, false, NM, true>, kMttkrpThreads, 0));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
+  if (!grid) return ALTO_OK;
+  mttkrp_tile_kernel<R, float, HW, false, NM, true><<<grid, kMttkrpThreads, 0, st>>>(a);
+  ALTO_LAUNCHED();
+  const uint32_t nslots = a.ntiles * kMttkrpWarps * LaneWidth<R>::NPW * 2;
+  ALTO_TRY_CUDA(cudaMemsetAsync(nlong, 0, sizeof(uint32_t), st));
+  const unsigned g1 = std::min<unsigned>((nslots + 7) / 8, (unsigned)num_sms() * 16);
+  det_fix_short_kernel<<<g1, 256, 0, st>>>(a.det_rows, a.det_vals, nslots, R, a.out, longs, nlong);
+  ALTO_LAUNCHED();
+  det_fix_long_kernel<<<(unsigned)num_sms(), 256, 0, st>>>(a.det_rows, a.det_vals, R, a.out, longs, nlong);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+template <int R, int HW>
+static alto_status launch_det(const MttkrpArgs& a, uint2* longs, uint32_t* nlong, cudaStream_t st) {
+  switch (a.dec.nmodes) {
+    case 3: return launch_det_nm<R, HW, 3>(a, longs, nlong, st);
+    case 4: return launch_det_nm<R, HW, 4>(a, longs, nlong, st);
+    case 5: return launch_det_nm<R, HW, 5>(a, longs, nlong, st);
+    default: return launch_det_nm<R, HW, ALTO_MAX_MODES>(a, longs, nlong, st);
+  }
+}
+
+template <int HW>
+static alto_status launch_det_rank(const MttkrpArgs& a, int rank, uint2* longs, uint32_t* nlong,
+                                   cudaStream_t st) {
+  switch (rank) {
+    case 8: return launch_det<8, HW>(a, longs, nlong, st);
+    case 16: return launch_det<16, HW>(a, longs, nlong, st);
+    case 32: return launch_det<32, HW>(a, longs, nlong, st);
+    case 64: return launch_det<64, HW>(a, longs, nlong, st);
+    case 128: return launch_det<128, HW>(a, longs, nlong, st);
+    default: break;
+  }
+  set_error("the deterministic MTTKRP takes rank 8, 16, 32, 64 or 128 (got %d)", rank);
+  return ALTO_ERR_UNSUPPORTED;
+}
+
+bool deterministic_supported(int rank, alto_dtype fdtype) {
+  return fdtype == ALTO_F32 && (rank == 8 || rank == 16 || rank == 32 || rank == 64 || rank == 128);
+}
+
 template <int R, typename FT, int HW>
 static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
                                 cudaStream_t st) {
@@ -574,6 +780,11 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     feed = e ? (e->bulk_feed ? 1 : 0) : 0;
   }
   if (variant == ALTO_MTTKRP_AUTO) variant = choose_variant(t, mode, rank, fdtype);
+  const bool det = variant == ALTO_MTTKRP_DETERMINISTIC;
+  if (det && !deterministic_supported(rank, fdtype)) {
+    set_error("the deterministic MTTKRP takes float32 factors at rank 8, 16, 32, 64 or 128");
+    return ALTO_ERR_UNSUPPORTED;
+  }
   if (!accumulate)
     ALTO_TRY_CUDA(cudaMemsetAsync(out, 0, (size_t)t->dims[mode] * rank * sizeof(float), st));
   if (!t->nnz) return ALTO_OK;
@@ -581,7 +792,8 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   a.line = t->line.p;
   a.tile_iv = t->tile_iv.as<uint32_t>();
   a.ntiles = t->ntiles;
-  if (variant == ALTO_MTTKRP_SORTED) {
+  // (a mode of length 1 is already in row order in the ALTO line)
+  if (variant == ALTO_MTTKRP_SORTED || (det && t->dims[mode] > 1)) {
     if (!t->sorted[mode].ready || t->sorted[mode].for_nnz != t->nnz)
       ALTO_TRY(build_sorted_line(t, mode, st));
     const SortedLine& s = t->sorted[mode];
@@ -607,6 +819,23 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
+  if (det) {
+    if (!aligned) {
+      set_error("the deterministic MTTKRP needs 16-byte aligned factors and output");
+      return ALTO_ERR_UNSUPPORTED;
+    }
+    const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * (128 / rank) * 2;
+    ALTO_TRY(t->det_rows.ensure(nslots * 4));
+    ALTO_TRY(t->det_vals.ensure(nslots * rank * 4));
+    ALTO_TRY(t->det_long.ensure((nslots / (kShortChain + 1) + 2) * sizeof(uint2) + 16));
+    a.det_rows = t->det_rows.as<uint32_t>();
+    a.det_vals = t->det_vals.as<float>();
+    uint32_t* nlong = t->det_long.as<uint32_t>();
+    uint2* longs = reinterpret_cast<uint2*>(t->det_long.as<char>() + 16);
+    if (hw == 0) return launch_det_rank<0>(a, rank, longs, nlong, st);
+    if (hw == 1) return launch_det_rank<1>(a, rank, longs, nlong, st);
+    return launch_det_rank<2>(a, rank, longs, nlong, st);
+  }
   const bool bulk = feed == 1;
   if (fdtype == ALTO_BF16) {
     if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);

@@ -361,13 +361,17 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
 
   const void* fac[ALTO_MAX_MODES];
   for (int n = 0; n < N; ++n) fac[n] = s->U[n].p;
+  // the deterministic MTTKRP where it runs, so a stream's results repeat
+  // bit for bit however many other streams share the device
+  const alto_mttkrp_variant mv =
+      deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
   const unsigned all = (1u << N) - 1;
   double* dstat = s->dstat.as<double>();  // [N][3]
   double delta = 0.0, prev_delta = 0.0;
   int it;
   for (it = 0; it < s->max_inner; ++it) {
     // time rows: MTTKRP of the stream mode, solve with the other Grams
-    ALTO_TRY(run_mttkrp(s->at, t, fac, ALTO_F32, R, s->buf32.as<float>(), 0, ALTO_MTTKRP_AUTO, st));
+    ALTO_TRY(run_mttkrp(s->at, t, fac, ALTO_F32, R, s->buf32.as<float>(), 0, mv, st));
     ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidge, 1e-12, s->W.as<double>(),
                          s->status.as<int>(), nullptr, st));
     ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->dims[t], R,
@@ -380,7 +384,7 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     for (int j = 0; j < N; ++j) {
       if (j == t) continue;
       const uint64_t I = s->dims[j];
-      ALTO_TRY(run_mttkrp(s->at, j, fac, ALTO_F32, R, s->buf32.as<float>(), 0, ALTO_MTTKRP_AUTO, st));
+      ALTO_TRY(run_mttkrp(s->at, j, fac, ALTO_F32, R, s->buf32.as<float>(), 0, mv, st));
       // historical term
       ALTO_TRY(rr_op(s->ata.as<double>(), s->old_gram.as<double>(), (int)RR, 0, 0.0, st));
       for (int m = 0; m < N; ++m) {
@@ -439,6 +443,15 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
 }
 
 }  // namespace
+
+namespace alto {
+// Point a session (and its encoded slice) at another CUDA stream; the
+// session's previous work must be complete (every push is synchronous).
+void stream_set_cuda_stream(alto_stream_session* s, cudaStream_t st) {
+  s->st = st;
+  if (s->at) s->at->stream = st;
+}
+}  // namespace alto
 
 extern "C" {
 

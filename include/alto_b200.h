@@ -49,7 +49,12 @@ typedef enum {
   ALTO_MTTKRP_ATOMIC = 1,   /* vector atomics per nonzero, consecutive equal rows merged in the warp */
   ALTO_MTTKRP_STAGED = 2,   /* partition-local output rows staged in shared memory (da_mem_pull)    */
   ALTO_MTTKRP_STREAM = 3,   /* single or few output rows held in registers (mttkrp_alto_stream)     */
-  ALTO_MTTKRP_SORTED = 4    /* a row-sorted copy of the line, runs reduced in registers (op_sched)  */
+  ALTO_MTTKRP_SORTED = 4,   /* a row-sorted copy of the line, runs reduced in registers (op_sched)  */
+  /* SORTED without atomics: runs split between lane groups are summed in a
+   * fixed order afterwards, so the output repeats bit for bit from run to
+   * run (float32 factors, rank 8/16/32/64/128, 16-byte aligned buffers).
+   * The reference's threaded variants are not reproducible run to run. */
+  ALTO_MTTKRP_DETERMINISTIC = 5
 } alto_mttkrp_variant;
 
 /* OR-ed into the variant given to alto_mttkrp_variant_run (ATOMIC or
@@ -232,6 +237,56 @@ alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_ou
                                uint64_t* rows);
 alto_status alto_stream_lambda(alto_stream_session* s, double* host_out);
 alto_status alto_stream_close(alto_stream_session* s);
+
+/* -------------------------------------------------------------- serving */
+
+/* A server for many independent CP-stream tensors (the reference has none;
+ * it runs one stream's slices one at a time, src/streaming_cpd.cpp:26-366).
+ * Slices are submitted as host COO batches and processed by `workers`
+ * threads, each on its own CUDA stream, so the updates of different streams
+ * overlap on the GPU; a stream's own slices run in submission order.  Each
+ * stream's model, Grams and ADMM state stay on the device.  Streams are
+ * admitted while the sum of their reserved footprints stays within
+ * hbm_budget_bytes; a stream that does not fit waits, with its slices
+ * queued, until earlier streams close. */
+typedef struct alto_server alto_server;
+
+typedef struct {
+  int nmodes;
+  int stream_mode;
+  int rank;
+  alto_constraint constraint;
+  double forgetting;
+  int max_inner_iters;
+  double epsilon;
+} alto_stream_config;
+
+typedef struct {
+  uint64_t submitted, completed;
+  double p50_ms, p99_ms, max_ms;  /* slice latency, submission to completion */
+  double slices_per_s;            /* completed slices over first submission .. last completion */
+  uint64_t reserved_bytes;
+  int admitted_streams, pending_streams;
+} alto_serving_stats;
+
+alto_status alto_server_create(uint64_t hbm_budget_bytes, int workers, alto_server** out);
+/* Open a stream; max_dims (nmodes) and max_slice_nnz bound its footprint
+ * estimate for admission.  *sid receives its id; it may wait for admission. */
+alto_status alto_server_open(alto_server* s, const alto_stream_config* cfg, const uint64_t* max_dims,
+                             uint64_t max_slice_nnz, int* sid);
+/* Queue one time batch (copied; host memory).  init_vals as alto_stream_push. */
+alto_status alto_server_submit(alto_server* s, int sid, const alto_coo* batch, const double* init_vals,
+                               uint64_t n_init, uint64_t* ticket);
+/* Wait for one slice; its status, inner iterations and latency. */
+alto_status alto_server_wait(alto_server* s, uint64_t ticket, int* inner_iters, double* latency_ms);
+/* Wait until every admitted stream has processed all its slices. */
+alto_status alto_server_drain(alto_server* s);
+alto_status alto_server_stats(alto_server* s, alto_serving_stats* out);
+/* A stream's factor (as alto_stream_factor) once its queued slices are done. */
+alto_status alto_server_factor(alto_server* s, int sid, int mode, double* host_out, uint64_t* rows);
+/* Finish a stream's queued slices, free its device state, admit waiting streams. */
+alto_status alto_server_close(alto_server* s, int sid);
+alto_status alto_server_destroy(alto_server* s);
 
 #ifdef __cplusplus
 }

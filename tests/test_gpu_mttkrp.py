@@ -171,3 +171,79 @@ def test_autotune_records_a_choice_per_mode():
         fs[m][:] = 0
         ref = O.mttkrp(enc, m, fs, R)[m]
         assert rel_err(t.mttkrp(m, Fd, R).cpu().numpy(), ref) <= TOL
+
+
+# ------------------------------------------------- deterministic variant
+
+def check_deterministic(dims, cidx, vals, R, seed=0, stream_mode=-1):
+    """DETERMINISTIC against the oracle, and bit-identical on a second run
+    with other MTTKRP work (atomic variants) launched in between."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    Fd = to_dev([rng.uniform(-1.0, 1.0, (int(d), R)) for d in dims], torch.float32)
+    Fo = seen_by_gpu(Fd)
+    t = A.init_salto(dims, cidx, vals, 1, stream_mode=stream_mode) if stream_mode >= 0 else \
+        A.create_alto(dims, cidx, vals)
+    enc = O.build(dims, cidx, vals.astype(np.float32).astype(np.float64))
+    for m in range(len(dims)):
+        fs = [f.copy() for f in Fo]
+        fs[m][:] = 0
+        ref = O.mttkrp(enc, m, fs, R)[m]
+        first = t.mttkrp(m, Fd, R, variant=A.DETERMINISTIC)
+        assert rel_err(first.cpu().numpy(), ref) <= TOL, (m, rel_err(first.cpu().numpy(), ref))
+        for v in (A.ATOMIC, A.SORTED):
+            t.mttkrp(m, Fd, R, variant=v)
+        again = t.mttkrp(m, Fd, R, variant=A.DETERMINISTIC)
+        assert torch.equal(first, again), m
+
+
+@pytest.mark.parametrize("name", FIXTURE_NAMES)
+def test_deterministic_fixtures(name):
+    dims, cidx, vals = load_fixture(name)
+    check_deterministic(dims, cidx, vals, 8)
+
+
+@pytest.mark.parametrize("R", [8, 16, 32, 64, 128])
+def test_deterministic_ranks(R):
+    dims = np.array([1000, 1000, 1000], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 150000, seed=R + 40)
+    check_deterministic(dims, cidx, vals, R, seed=R)
+
+
+def test_deterministic_hot_rows_and_128bit_keys():
+    """Zipf 2.0: a few rows hold most nonzeros, so their runs span many
+    lane-group sub-ranges (the long-chain fix-up)."""
+    dims = np.array([4800000, 1800000, 1800000], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 200000, [2.0, 1.2, 2.0], seed=13, values="lognormal")
+    check_deterministic(dims, cidx, vals, 32)
+
+
+def test_deterministic_five_modes_and_stream_row():
+    dims = np.array([100000, 100000, 10000, 1000, 100], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 150000, [1.1, 1.1, None, None, None], seed=14)
+    check_deterministic(dims, cidx, vals, 64)
+    dims = np.array([1, 3000, 4000, 500], np.uint64)  # every nonzero in one output row
+    cidx, vals = synth.uniform_coo(dims, 100000, seed=15)
+    check_deterministic(dims, cidx, vals, 16, stream_mode=0)
+
+
+def test_deterministic_accumulates_and_rejects_unsupported():
+    import torch
+
+    dims = np.array([300, 200, 100], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 30000, seed=16)
+    R = 16
+    rng = np.random.default_rng(5)
+    Fd = to_dev([rng.uniform(-1, 1, (int(d), R)) for d in dims], torch.float32)
+    t = A.create_alto(dims, cidx, vals)
+    base = torch.ones((200, R), device="cuda")
+    out = base.clone()
+    t.mttkrp(1, Fd, R, out=out, accumulate=True, variant=A.DETERMINISTIC)
+    fresh = t.mttkrp(1, Fd, R, variant=A.DETERMINISTIC)
+    np.testing.assert_allclose(out.cpu().numpy(), base.cpu().numpy() + fresh.cpu().numpy(), rtol=1e-6, atol=1e-6)
+    Fd10 = to_dev([rng.uniform(-1, 1, (int(d), 10)) for d in dims], torch.float32)
+    with pytest.raises(A.AltoError):
+        t.mttkrp(0, Fd10, 10, variant=A.DETERMINISTIC)
+    with pytest.raises(A.AltoError):
+        t.mttkrp(0, [f.to(torch.bfloat16) for f in Fd], R, variant=A.DETERMINISTIC)

@@ -1,0 +1,96 @@
+"""The CP-stream server: every stream's result is the same processed alone
+and in a mix with other streams -- bit for bit, since CP-stream sessions use
+the deterministic MTTKRP and fixed-order reductions throughout (the stated
+bound is 1e-4) --, slices of one stream keep their order, admission respects
+the HBM budget, and the alone result matches the FP64 oracle within 1e-4."""
+import numpy as np
+import pytest
+
+import alto_b200 as A
+import oracle as O
+from alto_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def make_stream(seed, space, nslices, rank):
+    b = synth.stream_batches(space, nslices, lambda rng, s: 300 + 40 * s, [1.1, None, 1.2], seed=seed,
+                             values="uniform")
+    n_init = sum(int(x) for x in b[-1]["dims"]) * rank + 64
+    return b, synth.init_values(n_init, seed=seed + 100)
+
+
+def submit_all(srv, sid, batches, iv, rank):
+    used, prev, tickets = 0, np.zeros(len(batches[0]["dims"]), np.int64), []
+    for b in batches:
+        d = b["dims"].astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * rank
+        tickets.append(srv.submit(sid, b["dims"], b["cidx"], b["vals"], iv[used:used + need]))
+        used += need
+        prev = np.maximum(prev, d)
+    return tickets
+
+
+def normwise(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+SPECS = [(11, [150, 200, 40], 8, A.NONNEG), (12, [300, 120, 60], 16, A.UNCONSTRAINED),
+         (13, [90, 400, 30], 8, A.UNCONSTRAINED), (14, [250, 250, 50], 16, A.NONNEG)]
+
+
+def run(specs, workers):
+    srv = A.Server(8 << 30, workers=workers)
+    sids, streams = [], []
+    for seed, space, rank, con in specs:
+        b, iv = make_stream(seed, space, 5, rank)
+        sid = srv.open(4, 0, rank, [len(b)] + [int(x) for x in b[-1]["dims"][1:]], 2000, constraint=con,
+                       forgetting=0.99, max_inner=10, epsilon=1e-5)
+        sids.append(sid)
+        streams.append((b, iv, rank))
+    tickets = [submit_all(srv, sid, b, iv, rank) for sid, (b, iv, rank) in zip(sids, streams)]
+    srv.drain()
+    out = [[srv.factor(sid, m) for m in range(4)] for sid in sids]
+    st = srv.stats()
+    srv.destroy()
+    return out, st, tickets
+
+
+def test_each_result_same_alone_and_in_the_mix():
+    mix, st, _ = run(SPECS, workers=4)
+    assert st["completed"] == 5 * len(SPECS)
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    for k, spec in enumerate(SPECS):
+        alone, _, _ = run([spec], workers=1)
+        for a, m in zip(alone[0], mix[k]):
+            assert a.shape == m.shape
+            assert np.array_equal(m, a), (k, normwise(m, a))
+
+
+def test_alone_result_matches_oracle():
+    seed, space, rank, con = SPECS[0]
+    res, _, _ = run([SPECS[0]], workers=1)
+    b, iv = make_stream(seed, space, 5, rank)
+    bo = [dict(dims=x["dims"], cidx=x["cidx"], vals=x["vals"].astype(np.float32).astype(np.float64)) for x in b]
+    oo, _, _ = O.cpstream(bo, 0, rank, 10, 1e-5, con == A.NONNEG, iv.astype(np.float32).astype(np.float64))
+    for g, o in zip(res[0], oo):
+        assert normwise(g, o) <= 1e-4
+
+
+def test_admission_waits_for_budget():
+    srv = A.Server(1, workers=2)  # room for one stream at a time
+    b1, iv1 = make_stream(21, [100, 100, 20], 3, 8)
+    b2, iv2 = make_stream(22, [100, 100, 20], 3, 8)
+    s1 = srv.open(4, 0, 8, [3, 200, 200, 40], 1000)
+    s2 = srv.open(4, 0, 8, [3, 200, 200, 40], 1000)
+    st = srv.stats()
+    assert st["admitted_streams"] == 1 and st["pending_streams"] == 1
+    t2 = submit_all(srv, s2, b2, iv2, 8)
+    submit_all(srv, s1, b1, iv1, 8)
+    srv.drain()
+    assert srv.stats()["completed"] == 3  # only the admitted stream ran
+    srv.close(s1)
+    srv.wait(t2[-1])
+    assert srv.stats()["completed"] == 6
+    srv.close(s2)
+    srv.destroy()

@@ -62,3 +62,15 @@ def test_forgetting_factor_is_a_parameter():
     oo, _, _ = O.cpstream(bo, 0, R, 10, 1e-5, 0, iv.astype(np.float32).astype(np.float64), forgetting=0.95)
     for a, c in zip(o1, oo):
         assert normwise(a, c) <= 1e-4
+
+
+def test_stream_repeats_bit_for_bit():
+    """Two sessions fed the same slices end with identical factors and
+    lambda, and take the same inner iterations."""
+    b = load_stream_fixture()[:4]
+    iv = synth.init_values(20000, seed=3)
+    o1, l1, i1 = run_gpu(b, 8, 10, 1e-5, 1, iv, forgetting=0.95)
+    o2, l2, i2 = run_gpu(b, 8, 10, 1e-5, 1, iv, forgetting=0.95)
+    assert i1 == i2 and np.array_equal(l1, l2)
+    for a, c in zip(o1, o2):
+        assert np.array_equal(a, c)
