@@ -41,7 +41,7 @@ EXPORTED = [
     "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
-    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_close",
+    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_graph", "alto_stream_close",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
@@ -383,6 +383,11 @@ class CPStream:
         rows = c_uint64()
         check(lib().alto_stream_factor(self.h, c_int(mode), out.ctypes.data_as(c_void_p), byref(rows)))
         return out[: rows.value]
+
+    def set_graph(self, enable):
+        """Inner iterations 2.. of each batch as one CUDA graph (default) or
+        launched one by one (alto_stream_set_graph)."""
+        check(lib().alto_stream_set_graph(self.h, c_int(1 if enable else 0)))
 
     def lam(self):
         out = np.zeros(self.rank, np.float64)

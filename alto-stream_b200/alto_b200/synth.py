@@ -266,3 +266,39 @@ def zipf_coo_device(dims, nnz, exponents, seed=0, values="lognormal", device="cu
     else:
         v = torch.rand(n, generator=g, device=device, dtype=torch.float32)
     return cidx, v
+
+
+def serving_streams(nstreams, slices_per_stream, seed=0, dim_range=(1e3, 1e6), nnz_range=(1e4, 1e6),
+                    nnz_median=5e4, ranks=(8, 16, 32)):
+    """Independent CP-stream tensors for the serving workload.
+
+    Per stream: three spatial modes with lengths log-uniform in dim_range, a
+    rank drawn from `ranks`, a constraint (0 unconstrained, 1 non-negative)
+    drawn with equal odds, and slices_per_stream slices of one time step each
+    whose nonzero counts are log-normal (median nnz_median, sigma 1) clipped
+    to nnz_range; coordinates are uniform over the stream's dims (unique),
+    values uniform(0, 1).  Every slice carries the stream's full dims (the
+    time mode has extent 1), so the model takes its final size with the
+    first slice.  Returns a list of dicts {dims, rank, constraint, slices}."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log10(dim_range[0]), np.log10(dim_range[1])
+    out = []
+    for k in range(nstreams):
+        d = [int(round(10 ** rng.uniform(lo, hi))) for _ in range(3)]
+        rank = int(rng.choice(ranks))
+        con = int(rng.integers(0, 2))
+        bits = [max(1, (x - 1).bit_length()) for x in d]
+        slices = []
+        for _ in range(slices_per_stream):
+            n = int(np.clip(rng.lognormal(np.log(nnz_median), 1.0), nnz_range[0], nnz_range[1]))
+            draw = int(n * 1.05) + 64
+            cols = [rng.integers(0, x, draw, dtype=np.uint64) for x in d]
+            key = cols[0] | (cols[1] << np.uint64(bits[0])) | (cols[2] << np.uint64(bits[0] + bits[1]))
+            _, first = np.unique(key, return_index=True)
+            keep = np.sort(first)[:n]
+            cidx = np.zeros((4, len(keep)), np.uint64)
+            for m in range(3):
+                cidx[m + 1] = cols[m][keep]
+            slices.append(dict(dims=np.array([1] + d, np.uint64), cidx=cidx, vals=rng.random(len(keep))))
+        out.append(dict(dims=[1] + d, rank=rank, constraint=con, slices=slices))
+    return out

@@ -85,13 +85,27 @@ __global__ void __launch_bounds__(kGramThreads)
   }
 }
 
-// out[p] = sum over blocks of partials[b][p], in block order.
-__global__ void reduce_partials_kernel(const double* __restrict__ partials, int nblocks, int n,
-                                       double* __restrict__ out) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * n + p];
-    out[p] = s;
+// out[p] = sum over blocks b of partials[b][p] in a fixed order: block x
+// takes 32 consecutive p (one per lane, coalesced), warp w sums blocks
+// w, w+8, w+16, ... and the 8 warp sums are added in warp order.  Launch with
+// reduce_grid(n) blocks of kReduceThreads threads.
+constexpr int kReduceThreads = 256;
+__host__ __device__ inline unsigned reduce_grid(int n) { return (unsigned)((n + 31) / 32); }
+
+__global__ void __launch_bounds__(kReduceThreads)
+    reduce_partials_kernel(const double* __restrict__ partials, int nblocks, int n, double* __restrict__ out) {
+  __shared__ double s[kReduceThreads / 32][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * 32 + lane;
+  double acc = 0.0;
+  if (p < n)
+    for (int b = w; b < nblocks; b += kReduceThreads / 32) acc += partials[(size_t)b * n + p];
+  s[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && p < n) {
+    double t = s[0][lane];
+    for (int k = 1; k < kReduceThreads / 32; ++k) t += s[k][lane];
+    out[p] = t;
   }
 }
 
@@ -111,11 +125,17 @@ static alto_status gram_launch(const TA* A, const TB* B, uint64_t I, int R, doub
     ALTO_TRY_CUDA(cudaMemsetAsync(out, 0, RR * sizeof(double), st));
     return ALTO_OK;
   }
+  // (the shared-memory limit is raised once per kernel, outside any capture)
 #define GRAM_CASE(P)                                                                             \
   case P:                                                                                        \
-    if (smem > 48 * 1024)                                                                        \
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(gram_partial_kernel<P, TA, TB>,                        \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    if (smem > 48 * 1024) {                                                                      \
+      static size_t raised = 0;                                                                  \
+      if (smem > raised) {                                                                       \
+        ALTO_TRY_CUDA(cudaFuncSetAttribute(gram_partial_kernel<P, TA, TB>,                      \
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        raised = smem;                                                                           \
+      }                                                                                          \
+    }                                                                                            \
     gram_partial_kernel<P, TA, TB><<<(unsigned)nb, kGramThreads, smem, st>>>(A, B, I, R, rpb, part); \
     break;
   switch (ppt <= 1 ? 1 : ppt <= 2 ? 2 : ppt <= 4 ? 4 : ppt <= 8 ? 8 : ppt <= 16 ? 16 : 64) {
@@ -128,7 +148,7 @@ static alto_status gram_launch(const TA* A, const TB* B, uint64_t I, int R, doub
   }
 #undef GRAM_CASE
   ALTO_LAUNCHED();
-  reduce_partials_kernel<<<(RR + 255) / 256, 256, 0, st>>>(part, (int)nb, RR, out);
+  reduce_partials_kernel<<<reduce_grid(RR), kReduceThreads, 0, st>>>(part, (int)nb, RR, out);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -255,9 +275,12 @@ __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes,
 alto_status solve_setup(const double* grams, int nmodes, unsigned mask, int R, int kind,
                         double ridge, double* W, int* status, double* rho, cudaStream_t st) {
   const size_t smem = (size_t)R * R * sizeof(double);
-  if (smem > 48 * 1024)
+  static size_t raised = 0;
+  if (smem > 48 * 1024 && smem > raised) {
     ALTO_TRY_CUDA(cudaFuncSetAttribute(solve_setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
+    raised = smem;
+  }
   solve_setup_kernel<<<1, 256, smem, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
   ALTO_LAUNCHED();
   return ALTO_OK;
@@ -463,7 +486,7 @@ alto_status dot_stats(const float* a, const float* b, uint64_t n, const double* 
   ALTO_TRY(scratch.ensure(kDotBlocks * 3 * sizeof(double)));
   dot_partial_kernel<float, float><<<kDotBlocks, 256, 0, st>>>(a, b, n, colw, R, scratch.as<double>());
   ALTO_LAUNCHED();
-  reduce_partials_kernel<<<1, 32, 0, st>>>(scratch.as<double>(), kDotBlocks, 3, out3);
+  reduce_partials_kernel<<<reduce_grid(3), kReduceThreads, 0, st>>>(scratch.as<double>(), kDotBlocks, 3, out3);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -473,7 +496,7 @@ alto_status dot_stats_f64(const double* a, const float* b, uint64_t n, double* o
   ALTO_TRY(scratch.ensure(kDotBlocks * 3 * sizeof(double)));
   dot_partial_kernel<double, float><<<kDotBlocks, 256, 0, st>>>(a, b, n, nullptr, 1, scratch.as<double>());
   ALTO_LAUNCHED();
-  reduce_partials_kernel<<<1, 32, 0, st>>>(scratch.as<double>(), kDotBlocks, 3, out3);
+  reduce_partials_kernel<<<reduce_grid(3), kReduceThreads, 0, st>>>(scratch.as<double>(), kDotBlocks, 3, out3);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -499,7 +522,7 @@ alto_status sum_squares(const float* v, uint64_t n, double* out, DevBuf& scratch
   ALTO_TRY(scratch.ensure(kDotBlocks * sizeof(double)));
   sumsq_partial_kernel<<<kDotBlocks, 256, 0, st>>>(v, n, scratch.as<double>());
   ALTO_LAUNCHED();
-  reduce_partials_kernel<<<1, 32, 0, st>>>(scratch.as<double>(), kDotBlocks, 1, out);
+  reduce_partials_kernel<<<reduce_grid(1), kReduceThreads, 0, st>>>(scratch.as<double>(), kDotBlocks, 1, out);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -670,7 +693,7 @@ extern "C" alto_status alto_gram_noalloc(const float* U, uint64_t rows, int rank
       break;
   }
   ALTO_LAUNCHED();
-  alto::reduce_partials_kernel<<<(RR + 255) / 256, 256, 0, st>>>(part, (int)nb, RR, G);
+  alto::reduce_partials_kernel<<<alto::reduce_grid(RR), alto::kReduceThreads, 0, st>>>(part, (int)nb, RR, G);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }

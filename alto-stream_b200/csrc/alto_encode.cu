@@ -685,6 +685,21 @@ __global__ void gather_line_kernel(const uint4* __restrict__ line, int words,
   }
 }
 
+// Gather line records in the given order, writing them with the rows
+// decoded (3-mode lines): {row 0, row 1, row 2, value}.
+__global__ void gather_decode3_kernel(const void* __restrict__ line, LineDecode dec,
+                                      const uint32_t* __restrict__ order, uint32_t nnz,
+                                      uint4* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    uint64_t lo, hi;
+    float v;
+    rec_read(line, dec.hi_words, order[i], lo, hi, v);
+    out[i] = make_uint4((uint32_t)line_field(lo, hi, dec.pos[0], dec.mask[0]),
+                        (uint32_t)line_field(lo, hi, dec.pos[1], dec.mask[1]),
+                        (uint32_t)line_field(lo, hi, dec.pos[2], dec.mask[2]), __float_as_uint(v));
+  }
+}
+
 // A copy of the line ordered by the row of `mode`, ALTO order kept among
 // equal rows (stable LSD sort over the mode's bits).  This is the device
 // form of the reference's op_sched traversal (include/alto.hpp:1708-1801,
@@ -694,7 +709,9 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   SortedLine& s = t->sorted[mode];
   const uint64_t nnz = t->nnz;
   const int hw = t->dec.hi_words;
-  ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(hw)));
+  // 3-mode copies store the rows decoded (same 16 bytes per record)
+  s.hw = t->nmodes == 3 ? kDecoded3 : hw;
+  ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(s.hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
   const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
   size_t off = 0;
@@ -723,13 +740,19 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
       ALTO_LAUNCHED();
       cur ^= 1;
     }
-    gather_line_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.as<uint4>(), rec_bytes(hw) / 16,
-                                                           pm[cur], n32, s.line.as<uint4>());
+    if (s.hw == kDecoded3)
+      gather_decode3_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, pm[cur], n32,
+                                                                 s.line.as<uint4>());
+    else
+      gather_line_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.as<uint4>(), rec_bytes(hw) / 16,
+                                                             pm[cur], n32, s.line.as<uint4>());
     ALTO_LAUNCHED();
   }
   s.ntiles = t->ntiles;
   ALTO_TRY(s.tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * t->nmodes * 2 * 4));
-  if (t->ntiles) {
+  // (tile intervals are read only by shared-memory staging, which never
+  // walks a sorted copy; the decoded copies carry none)
+  if (t->ntiles && s.hw != kDecoded3) {
     tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(s.line.p, t->dec, n32, t->tile_nnz,
                                                     s.tile_iv.as<uint32_t>());
     ALTO_LAUNCHED();

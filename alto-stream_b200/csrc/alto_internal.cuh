@@ -129,6 +129,12 @@ struct __align__(16) LineRec32 {
   uint32_t pad[3];
 };
 
+// Record format code 3: a 3-mode record with the rows stored decoded,
+// {row of mode 0, row of mode 1, row of mode 2, value} (16 bytes); used for
+// the row-sorted copies of 3-mode lines, where the kernels then skip the
+// bit-field decode.
+constexpr int kDecoded3 = 3;
+
 __host__ __device__ __forceinline__ int rec_bytes(int hi_words) { return hi_words == 2 ? 32 : 16; }
 
 // Read record i of a line with any key width.
@@ -184,6 +190,7 @@ namespace alto {
 // A copy of the line ordered by one mode's row (see build_sorted_line).
 struct SortedLine {
   DevBuf line, tile_iv;
+  int hw = 0;  // record format: the line's hi_words, or kDecoded3
   uint32_t ntiles = 0;
   uint64_t for_nnz = 0;
   bool ready = false;

@@ -96,6 +96,15 @@ __device__ __forceinline__ uint32_t field32(uint32_t w0, uint32_t w1, uint32_t w
   return v & mask;
 }
 
+// Row of mode m of a record held as words w (HW = kDecoded3: stored
+// decoded; else the field of the mode-contiguous key).
+template <int HW>
+__device__ __forceinline__ uint32_t rec_row(const uint32_t (&w)[4], const LineDecode& dec, int m) {
+  // (selects, not w[m]: a runtime index would move w to local memory)
+  if (HW == kDecoded3) return m == 0 ? w[0] : (m == 1 ? w[1] : w[2]);
+  return field32(w[0], w[1], w[2], w[3], dec.pos[m], (uint32_t)dec.mask[m]);
+}
+
 // This lane's V floats of a factor row: V/4 float4 pieces at columns
 // q*4G + 4*sub (q = 0..V/4-1), so that one load instruction of the G lanes of
 // a group reads 4G contiguous floats (whole 32-byte sectors).
@@ -247,7 +256,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
       for (int j = 0; j < NM - 1; ++j) {
         const int m = j < a.target ? j : j + 1;
         if (m < a.dec.nmodes && valid[u]) {
-          const uint32_t r = field32(w[u][0], w[u][1], w[u][2], w[u][3], a.dec.pos[m], (uint32_t)a.dec.mask[m]);
+          const uint32_t r = rec_row<HW>(w[u], a.dec, m);
           load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
         }
       }
@@ -257,7 +266,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
     bool ok[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      rows[u] = field32(w[u][0], w[u][1], w[u][2], w[u][3], a.dec.pos[a.target], (uint32_t)a.dec.mask[a.target]);
+      rows[u] = rec_row<HW>(w[u], a.dec, a.target);
       vals[u] = v[u];
       ok[u] = valid[u];
     }
@@ -301,8 +310,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
     bool ok0[1];
     const uint32_t at = gs > 0 ? gs - 1 : 0;
     load_keys<HW, 1, SMEM>(line, at, at + 1, w0, v0, ok0);
-    const uint32_t r0 = field32(w0[0][0], w0[0][1], w0[0][2], w0[0][3], a.dec.pos[a.target],
-                                (uint32_t)a.dec.mask[a.target]);
+    const uint32_t r0 = rec_row<HW>(w0[0], a.dec, a.target);
     det_slot<R, V, G>(a, slot0, r0, sub, acc, true);
     det_slot<R, V, G>(a, slot0 + 1, r0, sub, acc, true);
   } else if (nrun == 0) {
@@ -562,13 +570,23 @@ __global__ void __launch_bounds__(kMttkrpThreads)
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t i = gw; i < a.nnz; i += nw) {
-    uint64_t lo, hi;
-    float v;
-    rec_read(a.line, HW, i, lo, hi, v);
     uint32_t rows[ALTO_MAX_MODES];
+    float v;
+    if (HW == kDecoded3) {
+      const uint4 q = static_cast<const uint4*>(a.line)[i];
+      rows[0] = q.x;
+      rows[1] = q.y;
+      rows[2] = q.z;
 #pragma unroll
-    for (int m = 0; m < ALTO_MAX_MODES; ++m)
-      rows[m] = m < a.dec.nmodes ? (uint32_t)line_field(lo, hi, a.dec.pos[m], a.dec.mask[m]) : 0;
+      for (int m = 3; m < ALTO_MAX_MODES; ++m) rows[m] = 0;
+      v = __uint_as_float(q.w);
+    } else {
+      uint64_t lo, hi;
+      rec_read(a.line, HW, i, lo, hi, v);
+#pragma unroll
+      for (int m = 0; m < ALTO_MAX_MODES; ++m)
+        rows[m] = m < a.dec.nmodes ? (uint32_t)line_field(lo, hi, a.dec.pos[m], a.dec.mask[m]) : 0;
+    }
     for (int r = lane; r < rank; r += 32) {
       float x = v;
 #pragma unroll
@@ -664,6 +682,7 @@ static alto_status launch_det_nm(const MttkrpArgs& a, uint2* longs, uint32_t* nl
 
 template <int R, int HW>
 static alto_status launch_det(const MttkrpArgs& a, uint2* longs, uint32_t* nlong, cudaStream_t st) {
+  if constexpr (HW == kDecoded3) return launch_det_nm<R, HW, 3>(a, longs, nlong, st);
   switch (a.dec.nmodes) {
     case 3: return launch_det_nm<R, HW, 3>(a, longs, nlong, st);
     case 4: return launch_det_nm<R, HW, 4>(a, longs, nlong, st);
@@ -687,6 +706,17 @@ static alto_status launch_det_rank(const MttkrpArgs& a, int rank, uint2* longs, 
   return ALTO_ERR_UNSUPPORTED;
 }
 
+// Lane groups per warp of the specialised kernels at this rank.
+static uint32_t groups_per_warp(int rank) {
+  switch (rank) {
+    case 8: return LaneWidth<8>::NPW;
+    case 16: return LaneWidth<16>::NPW;
+    case 32: return LaneWidth<32>::NPW;
+    case 64: return LaneWidth<64>::NPW;
+    default: return LaneWidth<128>::NPW;
+  }
+}
+
 bool deterministic_supported(int rank, alto_dtype fdtype) {
   return fdtype == ALTO_F32 && (rank == 8 || rank == 16 || rank == 32 || rank == 64 || rank == 128);
 }
@@ -694,6 +724,9 @@ bool deterministic_supported(int rank, alto_dtype fdtype) {
 template <int R, typename FT, int HW>
 static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
                                 cudaStream_t st) {
+  if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
+    return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
+  } else {
 #define NM_CASE(NN)                                                                   \
   case NN:                                                                            \
     if (stage) return launch_tile<R, FT, HW, true, NN>(a, st);                        \
@@ -707,6 +740,7 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed,
                    : launch_tile<R, FT, HW, false, ALTO_MAX_MODES>(a, st);
   }
 #undef NM_CASE
+  }
 }
 
 template <typename FT, int HW>
@@ -792,6 +826,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   a.line = t->line.p;
   a.tile_iv = t->tile_iv.as<uint32_t>();
   a.ntiles = t->ntiles;
+  int hw = t->dec.hi_words;  // record format of the line walked
   // (a mode of length 1 is already in row order in the ALTO line)
   if (variant == ALTO_MTTKRP_SORTED || (det && t->dims[mode] > 1)) {
     if (!t->sorted[mode].ready || t->sorted[mode].for_nnz != t->nnz)
@@ -800,6 +835,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     a.line = s.line.p;
     a.tile_iv = s.tile_iv.as<uint32_t>();
     a.ntiles = s.ntiles;
+    hw = s.hw;
   }
   a.nnz = (uint32_t)t->nnz;
   a.tile_nnz = t->tile_nnz;
@@ -813,7 +849,6 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     if (m != mode && (reinterpret_cast<uintptr_t>(factors[m]) % (4 * esz)) != 0) aligned = false;
   }
   const bool stage = variant == ALTO_MTTKRP_STAGED || variant == ALTO_MTTKRP_STREAM;
-  const int hw = t->dec.hi_words;
   if (!t->err.p) {
     ALTO_TRY(t->err.ensure(16));
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
@@ -824,7 +859,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
       set_error("the deterministic MTTKRP needs 16-byte aligned factors and output");
       return ALTO_ERR_UNSUPPORTED;
     }
-    const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * (128 / rank) * 2;
+    const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * groups_per_warp(rank) * 2;
     ALTO_TRY(t->det_rows.ensure(nslots * 4));
     ALTO_TRY(t->det_vals.ensure(nslots * rank * 4));
     ALTO_TRY(t->det_long.ensure((nslots / (kShortChain + 1) + 2) * sizeof(uint2) + 16));
@@ -834,16 +869,19 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     uint2* longs = reinterpret_cast<uint2*>(t->det_long.as<char>() + 16);
     if (hw == 0) return launch_det_rank<0>(a, rank, longs, nlong, st);
     if (hw == 1) return launch_det_rank<1>(a, rank, longs, nlong, st);
+    if (hw == kDecoded3) return launch_det_rank<kDecoded3>(a, rank, longs, nlong, st);
     return launch_det_rank<2>(a, rank, longs, nlong, st);
   }
   const bool bulk = feed == 1;
   if (fdtype == ALTO_BF16) {
     if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
     if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == kDecoded3) return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, aligned, err, st);
     return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, aligned, err, st);
   }
   if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, aligned, err, st);
   if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, aligned, err, st);
   return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
 }
 

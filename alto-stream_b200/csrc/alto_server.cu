@@ -251,8 +251,10 @@ alto_status alto_server_open(alto_server* s, const alto_stream_config* cfg, cons
 
 alto_status alto_server_submit(alto_server* s, int sid, const alto_coo* batch, const double* init_vals,
                                uint64_t n_init, uint64_t* ticket) {
-  if (!s || !batch || batch->on_device || batch->nnz == 0) {
-    set_error("server batches are non-empty host COO tensors");
+  if (!s || !batch || batch->on_device || batch->nnz == 0 || !batch->cidx || !batch->vals || !batch->dims ||
+      (batch->index_bytes != 4 && batch->index_bytes != 8) ||
+      (batch->val_dtype != ALTO_F32 && batch->val_dtype != ALTO_F64)) {
+    set_error("server batches are non-empty host COO tensors (4- or 8-byte indices, float32/64 values)");
     return ALTO_ERR_INVALID;
   }
   SliceReq* q = new SliceReq();
@@ -260,14 +262,21 @@ alto_status alto_server_submit(alto_server* s, int sid, const alto_coo* batch, c
   q->dims.assign(batch->dims, batch->dims + batch->nmodes);
   q->cidx.resize(batch->nmodes);
   for (int m = 0; m < batch->nmodes; ++m) {
-    q->cidx[m].resize(batch->nnz);
-    for (uint64_t i = 0; i < batch->nnz; ++i)
-      q->cidx[m][i] = batch->index_bytes == 8 ? ((const uint64_t*)batch->cidx[m])[i]
-                                              : ((const uint32_t*)batch->cidx[m])[i];
+    if (batch->index_bytes == 8) {
+      const uint64_t* c = (const uint64_t*)batch->cidx[m];
+      q->cidx[m].assign(c, c + batch->nnz);
+    } else {
+      const uint32_t* c = (const uint32_t*)batch->cidx[m];
+      q->cidx[m].assign(c, c + batch->nnz);
+    }
   }
-  q->vals.resize(batch->nnz);
-  for (uint64_t i = 0; i < batch->nnz; ++i)
-    q->vals[i] = batch->val_dtype == ALTO_F64 ? ((const double*)batch->vals)[i] : ((const float*)batch->vals)[i];
+  if (batch->val_dtype == ALTO_F64) {
+    const double* v = (const double*)batch->vals;
+    q->vals.assign(v, v + batch->nnz);
+  } else {
+    const float* v = (const float*)batch->vals;
+    q->vals.assign(v, v + batch->nnz);
+  }
   if (n_init && init_vals) q->init.assign(init_vals, init_vals + n_init);
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->streams.find(sid);

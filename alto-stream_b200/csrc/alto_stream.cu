@@ -20,11 +20,19 @@
 // |delta - prev_delta| < epsilon.  After the batch: G_t *= forgetting,
 // prev_U <- U, time rows appended.
 //
-// ADMM runs as one launch per sweep over all rows (rows are independent
-// except for the four global sums of the stopping test).  Each launch writes
-// per-block partial sums; the last block to finish (ticket counter, no
-// waiting) adds them in block order and raises a converged flag that makes
-// the remaining launches return at once.
+// ADMM of a mode runs as three launches: a pass over the rows that runs all
+// 25 sweeps in registers and records every sweep's stopping-test sums, a
+// one-block kernel that picks the sweep count from them, and a second pass
+// that reruns that many sweeps and writes the result (admm_rows_kernel).
+//
+// Launch structure.  The first inner iteration of a batch is issued
+// directly (it sizes every buffer and builds the row-sorted lines); the
+// remaining iterations run as one CUDA graph: a while node whose body is one
+// inner iteration, ending in a kernel that computes delta and decides on the
+// device whether to go on.  A batch costs one eager iteration, one capture
+// and one graph launch, with no host synchronisation between inner
+// iterations.  alto_stream_set_graph(s, 0) issues every iteration directly
+// instead (the same kernels in the same order: identical results).
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -39,159 +47,295 @@ constexpr int kAdmmThreads = 256;
 constexpr int kAdmmMaxIters = 25;
 
 struct AdmmState {
-  int converged;
-  int iters;
-  unsigned ticket;
+  int iters;         // sweeps done
+  int stop;          // the test passed or 25 sweeps are done
+  int converged;     // the test passed
+  int chunk_start;   // sweeps done before the current chunk
+  int chunk_sweeps;  // sweeps of the current chunk that stand
   int pad;
 };
 
-// Shared row solve: x[c] = sum_k a[k] W[k][c] for the row held by the warp's
-// lanes (lane owns columns lane, lane+32, ...).  a is given per lane slot.
-template <int SLOTS>
+// Inner-iteration bookkeeping kept on the device.
+struct IterState {
+  int done;     // inner iterations executed in this batch
+  int stop;     // converged, or a solve failed
+  int info;     // Cholesky info of the failed ADMM solve (0 = none)
+  int pad;
+  double prev_delta;
+  double delta;
+};
+
+// Sets a conditional node's value from a kernel in its graph (no-op when the
+// kernel was launched outside a graph).
+__device__ __forceinline__ void set_condition(cudaGraphConditionalHandle h, int in_graph, bool go) {
+  if (in_graph) cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Rows are processed by lane segments of SEG lanes (SEG = 8 or 16 for rank
+// <= SEG, so 32/SEG rows share a warp; SEG = 32 otherwise, one row per warp
+// with SLOTS columns per lane): lane `col` of a segment owns columns col,
+// col + 32, ... of its row.
+template <int SEG>
+struct RowMap {
+  static constexpr int kRows = 32 / SEG;  // rows per warp
+  __device__ static int base(int lane) { return SEG < 32 ? (lane & ~(SEG - 1)) : 0; }
+  __device__ static int col(int lane) { return SEG < 32 ? (lane & (SEG - 1)) : lane; }
+  __device__ static int sub(int lane) { return SEG < 32 ? lane / SEG : 0; }
+};
+
+// Row solve: x[c] = sum_k a[k] W[k][c] for the row held by the segment
+// (a given per lane slot; W in shared memory), fused multiply-adds in k order.
+template <int SLOTS, int SEG>
 __device__ __forceinline__ void row_solve(const double (&a)[SLOTS], const double* sw, int R,
                                           int lane, double (&x)[SLOTS]) {
+  const int base = RowMap<SEG>::base(lane), col = RowMap<SEG>::col(lane);
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) x[s] = 0.0;
 #pragma unroll
   for (int ks = 0; ks < SLOTS; ++ks) {
     const int kbase = ks * 32;
-    const int kmax = min(32, R - kbase);
+    const int kmax = min(SEG, R - kbase);
     for (int k = 0; k < kmax; ++k) {
-      const double ak = __shfl_sync(0xffffffffu, a[ks], k);
+      const double ak = __shfl_sync(0xffffffffu, a[ks], base + k);
 #pragma unroll
       for (int s = 0; s < SLOTS; ++s) {
-        const int c = s * 32 + lane;
-        if (c < R) x[s] += ak * sw[(kbase + k) * R + c];
+        const int c = s * 32 + col;
+        if (c < R) x[s] = __fma_rn(ak, sw[(kbase + k) * R + c], x[s]);
       }
     }
   }
 }
 
-// First primal update (src/admm.cpp:288-327).
-template <int SLOTS>
-__global__ void __launch_bounds__(kAdmmThreads)
-    admm_first_kernel(const double* __restrict__ rhs, double* __restrict__ primal,
-                      const double* __restrict__ dual, double* __restrict__ aux,
-                      double* __restrict__ init, const double* __restrict__ W,
-                      const double* __restrict__ rho_p, uint64_t I, int R,
-                      AdmmState* __restrict__ state) {
-  extern __shared__ double sw[];
-  for (int p = threadIdx.x; p < R * R; p += blockDim.x) sw[p] = W[p];
-  __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    state->converged = 0;
-    state->iters = 0;
-    state->ticket = 0;
-  }
-  const double rho = *rho_p;
-  const int lane = threadIdx.x & 31;
-  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t i = gw; i < I; i += nw) {
-    double a[SLOTS], x[SLOTS];
-#pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-      const int c = s * 32 + lane;
-      a[s] = c < R ? rhs[i * R + c] + rho * (primal[i * R + c] + dual[i * R + c]) : 0.0;
-    }
-    row_solve<SLOTS>(a, sw, R, lane, x);
-#pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-      const int c = s * 32 + lane;
-      if (c < R) {
-        const size_t q = i * R + c;
-        init[q] = primal[q];
-        aux[q] = x[s];
-        const double v = x[s] - dual[q];
-        primal[q] = v < 0.0 ? 0.0 : v;
-      }
-    }
-  }
-}
+// ADMM of one mode (admm_cf_, src/admm.cpp:288-425) in chunks of up to
+// kAdmmChunk sweeps, each chunk two passes over the rows with the rows'
+// state in registers.  Rows are independent except for the stopping test,
+// which after every sweep compares four sums over all rows (p_res <= tol
+// p_norm and d_res <= tol d_norm).  Per chunk:
+//   pass 1  runs the chunk's sweeps for every row (the first chunk starts
+//           with the first update) without writing the rows back, and
+//           records each sweep's four sums (per block: warps in order);
+//   decide  adds the blocks' sums in block order and finds the first sweep
+//           of the chunk whose sums pass the test -- k sweeps, else the
+//           whole chunk (25 sweeps at most in all);
+//   pass 2  reruns the same k sweeps and writes primal, aux and dual.
+// Both passes run the same per-row code, so the result is that of stopping
+// after exactly the sweep the reference stops after.  Most solves stop
+// after one or two sweeps, i.e. within the first chunk: each row is then
+// read twice and written once.  Chunks repeat (a while node in the batch
+// graph, or launches that return at once when issued directly) until the
+// test passes or 25 sweeps are done.
+//
+// Per sweep, with the reference's variables (x = primal, z = aux, u = dual,
+// init = x before the sweep, W = (Phi + rho I)^{-1}):
+//   y = x - z;  u += y;  z = (rhs + rho (x + u)) W;  x = max(z - u, 0)
+//   p_res += y^2, p_norm += x_before^2, d_norm += u^2, d_res += (x - init)^2.
+// The reference sets init = x at the end of every sweep, so d_res is zero
+// from the second sweep on; only the first sweep's d_res term is formed.
+constexpr int kAdmmChunk = 3;
+constexpr int kAdmmSums = kAdmmChunk * 4;
 
-// One ADMM sweep (src/admm.cpp:331-425) with the stopping test.
 template <int SLOTS>
+struct AdmmBatch {
+  static constexpr int M = SLOTS == 1 ? 4 : (SLOTS == 2 ? 2 : 1);  // row groups per warp in registers
+};
+
+template <int SLOTS, int SEG, bool PASS1>
 __global__ void __launch_bounds__(kAdmmThreads)
-    admm_sweep_kernel(const double* __restrict__ rhs, double* __restrict__ primal,
-                      double* __restrict__ dual, double* __restrict__ aux,
-                      double* __restrict__ init, const double* __restrict__ W,
-                      const double* __restrict__ rho_p, uint64_t I, int R,
-                      double* __restrict__ partials, AdmmState* __restrict__ state, double tol) {
-  if (*(volatile int*)&state->converged) return;
+    admm_rows_kernel(const double* __restrict__ rhs, double* __restrict__ primal, double* __restrict__ aux,
+                     double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
+                     uint64_t I, int R, double* __restrict__ partials, const AdmmState* __restrict__ state) {
+  constexpr int M = AdmmBatch<SLOTS>::M;
+  constexpr int KR = RowMap<SEG>::kRows;
+  constexpr int NW = kAdmmThreads / 32;
+  if (PASS1 ? state->stop : state->chunk_sweeps == 0) return;
+  const int start = PASS1 ? state->iters : state->chunk_start;  // sweeps done before this chunk
+  const int nsweeps = PASS1 ? min(kAdmmChunk, kAdmmMaxIters - start) : state->chunk_sweeps;
+  const bool first = start == 0;
   extern __shared__ double sw[];
+  __shared__ double wsum[PASS1 ? NW : 1][PASS1 ? kAdmmSums : 1];
   for (int p = threadIdx.x; p < R * R; p += blockDim.x) sw[p] = W[p];
+  if (PASS1)
+    for (int p = threadIdx.x; p < NW * kAdmmSums; p += blockDim.x) (&wsum[0][0])[p] = 0.0;
   __syncthreads();
   const double rho = *rho_p;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int col = RowMap<SEG>::col(lane), sub = RowMap<SEG>::sub(lane);
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  double p_res = 0, d_res = 0, p_norm = 0, d_norm = 0;
-  for (uint64_t i = gw; i < I; i += nw) {
-    double a[SLOTS], x[SLOTS];
+  for (uint64_t b0 = gw * KR * M; b0 < I; b0 += nw * KR * M) {
+    double X[M][SLOTS], Z[M][SLOTS], U[M][SLOTS], H[M][SLOTS], X0[M][SLOTS];
 #pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-      const int c = s * 32 + lane;
-      a[s] = 0.0;
-      if (c < R) {
-        const size_t q = i * R + c;
-        const double xv = primal[q];
-        const double dd = xv - init[q];
-        d_res += dd * dd;
-        p_norm += xv * xv;
-        const double y = xv - aux[q];
-        const double di = dual[q] + y;
-        dual[q] = di;
-        d_norm += di * di;
-        p_res += y * y;
-        a[s] = rhs[q] + rho * (xv + di);
+    for (int m = 0; m < M; ++m) {
+      const uint64_t i = b0 + (uint64_t)m * KR + sub;
+      double a[SLOTS], z[SLOTS];
+#pragma unroll
+      for (int s = 0; s < SLOTS; ++s) {
+        const int c = s * 32 + col;
+        const bool ok = i < I && c < R;
+        H[m][s] = ok ? rhs[i * R + c] : 0.0;
+        X[m][s] = ok ? primal[i * R + c] : 0.0;
+        U[m][s] = ok ? dual[i * R + c] : 0.0;
+        Z[m][s] = ok && !first ? aux[i * R + c] : 0.0;
+        X0[m][s] = X[m][s];
+        // first update (src/admm.cpp:288-327): z = (rhs + rho (x + u)) W
+        a[s] = __fma_rn(rho, __dadd_rn(X[m][s], U[m][s]), H[m][s]);
+      }
+      if (first) {
+        row_solve<SLOTS, SEG>(a, sw, R, lane, z);
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+          Z[m][s] = z[s];
+          const double v = __dsub_rn(z[s], U[m][s]);
+          X[m][s] = v < 0.0 ? 0.0 : v;
+        }
       }
     }
-    row_solve<SLOTS>(a, sw, R, lane, x);
+    for (int k = 0; k < nsweeps; ++k) {
+      double p_res = 0, d_res = 0, p_norm = 0, d_norm = 0;
 #pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-      const int c = s * 32 + lane;
-      if (c < R) {
-        const size_t q = i * R + c;
-        aux[q] = x[s];
-        double v = x[s] - dual[q];
-        v = v > 0.0 ? v : 0.0;
-        init[q] = v;
-        primal[q] = v;
+      for (int m = 0; m < M; ++m) {
+        double a[SLOTS], z[SLOTS];
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+          const double xv = X[m][s];
+          if (PASS1) {
+            if (first && k == 0) {
+              const double dd = __dsub_rn(xv, X0[m][s]);
+              d_res = __fma_rn(dd, dd, d_res);
+            }
+            p_norm = __fma_rn(xv, xv, p_norm);
+          }
+          const double y = __dsub_rn(xv, Z[m][s]);
+          const double di = __dadd_rn(U[m][s], y);
+          U[m][s] = di;
+          if (PASS1) {
+            d_norm = __fma_rn(di, di, d_norm);
+            p_res = __fma_rn(y, y, p_res);
+          }
+          a[s] = __fma_rn(rho, __dadd_rn(xv, di), H[m][s]);
+        }
+        row_solve<SLOTS, SEG>(a, sw, R, lane, z);
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+          Z[m][s] = z[s];
+          const double v = __dsub_rn(z[s], U[m][s]);
+          X[m][s] = v < 0.0 ? 0.0 : v;
+        }
+      }
+      if (PASS1) {
+        double v4[4] = {p_res, d_res, p_norm, d_norm};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          for (int o = 16; o; o >>= 1) v4[q] += __shfl_xor_sync(0xffffffffu, v4[q], o);
+          if (lane == 0) wsum[warp][k * 4 + q] += v4[q];
+        }
+      }
+    }
+    if (!PASS1) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const uint64_t i = b0 + (uint64_t)m * KR + sub;
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+          const int c = s * 32 + col;
+          if (i < I && c < R) {
+            primal[i * R + c] = X[m][s];
+            aux[i * R + c] = Z[m][s];
+            dual[i * R + c] = U[m][s];
+          }
+        }
       }
     }
   }
-  // block partials of the four sums
-  __shared__ double sred[4][kAdmmThreads / 32];
-  double v4[4] = {p_res, d_res, p_norm, d_norm};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    double v = v4[k];
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) sred[k][warp] = v;
-  }
-  __syncthreads();
-  __shared__ bool last;
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < 4; ++k) {
-      double t = 0;
-      for (int w = 0; w < kAdmmThreads / 32; ++w) t += sred[k][w];
-      partials[(size_t)blockIdx.x * 4 + k] = t;
+  if (PASS1) {
+    __syncthreads();
+    for (int p = threadIdx.x; p < kAdmmSums; p += blockDim.x) {
+      double t = 0.0;
+      for (int w = 0; w < NW; ++w) t += wsum[w][p];
+      partials[(size_t)blockIdx.x * kAdmmSums + p] = t;
     }
-    __threadfence();
-    const unsigned ticket = atomicAdd(&state->ticket, 1u);
-    last = ticket == gridDim.x - 1;
+  }
+}
+
+// Start of an ADMM solve: clear the state, open the chunk loop.
+__global__ void admm_begin_kernel(AdmmState* __restrict__ state, cudaGraphConditionalHandle h, int in_graph) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    state->iters = 0;
+    state->stop = 0;
+    state->converged = 0;
+    state->chunk_start = 0;
+    state->chunk_sweeps = 0;
+    set_condition(h, in_graph, true);
+  }
+}
+
+// Adds the blocks' per-sweep partials in block order (one thread per sum,
+// blocks in order) and takes the chunk's sweep count: the first sweep whose
+// sums pass the test, else every sweep of the chunk.
+__global__ void admm_decide_kernel(const double* __restrict__ partials, int nblocks, double tol,
+                                   AdmmState* __restrict__ state, cudaGraphConditionalHandle h, int in_graph) {
+  __shared__ double S[kAdmmSums];
+  const bool idle = state->stop != 0;
+  for (int p = threadIdx.x; p < kAdmmSums && !idle; p += blockDim.x) {
+    double t = 0.0;
+    for (int b = 0; b < nblocks; ++b) t += partials[(size_t)b * kAdmmSums + p];
+    S[p] = t;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double t[4] = {0, 0, 0, 0};
-    for (unsigned b = 0; b < gridDim.x; ++b)
-      for (int k = 0; k < 4; ++k) t[k] += ((volatile double*)partials)[(size_t)b * 4 + k];
-    state->iters += 1;
-    state->ticket = 0;
-    if (t[0] <= tol * t[2] && t[1] <= tol * t[3]) state->converged = 1;
-    __threadfence();
+  if (threadIdx.x != 0) return;
+  if (idle) {
+    state->chunk_sweeps = 0;
+    set_condition(h, in_graph, false);
+    return;
   }
+  const int start = state->iters;
+  const int n = min(kAdmmChunk, kAdmmMaxIters - start);
+  int k = n, conv = 0;
+  for (int j = 0; j < n; ++j)
+    if (S[j * 4 + 0] <= tol * S[j * 4 + 2] && S[j * 4 + 1] <= tol * S[j * 4 + 3]) {
+      k = j + 1;
+      conv = 1;
+      break;
+    }
+  state->chunk_start = start;
+  state->chunk_sweeps = k;
+  state->iters = start + k;
+  state->converged = conv;
+  state->stop = conv || start + k >= kAdmmMaxIters;
+  set_condition(h, in_graph, !state->stop);
+}
+
+// End of an inner iteration (src/streaming_cpd.cpp:1457-1482): delta = sum
+// over the non-stream modes of ||U_j - prev_U_j|| / (||U_j|| + 1e-12) from
+// the per-mode statistics; stop once |prev_delta - delta| < epsilon after
+// the first iteration, when max_inner iterations are done, or when the
+// constrained solve's Cholesky failed.
+__global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, const int* __restrict__ status,
+                                int constrained, double eps, int max_inner, IterState* __restrict__ it,
+                                cudaGraphConditionalHandle h, int in_graph) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double delta = 0.0;
+  for (int j = 0; j < N; ++j)
+    if (j != t) delta += sqrt(dstat[3 * j + 1]) / (sqrt(dstat[3 * j + 2]) + 1e-12);
+  const int k = it->done;
+  bool stop = false;
+  if (constrained && status[0]) {
+    it->info = status[0];
+    stop = true;
+  } else if (k > 0 && fabs(it->prev_delta - delta) < eps) {
+    stop = true;
+  } else {
+    it->prev_delta = delta;
+  }
+  it->delta = delta;
+  it->done = k + 1;
+  if (stop) it->stop = 1;
+  set_condition(h, in_graph, !stop && k + 1 < max_inner);
+}
+
+// Head of the iteration graph: run the loop only if the batch goes on.
+__global__ void iter_begin_kernel(const IterState* __restrict__ it, int max_inner, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(h, (!it->stop && it->done < max_inner) ? 1u : 0u);
 }
 
 }  // namespace alto
@@ -209,11 +353,17 @@ struct alto_stream_session {
   uint64_t dims[ALTO_MAX_MODES] = {0};
   uint64_t cap[ALTO_MAX_MODES] = {0};
   DevBuf U[ALTO_MAX_MODES], P[ALTO_MAX_MODES], dual[ALTO_MAX_MODES];
-  DevBuf G, old_gram, ata, hist, W, status, rho, lam, dstat, buf32, rhs, aux, init, prim, time64;
-  DevBuf gscr, dscr, admm_part, admm_state, grow_stage, copy_tmp;
+  DevBuf G, old_gram, ata, hist, W, status, rho, lam, dstat, buf32, rhs, aux, prim, time64;
+  DevBuf gscr, dscr, admm_part, admm_state, grow_stage, copy_tmp, iter;
   std::vector<double> time_rows;  // concatenated time factor (host)
   alto_tensor* at = nullptr;
-  ~alto_stream_session() { delete at; }
+  bool use_graph = true;              // inner iterations 1.. as one graph per batch
+  cudaStream_t capst[2] = {nullptr, nullptr};  // capture-only streams (nothing runs on them)
+  ~alto_stream_session() {
+    delete at;
+    for (cudaStream_t c : capst)
+      if (c) cudaStreamDestroy(c);
+  }
 };
 
 namespace {
@@ -244,37 +394,210 @@ __global__ void fill_kernel(double* __restrict__ p, int n, double v) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) p[q] = v;
 }
 
-template <int SLOTS>
-alto_status admm_run(alto_stream_session* s, uint64_t I, double* primal, double* dual,
-                     cudaStream_t st) {
-  const int R = s->R;
-  const size_t smem = (size_t)R * R * sizeof(double);
-  uint64_t blocks = std::min<uint64_t>((I * 32 + kAdmmThreads - 1) / kAdmmThreads, 148ull * 8);
-  if (blocks < 1) blocks = 1;
-  ALTO_TRY(s->admm_part.ensure(blocks * 4 * sizeof(double)));
-  if (smem > 48 * 1024) {
-    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_first_kernel<SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_sweep_kernel<SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+// How an iteration is issued: directly, or captured into the batch graph
+// (then with the conditional handle of the inner loop).
+struct IterLaunch {
+  const void* fac[ALTO_MAX_MODES];
+  alto_mttkrp_variant mv;
+  int in_graph;
+  cudaGraphConditionalHandle outer;
+  cudaGraphConditionalHandle admm[ALTO_MAX_MODES];  // chunk loop of each constrained mode
+  cudaStream_t body_stream;                         // captures the chunk loop bodies
+};
+
+// In a stream being captured: append a while node on handle h after the
+// work captured so far, make later captured work depend on it, and return
+// its (empty) body graph.
+alto_status capture_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  ALTO_TRY_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &g, &deps, &nd));
+  if (cst != cudaStreamCaptureStatusActive) {
+    set_error("stream is not capturing");
+    return ALTO_ERR_CUDA;
   }
-  AdmmState* state = s->admm_state.as<AdmmState>();
-  admm_first_kernel<SLOTS><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(
-      s->rhs.as<double>(), primal, dual, s->aux.as<double>(), s->init.as<double>(),
-      s->W.as<double>(), s->rho.as<double>(), I, R, state);
-  ALTO_LAUNCHED();
-  const double tol = (double)1e-6f;
-  for (int k = 0; k < kAdmmMaxIters; ++k) {
-    admm_sweep_kernel<SLOTS><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(
-        s->rhs.as<double>(), primal, dual, s->aux.as<double>(), s->init.as<double>(),
-        s->W.as<double>(), s->rho.as<double>(), I, R, s->admm_part.as<double>(), state, tol);
-    ALTO_LAUNCHED();
-  }
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  ALTO_TRY_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  ALTO_TRY_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  *body = p.conditional.phGraph_out[0];
   return ALTO_OK;
 }
 
-alto_status admm(alto_stream_session* s, uint64_t I, double* primal, double* dual, cudaStream_t st) {
-  if (s->R <= 32) return admm_run<1>(s, I, primal, dual, st);
-  if (s->R <= 64) return admm_run<2>(s, I, primal, dual, st);
-  return admm_run<4>(s, I, primal, dual, st);
+template <int SLOTS, int SEG>
+alto_status admm_run(alto_stream_session* s, uint64_t I, double* primal, double* dual, cudaStream_t st,
+                     const IterLaunch& L, int mode) {
+  const int R = s->R;
+  const size_t smem = (size_t)R * R * sizeof(double);
+  constexpr uint64_t rows_per_block = (kAdmmThreads / 32) * RowMap<SEG>::kRows * AdmmBatch<SLOTS>::M;
+  uint64_t blocks = std::min<uint64_t>((I + rows_per_block - 1) / rows_per_block, 148ull * 4);
+  if (blocks < 1) blocks = 1;
+  ALTO_TRY(s->admm_part.ensure(blocks * kAdmmSums * sizeof(double)));
+  static size_t raised = 0;  // raised once per kernel, outside any capture
+  if (smem > 40 * 1024 && smem > raised) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_rows_kernel<SLOTS, SEG, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_rows_kernel<SLOTS, SEG, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raised = smem;
+  }
+  AdmmState* state = s->admm_state.as<AdmmState>();
+  double* part = s->admm_part.as<double>();
+  double* aux = s->aux.as<double>();
+  const double tol = (double)1e-6f;
+  const cudaGraphConditionalHandle h = L.in_graph ? L.admm[mode] : cudaGraphConditionalHandle{};
+  admm_begin_kernel<<<1, 32, 0, st>>>(state, h, L.in_graph);
+  ALTO_LAUNCHED();
+  auto chunk = [&](cudaStream_t cs) -> alto_status {
+    admm_rows_kernel<SLOTS, SEG, true><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
+        s->rhs.as<double>(), primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
+    ALTO_LAUNCHED();
+    admm_decide_kernel<<<1, 32, 0, cs>>>(part, (int)blocks, tol, state, h, L.in_graph);
+    ALTO_LAUNCHED();
+    admm_rows_kernel<SLOTS, SEG, false><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
+        s->rhs.as<double>(), primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
+    ALTO_LAUNCHED();
+    return ALTO_OK;
+  };
+  if (!L.in_graph) {
+    // every chunk issued; those after the stop return at once
+    for (int c = 0; c < (kAdmmMaxIters + kAdmmChunk - 1) / kAdmmChunk; ++c) ALTO_TRY(chunk(st));
+    return ALTO_OK;
+  }
+  // while (not stopped): one chunk
+  cudaGraph_t body;
+  ALTO_TRY(capture_while(st, h, &body));
+  ALTO_TRY_CUDA(cudaStreamBeginCaptureToGraph(L.body_stream, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+  const alto_status cst = chunk(L.body_stream);
+  cudaGraph_t done = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(L.body_stream, &done);
+  ALTO_TRY(cst);
+  ALTO_TRY_CUDA(ee);
+  return ALTO_OK;
+}
+
+alto_status admm(alto_stream_session* s, uint64_t I, double* primal, double* dual, cudaStream_t st,
+                 const IterLaunch& L, int mode) {
+  if (s->R <= 8) return admm_run<1, 8>(s, I, primal, dual, st, L, mode);
+  if (s->R <= 16) return admm_run<1, 16>(s, I, primal, dual, st, L, mode);
+  if (s->R <= 32) return admm_run<1, 32>(s, I, primal, dual, st, L, mode);
+  if (s->R <= 64) return admm_run<2, 32>(s, I, primal, dual, st, L, mode);
+  return admm_run<4, 32>(s, I, primal, dual, st, L, mode);
+}
+
+// One inner iteration of cpstream_alto_iter (src/streaming_cpd.cpp:1240-1482)
+// on stream st, ending with the convergence kernel.
+alto_status enqueue_iteration(alto_stream_session* s, const IterLaunch& L, cudaStream_t st) {
+  const int N = s->N, t = s->t, R = s->R;
+  const size_t RR = (size_t)R * R;
+  const unsigned all = (1u << N) - 1;
+  double* G = s->G.as<double>();
+  double* dstat = s->dstat.as<double>();  // [N][3]
+  // time rows: MTTKRP of the stream mode, solve with the other Grams
+  ALTO_TRY(run_mttkrp(s->at, t, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
+  ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidge, 1e-12, s->W.as<double>(),
+                       s->status.as<int>(), nullptr, st));
+  ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->dims[t], R,
+                            s->time64.as<double>(), st));
+  ALTO_TRY(convert_f64_to_f32(s->time64.as<double>(), s->dims[t] * R, s->U[t].as<float>(), st));
+  double* Gt = G + (size_t)t * RR;
+  ALTO_TRY(rr_op(s->old_gram.as<double>(), Gt, (int)RR, 0, 0.0, st));
+  ALTO_TRY(rank_update(Gt, s->time64.as<double>(), s->dims[t], R, st));
+
+  for (int j = 0; j < N; ++j) {
+    if (j == t) continue;
+    const uint64_t I = s->dims[j];
+    ALTO_TRY(run_mttkrp(s->at, j, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
+    // historical term
+    ALTO_TRY(rr_op(s->ata.as<double>(), s->old_gram.as<double>(), (int)RR, 0, 0.0, st));
+    for (int m = 0; m < N; ++m) {
+      if (m == j || m == t) continue;
+      ALTO_TRY(cross_gram(s->P[m].as<float>(), s->U[m].as<float>(), s->dims[m], R, s->hist.as<double>(),
+                          s->gscr, st));
+      ALTO_TRY(rr_op(s->ata.as<double>(), s->hist.as<double>(), (int)RR, 1, 0.0, st));
+    }
+    ALTO_TRY(apply_f32_to_f64(s->P[j].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), I, R,
+                              s->rhs.as<double>(), st));
+    if (s->con == ALTO_UNCONSTRAINED) {
+      ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveRidge, 1e-12, s->W.as<double>(),
+                           s->status.as<int>(), nullptr, st));
+      ALTO_TRY(apply_f64_to_f32(s->rhs.as<double>(), s->W.as<double>(), I, R, s->U[j].as<float>(), st));
+    } else {
+      ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveAdmm, 0.0, s->W.as<double>(), s->status.as<int>(),
+                           s->rho.as<double>(), st));
+      ALTO_TRY(convert_f32_to_f64(s->U[j].as<float>(), I * R, s->prim.as<double>(), st));
+      ALTO_TRY(admm(s, I, s->prim.as<double>(), s->dual[j].as<double>(), st, L, j));
+      ALTO_TRY(convert_f64_to_f32(s->prim.as<double>(), I * R, s->U[j].as<float>(), st));
+    }
+    ALTO_TRY(gram(s->U[j].as<float>(), I, R, G + (size_t)j * RR, s->gscr, st));
+    ALTO_TRY(dot_stats(s->P[j].as<float>(), s->U[j].as<float>(), I * R, nullptr, R, dstat + 3 * j, s->dscr, st));
+  }
+  converge_kernel<<<1, 32, 0, st>>>(dstat, N, t, s->status.as<int>(), s->con != ALTO_UNCONSTRAINED ? 1 : 0, s->eps,
+                                    s->max_inner, s->iter.as<IterState>(), L.outer, L.in_graph);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+// Inner iterations 1.. of the batch as one graph (see the file comment);
+// launched on the session stream, resources released after the launch is
+// queued (CUDA keeps an executable graph alive until its launches finish).
+alto_status run_graph(alto_stream_session* s, IterLaunch L) {
+  cudaStream_t cs = s->capst[0];
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  alto_status st = ALTO_OK;
+  auto end_open_captures = [&]() {
+    for (cudaStream_t c : s->capst) {
+      cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(c, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c, &junk);
+      }
+    }
+    cudaGetLastError();
+  };
+  do {
+    if ((st = cuda_status(cudaGraphCreate(&g, 0), "cudaGraphCreate", __FILE__, __LINE__))) break;
+    L.in_graph = 1;
+    L.body_stream = s->capst[1];
+    if ((st = cuda_status(cudaGraphConditionalHandleCreate(&L.outer, g, 0, 0), "conditional handle", __FILE__,
+                          __LINE__)))
+      break;
+    if (s->con != ALTO_UNCONSTRAINED)
+      for (int j = 0; j < s->N && st == ALTO_OK; ++j)
+        if (j != s->t)
+          st = cuda_status(cudaGraphConditionalHandleCreate(&L.admm[j], g, 0, 0), "conditional handle", __FILE__,
+                           __LINE__);
+    if (st) break;
+    if ((st = cuda_status(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                          "capture", __FILE__, __LINE__)))
+      break;
+    iter_begin_kernel<<<1, 32, 0, cs>>>(s->iter.as<IterState>(), s->max_inner, L.outer);
+    if ((st = cuda_status(cudaGetLastError(), "iter_begin_kernel", __FILE__, __LINE__))) break;
+    cudaGraph_t body = nullptr;
+    if ((st = capture_while(cs, L.outer, &body))) break;
+    cudaGraph_t tmp = nullptr;
+    if ((st = cuda_status(cudaStreamEndCapture(cs, &tmp), "end capture", __FILE__, __LINE__))) break;
+    if ((st = cuda_status(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                          "capture", __FILE__, __LINE__)))
+      break;
+    if ((st = enqueue_iteration(s, L, cs))) break;
+    if ((st = cuda_status(cudaStreamEndCapture(cs, &tmp), "end capture", __FILE__, __LINE__))) break;
+    if ((st = cuda_status(cudaGraphInstantiate(&exec, g, 0), "cudaGraphInstantiate", __FILE__, __LINE__))) break;
+    st = cuda_status(cudaGraphLaunch(exec, s->st), "cudaGraphLaunch", __FILE__, __LINE__);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  } while (false);
+  if (st) end_open_captures();
+  if (exec) cudaGraphExecDestroy(exec);
+  if (g) cudaGraphDestroy(g);
+  return st;
 }
 
 alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals,
@@ -316,8 +639,7 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   for (int n = 0; n < N; ++n) max_dim = std::max(max_dim, s->dims[n]);
   ALTO_TRY(s->buf32.ensure(max_dim * R * 4));
   ALTO_TRY(s->rhs.ensure(max_dim * R * 8));
-  ALTO_TRY(s->aux.ensure(max_dim * R * 8));
-  ALTO_TRY(s->init.ensure(max_dim * R * 8));
+  if (s->con != ALTO_UNCONSTRAINED) ALTO_TRY(s->aux.ensure(max_dim * R * 8));
   ALTO_TRY(s->prim.ensure(max_dim * R * 8));
   ALTO_TRY(s->time64.ensure(s->dims[t] * R * 8));
   double* G = s->G.as<double>();
@@ -359,76 +681,33 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     ALTO_LAUNCHED();
   }
 
-  const void* fac[ALTO_MAX_MODES];
-  for (int n = 0; n < N; ++n) fac[n] = s->U[n].p;
+  IterLaunch L{};
+  for (int n = 0; n < N; ++n) L.fac[n] = s->U[n].p;
   // the deterministic MTTKRP where it runs, so a stream's results repeat
   // bit for bit however many other streams share the device
-  const alto_mttkrp_variant mv =
-      deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
-  const unsigned all = (1u << N) - 1;
-  double* dstat = s->dstat.as<double>();  // [N][3]
-  double delta = 0.0, prev_delta = 0.0;
-  int it;
-  for (it = 0; it < s->max_inner; ++it) {
-    // time rows: MTTKRP of the stream mode, solve with the other Grams
-    ALTO_TRY(run_mttkrp(s->at, t, fac, ALTO_F32, R, s->buf32.as<float>(), 0, mv, st));
-    ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidge, 1e-12, s->W.as<double>(),
-                         s->status.as<int>(), nullptr, st));
-    ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->dims[t], R,
-                              s->time64.as<double>(), st));
-    ALTO_TRY(convert_f64_to_f32(s->time64.as<double>(), s->dims[t] * R, s->U[t].as<float>(), st));
-    double* Gt = G + (size_t)t * RR;
-    ALTO_TRY(rr_op(s->old_gram.as<double>(), Gt, (int)RR, 0, 0.0, st));
-    ALTO_TRY(rank_update(Gt, s->time64.as<double>(), s->dims[t], R, st));
-
-    for (int j = 0; j < N; ++j) {
-      if (j == t) continue;
-      const uint64_t I = s->dims[j];
-      ALTO_TRY(run_mttkrp(s->at, j, fac, ALTO_F32, R, s->buf32.as<float>(), 0, mv, st));
-      // historical term
-      ALTO_TRY(rr_op(s->ata.as<double>(), s->old_gram.as<double>(), (int)RR, 0, 0.0, st));
-      for (int m = 0; m < N; ++m) {
-        if (m == j || m == t) continue;
-        ALTO_TRY(cross_gram(s->P[m].as<float>(), s->U[m].as<float>(), s->dims[m], R,
-                            s->hist.as<double>(), s->gscr, st));
-        ALTO_TRY(rr_op(s->ata.as<double>(), s->hist.as<double>(), (int)RR, 1, 0.0, st));
-      }
-      ALTO_TRY(apply_f32_to_f64(s->P[j].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), I, R,
-                                s->rhs.as<double>(), st));
-      if (s->con == ALTO_UNCONSTRAINED) {
-        ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveRidge, 1e-12, s->W.as<double>(),
-                             s->status.as<int>(), nullptr, st));
-        ALTO_TRY(apply_f64_to_f32(s->rhs.as<double>(), s->W.as<double>(), I, R, s->U[j].as<float>(), st));
-      } else {
-        ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveAdmm, 0.0, s->W.as<double>(),
-                             s->status.as<int>(), s->rho.as<double>(), st));
-        ALTO_TRY(convert_f32_to_f64(s->U[j].as<float>(), I * R, s->prim.as<double>(), st));
-        ALTO_TRY(admm(s, I, s->prim.as<double>(), s->dual[j].as<double>(), st));
-        ALTO_TRY(convert_f64_to_f32(s->prim.as<double>(), I * R, s->U[j].as<float>(), st));
-      }
-      ALTO_TRY(gram(s->U[j].as<float>(), I, R, G + (size_t)j * RR, s->gscr, st));
-      ALTO_TRY(dot_stats(s->P[j].as<float>(), s->U[j].as<float>(), I * R, nullptr, R, dstat + 3 * j,
-                         s->dscr, st));
-    }
-    double h[3 * ALTO_MAX_MODES];
-    ALTO_TRY_CUDA(cudaMemcpyAsync(h, dstat, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
-    int info = 0;
-    ALTO_TRY_CUDA(cudaMemcpyAsync(&info, s->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
+  ALTO_TRY(s->iter.ensure(sizeof(IterState)));
+  ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
+  IterState hs{};
+  // iteration 0 directly: sizes every buffer and builds the sorted lines
+  ALTO_TRY(enqueue_iteration(s, L, st));
+  if (s->use_graph && s->max_inner > 1) {
+    ALTO_TRY(run_graph(s, L));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-    if (info && s->con != ALTO_UNCONSTRAINED) {
-      set_error("Cholesky of the ADMM normal equations failed (info %d)", info);
-      return ALTO_ERR_NOT_SPD;
+  } else {
+    while (true) {
+      ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+      if (hs.stop || hs.done >= s->max_inner) break;
+      ALTO_TRY(enqueue_iteration(s, L, st));
     }
-    delta = 0.0;
-    for (int j = 0; j < N; ++j)
-      if (j != t) delta += std::sqrt(h[3 * j + 1]) / (std::sqrt(h[3 * j + 2]) + 1e-12);
-    if (it > 0 && std::fabs(prev_delta - delta) < s->eps) {
-      ++it;
-      break;
-    }
-    prev_delta = delta;
   }
-  if (inner_out) *inner_out = it;
+  if (hs.info) {
+    set_error("Cholesky of the ADMM normal equations failed (info %d)", hs.info);
+    return ALTO_ERR_NOT_SPD;
+  }
+  if (inner_out) *inner_out = hs.done;
   // forgetting, prev <- current, time rows out
   ALTO_TRY(rr_op(G + (size_t)t * RR, nullptr, (int)RR, 2, s->forgetting, st));
   for (int n = 0; n < N; ++n)
@@ -499,9 +778,11 @@ alto_status alto_stream_open(int nmodes, int stream_mode, int rank, alto_constra
     return st;
   }
   if (cudaMemsetAsync(s->G.p, 0, nmodes * RR * 8, s->st) != cudaSuccess ||
-      cudaMemsetAsync(s->dstat.p, 0, 3 * ALTO_MAX_MODES * 8, s->st) != cudaSuccess) {
+      cudaMemsetAsync(s->dstat.p, 0, 3 * ALTO_MAX_MODES * 8, s->st) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->capst[0], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->capst[1], cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
-    set_error("cudaMemsetAsync failed");
+    set_error("session set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
     return ALTO_ERR_CUDA;
   }
   *out = s;
@@ -557,6 +838,15 @@ alto_status alto_stream_lambda(alto_stream_session* s, double* host_out) {
   }
   ALTO_TRY_CUDA(cudaMemcpyAsync(host_out, s->lam.p, s->R * 8, cudaMemcpyDeviceToHost, s->st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(s->st));
+  return ALTO_OK;
+}
+
+alto_status alto_stream_set_graph(alto_stream_session* s, int enable) {
+  if (!s) {
+    set_error("session is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  s->use_graph = enable != 0;
   return ALTO_OK;
 }
 

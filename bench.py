@@ -27,6 +27,25 @@ number of this library's kernel launches in the timed region.
 `--impl reference` times the reference's own OpenMP MTTKRP (oracle/_ref) on
 the host cores instead, on the bounded sample, and prints the same line
 with "impl": "reference".
+
+Two more workloads print their own line:
+
+  --workload cpstream   CP-stream over a 4-mode stream: 200 time slices of
+                        100,000 x 100,000 x 10,000, per-slice nonzero draws
+                        log-normal (median 2e5, sigma 1) clipped to
+                        [5e4, 2e6], Zipf(1.1) coordinates, Poisson(3) values
+                        (zero draws dropped), rank 16, non-negative ADMM,
+                        forgetting 0.95, at most 50 inner iterations, epsilon
+                        1e-5.  A step is one slice update through the session
+                        API (host COO in); metric slices/s, with p50/p99
+                        slice latency.
+  --workload serve      64 independent streams (spatial dims log-uniform in
+                        [1e3, 1e6], rank 8/16/32, non-negative or
+                        unconstrained), slices of log-normal size in
+                        [1e4, 1e6] arriving as a Poisson process at 2,000
+                        slices/s, served under an 80 GB HBM budget; metric
+                        slices/s with p50/p99 latency, against the plain path
+                        (one slice at a time, each stream's session in turn).
 """
 from __future__ import annotations
 
@@ -57,8 +76,15 @@ WORKLOAD = "powerlaw3d-4.8Mx1.8Mx1.8M-140Mnnz-zipf1.2-R32-allmode"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve"], default="mttkrp")
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (mttkrp: all-mode MTTKRPs, default 10; cpstream: slices, default 197; "
+                         "serve: slices per stream, default 7)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="untimed steps before (mttkrp 3; cpstream 3 slices; serve 1 slice per stream)")
+    ap.add_argument("--workers", type=int, default=16, help="serve: server worker threads")
+    ap.add_argument("--streams", type=int, default=64, help="serve: independent streams")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: aggregate Poisson arrival rate (slices/s)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nnz", type=int, default=NNZ)
     ap.add_argument("--rank", type=int, default=RANK)
@@ -70,7 +96,13 @@ def parse():
                     help="factor storage (bf16 halves gather bytes; accumulation stays f32)")
     ap.add_argument("--profile-small", action="store_true",
                     help="small tensor (for ncu captures): 20M nonzeros, 1 step")
-    return ap.parse_args()
+    args = ap.parse_args()
+    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1)}[args.workload]
+    if args.steps is None:
+        args.steps = defaults[0]
+    if args.warmup is None:
+        args.warmup = defaults[1]
+    return args
 
 
 def dist_env():
@@ -280,10 +312,12 @@ def ours(args):
     launches0 = A.kernel_launches()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
     t0.record(stream)
     for k in range(steps):
         step(events[k])
     t1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = A.kernel_launches() - launches0
     if world > 1:
@@ -377,8 +411,359 @@ def ours(args):
     return 0
 
 
+# ----------------------------------------------------------------- CP-stream
+
+C4_SPACE = [100000, 100000, 10000]
+C4_RANK = 16
+C4_SEED = 7
+CPSTREAM_METRIC = "CP-stream slices/s (rank 16, non-negative ADMM)"
+CPSTREAM_WORKLOAD = "cpstream4d-200slices-100Kx100Kx10K-zipf1.1-poisson3-R16-nonneg-f0.95-m50-e1e-5"
+
+
+def c4_batches(n):
+    """The first n slices of the CP-stream workload (host COO)."""
+    import numpy as np
+
+    from alto_b200 import synth
+
+    return synth.stream_batches(
+        C4_SPACE, n, lambda rng, s: int(np.clip(rng.lognormal(np.log(2e5), 1.0), 5e4, 2e6)),
+        [1.1, 1.1, 1.1], seed=C4_SEED, values="poisson3")
+
+
+def stream_need(batches, R):
+    """Initial values consumed per batch (new rows x rank, mode order)."""
+    import numpy as np
+
+    prev = np.zeros(len(batches[0]["dims"]), np.int64)
+    out = []
+    for b in batches:
+        d = b["dims"].astype(np.int64)
+        out.append(int(np.sum(np.maximum(d - prev, 0))) * R)
+        prev = np.maximum(prev, d)
+    return out
+
+
+def cpstream_bytes(b, R, inner):
+    """Algorithmic HBM bytes of one slice update: per inner iteration the
+    line once per mode (key + value) and, per non-stream mode, the factor,
+    previous factor and solve buffer read plus buffer and factor written."""
+    N = len(b["dims"])
+    nnz = len(b["vals"])
+    return inner * (N * nnz * 12 + sum(int(d) * R * 4 * 5 for m, d in enumerate(b["dims"]) if m != 0))
+
+
+class stdout_to_stderr:
+    """Sends what native code prints to file descriptor 1 (the reference's
+    per-slice tables) to stderr, so stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        import ctypes
+
+        ctypes.CDLL(None).fflush(None)  # C stdio buffers still hold the native prints
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def ref_cpstream_rate(batches, R, iv):
+    """Slices/s of the reference's cpstream (oracle/_ref, all host threads)."""
+    import oracle as O
+
+    L = O.ref_lib(64)
+    threads = os.cpu_count() or 1
+    L.ref_set_threads(threads)
+    with stdout_to_stderr():
+        _, _, secs = O.ref_cpstream(batches, 0, R, 50, 1e-5, 1, iv, bits=64)
+    return len(batches) / float(secs.sum()), threads, [round(float(x) * 1e3, 1) for x in secs]
+
+
+def ours_cpstream(args):
+    import numpy as np
+    import torch
+
+    import alto_b200 as A
+    from alto_b200 import synth
+
+    torch.cuda.set_device(0)
+    W, K = args.warmup, args.steps
+    batches = c4_batches(W + K)
+    R = C4_RANK
+    need = stream_need(batches, R)
+    iv = synth.init_values(sum(need) + 64, seed=1)
+    s = A.CPStream(4, 0, R, constraint=A.NONNEG, forgetting=0.95, max_inner=50, epsilon=1e-5)
+    used = 0
+    lat, inner, dev_ms, nbytes, h2d = [], [], [], 0, 0
+    stream = torch.cuda.current_stream()
+    sampler = None
+    launches0 = 0
+    for k, b in enumerate(batches):
+        if k == W:
+            torch.cuda.synchronize()
+            sampler = ClockSampler(0)
+            sampler.start()
+            time.sleep(0.3)
+            launches0 = A.kernel_launches()
+            t_start = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ts = time.perf_counter()
+        it = s.push(b["dims"], b["cidx"], b["vals"], iv[used:used + need[k]])
+        te = time.perf_counter() - ts
+        e1.record(stream)
+        used += need[k]
+        if k >= W:
+            e1.synchronize()
+            lat.append(te * 1e3)
+            dev_ms.append(e0.elapsed_time(e1))
+            inner.append(it)
+            nbytes += cpstream_bytes(b, R, it)
+            h2d += b["cidx"].nbytes + b["vals"].nbytes + need[k] * 8
+    t_total = time.perf_counter() - t_start
+    launches = A.kernel_launches() - launches0
+    clocks = sampler.stop()
+    s.close()
+    dev_total = sum(dev_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            nb = 6
+            rate, threads, secs = ref_cpstream_rate(batches[:nb], R, iv)
+            cpu = {"value": rate, "unit": "slices/s", "cores": threads, "kind": "reference",
+                   "sample": f"first {nb} slices of the same stream through the reference's cpstream "
+                             f"(its forgetting factor is fixed at 0.99); per-slice ms {secs}"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "slices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+    line = {
+        "metric": CPSTREAM_METRIC, "value": K / dev_total, "unit": "slices/s", "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": dev_total / K * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": CPSTREAM_WORKLOAD, "space_dims": C4_SPACE, "rank": R, "constraint": "nonneg",
+                   "forgetting": 0.95, "max_inner": 50, "epsilon": 1e-5,
+                   "slice_nnz_mean": float(np.mean([len(b["vals"]) for b in batches[W:]])),
+                   "inner_iters_mean": float(np.mean(inner)), "inner_iters_max": int(np.max(inner)),
+                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                   "launch": "first inner iteration direct, the rest one CUDA graph per slice",
+                   "l2": "per-slice work streams the slice and the factors (> L2 in total over a slice); no flush"},
+        "roofline": {"bound": "hbm", "achieved": nbytes / dev_total / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": nbytes / dev_total / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "note": "algorithmic bytes per inner iteration: N*nnz*12 + sum_j I_j*R*4*5"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": K / t_total, "unit": "slices/s", "h2d_bytes_per_step": h2d // K,
+                "d2h_bytes_per_step": R * 8, "api": "alto_stream_push (host COO batch in, time row out)"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------- serving
+
+SERVE_METRIC = "CP-stream serving slices/s (64 streams, Poisson 2000 slices/s)"
+SERVE_WORKLOAD = "serve-64streams-dims1e3..1e6-R8/16/32-nnz1e4..1e6-poisson2000-budget80GB"
+SERVE_SEED = 11
+
+
+def serve_setup(args):
+    import numpy as np
+
+    from alto_b200 import synth
+
+    streams = synth.serving_streams(args.streams, args.warmup + args.steps, seed=SERVE_SEED)
+    rng = np.random.default_rng(SERVE_SEED + 1)
+    need = [sum(st["dims"][1:]) * st["rank"] for st in streams]
+    pool = rng.uniform(0.0, 3.0, max(need) + 1024) * np.where(rng.random(max(need) + 1024) < 0.5, -1.0, 1.0)
+    offs = [int(rng.integers(0, len(pool) - n)) for n in need]
+    # arrival order of the timed slices: a random interleaving that keeps each
+    # stream's slices in order, at exponential gaps
+    order = np.repeat(np.arange(len(streams)), args.steps)
+    rng.shuffle(order)
+    gaps = rng.exponential(1.0 / args.rate, len(order))
+    return streams, pool, offs, need, order, np.cumsum(gaps)
+
+
+def ours_serve(args):
+    import numpy as np
+    import torch
+
+    import alto_b200 as A
+
+    torch.cuda.set_device(0)
+    streams, pool, offs, need, order, arrive = serve_setup(args)
+    W, K = args.warmup, args.steps
+    cons = {0: A.UNCONSTRAINED, 1: A.NONNEG}
+
+    def init_for(k, j):  # initial values with the first slice only
+        return pool[offs[k]:offs[k] + need[k]] if j == 0 else None
+
+    # plain path: one session per stream, one slice at a time, arrival order
+    sess = [A.CPStream(4, 0, st["rank"], constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10,
+                       epsilon=1e-5) for st in streams]
+    for j in range(W):
+        for k, st in enumerate(streams):
+            b = st["slices"][j]
+            sess[k].push(b["dims"], b["cidx"], b["vals"], init_for(k, j))
+    torch.cuda.synchronize()
+    nxt = [W] * len(streams)
+    iso = []
+    t0 = time.perf_counter()
+    for k in order:
+        b = streams[k]["slices"][nxt[k]]
+        ts = time.perf_counter()
+        sess[k].push(b["dims"], b["cidx"], b["vals"])
+        iso.append((time.perf_counter() - ts) * 1e3)
+        nxt[k] += 1
+    plain_s = time.perf_counter() - t0
+    check = list(range(min(8, len(streams))))
+    plain_out = {k: [sess[k].factor(m, int(streams[k]["dims"][m]) + 1) for m in (1, 2, 3)] for k in check}
+    for x in sess:
+        x.close()
+    del sess
+    torch.cuda.synchronize()
+
+    # server: warm-up slices, then the timed slices at their arrival times
+    srv = A.Server(80 << 30, workers=args.workers)
+    sids = [srv.open(4, 0, st["rank"], st["dims"], max(len(b["vals"]) for b in st["slices"]),
+                     constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10, epsilon=1e-5)
+            for st in streams]
+    for j in range(W):
+        for k, st in enumerate(streams):
+            b = st["slices"][j]
+            srv.submit(sids[k], b["dims"], b["cidx"], b["vals"], init_for(k, j))
+    srv.drain()
+    st0 = srv.stats()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = A.kernel_launches()
+    nxt = [W] * len(streams)
+    tickets = []
+    h2d = 0
+    t0 = time.perf_counter()
+    for k, ta in zip(order, arrive):
+        while time.perf_counter() - t0 < ta:
+            pass
+        b = streams[k]["slices"][nxt[k]]
+        tickets.append(srv.submit(sids[k], b["dims"], b["cidx"], b["vals"]))
+        h2d += b["cidx"].nbytes + b["vals"].nbytes
+        nxt[k] += 1
+    srv.drain()
+    served_s = time.perf_counter() - t0
+    launches = A.kernel_launches() - launches0
+    clocks = sampler.stop()
+    lat = [srv.wait(t)[1] for t in tickets]
+    st1 = srv.stats()
+    same = all(np.array_equal(srv.factor(sids[k], m), plain_out[k][i]) for k in check
+               for i, m in enumerate((1, 2, 3)))
+    srv.destroy()
+
+    n = len(order)
+    value = n / served_s
+    plain_rate = n / plain_s
+    p99_iso = float(np.percentile(iso, 99))
+    line = {
+        "metric": SERVE_METRIC, "value": value, "unit": "slices/s", "n_gpus": 1, "steps": n, "warmup": W * len(streams),
+        "ms_per_step": served_s / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "streams": len(streams), "slices_per_stream": W + K,
+                   "workers": args.workers, "arrival_rate": args.rate, "hbm_budget_bytes": 80 << 30,
+                   "max_inner": 10, "epsilon": 1e-5,
+                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                   "plain_slices_per_s": plain_rate, "speedup_vs_plain": value / plain_rate,
+                   "isolated_p50_ms": float(np.percentile(iso, 50)), "isolated_p99_ms": p99_iso,
+                   "p99_vs_isolated_p99": float(np.percentile(lat, 99)) / p99_iso,
+                   "results_identical_to_plain": bool(same), "checked_streams": len(check),
+                   "reserved_bytes": st1["reserved_bytes"], "admitted_streams": st1["admitted_streams"],
+                   "warmup_completed": st0["completed"],
+                   "timing": "host clock from the first timed arrival to the drained server",
+                   "l2": "per-slice data and factors exceed L2 across streams; no flush"},
+        "roofline": None,
+        "cpu_baseline": None,
+        "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": h2d // n, "d2h_bytes_per_step": 0,
+                "api": "alto_server_submit / alto_server_drain (host COO batches)"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = serve_reference_sample(streams, pool, offs, need)
+    print(json.dumps(line))
+    return 0
+
+
+def serve_reference_sample(streams, pool, offs, need, nstreams=6, nslices=3):
+    """The reference's cpstream run stream after stream (its plain path) on a
+    bounded sample: the first nslices slices of the first nstreams streams."""
+    import oracle as O
+
+    try:
+        L = O.ref_lib(64)
+        threads = os.cpu_count() or 1
+        L.ref_set_threads(threads)
+        total, count = 0.0, 0
+        for k in range(min(nstreams, len(streams))):
+            st = streams[k]
+            iv = pool[offs[k]:offs[k] + need[k]]
+            with stdout_to_stderr():
+                _, _, secs = O.ref_cpstream(st["slices"][:nslices], 0, st["rank"], 10, 1e-5, st["constraint"], iv,
+                                            bits=64)
+            total += float(secs.sum())
+            count += nslices
+        return {"value": count / total, "unit": "slices/s", "cores": threads, "kind": "reference",
+                "sample": f"first {nslices} slices of the first {nstreams} streams, one stream after another"}
+    except Exception as e:
+        return {"value": None, "unit": "slices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+
+def reference_stream_arm(args):
+    """--impl reference for the cpstream and serve workloads."""
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
+    try:
+        if args.workload == "cpstream":
+            from alto_b200 import synth
+
+            nb = 6
+            batches = c4_batches(nb)
+            iv = synth.init_values(sum(stream_need(batches, C4_RANK)) + 64, seed=1)
+            rate, threads, secs = ref_cpstream_rate(batches, C4_RANK, iv)
+            metric, unit, workload = CPSTREAM_METRIC, "slices/s", CPSTREAM_WORKLOAD
+            sample = f"first {nb} slices; per-slice ms {secs}"
+        else:
+            steps = args.steps
+            args.steps = 2  # only the sample's slices are generated
+            streams, pool, offs, need, _, _ = serve_setup(args)
+            args.steps = steps
+            cb = serve_reference_sample(streams, pool, offs, need)
+            if cb["value"] is None:
+                raise RuntimeError(cb["sample"])
+            rate, threads, sample = cb["value"], cb["cores"], cb["sample"]
+            metric, unit, workload = SERVE_METRIC, "slices/s", SERVE_WORKLOAD
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
+        return 0
+    print(json.dumps({
+        "impl": "reference", "metric": metric, "value": rate, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": workload},
+        "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload != "mttkrp":
+        if args.impl == "reference":
+            return reference_stream_arm(args)
+        return ours_cpstream(args) if args.workload == "cpstream" else ours_serve(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours(args)

@@ -236,6 +236,15 @@ alto_status alto_stream_push(alto_stream_session* s, const alto_coo* batch,
 alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_out,
                                uint64_t* rows);
 alto_status alto_stream_lambda(alto_stream_session* s, double* host_out);
+
+/* How alto_stream_push issues a batch's inner iterations (the reference's
+ * loop, src/streaming_cpd.cpp:1240-1482).  enable = 1 (the default): the
+ * first directly, the rest as one CUDA graph per batch whose while nodes
+ * run the inner loop and the ADMM sweeps, with the stopping tests on the
+ * device.  enable = 0: every launch directly, one host synchronisation per
+ * inner iteration.  Both issue the same kernels in the same order and give
+ * identical results. */
+alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
 alto_status alto_stream_close(alto_stream_session* s);
 
 /* -------------------------------------------------------------- serving */

@@ -12,10 +12,11 @@ from conftest import load_stream_fixture
 pytestmark = pytest.mark.gpu
 
 
-def run_gpu(batches, R, max_iters, eps, nonneg, iv, forgetting=0.99):
+def run_gpu(batches, R, max_iters, eps, nonneg, iv, forgetting=0.99, graph=True):
     N = len(batches[0]["dims"])
     s = A.CPStream(N, 0, R, constraint=A.NONNEG if nonneg else A.UNCONSTRAINED, forgetting=forgetting,
                    max_inner=max_iters, epsilon=eps)
+    s.set_graph(graph)
     used = 0
     prev = np.zeros(N, np.int64)
     inner = []
@@ -73,4 +74,17 @@ def test_stream_repeats_bit_for_bit():
     o2, l2, i2 = run_gpu(b, 8, 10, 1e-5, 1, iv, forgetting=0.95)
     assert i1 == i2 and np.array_equal(l1, l2)
     for a, c in zip(o1, o2):
+        assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("nonneg", [0, 1])
+def test_graph_and_direct_launches_agree(nonneg):
+    """The batch graph (device-side inner loop and ADMM sweep loop) and the
+    directly launched loop give identical factors and iteration counts."""
+    b = load_stream_fixture()[:4]
+    iv = synth.init_values(20000, seed=4)
+    og, lg, ig = run_gpu(b, 16, 10, 1e-5, nonneg, iv, forgetting=0.95, graph=True)
+    od, ld, id_ = run_gpu(b, 16, 10, 1e-5, nonneg, iv, forgetting=0.95, graph=False)
+    assert ig == id_ and np.array_equal(lg, ld)
+    for a, c in zip(og, od):
         assert np.array_equal(a, c)
