@@ -153,6 +153,149 @@ static alto_status gram_launch(const TA* A, const TB* B, uint64_t I, int R, doub
   return ALTO_OK;
 }
 
+// One pass over P and U (float32, I x R): per-block partials of U^T U,
+// P^T U and {sum p u, sum (p - u)^2, sum u^2} (the CP-stream Gram, cross
+// Gram and change statistics of a freshly updated factor), layout
+// [block][2 R^2 + 3].
+template <int PPT>
+__global__ void __launch_bounds__(kGramThreads)
+    gram_cross_partial_kernel(const float* __restrict__ P, const float* __restrict__ U, uint64_t I, int R,
+                              uint64_t rows_per_block, double* __restrict__ partials) {
+  extern __shared__ double sm[];
+  double* sp = sm;
+  double* su = sm + kGramRows * R;
+  double g[PPT], c[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) g[k] = c[k] = 0.0;
+  double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+  const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_block;
+  const uint64_t r1 = min(r0 + rows_per_block, I);
+  const int RR = R * R;
+  for (uint64_t t0 = r0; t0 < r1; t0 += kGramRows) {
+    const int nr = (int)min((uint64_t)kGramRows, r1 - t0);
+    for (int q = threadIdx.x; q < nr * R; q += kGramThreads) {
+      const double pv = (double)P[t0 * R + q], uv = (double)U[t0 * R + q];
+      sp[q] = pv;
+      su[q] = uv;
+      q0 += pv * uv;
+      q1 += (pv - uv) * (pv - uv);
+      q2 += uv * uv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int p = threadIdx.x + k * kGramThreads;
+      if (p < RR) {
+        const int a = p / R, b = p % R;
+        double sg = 0.0, sc = 0.0;
+        for (int r = 0; r < nr; ++r) {
+          const double ub = su[r * R + b];
+          sg += su[r * R + a] * ub;
+          sc += sp[r * R + a] * ub;
+        }
+        g[k] += sg;
+        c[k] += sc;
+      }
+    }
+    __syncthreads();
+  }
+  double* out = partials + (size_t)blockIdx.x * (2 * RR + 3);
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    const int p = threadIdx.x + k * kGramThreads;
+    if (p < RR) {
+      out[p] = g[k];
+      out[RR + p] = c[k];
+    }
+  }
+  // the three statistics: warp butterflies, then warps in order
+  __shared__ double wq[3][kGramThreads / 32];
+  for (int o = 16; o; o >>= 1) {
+    q0 += __shfl_xor_sync(0xffffffffu, q0, o);
+    q1 += __shfl_xor_sync(0xffffffffu, q1, o);
+    q2 += __shfl_xor_sync(0xffffffffu, q2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    wq[0][threadIdx.x >> 5] = q0;
+    wq[1][threadIdx.x >> 5] = q1;
+    wq[2][threadIdx.x >> 5] = q2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int w = 0; w < kGramThreads / 32; ++w) t += wq[threadIdx.x][w];
+    out[2 * RR + threadIdx.x] = t;
+  }
+}
+
+// reduce_partials_kernel with the result split over three outputs:
+// [0, n1) -> o1, [n1, 2 n1) -> o2, the rest -> o3.
+__global__ void __launch_bounds__(kReduceThreads)
+    reduce_split_kernel(const double* __restrict__ partials, int nblocks, int n1, int n, double* __restrict__ o1,
+                        double* __restrict__ o2, double* __restrict__ o3) {
+  __shared__ double s[kReduceThreads / 32][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * 32 + lane;
+  double acc = 0.0;
+  if (p < n)
+    for (int b = w; b < nblocks; b += kReduceThreads / 32) acc += partials[(size_t)b * n + p];
+  s[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && p < n) {
+    double t = s[0][lane];
+    for (int k = 1; k < kReduceThreads / 32; ++k) t += s[k][lane];
+    if (p < n1)
+      o1[p] = t;
+    else if (p < 2 * n1)
+      o2[p - n1] = t;
+    else if (o3)
+      o3[p - 2 * n1] = t;
+  }
+}
+
+alto_status gram_cross_stats(const float* P, const float* U, uint64_t I, int R, double* G, double* C,
+                             double* stats3, DevBuf& scratch, cudaStream_t st) {
+  const int RR = R * R;
+  const int n = 2 * RR + 3;
+  const int ppt = (RR + kGramThreads - 1) / kGramThreads;
+  // at least 64 rows per block, at most 4 blocks per SM
+  uint64_t nb = std::min<uint64_t>((I + 63) / 64, (uint64_t)sms() * 4);
+  if (nb < 1) nb = 1;
+  const uint64_t rpb = (I + nb - 1) / nb;
+  nb = I ? (I + rpb - 1) / rpb : 1;
+  ALTO_TRY(scratch.ensure(nb * n * sizeof(double)));
+  double* part = scratch.as<double>();
+  const size_t smem = 2 * kGramRows * R * sizeof(double);
+  if (I == 0) {
+    ALTO_TRY_CUDA(cudaMemsetAsync(part, 0, n * sizeof(double), st));
+    nb = 1;
+  } else {
+#define GC_CASE(PP)                                                                                  \
+  case PP: {                                                                                         \
+    static size_t raised = 0;                                                                        \
+    if (smem > 48 * 1024 && smem > raised) {                                                         \
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(gram_cross_partial_kernel<PP>,                             \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
+      raised = smem;                                                                                 \
+    }                                                                                                \
+    gram_cross_partial_kernel<PP><<<(unsigned)nb, kGramThreads, smem, st>>>(P, U, I, R, rpb, part); \
+    break;                                                                                           \
+  }
+    switch (ppt <= 1 ? 1 : ppt <= 2 ? 2 : ppt <= 4 ? 4 : ppt <= 16 ? 16 : 64) {
+      GC_CASE(1)
+      GC_CASE(2)
+      GC_CASE(4)
+      GC_CASE(16)
+      GC_CASE(64)
+    }
+#undef GC_CASE
+    ALTO_LAUNCHED();
+  }
+  reduce_split_kernel<<<reduce_grid(n), kReduceThreads, 0, st>>>(part, (int)nb, RR, n, G, C, stats3);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
 alto_status gram(const float* A, uint64_t I, int R, double* out, DevBuf& scratch, cudaStream_t st) {
   return gram_launch<float, float>(A, A, I, R, out, scratch, st);
 }
@@ -272,8 +415,128 @@ __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes,
   }
 }
 
+// The same set-up for R <= RMAX <= 32 in one warp: solve_setup_kernel's
+// steps and operation order (so identical results), with the loops bounded
+// by RMAX and unrolled so the dot products' shared-memory loads overlap.
+template <int RMAX>
+__global__ void __launch_bounds__(32)
+    solve_setup_small_kernel(const double* __restrict__ grams, int nmodes, unsigned mask, int R, int kind,
+                             double ridge, double* __restrict__ W, int* __restrict__ status,
+                             double* __restrict__ rho_out) {
+  __shared__ double A[RMAX * RMAX];
+  __shared__ double s_rho;
+  __shared__ int s_info;
+  const int RR = R * R;
+  const int tid = threadIdx.x;
+  for (int p = tid; p < RR; p += 32) {
+    double v = 1.0;
+    for (int m = 0; m < nmodes; ++m)
+      if (mask & (1u << m)) v *= grams[(size_t)m * RR + p];
+    A[p] = v;
+  }
+  __syncwarp();
+  if (tid == 0) {
+    double add = ridge;
+    if (kind == kSolveAdmm) {
+      double tr = 0.0;
+      for (int r = 0; r < R; ++r) tr += A[r * R + r];
+      add = tr / (double)R;
+    }
+    s_rho = add;
+    s_info = 0;
+  }
+  __syncwarp();
+  if (kind == kSolveRidgeDiagFallback && tid < R) W[tid * R + tid] = A[tid * R + tid];
+  if (tid < R) A[tid * R + tid] += s_rho;
+  __syncwarp();
+  for (int j = 0; j < R; ++j) {
+    if (tid == 0) {
+      double d = A[j * R + j];
+#pragma unroll
+      for (int k = 0; k < RMAX; ++k)
+        if (k < j) d -= A[j * R + k] * A[j * R + k];
+      if (!(d > 0.0)) {
+        if (!s_info) s_info = j + 1;
+        d = 1.0;
+      }
+      A[j * R + j] = sqrt(d);
+    }
+    __syncwarp();
+    const double djj = A[j * R + j];
+    const int i = j + 1 + tid;
+    if (i < R) {
+      double sv = A[j * R + i];
+#pragma unroll
+      for (int k = 0; k < RMAX; ++k)
+        if (k < j) sv -= A[i * R + k] * A[j * R + k];
+      A[i * R + j] = sv / djj;
+    }
+    __syncwarp();
+  }
+  const int info = s_info;
+  if (info) {
+    for (int p = tid; p < RR; p += 32) {
+      const int a = p / R, b = p % R;
+      if (kind == kSolveRidgeDiagFallback) {
+        if (a != b) W[p] = 0.0;
+      } else {
+        W[p] = 0.0;
+      }
+    }
+    __syncwarp();
+    if (kind == kSolveRidgeDiagFallback && tid < R) {
+      const double d = W[tid * R + tid];
+      W[tid * R + tid] = d != 0.0 ? 1.0 / d : 0.0;
+    }
+  } else {
+    if (tid < R) {
+      const int c = tid;
+      double x[RMAX];
+#pragma unroll
+      for (int i = 0; i < RMAX; ++i) {
+        if (i < c || i >= R) {
+          x[i] = 0.0;
+          continue;
+        }
+        double sv = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k)
+          if (k >= c && k < i) sv -= A[i * R + k] * x[k];
+        x[i] = sv / A[i * R + i];
+      }
+      __syncwarp(0xffffffffu >> (32 - R));
+      // L^{-1} column c into A's lower triangle
+#pragma unroll
+      for (int i = 0; i < RMAX; ++i)
+        if (i >= c && i < R) A[i * R + c] = x[i];
+    }
+    __syncwarp();
+    for (int p = tid; p < RR; p += 32) {
+      const int a = p / R, b = p % R;
+      const int k0 = a > b ? a : b;
+      double sv = 0.0;
+      for (int k = k0; k < R; ++k) sv += A[k * R + a] * A[k * R + b];
+      W[p] = sv;
+    }
+  }
+  if (tid == 0) {
+    status[0] = info;
+    if (rho_out) rho_out[0] = s_rho;
+  }
+}
+
 alto_status solve_setup(const double* grams, int nmodes, unsigned mask, int R, int kind,
                         double ridge, double* W, int* status, double* rho, cudaStream_t st) {
+  if (R <= 32) {
+    if (R <= 8)
+      solve_setup_small_kernel<8><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+    else if (R <= 16)
+      solve_setup_small_kernel<16><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+    else
+      solve_setup_small_kernel<32><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+    ALTO_LAUNCHED();
+    return ALTO_OK;
+  }
   const size_t smem = (size_t)R * R * sizeof(double);
   static size_t raised = 0;
   if (smem > 48 * 1024 && smem > raised) {
@@ -361,9 +624,12 @@ static alto_status apply_launch(const TB* B, const TC* C, const double* W, uint6
   }
   if (nblocks_out) *nblocks_out = (int)nb;
   const size_t smem = ((size_t)R * R + 2 * 8 * R) * sizeof(double);
-  if (smem > 48 * 1024)
+  static size_t raised = 0;  // raised once per kernel, outside any capture
+  if (smem > 48 * 1024 && smem > raised) {
     ALTO_TRY_CUDA(cudaFuncSetAttribute(apply_kernel<TB, TC, TX>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raised = smem;
+  }
   apply_kernel<TB, TC, TX><<<(unsigned)nb, 256, smem, st>>>(B, C, W, I, R, X, sp, rpb);
   ALTO_LAUNCHED();
   return ALTO_OK;

@@ -12,6 +12,10 @@ alto_status gram(const float* A, uint64_t I, int R, double* out, DevBuf& scratch
 // G = A^T B.
 alto_status cross_gram(const float* A, const float* B, uint64_t I, int R, double* out,
                        DevBuf& scratch, cudaStream_t st);
+// One pass over P and U: G = U^T U, C = P^T U and stats3 = {sum p u,
+// sum (p - u)^2, sum u^2} (stats3 may be NULL).
+alto_status gram_cross_stats(const float* P, const float* U, uint64_t I, int R, double* G, double* C,
+                             double* stats3, DevBuf& scratch, cudaStream_t st);
 // W = (prod_{m in mask} grams[m] + shift I)^{-1}; see the kernel comment.
 alto_status solve_setup(const double* grams, int nmodes, unsigned mask, int R, int kind,
                         double ridge, double* W, int* status, double* rho, cudaStream_t st);

@@ -611,7 +611,22 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
     ALTO_LAUNCHED();
   }
 
-  // MTTKRP tiles and their intervals
+  // MTTKRP tiles and their intervals.  Tiles hold 4096 nonzeros, fewer for
+  // small tensors (down to 256) so the grid still has two tiles per SM: a
+  // lane group walks tile/64 nonzeros in order, so the tile size is also the
+  // length of the kernel's latency chain.
+  {
+    static int sm_count = 0;
+    if (!sm_count) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+      if (sm_count <= 0) sm_count = 148;
+    }
+    uint32_t tile = 4096;
+    while (tile > 256 && (nnz + tile - 1) / tile < 2ull * (uint64_t)sm_count) tile >>= 1;
+    t->tile_nnz = tile;
+  }
   t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
   ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
   for (int m = 0; m < ALTO_MAX_MODES; ++m) {

@@ -375,10 +375,21 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
 // bit from run to run and whatever else runs on the device.
 
 constexpr uint32_t kShortChain = 64;
+constexpr uint32_t kChainSeg = 2048;  // slots per segment of a long chain
+
+// Workspace of the long chains (device): counters, then the chains
+// {first slot, end slot, first segment, segments}, then the segments
+// {chain, index in chain}, then each segment's R partial sums.
+struct DetLong {
+  uint32_t* counters;  // [0] long chains, [1] segments
+  uint4* chains;
+  uint2* segs;
+  float* segpart;
+};
 
 __global__ void __launch_bounds__(256)
     det_fix_short_kernel(const uint32_t* __restrict__ rows, const float* __restrict__ vals, uint32_t nslots,
-                         int R, float* __restrict__ out, uint2* __restrict__ longs, uint32_t* __restrict__ nlong) {
+                         int R, float* __restrict__ out, DetLong dl) {
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -394,7 +405,18 @@ __global__ void __launch_bounds__(256)
         hi = mid;
     }
     if (lo - i > kShortChain) {
-      if (lane == 0) longs[atomicAdd(nlong, 1u)] = make_uint2(i, lo);
+      // long chain: register it and its segments (the order of the lists
+      // varies from run to run; what each entry sums does not)
+      const uint32_t nseg = (lo - i + kChainSeg - 1) / kChainSeg;
+      uint32_t c = 0, base = 0;
+      if (lane == 0) {
+        c = atomicAdd(&dl.counters[0], 1u);
+        base = atomicAdd(&dl.counters[1], nseg);
+        dl.chains[c] = make_uint4(i, lo, base, nseg);
+      }
+      c = __shfl_sync(0xffffffffu, c, 0);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      for (uint32_t k = lane; k < nseg; k += 32) dl.segs[base + k] = make_uint2(c, k);
       continue;
     }
     for (int r = lane; r < R; r += 32) {
@@ -405,21 +427,23 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// One block per long chain: thread (s, q) sums slots first+s, first+s+S, ...
-// of rank quad q (S = 256 / (R/4)), then a fixed tree over s.
+// One block per segment of a long chain: thread (s, q) sums slots
+// start+s, start+s+S, ... of rank quad q (S = 256 / (R/4)), then a fixed tree
+// over s; the segment's R sums go to segpart.
 __global__ void __launch_bounds__(256)
-    det_fix_long_kernel(const uint32_t* __restrict__ rows, const float* __restrict__ vals, int R,
-                        float* __restrict__ out, const uint2* __restrict__ longs,
-                        const uint32_t* __restrict__ nlong) {
+    det_fix_seg_kernel(const float* __restrict__ vals, int R, DetLong dl) {
   __shared__ float4 part[256];
   const int Q = R / 4, S = 256 / Q;
   const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
-  const uint32_t n = *nlong;
-  for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
-    const uint2 ch = longs[c];
+  const uint32_t nseg = dl.counters[1];
+  for (uint32_t g = blockIdx.x; g < nseg; g += gridDim.x) {
+    const uint2 sg = dl.segs[g];
+    const uint4 ch = dl.chains[sg.x];
+    const uint32_t s0 = ch.x + sg.y * kChainSeg;
+    const uint32_t s1 = min(s0 + kChainSeg, ch.y);
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (sidx < S)
-      for (uint32_t k = ch.x + sidx; k < ch.y; k += S) {
+      for (uint32_t k = s0 + sidx; k < s1; k += S) {
         const float4 v = *reinterpret_cast<const float4*>(vals + (size_t)k * R + q * 4);
         acc.x += v.x;
         acc.y += v.y;
@@ -439,17 +463,27 @@ __global__ void __launch_bounds__(256)
       }
       __syncthreads();
     }
-    if (sidx == 0) {
-      float4* o = reinterpret_cast<float4*>(out + (size_t)rows[ch.x] * R + q * 4);
-      float4 x = *o;
-      const float4 p = part[q];
-      x.x += p.x;
-      x.y += p.y;
-      x.z += p.z;
-      x.w += p.w;
-      *o = x;
-    }
+    if (sidx == 0) *reinterpret_cast<float4*>(dl.segpart + (size_t)(ch.z + sg.y) * R + q * 4) = part[q];
     __syncthreads();
+  }
+}
+
+// One warp per long chain: its segments' sums added in segment order, then
+// added to the chain's output row.
+__global__ void __launch_bounds__(256)
+    det_fix_final_kernel(const uint32_t* __restrict__ rows, int R, float* __restrict__ out, DetLong dl) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nlong = dl.counters[0];
+  for (uint32_t c = gw; c < nlong; c += nw) {
+    const uint4 ch = dl.chains[c];
+    const uint32_t row = rows[ch.x];
+    for (int r = lane; r < R; r += 32) {
+      float x = 0.f;
+      for (uint32_t k = 0; k < ch.w; ++k) x += dl.segpart[(size_t)(ch.z + k) * R + r];
+      out[(size_t)row * R + r] += x;
+    }
   }
 }
 
@@ -659,7 +693,7 @@ static alto_status launch_tma(const MttkrpArgs& a, int* err, cudaStream_t st) {
 // Deterministic MTTKRP: the tile kernel in DET mode (float32 factors, the
 // specialised ranks) followed by the two fix-up kernels.
 template <int R, int HW, int NM>
-static alto_status launch_det_nm(const MttkrpArgs& a, uint2* longs, uint32_t* nlong, cudaStream_t st) {
+static alto_status launch_det_nm(const MttkrpArgs& a, const DetLong& dl, cudaStream_t st) {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -671,35 +705,37 @@ static alto_status launch_det_nm(const MttkrpArgs& a, uint2* longs, uint32_t* nl
   mttkrp_tile_kernel<R, float, HW, false, NM, true><<<grid, kMttkrpThreads, 0, st>>>(a);
   ALTO_LAUNCHED();
   const uint32_t nslots = a.ntiles * kMttkrpWarps * LaneWidth<R>::NPW * 2;
-  ALTO_TRY_CUDA(cudaMemsetAsync(nlong, 0, sizeof(uint32_t), st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(dl.counters, 0, 2 * sizeof(uint32_t), st));
   const unsigned g1 = std::min<unsigned>((nslots + 7) / 8, (unsigned)num_sms() * 16);
-  det_fix_short_kernel<<<g1, 256, 0, st>>>(a.det_rows, a.det_vals, nslots, R, a.out, longs, nlong);
+  det_fix_short_kernel<<<g1, 256, 0, st>>>(a.det_rows, a.det_vals, nslots, R, a.out, dl);
   ALTO_LAUNCHED();
-  det_fix_long_kernel<<<(unsigned)num_sms(), 256, 0, st>>>(a.det_rows, a.det_vals, R, a.out, longs, nlong);
+  det_fix_seg_kernel<<<(unsigned)num_sms() * 2, 256, 0, st>>>(a.det_vals, R, dl);
+  ALTO_LAUNCHED();
+  det_fix_final_kernel<<<(unsigned)num_sms(), 256, 0, st>>>(a.det_rows, R, a.out, dl);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
 
 template <int R, int HW>
-static alto_status launch_det(const MttkrpArgs& a, uint2* longs, uint32_t* nlong, cudaStream_t st) {
-  if constexpr (HW == kDecoded3) return launch_det_nm<R, HW, 3>(a, longs, nlong, st);
+static alto_status launch_det(const MttkrpArgs& a, const DetLong& dl, cudaStream_t st) {
+  if constexpr (HW == kDecoded3) return launch_det_nm<R, HW, 3>(a, dl, st);
   switch (a.dec.nmodes) {
-    case 3: return launch_det_nm<R, HW, 3>(a, longs, nlong, st);
-    case 4: return launch_det_nm<R, HW, 4>(a, longs, nlong, st);
-    case 5: return launch_det_nm<R, HW, 5>(a, longs, nlong, st);
-    default: return launch_det_nm<R, HW, ALTO_MAX_MODES>(a, longs, nlong, st);
+    case 3: return launch_det_nm<R, HW, 3>(a, dl, st);
+    case 4: return launch_det_nm<R, HW, 4>(a, dl, st);
+    case 5: return launch_det_nm<R, HW, 5>(a, dl, st);
+    default: return launch_det_nm<R, HW, ALTO_MAX_MODES>(a, dl, st);
   }
 }
 
 template <int HW>
-static alto_status launch_det_rank(const MttkrpArgs& a, int rank, uint2* longs, uint32_t* nlong,
+static alto_status launch_det_rank(const MttkrpArgs& a, int rank, const DetLong& dl,
                                    cudaStream_t st) {
   switch (rank) {
-    case 8: return launch_det<8, HW>(a, longs, nlong, st);
-    case 16: return launch_det<16, HW>(a, longs, nlong, st);
-    case 32: return launch_det<32, HW>(a, longs, nlong, st);
-    case 64: return launch_det<64, HW>(a, longs, nlong, st);
-    case 128: return launch_det<128, HW>(a, longs, nlong, st);
+    case 8: return launch_det<8, HW>(a, dl, st);
+    case 16: return launch_det<16, HW>(a, dl, st);
+    case 32: return launch_det<32, HW>(a, dl, st);
+    case 64: return launch_det<64, HW>(a, dl, st);
+    case 128: return launch_det<128, HW>(a, dl, st);
     default: break;
   }
   set_error("the deterministic MTTKRP takes rank 8, 16, 32, 64 or 128 (got %d)", rank);
@@ -862,15 +898,23 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * groups_per_warp(rank) * 2;
     ALTO_TRY(t->det_rows.ensure(nslots * 4));
     ALTO_TRY(t->det_vals.ensure(nslots * rank * 4));
-    ALTO_TRY(t->det_long.ensure((nslots / (kShortChain + 1) + 2) * sizeof(uint2) + 16));
+    // long chains: each has more than kShortChain slots; segments:
+    // sum over chains of ceil(len / kChainSeg)
+    const uint64_t max_chains = nslots / (kShortChain + 1) + 1;
+    const uint64_t max_segs = nslots / kChainSeg + max_chains;
+    auto up = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    const uint64_t o_chains = 256, o_segs = o_chains + up(max_chains * sizeof(uint4)),
+                   o_part = o_segs + up(max_segs * sizeof(uint2)), bytes = o_part + max_segs * rank * 4;
+    ALTO_TRY(t->det_long.ensure(bytes));
     a.det_rows = t->det_rows.as<uint32_t>();
     a.det_vals = t->det_vals.as<float>();
-    uint32_t* nlong = t->det_long.as<uint32_t>();
-    uint2* longs = reinterpret_cast<uint2*>(t->det_long.as<char>() + 16);
-    if (hw == 0) return launch_det_rank<0>(a, rank, longs, nlong, st);
-    if (hw == 1) return launch_det_rank<1>(a, rank, longs, nlong, st);
-    if (hw == kDecoded3) return launch_det_rank<kDecoded3>(a, rank, longs, nlong, st);
-    return launch_det_rank<2>(a, rank, longs, nlong, st);
+    char* base = t->det_long.as<char>();
+    DetLong dl{reinterpret_cast<uint32_t*>(base), reinterpret_cast<uint4*>(base + o_chains),
+               reinterpret_cast<uint2*>(base + o_segs), reinterpret_cast<float*>(base + o_part)};
+    if (hw == 0) return launch_det_rank<0>(a, rank, dl, st);
+    if (hw == 1) return launch_det_rank<1>(a, rank, dl, st);
+    if (hw == kDecoded3) return launch_det_rank<kDecoded3>(a, rank, dl, st);
+    return launch_det_rank<2>(a, rank, dl, st);
   }
   const bool bulk = feed == 1;
   if (fdtype == ALTO_BF16) {

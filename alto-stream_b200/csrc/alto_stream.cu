@@ -139,9 +139,71 @@ struct AdmmBatch {
   static constexpr int M = SLOTS == 1 ? 4 : (SLOTS == 2 ? 2 : 1);  // row groups per warp in registers
 };
 
+// Right-hand side of row i, mode j (src/streaming_cpd.cpp:1375-1415 and
+// :1346-1373): rhs = prev_U_j[i] A + mttkrp[i], A the historical Gram
+// product (global memory, L1-resident), in float64 from float32 inputs.
+template <int SLOTS, int SEG>
+__device__ __forceinline__ void row_rhs(const float* __restrict__ P32, const float* __restrict__ B32,
+                                        const double* __restrict__ A, uint64_t i, uint64_t I, int R, int lane,
+                                        double (&h)[SLOTS]) {
+  const int col = RowMap<SEG>::col(lane);
+  double p[SLOTS], b[SLOTS];
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    const int c = s * 32 + col;
+    const bool ok = i < I && c < R;
+    p[s] = ok ? (double)P32[i * R + c] : 0.0;
+    b[s] = ok ? (double)B32[i * R + c] : 0.0;
+  }
+  row_solve<SLOTS, SEG>(p, A, R, lane, h);
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) h[s] = __dadd_rn(h[s], b[s]);
+}
+
+// Unconstrained solve of mode j (src/streaming_cpd.cpp:1423-1431):
+// U_j[i] = (prev_U_j[i] A + mttkrp[i]) W, W = (Phi + 1e-12 I)^{-1}.
+template <int SLOTS, int SEG>
+__global__ void __launch_bounds__(kAdmmThreads)
+    stream_solve_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                        const double* __restrict__ W, uint64_t I, int R, float* __restrict__ U32) {
+  extern __shared__ double sw[];
+  for (int p = threadIdx.x; p < R * R; p += blockDim.x) sw[p] = W[p];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, col = RowMap<SEG>::col(lane), sub = RowMap<SEG>::sub(lane);
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i0 = gw * RowMap<SEG>::kRows; i0 < I; i0 += nw * RowMap<SEG>::kRows) {
+    const uint64_t i = i0 + sub;
+    double h[SLOTS], x[SLOTS];
+    row_rhs<SLOTS, SEG>(P32, B32, A, i, I, R, lane, h);
+    row_solve<SLOTS, SEG>(h, sw, R, lane, x);
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+      const int c = s * 32 + col;
+      if (i < I && c < R) U32[i * R + c] = (float)x[s];
+    }
+  }
+}
+
+// The historical Gram product of mode j: A = G_t(old) * prod_{m in mask}
+// (prev_U_m^T U_m), the cross Grams cached per mode.
+__global__ void hist_product_kernel(const double* __restrict__ old_gram, const double* __restrict__ cross,
+                                    unsigned mask, int N, int RR, double* __restrict__ A) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < RR; p += gridDim.x * blockDim.x) {
+    double v = old_gram[p];
+    for (int m = 0; m < N; ++m)
+      if (mask & (1u << m)) v *= cross[(size_t)m * RR + p];
+    A[p] = v;
+  }
+}
+
+// The ADMM rows of mode j: rhs formed on the fly from prev_U_j, the MTTKRP
+// and A; the primal starts from U_j (float32) and ends in U_j; between
+// chunks it is kept in float64 (prim), with aux.
 template <int SLOTS, int SEG, bool PASS1>
 __global__ void __launch_bounds__(kAdmmThreads)
-    admm_rows_kernel(const double* __restrict__ rhs, double* __restrict__ primal, double* __restrict__ aux,
+    admm_rows_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                     float* __restrict__ U32, double* __restrict__ primal, double* __restrict__ aux,
                      double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
                      uint64_t I, int R, double* __restrict__ partials, const AdmmState* __restrict__ state) {
   constexpr int M = AdmmBatch<SLOTS>::M;
@@ -168,12 +230,12 @@ __global__ void __launch_bounds__(kAdmmThreads)
     for (int m = 0; m < M; ++m) {
       const uint64_t i = b0 + (uint64_t)m * KR + sub;
       double a[SLOTS], z[SLOTS];
+      row_rhs<SLOTS, SEG>(P32, B32, A, i, I, R, lane, H[m]);
 #pragma unroll
       for (int s = 0; s < SLOTS; ++s) {
         const int c = s * 32 + col;
         const bool ok = i < I && c < R;
-        H[m][s] = ok ? rhs[i * R + c] : 0.0;
-        X[m][s] = ok ? primal[i * R + c] : 0.0;
+        X[m][s] = ok ? (first ? (double)U32[i * R + c] : primal[i * R + c]) : 0.0;
         U[m][s] = ok ? dual[i * R + c] : 0.0;
         Z[m][s] = ok && !first ? aux[i * R + c] : 0.0;
         X0[m][s] = X[m][s];
@@ -232,6 +294,7 @@ __global__ void __launch_bounds__(kAdmmThreads)
       }
     }
     if (!PASS1) {
+      const bool final_chunk = state->stop != 0;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         const uint64_t i = b0 + (uint64_t)m * KR + sub;
@@ -239,9 +302,13 @@ __global__ void __launch_bounds__(kAdmmThreads)
         for (int s = 0; s < SLOTS; ++s) {
           const int c = s * 32 + col;
           if (i < I && c < R) {
-            primal[i * R + c] = X[m][s];
-            aux[i * R + c] = Z[m][s];
             dual[i * R + c] = U[m][s];
+            if (final_chunk) {
+              U32[i * R + c] = (float)X[m][s];
+            } else {
+              primal[i * R + c] = X[m][s];
+              aux[i * R + c] = Z[m][s];
+            }
           }
         }
       }
@@ -269,17 +336,20 @@ __global__ void admm_begin_kernel(AdmmState* __restrict__ state, cudaGraphCondit
   }
 }
 
-// Adds the blocks' per-sweep partials in block order (one thread per sum,
-// blocks in order) and takes the chunk's sweep count: the first sweep whose
-// sums pass the test, else every sweep of the chunk.
+// Adds the blocks' per-sweep partials (one warp per sum: lane l takes blocks
+// l, l + 32, ... in order, then a fixed butterfly; lane 0's value stands)
+// and takes the chunk's sweep count: the first sweep whose sums pass the
+// test, else every sweep of the chunk.  Launch with kAdmmSums warps.
 __global__ void admm_decide_kernel(const double* __restrict__ partials, int nblocks, double tol,
                                    AdmmState* __restrict__ state, cudaGraphConditionalHandle h, int in_graph) {
   __shared__ double S[kAdmmSums];
   const bool idle = state->stop != 0;
-  for (int p = threadIdx.x; p < kAdmmSums && !idle; p += blockDim.x) {
+  const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+  if (!idle && p < kAdmmSums) {
     double t = 0.0;
-    for (int b = 0; b < nblocks; ++b) t += partials[(size_t)b * kAdmmSums + p];
-    S[p] = t;
+    for (int b = lane; b < nblocks; b += 32) t += partials[(size_t)b * kAdmmSums + p];
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) S[p] = t;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
@@ -353,7 +423,7 @@ struct alto_stream_session {
   uint64_t dims[ALTO_MAX_MODES] = {0};
   uint64_t cap[ALTO_MAX_MODES] = {0};
   DevBuf U[ALTO_MAX_MODES], P[ALTO_MAX_MODES], dual[ALTO_MAX_MODES];
-  DevBuf G, old_gram, ata, hist, W, status, rho, lam, dstat, buf32, rhs, aux, prim, time64;
+  DevBuf G, old_gram, ata, cross, W, status, rho, lam, dstat, buf32, aux, prim, time64;
   DevBuf gscr, dscr, admm_part, admm_state, grow_stage, copy_tmp, iter;
   std::vector<double> time_rows;  // concatenated time factor (host)
   alto_tensor* at = nullptr;
@@ -431,8 +501,13 @@ alto_status capture_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGra
 }
 
 template <int SLOTS, int SEG>
-alto_status admm_run(alto_stream_session* s, uint64_t I, double* primal, double* dual, cudaStream_t st,
-                     const IterLaunch& L, int mode) {
+alto_status admm_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st, const IterLaunch& L) {
+  double* primal = s->prim.as<double>();
+  double* dual = s->dual[mode].as<double>();
+  const float* P32 = s->P[mode].as<float>();
+  const float* B32 = s->buf32.as<float>();
+  const double* A = s->ata.as<double>();
+  float* U32 = s->U[mode].as<float>();
   const int R = s->R;
   const size_t smem = (size_t)R * R * sizeof(double);
   constexpr uint64_t rows_per_block = (kAdmmThreads / 32) * RowMap<SEG>::kRows * AdmmBatch<SLOTS>::M;
@@ -456,12 +531,12 @@ alto_status admm_run(alto_stream_session* s, uint64_t I, double* primal, double*
   ALTO_LAUNCHED();
   auto chunk = [&](cudaStream_t cs) -> alto_status {
     admm_rows_kernel<SLOTS, SEG, true><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
-        s->rhs.as<double>(), primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
     ALTO_LAUNCHED();
-    admm_decide_kernel<<<1, 32, 0, cs>>>(part, (int)blocks, tol, state, h, L.in_graph);
+    admm_decide_kernel<<<1, 32 * kAdmmSums, 0, cs>>>(part, (int)blocks, tol, state, h, L.in_graph);
     ALTO_LAUNCHED();
     admm_rows_kernel<SLOTS, SEG, false><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
-        s->rhs.as<double>(), primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
     ALTO_LAUNCHED();
     return ALTO_OK;
   };
@@ -483,13 +558,40 @@ alto_status admm_run(alto_stream_session* s, uint64_t I, double* primal, double*
   return ALTO_OK;
 }
 
-alto_status admm(alto_stream_session* s, uint64_t I, double* primal, double* dual, cudaStream_t st,
-                 const IterLaunch& L, int mode) {
-  if (s->R <= 8) return admm_run<1, 8>(s, I, primal, dual, st, L, mode);
-  if (s->R <= 16) return admm_run<1, 16>(s, I, primal, dual, st, L, mode);
-  if (s->R <= 32) return admm_run<1, 32>(s, I, primal, dual, st, L, mode);
-  if (s->R <= 64) return admm_run<2, 32>(s, I, primal, dual, st, L, mode);
-  return admm_run<4, 32>(s, I, primal, dual, st, L, mode);
+alto_status admm(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st, const IterLaunch& L) {
+  if (s->R <= 8) return admm_run<1, 8>(s, I, mode, st, L);
+  if (s->R <= 16) return admm_run<1, 16>(s, I, mode, st, L);
+  if (s->R <= 32) return admm_run<1, 32>(s, I, mode, st, L);
+  if (s->R <= 64) return admm_run<2, 32>(s, I, mode, st, L);
+  return admm_run<4, 32>(s, I, mode, st, L);
+}
+
+template <int SLOTS, int SEG>
+alto_status solve_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st) {
+  const int R = s->R;
+  const size_t smem = (size_t)R * R * sizeof(double);
+  static size_t raised = 0;  // raised once per kernel, outside any capture
+  if (smem > 40 * 1024 && smem > raised) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(stream_solve_kernel<SLOTS, SEG>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raised = smem;
+  }
+  const uint64_t warps = (I + RowMap<SEG>::kRows - 1) / RowMap<SEG>::kRows;
+  uint64_t blocks = std::min<uint64_t>((warps * 32 + kAdmmThreads - 1) / kAdmmThreads, 148ull * 8);
+  if (blocks < 1) blocks = 1;
+  stream_solve_kernel<SLOTS, SEG><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(
+      s->P[mode].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), s->W.as<double>(), I, R,
+      s->U[mode].as<float>());
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+alto_status stream_solve(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st) {
+  if (s->R <= 8) return solve_run<1, 8>(s, I, mode, st);
+  if (s->R <= 16) return solve_run<1, 16>(s, I, mode, st);
+  if (s->R <= 32) return solve_run<1, 32>(s, I, mode, st);
+  if (s->R <= 64) return solve_run<2, 32>(s, I, mode, st);
+  return solve_run<4, 32>(s, I, mode, st);
 }
 
 // One inner iteration of cpstream_alto_iter (src/streaming_cpd.cpp:1240-1482)
@@ -515,29 +617,23 @@ alto_status enqueue_iteration(alto_stream_session* s, const IterLaunch& L, cudaS
     if (j == t) continue;
     const uint64_t I = s->dims[j];
     ALTO_TRY(run_mttkrp(s->at, j, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
-    // historical term
-    ALTO_TRY(rr_op(s->ata.as<double>(), s->old_gram.as<double>(), (int)RR, 0, 0.0, st));
-    for (int m = 0; m < N; ++m) {
-      if (m == j || m == t) continue;
-      ALTO_TRY(cross_gram(s->P[m].as<float>(), s->U[m].as<float>(), s->dims[m], R, s->hist.as<double>(),
-                          s->gscr, st));
-      ALTO_TRY(rr_op(s->ata.as<double>(), s->hist.as<double>(), (int)RR, 1, 0.0, st));
-    }
-    ALTO_TRY(apply_f32_to_f64(s->P[j].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), I, R,
-                              s->rhs.as<double>(), st));
+    // historical term: A = G_t(old) * prod_{m != j, t} prev_U_m^T U_m
+    hist_product_kernel<<<(unsigned)((RR + 255) / 256), 256, 0, st>>>(
+        s->old_gram.as<double>(), s->cross.as<double>(), all & ~(1u << j) & ~(1u << t), N, (int)RR,
+        s->ata.as<double>());
+    ALTO_LAUNCHED();
     if (s->con == ALTO_UNCONSTRAINED) {
       ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveRidge, 1e-12, s->W.as<double>(),
                            s->status.as<int>(), nullptr, st));
-      ALTO_TRY(apply_f64_to_f32(s->rhs.as<double>(), s->W.as<double>(), I, R, s->U[j].as<float>(), st));
+      ALTO_TRY(stream_solve(s, I, j, st));
     } else {
       ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveAdmm, 0.0, s->W.as<double>(), s->status.as<int>(),
                            s->rho.as<double>(), st));
-      ALTO_TRY(convert_f32_to_f64(s->U[j].as<float>(), I * R, s->prim.as<double>(), st));
-      ALTO_TRY(admm(s, I, s->prim.as<double>(), s->dual[j].as<double>(), st, L, j));
-      ALTO_TRY(convert_f64_to_f32(s->prim.as<double>(), I * R, s->U[j].as<float>(), st));
+      ALTO_TRY(admm(s, I, j, st, L));
     }
-    ALTO_TRY(gram(s->U[j].as<float>(), I, R, G + (size_t)j * RR, s->gscr, st));
-    ALTO_TRY(dot_stats(s->P[j].as<float>(), s->U[j].as<float>(), I * R, nullptr, R, dstat + 3 * j, s->dscr, st));
+    // G_j, the cross Gram prev_U_j^T U_j and the change statistics, one pass
+    ALTO_TRY(gram_cross_stats(s->P[j].as<float>(), s->U[j].as<float>(), I, R, G + (size_t)j * RR,
+                              s->cross.as<double>() + (size_t)j * RR, dstat + 3 * j, s->gscr, st));
   }
   converge_kernel<<<1, 32, 0, st>>>(dstat, N, t, s->status.as<int>(), s->con != ALTO_UNCONSTRAINED ? 1 : 0, s->eps,
                                     s->max_inner, s->iter.as<IterState>(), L.outer, L.in_graph);
@@ -638,9 +734,10 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   uint64_t max_dim = 0;
   for (int n = 0; n < N; ++n) max_dim = std::max(max_dim, s->dims[n]);
   ALTO_TRY(s->buf32.ensure(max_dim * R * 4));
-  ALTO_TRY(s->rhs.ensure(max_dim * R * 8));
-  if (s->con != ALTO_UNCONSTRAINED) ALTO_TRY(s->aux.ensure(max_dim * R * 8));
-  ALTO_TRY(s->prim.ensure(max_dim * R * 8));
+  if (s->con != ALTO_UNCONSTRAINED) {  // the ADMM primal and aux between chunks
+    ALTO_TRY(s->aux.ensure(max_dim * R * 8));
+    ALTO_TRY(s->prim.ensure(max_dim * R * 8));
+  }
   ALTO_TRY(s->time64.ensure(s->dims[t] * R * 8));
   double* G = s->G.as<double>();
   if (first) {
@@ -650,8 +747,12 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     ALTO_TRY_CUDA(cudaMemsetAsync(s->U[t].p, 0, s->dims[t] * R * 4, st));
     ALTO_TRY_CUDA(cudaMemsetAsync(G + (size_t)t * RR, 0, RR * 8, st));
   }
+  // Grams and cross Grams (prev_U^T U) of the non-stream modes
+  double* C = s->cross.as<double>();
   for (int n = 0; n < N; ++n)
-    if (n != t) ALTO_TRY(gram(s->U[n].as<float>(), s->dims[n], R, G + (size_t)n * RR, s->gscr, st));
+    if (n != t)
+      ALTO_TRY(gram_cross_stats(s->P[n].as<float>(), s->U[n].as<float>(), s->dims[n], R, G + (size_t)n * RR,
+                                C + (size_t)n * RR, nullptr, s->gscr, st));
   for (int n = 0; n < N; ++n) ALTO_TRY_CUDA(cudaMemsetAsync(s->dual[n].p, 0, s->dims[n] * R * 8, st));
 
   // update_salto
@@ -675,7 +776,8 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
       lambda_from_gram_kernel<<<1, 128, 0, st>>>(Gm, R, s->lam.as<double>());
       ALTO_LAUNCHED();
       ALTO_TRY(scale_columns(s->U[m].as<float>(), s->dims[m], R, s->lam.as<double>(), nullptr, st));
-      ALTO_TRY(gram(s->U[m].as<float>(), s->dims[m], R, Gm, s->gscr, st));
+      ALTO_TRY(gram_cross_stats(s->P[m].as<float>(), s->U[m].as<float>(), s->dims[m], R, Gm, C + (size_t)m * RR,
+                                nullptr, s->gscr, st));
     }
     fill_kernel<<<1, 128, 0, st>>>(s->lam.as<double>(), R, 1.0);
     ALTO_LAUNCHED();
@@ -771,7 +873,7 @@ alto_status alto_stream_open(int nmodes, int stream_mode, int rank, alto_constra
   const size_t RR = (size_t)rank * rank;
   alto_status st = ALTO_OK;
   if ((st = s->G.ensure(nmodes * RR * 8)) || (st = s->old_gram.ensure(RR * 8)) ||
-      (st = s->ata.ensure(RR * 8)) || (st = s->hist.ensure(RR * 8)) || (st = s->W.ensure(RR * 8)) ||
+      (st = s->ata.ensure(RR * 8)) || (st = s->cross.ensure(nmodes * RR * 8)) || (st = s->W.ensure(RR * 8)) ||
       (st = s->status.ensure(16)) || (st = s->rho.ensure(16)) || (st = s->lam.ensure(rank * 8)) ||
       (st = s->dstat.ensure(3 * ALTO_MAX_MODES * 8)) || (st = s->admm_state.ensure(sizeof(AdmmState)))) {
     delete s;
