@@ -671,3 +671,272 @@ int ora_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_
   free(time_rows);
   return status == 0 ? (int)total_time : -1;
 }
+
+/* ------------------------------------------------------------ spCP-stream */
+
+/* C = A^T B over the rows listed in `rows` (or all I rows when rows is
+ * NULL) of row-major I x R matrices (full R x R result). */
+static void rows_atb(const double* A, const double* B, const uint64_t* rows, uint64_t n, int R, double* C) {
+  memset(C, 0, sizeof(double) * R * R);
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint64_t i = rows ? rows[k] : k;
+    for (int a = 0; a < R; ++a)
+      for (int b = 0; b < R; ++b) C[a * R + b] += A[i * R + a] * B[i * R + b];
+  }
+}
+
+/* C = A B (R x R). */
+static void mm(const double* A, const double* B, int R, double* C) {
+  for (int a = 0; a < R; ++a)
+    for (int b = 0; b < R; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < R; ++k) s += A[a * R + k] * B[k * R + b];
+      C[a * R + b] = s;
+    }
+}
+
+/* pseudo_inverse (src/matrix.cpp:226-250): rows of B <- rows of B times
+ * Phi^{-1} by Cholesky; on failure B is left as it is. */
+static void solve_rows_keep(const double* Phi, int R, double* B, uint64_t nrows, double* work) {
+  memcpy(work, Phi, sizeof(double) * R * R);
+  if (cholesky(work, R) == 0) cholesky_solve(work, R, B, nrows);
+}
+
+static double trace(const double* A, int R) {
+  double s = 0.0;
+  for (int r = 0; r < R; ++r) s += A[r * R + r];
+  return s;
+}
+
+/* spCP-stream: cpstream (src/streaming_cpd.cpp:26-366) with use_spcpstream,
+ * each batch through spcpstream_alto_iter (:466-1085).  Per batch, for every
+ * mode, the rows the batch touches (nonzero_slices, :1127-1161) are
+ * gathered into compact factors A_nz (and A_nz_prev from the previous
+ * model); the MTTKRPs run over the batch with its indices renumbered to
+ * those rows (update_salto_rowsparse).  The Gram bookkeeping keeps, per
+ * mode, c = U^T U and h = prev_U^T U split into the touched rows (c_nz,
+ * h_nz) and the untouched rows (c_z, h_z, updated in closed form through
+ * Q Phi^{-1}); after the inner loop the untouched rows become
+ * prev_U Q Phi^{-1} and the touched rows A_nz.  The constraint is not used
+ * (the reference solves with pseudo_inverse).  Initial and growth values as
+ * in ora_cpstream; forgetting as there.  Returns the total time steps, or
+ * -1 on failure. */
+int ora_spcpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_dims,
+                   const uint64_t* batch_nnz, const uint64_t* cidx, const double* vals, int rank,
+                   int max_iters, double epsilon, double forgetting, const double* init_vals,
+                   uint64_t n_init_vals, double** out_U, double* out_lambda, int* inner_iters) {
+  const int R = rank, t = stream_mode, RR = rank * rank;
+  Stream st = {init_vals, n_init_vals, 0};
+  uint64_t dims[8] = {0}, old_dims[8] = {0};
+  double *U[8] = {0}, *P[8] = {0}, *G[8];
+  double *c[8], *h[8], *c_prev[8], *c_nz_prev[8], *c_nz[8], *c_z[8], *h_nz[8], *h_z[8], *c_z_prev[8], *QPi[8];
+  double** all[] = {G, c, h, c_prev, c_nz_prev, c_nz, c_z, h_nz, h_z, c_z_prev, QPi};
+  for (size_t k = 0; k < sizeof(all) / sizeof(all[0]); ++k)
+    for (int n = 0; n < nmodes; ++n) all[k][n] = (double*)calloc(RR, sizeof(double));
+  double* lambda = out_lambda;
+  double* Phi = (double*)malloc(sizeof(double) * RR);
+  double* Q = (double*)malloc(sizeof(double) * RR);
+  double* work = (double*)malloc(sizeof(double) * RR);
+  double* tmp = (double*)malloc(sizeof(double) * RR);
+  double* old_gram = (double*)malloc(sizeof(double) * RR);
+  double* time_rows = NULL;
+  uint64_t total_time = 0;
+  size_t off_idx = 0, off_val = 0;
+
+  for (int s = 0; s < nbatch; ++s) {
+    const uint64_t* bd = batch_dims + (size_t)s * nmodes;
+    const uint64_t nnz = batch_nnz[s];
+    const uint64_t* bc = cidx + off_idx;
+    const double* bv = vals + off_val;
+    off_idx += (size_t)nmodes * nnz;
+    off_val += nnz;
+    for (int n = 0; n < nmodes; ++n) {
+      old_dims[n] = dims[n];
+      dims[n] = bd[n];
+      U[n] = (double*)realloc(U[n], sizeof(double) * (dims[n] ? dims[n] : 1) * R);
+      P[n] = (double*)realloc(P[n], sizeof(double) * (dims[n] ? dims[n] : 1) * R);
+      for (uint64_t q = old_dims[n] * R; q < dims[n] * R; ++q) {
+        U[n][q] = next_val(&st);
+        P[n][q] = 0.0;
+      }
+    }
+    if (s == 0) {
+      for (int r = 0; r < R; ++r) lambda[r] = 1.0;
+      memset(U[t], 0, sizeof(double) * dims[t] * R);
+      memset(G[t], 0, sizeof(double) * RR);
+      /* iteration 0: 2-norm normalise the non-stream factors (:585-598) */
+      for (int m = 0; m < nmodes; ++m) {
+        if (m == t) continue;
+        normalize_cols(U[m], dims[m], R, 0, lambda);
+        gram(U[m], dims[m], R, G[m]);
+      }
+      for (int r = 0; r < R; ++r) lambda[r] = 1.0;
+    }
+
+    /* nonzero_slices for every mode: sorted touched rows and their map */
+    uint64_t* nz[8];
+    int64_t* ridx[8];
+    uint64_t nnzr[8];
+    for (int m = 0; m < nmodes; ++m) {
+      ridx[m] = (int64_t*)malloc(sizeof(int64_t) * (dims[m] ? dims[m] : 1));
+      for (uint64_t i = 0; i < dims[m]; ++i) ridx[m][i] = -1;
+      for (uint64_t q = 0; q < nnz; ++q) ridx[m][bc[(size_t)m * nnz + q]] = 0;
+      nnzr[m] = 0;
+      for (uint64_t i = 0; i < dims[m]; ++i)
+        if (ridx[m][i] == 0) ++nnzr[m];
+      nz[m] = (uint64_t*)malloc(sizeof(uint64_t) * (nnzr[m] ? nnzr[m] : 1));
+      uint64_t k = 0;
+      for (uint64_t i = 0; i < dims[m]; ++i)
+        if (ridx[m][i] == 0) {
+          nz[m][k] = i;
+          ridx[m][i] = (int64_t)k++;
+        }
+    }
+    /* A_nz_prev, c = U^T U, h = prev_U^T U, A_nz (:614-676) */
+    double *Anz[8], *Aprev[8];
+    for (int m = 0; m < nmodes; ++m) {
+      Anz[m] = (double*)malloc(sizeof(double) * (nnzr[m] ? nnzr[m] : 1) * R);
+      Aprev[m] = (double*)malloc(sizeof(double) * (nnzr[m] ? nnzr[m] : 1) * R);
+      for (uint64_t k = 0; k < nnzr[m]; ++k)
+        for (int r = 0; r < R; ++r) {
+          Anz[m][k * R + r] = U[m][nz[m][k] * R + r];
+          Aprev[m][k * R + r] = P[m][nz[m][k] * R + r];
+        }
+      rows_atb(U[m], U[m], NULL, dims[m], R, c[m]);
+      rows_atb(P[m], U[m], NULL, dims[m], R, h[m]);
+    }
+    /* c_z_prev = c_prev - c_nz_prev over the touched rows (:679-693) */
+    if (s > 0)
+      for (int m = 0; m < nmodes; ++m) {
+        if (m == t) continue;
+        rows_atb(P[m], P[m], nz[m], nnzr[m], R, c_nz_prev[m]);
+        for (int q = 0; q < RR; ++q) c_z_prev[m][q] = c_prev[m][q] - c_nz_prev[m][q];
+      }
+    /* the batch with its indices renumbered to the touched rows */
+    uint64_t* cc = (uint64_t*)malloc(sizeof(uint64_t) * nmodes * (nnz ? nnz : 1));
+    for (int m = 0; m < nmodes; ++m)
+      for (uint64_t q = 0; q < nnz; ++q) cc[(size_t)m * nnz + q] = (uint64_t)ridx[m][bc[(size_t)m * nnz + q]];
+
+    double delta = 0.0, prev_delta = 0.0;
+    int it, done = 0;
+    for (it = 0; it < max_iters; ++it) {
+      delta = 0.0;
+      /* s_t: MTTKRP of the stream mode, solve with Hadamard(c) but t (:716-744) */
+      memset(Anz[t], 0, sizeof(double) * nnzr[t] * R);
+      ora_coo_mttkrp(nmodes, nnz, cc, bv, t, Anz, R);
+      for (int q = 0; q < RR; ++q) Phi[q] = 1.0;
+      for (int m = 0; m < nmodes; ++m)
+        if (m != t)
+          for (int q = 0; q < RR; ++q) Phi[q] *= c[m][q];
+      for (int r = 0; r < R; ++r) Phi[r * R + r] += 1e-12;
+      solve_rows_keep(Phi, R, Anz[t], nnzr[t], work);
+      /* G_t: old_gram, then += s s^T over the stream rows (:748-780) */
+      memcpy(old_gram, G[t], sizeof(double) * RR);
+      for (uint64_t q = 0; q < dims[t]; ++q) {
+        const double* sr = Anz[t] + q * R;
+        for (int a = 0; a < R; ++a)
+          for (int b = 0; b < R; ++b) G[t][a * R + b] += sr[b] * sr[a];
+      }
+      memcpy(h[t], old_gram, sizeof(double) * RR);
+      memcpy(c[t], G[t], sizeof(double) * RR);
+      for (int m = 0; m < nmodes; ++m) {
+        if (m == t) continue;
+        /* Q = Hadamard(h) but m, Phi = Hadamard(c) but m + 1e-12 I (:800-806) */
+        for (int q = 0; q < RR; ++q) Q[q] = Phi[q] = 1.0;
+        for (int k = 0; k < nmodes; ++k)
+          if (k != m)
+            for (int q = 0; q < RR; ++q) {
+              Q[q] *= h[k][q];
+              Phi[q] *= c[k][q];
+            }
+        for (int r = 0; r < R; ++r) Phi[r * R + r] += 1e-12;
+        /* row-sparse MTTKRP, historical term, solve (:826-892) */
+        memset(Anz[m], 0, sizeof(double) * nnzr[m] * R);
+        ora_coo_mttkrp(nmodes, nnz, cc, bv, m, Anz, R);
+        for (uint64_t k = 0; k < nnzr[m]; ++k)
+          for (int b = 0; b < R; ++b) {
+            double acc = 0.0;
+            for (int a = 0; a < R; ++a) acc += Aprev[m][k * R + a] * Q[a * R + b];
+            Anz[m][k * R + b] += acc;
+          }
+        solve_rows_keep(Phi, R, Anz[m], nnzr[m], work);
+        /* c_nz, h_nz; Q Phi^{-1}; h_z = c_z_prev Q Phi^{-1}; c_z = (Q Phi^{-1})^T h_z (:903-942) */
+        rows_atb(Anz[m], Anz[m], NULL, nnzr[m], R, c_nz[m]);
+        rows_atb(Aprev[m], Anz[m], NULL, nnzr[m], R, h_nz[m]);
+        memcpy(QPi[m], Q, sizeof(double) * RR);
+        solve_rows_keep(Phi, R, QPi[m], R, work);
+        mm(c_z_prev[m], QPi[m], R, h_z[m]);
+        for (int a = 0; a < R; ++a)
+          for (int b = 0; b < R; ++b) {
+            double sum = 0.0;
+            for (int k = 0; k < R; ++k) sum += QPi[m][k * R + a] * h_z[m][k * R + b];
+            tmp[a * R + b] = sum;
+          }
+        memcpy(c_z[m], tmp, sizeof(double) * RR);
+        for (int q = 0; q < RR; ++q) {
+          c[m][q] = c_nz[m][q] + c_z[m][q];
+          h[m][q] = h_nz[m][q] + h_z[m][q];
+        }
+        const double trc = trace(c[m], R), trh = trace(h[m], R), trp = trace(c_prev[m], R);
+        delta += sqrt(fabs((trc + trp - 2.0 * trh) / (trc + 1e-12)));
+      }
+      if (it > 0 && fabs(prev_delta - delta) < epsilon) {
+        done = it + 1;
+        break;
+      }
+      prev_delta = delta;
+      done = it + 1;
+    }
+    if (inner_iters) inner_iters[s] = done;
+    /* untouched rows <- prev rows Q Phi^{-1}; touched rows <- A_nz (:985-1024) */
+    for (int m = 0; m < nmodes; ++m) {
+      for (uint64_t i = 0; i < dims[m]; ++i) {
+        if (ridx[m][i] >= 0) {
+          memcpy(U[m] + i * R, Anz[m] + (uint64_t)ridx[m][i] * R, sizeof(double) * R);
+        } else if (m != t) {
+          for (int b = 0; b < R; ++b) {
+            double acc = 0.0;
+            for (int a = 0; a < R; ++a) acc += P[m][i * R + a] * QPi[m][a * R + b];
+            U[m][i * R + b] = acc;
+          }
+        }
+      }
+    }
+    for (int q = 0; q < RR; ++q) G[t][q] *= forgetting;
+    for (int m = 0; m < nmodes; ++m) {
+      if (m == t) continue;
+      memcpy(c_prev[m], c[m], sizeof(double) * RR);
+      memcpy(c_nz_prev[m], c_nz[m], sizeof(double) * RR);
+    }
+    for (int n = 0; n < nmodes; ++n) memcpy(P[n], U[n], sizeof(double) * dims[n] * R);
+    time_rows = (double*)realloc(time_rows, sizeof(double) * (total_time + dims[t]) * R);
+    memcpy(time_rows + total_time * R, U[t], sizeof(double) * dims[t] * R);
+    total_time += dims[t];
+    for (int m = 0; m < nmodes; ++m) {
+      free(nz[m]);
+      free(ridx[m]);
+      free(Anz[m]);
+      free(Aprev[m]);
+    }
+    free(cc);
+  }
+  for (int n = 0; n < nmodes; ++n) {
+    if (n == t)
+      memcpy(out_U[n], time_rows, sizeof(double) * total_time * R);
+    else
+      memcpy(out_U[n], U[n], sizeof(double) * dims[n] * R);
+  }
+  for (size_t k = 0; k < sizeof(all) / sizeof(all[0]); ++k)
+    for (int n = 0; n < nmodes; ++n) free(all[k][n]);
+  for (int n = 0; n < nmodes; ++n) {
+    free(U[n]);
+    free(P[n]);
+  }
+  free(Phi);
+  free(Q);
+  free(work);
+  free(tmp);
+  free(old_gram);
+  free(time_rows);
+  return (int)total_time;
+}

@@ -217,6 +217,23 @@ def cpstream(batches, stream_mode, rank, max_iters, eps, nonneg, init_vals, forg
     return outs, lam, inner
 
 
+def spcpstream(batches, stream_mode, rank, max_iters, eps, init_vals, forgetting=0.99):
+    """spCP-stream (row-sparse updates) over a list of batches."""
+    N = len(batches[0]["dims"])
+    dims, nnz, cidx, vals = _stream_args(batches)
+    init_vals = np.ascontiguousarray(init_vals, dtype=np.float64)
+    outs = _stream_outputs(batches, stream_mode, rank)
+    lam = np.zeros(rank, np.float64)
+    inner = np.zeros(len(batches), np.int32)
+    tt = lib().ora_spcpstream(c_int(N), c_int(stream_mode), c_int(len(batches)), _ptr(dims), _ptr(nnz),
+                              _ptr(cidx), _ptr(vals), c_int(rank), c_int(max_iters), c_double(eps),
+                              c_double(forgetting), _ptr(init_vals), c_uint64(len(init_vals)), _dptrs(outs),
+                              _ptr(lam), _ptr(inner))
+    if tt < 0:
+        raise RuntimeError("oracle spCP-stream failed")
+    return outs, lam, inner
+
+
 # ------------------------------------------------------ compiled reference
 
 class RefTensor:
@@ -281,6 +298,21 @@ class RefTensor:
             self.close()
         except Exception:
             pass
+
+
+def ref_spcpstream(batches, stream_mode, rank, max_iters, eps, init_vals, bits=64):
+    """The reference's spCP-stream (ALTO) over the same batches (forgetting 0.99)."""
+    L = ref_lib(bits)
+    N = len(batches[0]["dims"])
+    dims, nnz, cidx, vals = _stream_args(batches)
+    init_vals = np.ascontiguousarray(init_vals, dtype=np.float64)
+    outs = _stream_outputs(batches, stream_mode, rank)
+    lam = np.zeros(rank, np.float64)
+    secs = np.zeros(len(batches), np.float64)
+    L.ref_spcpstream(c_int(N), c_int(stream_mode), c_int(len(batches)), _ptr(dims), _ptr(nnz), _ptr(cidx),
+                     _ptr(vals), c_int(rank), c_int(max_iters), c_double(eps), _ptr(init_vals),
+                     c_uint64(len(init_vals)), _dptrs(outs), _ptr(lam), _ptr(secs))
+    return outs, lam, secs
 
 
 def ref_cpstream(batches, stream_mode, rank, max_iters, eps, nonneg, init_vals, bits=64):

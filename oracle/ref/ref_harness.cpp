@@ -248,11 +248,11 @@ int ref_cpd_als(void* p, double** U, double* lambda, int rank, int max_iters, do
 // Outputs: out_U[m] (final dims[m] x rank for m != stream_mode; for the stream
 // mode the concatenated time factor, total_time x rank), out_lambda (rank),
 // slice_seconds (nbatch, may be NULL).  Returns the total time steps.
-int ref_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_dims,
-                 const uint64_t* batch_nnz, const uint64_t* cidx, const double* vals, int rank,
-                 int max_iters, double epsilon, int nonneg, const double* init_vals,
-                 uint64_t n_init_vals, double** out_U, double* out_lambda,
-                 double* slice_seconds) {
+static int run_stream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_dims,
+                      const uint64_t* batch_nnz, const uint64_t* cidx, const double* vals, int rank,
+                      int max_iters, double epsilon, int nonneg, const double* init_vals,
+                      uint64_t n_init_vals, double** out_U, double* out_lambda, double* slice_seconds,
+                      bool sparse) {
   ValueStream vs{init_vals, (size_t)n_init_vals, 0};
   cpd_constraint* con = init_constraint();
   if (nonneg) apply_nonneg_constraint(con);
@@ -263,6 +263,7 @@ int ref_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_
   Matrix** grams = NULL;
   StreamMatrix* global_time = new StreamMatrix(rank);
   admm_ws* ws = admm_ws_init(nmodes);
+  SparseCPGrams* scpgrams = sparse ? InitSparseCPGrams(nmodes, rank) : NULL;
   double t_tensor = 0.0;
 
   size_t off_idx = 0, off_val = 0;
@@ -308,13 +309,18 @@ int ref_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_
     ws->auxil = zero_mat(max_dim, rank);
     ws->mat_init = zero_mat(max_dim, rank);
 
-    int num_partitions = get_num_ptrn(t_batch->nnz);
-    FType** ofibs = NULL;
-    update_salto(t_batch, AT, num_partitions);
-    create_da_mem(-1, rank, AT, &ofibs);
-    cpstream_alto_iter(AT, ofibs, M, prev_M, grams, max_iters, epsilon, stream_mode, it, con, ws,
-                       &t_tensor);
-    destroy_da_mem(AT, ofibs, rank, -1);
+    if (sparse) {
+      spcpstream_alto_iter(t_batch, AT, M, prev_M, grams, scpgrams, max_iters, epsilon, stream_mode, it, con, ws,
+                           &t_tensor);
+    } else {
+      int num_partitions = get_num_ptrn(t_batch->nnz);
+      FType** ofibs = NULL;
+      update_salto(t_batch, AT, num_partitions);
+      create_da_mem(-1, rank, AT, &ofibs);
+      cpstream_alto_iter(AT, ofibs, M, prev_M, grams, max_iters, epsilon, stream_mode, it, con, ws,
+                         &t_tensor);
+      destroy_da_mem(AT, ofibs, rank, -1);
+    }
 
     it += t_batch->dims[stream_mode];
     CopyKruskalModel(prev_M, M);
@@ -344,10 +350,31 @@ int ref_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_
     DestroyKruskalModel(prev_M);
   }
   if (AT) destroy_alto(AT);
+  if (scpgrams) DeleteSparseCPGrams(scpgrams, nmodes);
   delete global_time;
   free(ws);
   free_constraint(con);
   return it;
+}
+
+int ref_cpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_dims,
+                 const uint64_t* batch_nnz, const uint64_t* cidx, const double* vals, int rank,
+                 int max_iters, double epsilon, int nonneg, const double* init_vals,
+                 uint64_t n_init_vals, double** out_U, double* out_lambda,
+                 double* slice_seconds) {
+  return run_stream(nmodes, stream_mode, nbatch, batch_dims, batch_nnz, cidx, vals, rank, max_iters, epsilon,
+                    nonneg, init_vals, n_init_vals, out_U, out_lambda, slice_seconds, false);
+}
+
+// spcpstream (cpstream with use_spcpstream, src/streaming_cpd.cpp:26-366,
+// each batch through spcpstream_alto_iter :466-1085); the constraint is
+// not used by the reference on this path.
+int ref_spcpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batch_dims,
+                   const uint64_t* batch_nnz, const uint64_t* cidx, const double* vals, int rank,
+                   int max_iters, double epsilon, const double* init_vals, uint64_t n_init_vals,
+                   double** out_U, double* out_lambda, double* slice_seconds) {
+  return run_stream(nmodes, stream_mode, nbatch, batch_dims, batch_nnz, cidx, vals, rank, max_iters, epsilon, 0,
+                    init_vals, n_init_vals, out_U, out_lambda, slice_seconds, true);
 }
 
 }  // extern "C"

@@ -126,8 +126,17 @@ def main(ref_root):
             "norms": [float(np.linalg.norm(o)) for o in outs],
             "colsums": [o.sum(0).tolist() for o in outs]}
 
+    out_json["spcpstream_small"] = spcpstream_golden(b, iv, ntot)
+
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out_json, f, indent=1)
+
+
+def spcpstream_golden(b, iv, ntot):
+    """spCP-stream (the reference's row-sparse model) on the small stream."""
+    outs, lam, _ = O.ref_spcpstream(b, 0, RANK, 10, 1e-5, iv)
+    return {"rank": RANK, "max_iters": 10, "eps": 1e-5, "init_seed": 7, "n_init": ntot,
+            "norms": [float(np.linalg.norm(o)) for o in outs], "colsums": [o.sum(0).tolist() for o in outs]}
 
 
 if __name__ == "__main__":

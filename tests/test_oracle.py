@@ -100,6 +100,19 @@ def test_cpstream_matches_reference(nonneg, golden):
         np.testing.assert_allclose(o.sum(0), cs, rtol=1e-7, atol=1e-9)
 
 
+def test_spcpstream_matches_reference(golden):
+    """The spCP-stream restatement against the compiled reference's
+    spcpstream_alto_iter on the small stream (row-sparse updates, closed-form
+    untouched rows, c/h Gram bookkeeping)."""
+    g = golden["spcpstream_small"]
+    b = load_stream_fixture()
+    iv = synth.init_values(g["n_init"], seed=g["init_seed"])
+    outs, lam, inner = O.spcpstream(b, 0, g["rank"], g["max_iters"], g["eps"], iv)
+    np.testing.assert_allclose([np.linalg.norm(o) for o in outs], g["norms"], rtol=1e-9)
+    for o, cs in zip(outs, g["colsums"]):
+        np.testing.assert_allclose(o.sum(0), cs, rtol=1e-7, atol=1e-9)
+
+
 def test_partition_rules():
     """prtn_alto: equal-nnz partitions, empty tail partitions, clamped intervals."""
     dims = np.array([4, 5, 6], np.uint64)
