@@ -33,6 +33,7 @@ F32, BF16, F64 = 0, 1, 2
 AUTO, ATOMIC, STAGED, STREAM, SORTED, DETERMINISTIC = range(6)
 FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
 UNCONSTRAINED, NONNEG, LASSO = range(3)
+CPSTREAM, SPCPSTREAM = range(2)  # streaming models (alto_stream_set_model)
 FIT_REFERENCE, FIT_EXACT = 0, 1
 
 EXPORTED = [
@@ -41,7 +42,8 @@ EXPORTED = [
     "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
-    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_graph", "alto_stream_close",
+    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph",
+    "alto_stream_close",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
@@ -384,6 +386,10 @@ class CPStream:
         check(lib().alto_stream_factor(self.h, c_int(mode), out.ctypes.data_as(c_void_p), byref(rows)))
         return out[: rows.value]
 
+    def set_model(self, model):
+        """CPSTREAM (default) or SPCPSTREAM, before the first push (alto_stream_set_model)."""
+        check(lib().alto_stream_set_model(self.h, c_int(model)))
+
     def set_graph(self, enable):
         """Inner iterations 2.. of each batch as one CUDA graph (default) or
         launched one by one (alto_stream_set_graph)."""
@@ -410,7 +416,7 @@ class CPStream:
 
 class alto_stream_config(ctypes.Structure):
     _fields_ = [("nmodes", c_int), ("stream_mode", c_int), ("rank", c_int), ("constraint", c_int),
-                ("forgetting", c_double), ("max_inner_iters", c_int), ("epsilon", c_double)]
+                ("forgetting", c_double), ("max_inner_iters", c_int), ("epsilon", c_double), ("model", c_int)]
 
 
 class alto_serving_stats(ctypes.Structure):
@@ -431,8 +437,8 @@ class Server:
         self.rank = {}
 
     def open(self, nmodes, stream_mode, rank, max_dims, max_slice_nnz, constraint=UNCONSTRAINED,
-             forgetting=0.99, max_inner=10, epsilon=1e-5):
-        cfg = alto_stream_config(nmodes, stream_mode, rank, constraint, forgetting, max_inner, epsilon)
+             forgetting=0.99, max_inner=10, epsilon=1e-5, model=0):
+        cfg = alto_stream_config(nmodes, stream_mode, rank, constraint, forgetting, max_inner, epsilon, model)
         md = np.ascontiguousarray(max_dims, dtype=np.uint64)
         sid = c_int()
         check(lib().alto_server_open(self.h, byref(cfg), md.ctypes.data_as(c_void_p), c_uint64(int(max_slice_nnz)),

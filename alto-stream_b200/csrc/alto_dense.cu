@@ -313,7 +313,8 @@ alto_status cross_gram(const float* A, const float* B, uint64_t I, int R, double
 // view); on success W = V^{-1}.  On failure: kind SOLVE_RIDGE_DIAG_FALLBACK
 // writes the reference's dgelsy fallback for CP-ALS, W = diag(1/V_rr) of V
 // without the ridge (include/cpd.hpp:436-476: its restored V has zero
-// lower triangles mirrored over the upper one); otherwise W = 0.
+// lower triangles mirrored over the upper one); kind kSolveRidgeKeep writes
+// W = I (the right-hand side is left as it is); otherwise W = 0.
 // status[0] = LAPACK-style info (0 = success), rho_out[0] = rho.
 __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes, unsigned mask,
                                    int R, int kind, double ridge, double* __restrict__ W,
@@ -372,7 +373,7 @@ __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes,
       if (kind == kSolveRidgeDiagFallback) {
         if (a != b) W[p] = 0.0;
       } else {
-        W[p] = 0.0;
+        W[p] = (kind == kSolveRidgeKeep && a == b) ? 1.0 : 0.0;
       }
     }
     __syncthreads();
@@ -480,7 +481,7 @@ __global__ void __launch_bounds__(32)
       if (kind == kSolveRidgeDiagFallback) {
         if (a != b) W[p] = 0.0;
       } else {
-        W[p] = 0.0;
+        W[p] = (kind == kSolveRidgeKeep && a == b) ? 1.0 : 0.0;
       }
     }
     __syncwarp();

@@ -5,7 +5,11 @@
 
 namespace alto {
 
-enum { kSolveRidge = 0, kSolveRidgeDiagFallback = 1, kSolveAdmm = 2 };
+// Solve set-up kinds.  On a failed Cholesky: kSolveRidge gives W = 0,
+// kSolveRidgeDiagFallback the CP-ALS diagonal fallback, kSolveRidgeKeep
+// W = I (the right-hand side stays as it is, as pseudo_inverse leaves it,
+// src/matrix.cpp:226-250).
+enum { kSolveRidge = 0, kSolveRidgeDiagFallback = 1, kSolveAdmm = 2, kSolveRidgeKeep = 3 };
 
 // G = A^T A (R x R float64) of a float32 I x R matrix.
 alto_status gram(const float* A, uint64_t I, int R, double* out, DevBuf& scratch, cudaStream_t st);

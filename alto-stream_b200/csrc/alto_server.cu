@@ -149,6 +149,7 @@ void worker_main(alto_server* s) {
       const alto_stream_config& c = r->cfg;
       st = alto_stream_open(c.nmodes, c.stream_mode, c.rank, c.constraint, c.forgetting, c.max_inner_iters,
                             c.epsilon, cs, &r->sess);
+      if (st == ALTO_OK) st = alto_stream_set_model(r->sess, c.model);
     }
     if (st == ALTO_OK) {
       stream_set_cuda_stream(r->sess, cs);
@@ -233,7 +234,8 @@ alto_status alto_server_open(alto_server* s, const alto_stream_config* cfg, cons
     return ALTO_ERR_INVALID;
   }
   if (cfg->nmodes < 2 || cfg->nmodes > ALTO_MAX_MODES || cfg->stream_mode < 0 ||
-      cfg->stream_mode >= cfg->nmodes || cfg->rank < 1 || cfg->rank > 128 || cfg->max_inner_iters < 1) {
+      cfg->stream_mode >= cfg->nmodes || cfg->rank < 1 || cfg->rank > 128 || cfg->max_inner_iters < 1 ||
+      (cfg->model != ALTO_MODEL_CPSTREAM && cfg->model != ALTO_MODEL_SPCPSTREAM)) {
     set_error("bad stream configuration");
     return ALTO_ERR_INVALID;
   }

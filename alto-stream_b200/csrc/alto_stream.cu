@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kAdmmThreads)
 __global__ void hist_product_kernel(const double* __restrict__ old_gram, const double* __restrict__ cross,
                                     unsigned mask, int N, int RR, double* __restrict__ A) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < RR; p += gridDim.x * blockDim.x) {
-    double v = old_gram[p];
+    double v = old_gram ? old_gram[p] : 1.0;
     for (int m = 0; m < N; ++m)
       if (mask & (1u << m)) v *= cross[(size_t)m * RR + p];
     A[p] = v;
@@ -382,11 +382,12 @@ __global__ void admm_decide_kernel(const double* __restrict__ partials, int nblo
 // constrained solve's Cholesky failed.
 __global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, const int* __restrict__ status,
                                 int constrained, double eps, int max_inner, IterState* __restrict__ it,
-                                cudaGraphConditionalHandle h, int in_graph) {
+                                cudaGraphConditionalHandle h, int in_graph, int sparse) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double delta = 0.0;
   for (int j = 0; j < N; ++j)
-    if (j != t) delta += sqrt(dstat[3 * j + 1]) / (sqrt(dstat[3 * j + 2]) + 1e-12);
+    if (j != t)
+      delta += sparse ? dstat[3 * j] : sqrt(dstat[3 * j + 1]) / (sqrt(dstat[3 * j + 2]) + 1e-12);
   const int k = it->done;
   bool stop = false;
   if (constrained && status[0]) {
@@ -406,6 +407,127 @@ __global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, 
 // Head of the iteration graph: run the loop only if the batch goes on.
 __global__ void iter_begin_kernel(const IterState* __restrict__ it, int max_inner, cudaGraphConditionalHandle h) {
   if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(h, (!it->stop && it->done < max_inner) ? 1u : 0u);
+}
+
+
+// ------------------------------------------------------------ spCP-stream
+//
+// spcpstream_alto_iter (src/streaming_cpd.cpp:466-1085) works on the rows a
+// batch touches.  Per batch and mode: a row map (nonzero_slices,
+// :1127-1161; here flags, an exclusive scan and a list), the batch with its
+// indices renumbered to those rows and encoded (update_salto_rowsparse), the
+// touched rows of the model and the previous model gathered into compact
+// factors (A_nz, A_nz_prev).  Per inner iteration only the compact rows are
+// solved; the untouched rows enter through R x R Grams kept per mode:
+// c = U^T U and h = prev_U^T U, split into touched (c_nz, h_nz) and
+// untouched parts (c_z, h_z), the latter updated in closed form through
+// Q Phi^{-1}.  After the loop the untouched rows become prev_U Q Phi^{-1}.
+
+// R x R float64 state of spCP-stream per mode, [kind][mode][R][R].
+enum { kSpCPrev = 0, kSpCNzPrev, kSpCNz, kSpCZ, kSpHNz, kSpHZ, kSpCZPrev, kSpQPi, kSpKinds };
+
+__global__ void mark_rows_kernel(const uint64_t* __restrict__ idx, uint64_t nnz, uint32_t* __restrict__ flags) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < nnz; q += (uint64_t)gridDim.x * blockDim.x)
+    flags[idx[q]] = 1u;
+}
+
+// After the exclusive scan of the flags (dims + 1 entries): row i is touched
+// iff ridx[i + 1] != ridx[i], and then its compact index is ridx[i].
+__global__ void row_list_kernel(const uint32_t* __restrict__ ridx, uint64_t dims, uint32_t* __restrict__ nz) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dims; i += (uint64_t)gridDim.x * blockDim.x)
+    if (ridx[i + 1] != ridx[i]) nz[ridx[i]] = (uint32_t)i;
+}
+
+__global__ void renumber_kernel(uint64_t* __restrict__ idx, uint64_t nnz, const uint32_t* __restrict__ ridx) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < nnz; q += (uint64_t)gridDim.x * blockDim.x)
+    idx[q] = ridx[idx[q]];
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ src, const uint32_t* __restrict__ nz, uint64_t n, int R,
+                                   float* __restrict__ dst) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < n * R; q += (uint64_t)gridDim.x * blockDim.x)
+    dst[q] = src[(uint64_t)nz[q / R] * R + q % R];
+}
+
+__global__ void sub_kernel(const double* __restrict__ a, const double* __restrict__ b, int n, double* __restrict__ out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) out[p] = a[p] - b[p];
+}
+
+// The Gram bookkeeping of mode m after its rows were solved (:903-975):
+// QPi = Q W (Q Phi^{-1}); h_z = c_z_prev QPi; c_z = QPi^T h_z; c = c_nz + c_z;
+// h = h_nz + h_z; delta_m = sqrt(|(tr c + tr c_prev - 2 tr h) / (tr c + 1e-12)|).
+// One block; products in k order.
+__global__ void __launch_bounds__(256)
+    sp_gram_update_kernel(const double* __restrict__ Q, const double* __restrict__ W, const double* __restrict__ c_z_prev,
+                          const double* __restrict__ c_nz, const double* __restrict__ h_nz,
+                          const double* __restrict__ c_prev, int R, double* __restrict__ QPi, double* __restrict__ h_z,
+                          double* __restrict__ c_z, double* __restrict__ c, double* __restrict__ h,
+                          double* __restrict__ delta_out) {
+  const int RR = R * R;
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) {
+    const int a = p / R, b = p % R;
+    double x = 0.0;
+    for (int k = 0; k < R; ++k) x += Q[a * R + k] * W[k * R + b];
+    QPi[p] = x;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) {
+    const int a = p / R, b = p % R;
+    double x = 0.0;
+    for (int k = 0; k < R; ++k) x += c_z_prev[a * R + k] * QPi[k * R + b];
+    h_z[p] = x;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) {
+    const int a = p / R, b = p % R;
+    double x = 0.0;
+    for (int k = 0; k < R; ++k) x += QPi[k * R + a] * h_z[k * R + b];
+    c_z[p] = x;
+    c[p] = c_nz[p] + x;
+    h[p] = h_nz[p] + h_z[p];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double trc = 0.0, trh = 0.0, trp = 0.0;
+    for (int r = 0; r < R; ++r) {
+      trc += c[r * R + r];
+      trh += h[r * R + r];
+      trp += c_prev[r * R + r];
+    }
+    *delta_out = sqrt(fabs((trc + trp - 2.0 * trh) / (trc + 1e-12)));
+  }
+}
+
+// The model after the inner loop (:985-1024): touched rows from A_nz,
+// untouched rows prev_U QPi.
+template <int SLOTS, int SEG>
+__global__ void __launch_bounds__(kAdmmThreads)
+    sp_final_rows_kernel(const float* __restrict__ P32, const float* __restrict__ Anz, const uint32_t* __restrict__ ridx,
+                         const double* __restrict__ QPi, uint64_t I, int R, float* __restrict__ U32) {
+  extern __shared__ double sw[];
+  for (int p = threadIdx.x; p < R * R; p += blockDim.x) sw[p] = QPi[p];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, col = RowMap<SEG>::col(lane), sub = RowMap<SEG>::sub(lane);
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i0 = gw * RowMap<SEG>::kRows; i0 < I; i0 += nw * RowMap<SEG>::kRows) {
+    const uint64_t i = i0 + sub;
+    const bool ok = i < I;
+    double p[SLOTS], x[SLOTS];
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+      const int c = s * 32 + col;
+      p[s] = ok && c < R ? (double)P32[i * R + c] : 0.0;
+    }
+    row_solve<SLOTS, SEG>(p, sw, R, lane, x);
+    if (!ok) continue;
+    const uint32_t r0 = ridx[i], r1 = ridx[i + 1];
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+      const int c = s * 32 + col;
+      if (c < R) U32[i * R + c] = r1 != r0 ? Anz[(uint64_t)r0 * R + c] : (float)x[s];
+    }
+  }
 }
 
 }  // namespace alto
@@ -428,6 +550,12 @@ struct alto_stream_session {
   std::vector<double> time_rows;  // concatenated time factor (host)
   alto_tensor* at = nullptr;
   bool use_graph = true;              // inner iterations 1.. as one graph per batch
+  // spCP-stream (alto_stream_set_model): rows the batch touches, their maps
+  // and compact factors, the R x R Gram state, the batch on the device
+  bool sparse = false;
+  uint64_t nnzr[ALTO_MAX_MODES] = {0};
+  DevBuf ridx[ALTO_MAX_MODES], nzl[ALTO_MAX_MODES], Anz[ALTO_MAX_MODES], Aprev[ALTO_MAX_MODES];
+  DevBuf spg, coo_idx, coo_val;
   cudaStream_t capst[2] = {nullptr, nullptr};  // capture-only streams (nothing runs on them)
   ~alto_stream_session() {
     delete at;
@@ -567,8 +695,8 @@ alto_status admm(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st, 
 }
 
 template <int SLOTS, int SEG>
-alto_status solve_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st) {
-  const int R = s->R;
+alto_status solve_run(const float* P32, const float* B32, const double* A, const double* W, uint64_t I, int R,
+                      float* U32, cudaStream_t st) {
   const size_t smem = (size_t)R * R * sizeof(double);
   static size_t raised = 0;  // raised once per kernel, outside any capture
   if (smem > 40 * 1024 && smem > raised) {
@@ -579,24 +707,32 @@ alto_status solve_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t
   const uint64_t warps = (I + RowMap<SEG>::kRows - 1) / RowMap<SEG>::kRows;
   uint64_t blocks = std::min<uint64_t>((warps * 32 + kAdmmThreads - 1) / kAdmmThreads, 148ull * 8);
   if (blocks < 1) blocks = 1;
-  stream_solve_kernel<SLOTS, SEG><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(
-      s->P[mode].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), s->W.as<double>(), I, R,
-      s->U[mode].as<float>());
+  stream_solve_kernel<SLOTS, SEG><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(P32, B32, A, W, I, R, U32);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
 
+// U32 = (P32 A + B32) W row by row (float64 arithmetic, float32 in and out).
+alto_status rows_solve(const float* P32, const float* B32, const double* A, const double* W, uint64_t I, int R,
+                       float* U32, cudaStream_t st) {
+  if (R <= 8) return solve_run<1, 8>(P32, B32, A, W, I, R, U32, st);
+  if (R <= 16) return solve_run<1, 16>(P32, B32, A, W, I, R, U32, st);
+  if (R <= 32) return solve_run<1, 32>(P32, B32, A, W, I, R, U32, st);
+  if (R <= 64) return solve_run<2, 32>(P32, B32, A, W, I, R, U32, st);
+  return solve_run<4, 32>(P32, B32, A, W, I, R, U32, st);
+}
+
 alto_status stream_solve(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st) {
-  if (s->R <= 8) return solve_run<1, 8>(s, I, mode, st);
-  if (s->R <= 16) return solve_run<1, 16>(s, I, mode, st);
-  if (s->R <= 32) return solve_run<1, 32>(s, I, mode, st);
-  if (s->R <= 64) return solve_run<2, 32>(s, I, mode, st);
-  return solve_run<4, 32>(s, I, mode, st);
+  return rows_solve(s->P[mode].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), s->W.as<double>(), I, s->R,
+                    s->U[mode].as<float>(), st);
 }
 
 // One inner iteration of cpstream_alto_iter (src/streaming_cpd.cpp:1240-1482)
 // on stream st, ending with the convergence kernel.
+alto_status enqueue_iteration_sparse(alto_stream_session* s, const IterLaunch& L, cudaStream_t st);
+
 alto_status enqueue_iteration(alto_stream_session* s, const IterLaunch& L, cudaStream_t st) {
+  if (s->sparse) return enqueue_iteration_sparse(s, L, st);
   const int N = s->N, t = s->t, R = s->R;
   const size_t RR = (size_t)R * R;
   const unsigned all = (1u << N) - 1;
@@ -636,8 +772,212 @@ alto_status enqueue_iteration(alto_stream_session* s, const IterLaunch& L, cudaS
                               s->cross.as<double>() + (size_t)j * RR, dstat + 3 * j, s->gscr, st));
   }
   converge_kernel<<<1, 32, 0, st>>>(dstat, N, t, s->status.as<int>(), s->con != ALTO_UNCONSTRAINED ? 1 : 0, s->eps,
-                                    s->max_inner, s->iter.as<IterState>(), L.outer, L.in_graph);
+                                    s->max_inner, s->iter.as<IterState>(), L.outer, L.in_graph, 0);
   ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+// spCP-stream, per batch before the inner loop (:607-709): row maps, the
+// renumbered batch encoded, compact factors, c_z_prev.  The session's G
+// holds c (G_t the temporal Gram) and its cross Grams hold h.
+alto_status sparse_prepare(alto_stream_session* s, const alto_coo* b, bool first) {
+  const int N = s->N, R = s->R;
+  const size_t RR = (size_t)R * R;
+  cudaStream_t st = s->st;
+  const uint64_t nnz = b->nnz;
+  if (b->on_device) {
+    set_error("spCP-stream batches are host COO tensors");
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  ALTO_TRY(s->spg.ensure(kSpKinds * N * RR * 8));
+  double* spg = s->spg.as<double>();
+  auto SG = [&](int kind, int m) { return spg + ((size_t)kind * N + m) * RR; };
+  if (first) ALTO_TRY_CUDA(cudaMemsetAsync(spg, 0, kSpKinds * N * RR * 8, st));
+  // the batch on the device: uint64 indices, float64 values
+  ALTO_TRY(s->coo_idx.ensure((size_t)N * nnz * 8));
+  ALTO_TRY(s->coo_val.ensure(nnz * 8));
+  uint64_t* ci = s->coo_idx.as<uint64_t>();
+  std::vector<uint64_t> h64;
+  for (int m = 0; m < N; ++m) {
+    const void* src = b->cidx[m];
+    if (b->index_bytes == 4) {
+      h64.resize(nnz);
+      for (uint64_t q = 0; q < nnz; ++q) h64[q] = static_cast<const uint32_t*>(b->cidx[m])[q];
+      src = h64.data();
+    }
+    ALTO_TRY_CUDA(cudaMemcpyAsync(ci + (size_t)m * nnz, src, nnz * 8, cudaMemcpyHostToDevice, st));
+    if (b->index_bytes == 4) ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // h64 is reused
+  }
+  if (b->val_dtype == ALTO_F64) {
+    ALTO_TRY_CUDA(cudaMemcpyAsync(s->coo_val.p, b->vals, nnz * 8, cudaMemcpyHostToDevice, st));
+  } else {
+    std::vector<double> v(nnz);
+    for (uint64_t q = 0; q < nnz; ++q) v[q] = static_cast<const float*>(b->vals)[q];
+    ALTO_TRY_CUDA(cudaMemcpyAsync(s->coo_val.p, v.data(), nnz * 8, cudaMemcpyHostToDevice, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  }
+  // row maps: flags, exclusive scan (dims + 1 entries), touched-row count
+  for (int m = 0; m < N; ++m) {
+    const uint64_t d = s->dims[m];
+    ALTO_TRY(s->ridx[m].ensure((d + 1) * 4));
+    ALTO_TRY_CUDA(cudaMemsetAsync(s->ridx[m].p, 0, (d + 1) * 4, st));
+    mark_rows_kernel<<<(unsigned)std::min<uint64_t>((nnz + 255) / 256, 148ull * 8), 256, 0, st>>>(
+        ci + (size_t)m * nnz, nnz, s->ridx[m].as<uint32_t>());
+    ALTO_LAUNCHED();
+    ALTO_TRY(exclusive_scan_u32(s->ridx[m].as<uint32_t>(), d + 1, s->copy_tmp, st));
+  }
+  uint32_t cnt[ALTO_MAX_MODES];
+  for (int m = 0; m < N; ++m)
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&cnt[m], s->ridx[m].as<uint32_t>() + s->dims[m], 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  uint64_t max_r = 1;
+  for (int m = 0; m < N; ++m) {
+    s->nnzr[m] = cnt[m];
+    max_r = std::max<uint64_t>(max_r, cnt[m]);
+    const uint64_t d = s->dims[m];
+    ALTO_TRY(s->nzl[m].ensure(std::max<uint64_t>(cnt[m], 1) * 4));
+    row_list_kernel<<<(unsigned)std::min<uint64_t>((d + 255) / 256, 148ull * 8), 256, 0, st>>>(
+        s->ridx[m].as<uint32_t>(), d, s->nzl[m].as<uint32_t>());
+    ALTO_LAUNCHED();
+    renumber_kernel<<<(unsigned)std::min<uint64_t>((nnz + 255) / 256, 148ull * 8), 256, 0, st>>>(
+        ci + (size_t)m * nnz, nnz, s->ridx[m].as<uint32_t>());
+    ALTO_LAUNCHED();
+    ALTO_TRY(s->Anz[m].ensure(std::max<uint64_t>(cnt[m], 1) * R * 4));
+    ALTO_TRY(s->Aprev[m].ensure(std::max<uint64_t>(cnt[m], 1) * R * 4));
+    const unsigned gg = (unsigned)std::min<uint64_t>((cnt[m] * R + 255) / 256 + 1, 148ull * 8);
+    gather_rows_kernel<<<gg, 256, 0, st>>>(s->U[m].as<float>(), s->nzl[m].as<uint32_t>(), cnt[m], R,
+                                           s->Anz[m].as<float>());
+    ALTO_LAUNCHED();
+    gather_rows_kernel<<<gg, 256, 0, st>>>(s->P[m].as<float>(), s->nzl[m].as<uint32_t>(), cnt[m], R,
+                                           s->Aprev[m].as<float>());
+    ALTO_LAUNCHED();
+  }
+  // the renumbered batch, encoded (update_salto_rowsparse)
+  const void* ptrs[ALTO_MAX_MODES];
+  for (int m = 0; m < N; ++m) ptrs[m] = ci + (size_t)m * nnz;
+  alto_coo c;
+  c.nmodes = N;
+  c.dims = s->nnzr;
+  c.nnz = nnz;
+  c.cidx = ptrs;
+  c.index_bytes = 8;
+  c.vals = s->coo_val.p;
+  c.val_dtype = ALTO_F64;
+  c.on_device = 1;
+  ALTO_TRY(encode_tensor(s->at, &c, 1, st));
+  // c_z_prev = c_prev - c_nz_prev over the touched rows (:679-693)
+  if (!first)
+    for (int m = 0; m < N; ++m) {
+      if (m == s->t) continue;
+      ALTO_TRY(gram(s->Aprev[m].as<float>(), s->nnzr[m], R, SG(kSpCNzPrev, m), s->gscr, st));
+      sub_kernel<<<(unsigned)((RR + 255) / 256), 256, 0, st>>>(SG(kSpCPrev, m), SG(kSpCNzPrev, m), (int)RR,
+                                                               SG(kSpCZPrev, m));
+      ALTO_LAUNCHED();
+    }
+  ALTO_TRY(s->buf32.ensure(max_r * R * 4));
+  ALTO_TRY(s->time64.ensure(std::max<uint64_t>(s->nnzr[s->t], s->dims[s->t]) * R * 8));
+  return ALTO_OK;
+}
+
+// One inner iteration of spcpstream_alto_iter (:716-975), ending with the
+// convergence kernel.
+alto_status enqueue_iteration_sparse(alto_stream_session* s, const IterLaunch& L, cudaStream_t st) {
+  const int N = s->N, t = s->t, R = s->R;
+  const size_t RR = (size_t)R * R;
+  const unsigned all = (1u << N) - 1;
+  double* G = s->G.as<double>();        // c (and G_t)
+  double* H = s->cross.as<double>();    // h
+  double* spg = s->spg.as<double>();
+  auto SG = [&](int kind, int m) { return spg + ((size_t)kind * N + m) * RR; };
+  double* dstat = s->dstat.as<double>();
+  // s_t: MTTKRP of the stream mode over the compact factors, solve with
+  // Hadamard(c) but t (+1e-12 I); the rows stay as they are if it fails
+  ALTO_TRY(run_mttkrp(s->at, t, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
+  ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidgeKeep, 1e-12, s->W.as<double>(), s->status.as<int>(),
+                       nullptr, st));
+  ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->nnzr[t], R, s->time64.as<double>(),
+                            st));
+  ALTO_TRY(convert_f64_to_f32(s->time64.as<double>(), s->nnzr[t] * R, s->Anz[t].as<float>(), st));
+  // h_t = G_t (old), then G_t += s s^T (= c_t)
+  double* Gt = G + (size_t)t * RR;
+  ALTO_TRY(rr_op(H + (size_t)t * RR, Gt, (int)RR, 0, 0.0, st));
+  ALTO_TRY(rank_update(Gt, s->time64.as<double>(), s->nnzr[t], R, st));
+  for (int m = 0; m < N; ++m) {
+    if (m == t) continue;
+    const uint64_t I = s->nnzr[m];
+    // Q = Hadamard(h) but m; Phi = Hadamard(c) but m + 1e-12 I
+    hist_product_kernel<<<(unsigned)((RR + 255) / 256), 256, 0, st>>>(nullptr, H, all & ~(1u << m), N, (int)RR,
+                                                                       s->ata.as<double>());
+    ALTO_LAUNCHED();
+    ALTO_TRY(solve_setup(G, N, all & ~(1u << m), R, kSolveRidgeKeep, 1e-12, s->W.as<double>(),
+                         s->status.as<int>(), nullptr, st));
+    // A_nz = (mttkrp + A_nz_prev Q) Phi^{-1}
+    ALTO_TRY(run_mttkrp(s->at, m, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
+    ALTO_TRY(rows_solve(s->Aprev[m].as<float>(), s->buf32.as<float>(), s->ata.as<double>(), s->W.as<double>(), I, R,
+                        s->Anz[m].as<float>(), st));
+    // c_nz = A_nz^T A_nz, h_nz = A_nz_prev^T A_nz; then c, h, delta
+    ALTO_TRY(gram_cross_stats(s->Aprev[m].as<float>(), s->Anz[m].as<float>(), I, R, SG(kSpCNz, m), SG(kSpHNz, m),
+                              nullptr, s->gscr, st));
+    sp_gram_update_kernel<<<1, 256, 0, st>>>(s->ata.as<double>(), s->W.as<double>(), SG(kSpCZPrev, m),
+                                             SG(kSpCNz, m), SG(kSpHNz, m), SG(kSpCPrev, m), R, SG(kSpQPi, m),
+                                             SG(kSpHZ, m), SG(kSpCZ, m), G + (size_t)m * RR, H + (size_t)m * RR,
+                                             dstat + 3 * m);
+    ALTO_LAUNCHED();
+  }
+  converge_kernel<<<1, 32, 0, st>>>(dstat, N, t, s->status.as<int>(), 0, s->eps, s->max_inner,
+                                    s->iter.as<IterState>(), L.outer, L.in_graph, 1);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+template <int SLOTS, int SEG>
+alto_status sp_final_run(alto_stream_session* s, int m, cudaStream_t st) {
+  const int R = s->R;
+  const uint64_t I = s->dims[m];
+  const size_t smem = (size_t)R * R * sizeof(double);
+  static size_t raised = 0;  // raised once per kernel, outside any capture
+  if (smem > 40 * 1024 && smem > raised) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(sp_final_rows_kernel<SLOTS, SEG>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raised = smem;
+  }
+  const uint64_t warps = (I + RowMap<SEG>::kRows - 1) / RowMap<SEG>::kRows;
+  uint64_t blocks = std::min<uint64_t>((warps * 32 + kAdmmThreads - 1) / kAdmmThreads, 148ull * 8);
+  if (blocks < 1) blocks = 1;
+  const double* QPi = s->spg.as<double>() + ((size_t)kSpQPi * s->N + m) * R * R;
+  sp_final_rows_kernel<SLOTS, SEG><<<(unsigned)blocks, kAdmmThreads, smem, st>>>(
+      s->P[m].as<float>(), s->Anz[m].as<float>(), s->ridx[m].as<uint32_t>(), QPi, I, R, s->U[m].as<float>());
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+// After the inner loop (:985-1047): the model's rows; c_prev <- c,
+// c_nz_prev <- c_nz.
+alto_status sparse_finish(alto_stream_session* s) {
+  const int N = s->N, t = s->t, R = s->R;
+  const size_t RR = (size_t)R * R;
+  cudaStream_t st = s->st;
+  double* spg = s->spg.as<double>();
+  auto SG = [&](int kind, int m) { return spg + ((size_t)kind * N + m) * RR; };
+  for (int m = 0; m < N; ++m) {
+    if (m == t) {
+      // the stream mode's rows are the batch's (a batch touches its time rows)
+      ALTO_TRY_CUDA(cudaMemsetAsync(SG(kSpQPi, m), 0, RR * 8, st));
+    }
+    if (R <= 8)
+      ALTO_TRY((sp_final_run<1, 8>(s, m, st)));
+    else if (R <= 16)
+      ALTO_TRY((sp_final_run<1, 16>(s, m, st)));
+    else if (R <= 32)
+      ALTO_TRY((sp_final_run<1, 32>(s, m, st)));
+    else if (R <= 64)
+      ALTO_TRY((sp_final_run<2, 32>(s, m, st)));
+    else
+      ALTO_TRY((sp_final_run<4, 32>(s, m, st)));
+    if (m == t) continue;
+    ALTO_TRY(rr_op(SG(kSpCPrev, m), s->G.as<double>() + (size_t)m * RR, (int)RR, 0, 0.0, st));
+    ALTO_TRY(rr_op(SG(kSpCNzPrev, m), SG(kSpCNz, m), (int)RR, 0, 0.0, st));
+  }
   return ALTO_OK;
 }
 
@@ -753,20 +1093,21 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     if (n != t)
       ALTO_TRY(gram_cross_stats(s->P[n].as<float>(), s->U[n].as<float>(), s->dims[n], R, G + (size_t)n * RR,
                                 C + (size_t)n * RR, nullptr, s->gscr, st));
-  for (int n = 0; n < N; ++n) ALTO_TRY_CUDA(cudaMemsetAsync(s->dual[n].p, 0, s->dims[n] * R * 8, st));
-
-  // update_salto
-  alto_coo c = *b;
-  uint64_t bd[ALTO_MAX_MODES];
-  for (int n = 0; n < N; ++n) bd[n] = s->dims[n];
-  c.dims = bd;
+  if (!s->sparse)
+    for (int n = 0; n < N; ++n) ALTO_TRY_CUDA(cudaMemsetAsync(s->dual[n].p, 0, s->dims[n] * R * 8, st));
   if (!s->at) {
     s->at = new alto_tensor();
     s->at->key_bits = 128;
     s->at->stream_mode = t;
     s->at->stream = st;
   }
-  ALTO_TRY(encode_tensor(s->at, &c, 1, st));
+  if (!s->sparse) {  // update_salto
+    alto_coo c = *b;
+    uint64_t bd[ALTO_MAX_MODES];
+    for (int n = 0; n < N; ++n) bd[n] = s->dims[n];
+    c.dims = bd;
+    ALTO_TRY(encode_tensor(s->at, &c, 1, st));
+  }
 
   // first batch: 2-norm normalise the non-stream factors, lambda = 1
   if (first) {
@@ -783,8 +1124,10 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     ALTO_LAUNCHED();
   }
 
+  if (s->sparse) ALTO_TRY(sparse_prepare(s, b, first));
+
   IterLaunch L{};
-  for (int n = 0; n < N; ++n) L.fac[n] = s->U[n].p;
+  for (int n = 0; n < N; ++n) L.fac[n] = s->sparse ? s->Anz[n].p : s->U[n].p;
   // the deterministic MTTKRP where it runs, so a stream's results repeat
   // bit for bit however many other streams share the device
   L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
@@ -810,6 +1153,7 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     return ALTO_ERR_NOT_SPD;
   }
   if (inner_out) *inner_out = hs.done;
+  if (s->sparse) ALTO_TRY(sparse_finish(s));
   // forgetting, prev <- current, time rows out
   ALTO_TRY(rr_op(G + (size_t)t * RR, nullptr, (int)RR, 2, s->forgetting, st));
   for (int n = 0; n < N; ++n)
@@ -940,6 +1284,19 @@ alto_status alto_stream_lambda(alto_stream_session* s, double* host_out) {
   }
   ALTO_TRY_CUDA(cudaMemcpyAsync(host_out, s->lam.p, s->R * 8, cudaMemcpyDeviceToHost, s->st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(s->st));
+  return ALTO_OK;
+}
+
+alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model model) {
+  if (!s || (model != ALTO_MODEL_CPSTREAM && model != ALTO_MODEL_SPCPSTREAM)) {
+    set_error("bad session or model");
+    return ALTO_ERR_INVALID;
+  }
+  if (s->batches > 0) {
+    set_error("the model is chosen before the first batch");
+    return ALTO_ERR_INVALID;
+  }
+  s->sparse = model == ALTO_MODEL_SPCPSTREAM;
   return ALTO_OK;
 }
 

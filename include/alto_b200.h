@@ -237,6 +237,16 @@ alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_ou
                                uint64_t* rows);
 alto_status alto_stream_lambda(alto_stream_session* s, double* host_out);
 
+/* The streaming model of a session (the reference's -l cpstream_alto |
+ * spcpstream_alto, src/main.cpp:158-165; cpstream(..., use_spcpstream, ...),
+ * src/streaming_cpd.cpp:26).  CP-stream solves every row of every mode in
+ * each inner iteration and applies the constraint; spCP-stream
+ * (spcpstream_alto_iter, src/streaming_cpd.cpp:466-1085) solves only the
+ * rows a batch touches and moves the others in closed form, and, as in the
+ * reference, does not use the constraint.  Set before the first push. */
+typedef enum { ALTO_MODEL_CPSTREAM = 0, ALTO_MODEL_SPCPSTREAM = 1 } alto_stream_model;
+alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model model);
+
 /* How alto_stream_push issues a batch's inner iterations (the reference's
  * loop, src/streaming_cpd.cpp:1240-1482).  enable = 1 (the default): the
  * first directly, the rest as one CUDA graph per batch whose while nodes
@@ -268,6 +278,7 @@ typedef struct {
   double forgetting;
   int max_inner_iters;
   double epsilon;
+  alto_stream_model model;  /* ALTO_MODEL_CPSTREAM or ALTO_MODEL_SPCPSTREAM */
 } alto_stream_config;
 
 typedef struct {

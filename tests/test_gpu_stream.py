@@ -88,3 +88,64 @@ def test_graph_and_direct_launches_agree(nonneg):
     assert ig == id_ and np.array_equal(lg, ld)
     for a, c in zip(og, od):
         assert np.array_equal(a, c)
+
+
+# ------------------------------------------------------------ spCP-stream
+
+def run_sparse(batches, R, max_iters, eps, iv, graph=True):
+    N = len(batches[0]["dims"])
+    s = A.CPStream(N, 0, R, constraint=A.UNCONSTRAINED, forgetting=0.99, max_inner=max_iters, epsilon=eps)
+    s.set_model(A.SPCPSTREAM)
+    s.set_graph(graph)
+    used, prev, inner = 0, np.zeros(N, np.int64), []
+    for b in batches:
+        d = b["dims"].astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * R
+        inner.append(s.push(b["dims"], b["cidx"], b["vals"], iv[used:used + need]))
+        used += need
+        prev = np.maximum(prev, d)
+    outs = []
+    for m in range(N):
+        rows = int(sum(int(b["dims"][0]) for b in batches)) if m == 0 else int(batches[-1]["dims"][m])
+        outs.append(s.factor(m, rows))
+    s.close()
+    return outs, inner
+
+
+def test_spcpstream_matches_oracle_and_reference(golden):
+    """Row-sparse updates (spcpstream_alto_iter) against the FP64 oracle fed
+    the same float32 batches and initial values, and the reference's norms."""
+    g = golden["spcpstream_small"]
+    b = load_stream_fixture()
+    iv = synth.init_values(g["n_init"], seed=g["init_seed"])
+    outs, inner = run_sparse(b, g["rank"], g["max_iters"], g["eps"], iv)
+    bo = [dict(dims=x["dims"], cidx=x["cidx"], vals=x["vals"].astype(np.float32).astype(np.float64)) for x in b]
+    oo, _, inner_o = O.spcpstream(bo, 0, g["rank"], g["max_iters"], g["eps"],
+                                  iv.astype(np.float32).astype(np.float64))
+    assert list(inner) == list(inner_o)
+    for a, c in zip(outs, oo):
+        assert normwise(a, c) <= 1e-4, normwise(a, c)
+    np.testing.assert_allclose([np.linalg.norm(o) for o in outs], g["norms"], rtol=1e-4)
+
+
+def test_spcpstream_graph_direct_and_server_agree():
+    b = load_stream_fixture()[:4]
+    iv = synth.init_values(20000, seed=6)
+    og, ig = run_sparse(b, 16, 10, 1e-5, iv, graph=True)
+    od, id_ = run_sparse(b, 16, 10, 1e-5, iv, graph=False)
+    assert ig == id_
+    for a, c in zip(og, od):
+        assert np.array_equal(a, c)
+    srv = A.Server(4 << 30, workers=2)
+    sid = srv.open(4, 0, 16, [len(b)] + [int(x) for x in b[-1]["dims"][1:]], 2000, model=A.SPCPSTREAM)
+    used, prev = 0, np.zeros(4, np.int64)
+    for x in b:
+        d = x["dims"].astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * 16
+        srv.submit(sid, x["dims"], x["cidx"], x["vals"], iv[used:used + need])
+        used += need
+        prev = np.maximum(prev, d)
+    srv.drain()
+    for m in range(4):
+        assert np.array_equal(srv.factor(sid, m), og[m])
+    srv.destroy()
