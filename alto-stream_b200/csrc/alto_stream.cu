@@ -1006,7 +1006,7 @@ alto_status run_graph(alto_stream_session* s, IterLaunch L) {
     if ((st = cuda_status(cudaGraphConditionalHandleCreate(&L.outer, g, 0, 0), "conditional handle", __FILE__,
                           __LINE__)))
       break;
-    if (s->con != ALTO_UNCONSTRAINED)
+    if (s->con != ALTO_UNCONSTRAINED && !s->sparse)  // (spCP-stream has no ADMM loop)
       for (int j = 0; j < s->N && st == ALTO_OK; ++j)
         if (j != s->t)
           st = cuda_status(cudaGraphConditionalHandleCreate(&L.admm[j], g, 0, 0), "conditional handle", __FILE__,

@@ -217,7 +217,7 @@ int run_als(alto_tensor* t, const Coo& X, int R, int iters, double eps) {
 // stream mode then the following modes cyclically, relabel the non-stream
 // indices in first-seen order, and cut batches of timeslice_limit time steps
 // (or until nnz_threshold).
-int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_constraint con,
+int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_constraint con, bool sparse,
                  uint64_t nnz_threshold, uint64_t limit, double forgetting) {
   Coo X = X0;
   const int N = X.nmodes;
@@ -245,6 +245,7 @@ int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_co
   }
   alto_stream_session* s = nullptr;
   CHECK(alto_stream_open(N, tmode, R, con, forgetting, iters, eps, nullptr, &s));
+  if (sparse) CHECK(alto_stream_set_model(s, ALTO_MODEL_SPCPSTREAM));
   std::vector<uint64_t> prev(N, 0);
   uint64_t ptr = 0, batch_num = 0;
   int nb = 0;
@@ -290,7 +291,8 @@ int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_co
     fprintf(stderr, "batch %d: %llu nnz, %d inner iterations\n", nb, (unsigned long long)B.nnz(), inner);
   }
   double el = now() - t0;
-  printf("CPSTREAM (ALTO) on the GPU: %d batches in %f s (%f s/batch)\n", nb, el, nb ? el / nb : 0.0);
+  printf("%s (ALTO) on the GPU: %d batches in %f s (%f s/batch)\n", sparse ? "spCPSTREAM" : "CPSTREAM", nb, el,
+         nb ? el / nb : 0.0);
   alto_stream_close(s);
   return 0;
 }
@@ -353,11 +355,11 @@ int main(int argc, char** argv) {
   printf("tensor: %d modes, %llu nonzeros, rank %d\n", X.nmodes, (unsigned long long)X.nnz(), R);
   if (model == "cpstream_alto" || model == "CPSTREAM_ALTO") {
     if (tmode < 0 || tmode >= X.nmodes) { fprintf(stderr, "need -a streaming mode\n"); return 1; }
-    return run_cpstream(X, R, iters, eps, tmode, con, nnz_threshold, limit ? limit : 1, forgetting);
+    return run_cpstream(X, R, iters, eps, tmode, con, false, nnz_threshold, limit ? limit : 1, forgetting);
   }
   if (model == "spcpstream_alto" || model == "SPCPSTREAM_ALTO") {
-    fprintf(stderr, "spcpstream_alto is not available in this build\n");
-    return 2;
+    if (tmode < 0 || tmode >= X.nmodes) { fprintf(stderr, "need -a streaming mode\n"); return 1; }
+    return run_cpstream(X, R, iters, eps, tmode, con, true, nnz_threshold, limit ? limit : 1, forgetting);
   }
   std::vector<const void*> ptrs;
   alto_coo coo = view(X, ptrs);

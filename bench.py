@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed steps before (mttkrp 3; cpstream 3 slices; serve 1 slice per stream)")
     ap.add_argument("--workers", type=int, default=16, help="serve: server worker threads")
+    ap.add_argument("--model", choices=["cpstream", "spcpstream"], default="cpstream",
+                    help="cpstream/serve: the streaming model (spcpstream: row-sparse updates, no constraint)")
     ap.add_argument("--streams", type=int, default=64, help="serve: independent streams")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: aggregate Poisson arrival rate (slices/s)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
@@ -471,15 +473,19 @@ class stdout_to_stderr:
         os.close(self.saved)
 
 
-def ref_cpstream_rate(batches, R, iv):
-    """Slices/s of the reference's cpstream (oracle/_ref, all host threads)."""
+def ref_cpstream_rate(batches, R, iv, model="cpstream"):
+    """Slices/s of the reference's cpstream or spcpstream (oracle/_ref, all
+    host threads)."""
     import oracle as O
 
     L = O.ref_lib(64)
     threads = os.cpu_count() or 1
     L.ref_set_threads(threads)
     with stdout_to_stderr():
-        _, _, secs = O.ref_cpstream(batches, 0, R, 50, 1e-5, 1, iv, bits=64)
+        if model == "spcpstream":
+            _, _, secs = O.ref_spcpstream(batches, 0, R, 50, 1e-5, iv, bits=64)
+        else:
+            _, _, secs = O.ref_cpstream(batches, 0, R, 50, 1e-5, 1, iv, bits=64)
     return len(batches) / float(secs.sum()), threads, [round(float(x) * 1e3, 1) for x in secs]
 
 
@@ -497,6 +503,8 @@ def ours_cpstream(args):
     need = stream_need(batches, R)
     iv = synth.init_values(sum(need) + 64, seed=1)
     s = A.CPStream(4, 0, R, constraint=A.NONNEG, forgetting=0.95, max_inner=50, epsilon=1e-5)
+    if args.model == "spcpstream":
+        s.set_model(A.SPCPSTREAM)
     used = 0
     lat, inner, dev_ms, nbytes, h2d = [], [], [], 0, 0
     stream = torch.cuda.current_stream()
@@ -534,17 +542,19 @@ def ours_cpstream(args):
     if not args.no_cpu_baseline:
         try:
             nb = 6
-            rate, threads, secs = ref_cpstream_rate(batches[:nb], R, iv)
+            rate, threads, secs = ref_cpstream_rate(batches[:nb], R, iv, args.model)
             cpu = {"value": rate, "unit": "slices/s", "cores": threads, "kind": "reference",
                    "sample": f"first {nb} slices of the same stream through the reference's cpstream "
                              f"(its forgetting factor is fixed at 0.99); per-slice ms {secs}"}
         except Exception as e:
             cpu = {"value": None, "unit": "slices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
     line = {
-        "metric": CPSTREAM_METRIC, "value": K / dev_total, "unit": "slices/s", "n_gpus": 1, "steps": K,
+        "metric": CPSTREAM_METRIC + (" [spCP-stream model]" if args.model == "spcpstream" else ""),
+        "value": K / dev_total, "unit": "slices/s", "n_gpus": 1, "steps": K,
         "warmup": W, "ms_per_step": dev_total / K * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": CPSTREAM_WORKLOAD, "space_dims": C4_SPACE, "rank": R, "constraint": "nonneg",
+        "config": {"workload": CPSTREAM_WORKLOAD, "model": args.model, "space_dims": C4_SPACE, "rank": R,
+                   "constraint": "nonneg" if args.model == "cpstream" else "none (spCP-stream does not constrain)",
                    "forgetting": 0.95, "max_inner": 50, "epsilon": 1e-5,
                    "slice_nnz_mean": float(np.mean([len(b["vals"]) for b in batches[W:]])),
                    "inner_iters_mean": float(np.mean(inner)), "inner_iters_max": int(np.max(inner)),
@@ -604,8 +614,11 @@ def ours_serve(args):
         return pool[offs[k]:offs[k] + need[k]] if j == 0 else None
 
     # plain path: one session per stream, one slice at a time, arrival order
+    model = A.SPCPSTREAM if args.model == "spcpstream" else A.CPSTREAM
     sess = [A.CPStream(4, 0, st["rank"], constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10,
                        epsilon=1e-5) for st in streams]
+    for x in sess:
+        x.set_model(model)
     for j in range(W):
         for k, st in enumerate(streams):
             b = st["slices"][j]
@@ -631,7 +644,7 @@ def ours_serve(args):
     # server: warm-up slices, then the timed slices at their arrival times
     srv = A.Server(80 << 30, workers=args.workers)
     sids = [srv.open(4, 0, st["rank"], st["dims"], max(len(b["vals"]) for b in st["slices"]),
-                     constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10, epsilon=1e-5)
+                     constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10, epsilon=1e-5, model=model)
             for st in streams]
     for j in range(W):
         for k, st in enumerate(streams):
@@ -669,10 +682,11 @@ def ours_serve(args):
     plain_rate = n / plain_s
     p99_iso = float(np.percentile(iso, 99))
     line = {
-        "metric": SERVE_METRIC, "value": value, "unit": "slices/s", "n_gpus": 1, "steps": n, "warmup": W * len(streams),
+        "metric": SERVE_METRIC + (" [spCP-stream model]" if args.model == "spcpstream" else ""),
+        "value": value, "unit": "slices/s", "n_gpus": 1, "steps": n, "warmup": W * len(streams),
         "ms_per_step": served_s / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": SERVE_WORKLOAD, "streams": len(streams), "slices_per_stream": W + K,
+        "config": {"workload": SERVE_WORKLOAD, "model": args.model, "streams": len(streams), "slices_per_stream": W + K,
                    "workers": args.workers, "arrival_rate": args.rate, "hbm_budget_bytes": 80 << 30,
                    "max_inner": 10, "epsilon": 1e-5,
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
@@ -692,12 +706,12 @@ def ours_serve(args):
         "gpu_launches": launches,
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = serve_reference_sample(streams, pool, offs, need)
+        line["cpu_baseline"] = serve_reference_sample(streams, pool, offs, need, model=args.model)
     print(json.dumps(line))
     return 0
 
 
-def serve_reference_sample(streams, pool, offs, need, nstreams=6, nslices=3):
+def serve_reference_sample(streams, pool, offs, need, nstreams=6, nslices=3, model="cpstream"):
     """The reference's cpstream run stream after stream (its plain path) on a
     bounded sample: the first nslices slices of the first nstreams streams."""
     import oracle as O
@@ -711,8 +725,11 @@ def serve_reference_sample(streams, pool, offs, need, nstreams=6, nslices=3):
             st = streams[k]
             iv = pool[offs[k]:offs[k] + need[k]]
             with stdout_to_stderr():
-                _, _, secs = O.ref_cpstream(st["slices"][:nslices], 0, st["rank"], 10, 1e-5, st["constraint"], iv,
-                                            bits=64)
+                if model == "spcpstream":
+                    _, _, secs = O.ref_spcpstream(st["slices"][:nslices], 0, st["rank"], 10, 1e-5, iv, bits=64)
+                else:
+                    _, _, secs = O.ref_cpstream(st["slices"][:nslices], 0, st["rank"], 10, 1e-5, st["constraint"],
+                                                iv, bits=64)
             total += float(secs.sum())
             count += nslices
         return {"value": count / total, "unit": "slices/s", "cores": threads, "kind": "reference",
@@ -733,7 +750,7 @@ def reference_stream_arm(args):
             nb = 6
             batches = c4_batches(nb)
             iv = synth.init_values(sum(stream_need(batches, C4_RANK)) + 64, seed=1)
-            rate, threads, secs = ref_cpstream_rate(batches, C4_RANK, iv)
+            rate, threads, secs = ref_cpstream_rate(batches, C4_RANK, iv, args.model)
             metric, unit, workload = CPSTREAM_METRIC, "slices/s", CPSTREAM_WORKLOAD
             sample = f"first {nb} slices; per-slice ms {secs}"
         else:
@@ -741,7 +758,7 @@ def reference_stream_arm(args):
             args.steps = 2  # only the sample's slices are generated
             streams, pool, offs, need, _, _ = serve_setup(args)
             args.steps = steps
-            cb = serve_reference_sample(streams, pool, offs, need)
+            cb = serve_reference_sample(streams, pool, offs, need, model=args.model)
             if cb["value"] is None:
                 raise RuntimeError(cb["sample"])
             rate, threads, sample = cb["value"], cb["cores"], cb["sample"]

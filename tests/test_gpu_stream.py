@@ -92,9 +92,9 @@ def test_graph_and_direct_launches_agree(nonneg):
 
 # ------------------------------------------------------------ spCP-stream
 
-def run_sparse(batches, R, max_iters, eps, iv, graph=True):
+def run_sparse(batches, R, max_iters, eps, iv, graph=True, constraint=A.UNCONSTRAINED):
     N = len(batches[0]["dims"])
-    s = A.CPStream(N, 0, R, constraint=A.UNCONSTRAINED, forgetting=0.99, max_inner=max_iters, epsilon=eps)
+    s = A.CPStream(N, 0, R, constraint=constraint, forgetting=0.99, max_inner=max_iters, epsilon=eps)
     s.set_model(A.SPCPSTREAM)
     s.set_graph(graph)
     used, prev, inner = 0, np.zeros(N, np.int64), []
@@ -133,9 +133,10 @@ def test_spcpstream_graph_direct_and_server_agree():
     iv = synth.init_values(20000, seed=6)
     og, ig = run_sparse(b, 16, 10, 1e-5, iv, graph=True)
     od, id_ = run_sparse(b, 16, 10, 1e-5, iv, graph=False)
-    assert ig == id_
-    for a, c in zip(og, od):
-        assert np.array_equal(a, c)
+    on, in_ = run_sparse(b, 16, 10, 1e-5, iv, graph=True, constraint=A.NONNEG)  # not used by spCP-stream
+    assert ig == id_ == in_
+    for a, c, d in zip(og, od, on):
+        assert np.array_equal(a, c) and np.array_equal(a, d)
     srv = A.Server(4 << 30, workers=2)
     sid = srv.open(4, 0, 16, [len(b)] + [int(x) for x in b[-1]["dims"][1:]], 2000, model=A.SPCPSTREAM)
     used, prev = 0, np.zeros(4, np.int64)
@@ -149,3 +150,27 @@ def test_spcpstream_graph_direct_and_server_agree():
     for m in range(4):
         assert np.array_equal(srv.factor(sid, m), og[m])
     srv.destroy()
+
+
+@pytest.mark.parametrize("model,label", [("cpstream_alto", "CPSTREAM"), ("spcpstream_alto", "spCPSTREAM")])
+def test_cpd64_streaming_models(tmp_path, model, label):
+    """The rebuilt cpd64 driver runs both streaming models of the reference's
+    -l flag on a .tns file (1-based indices, time mode 0)."""
+    import os
+    import subprocess
+
+    rng = np.random.default_rng(3)
+    dims = [5, 40, 30, 20]
+    n = 600
+    cols = [rng.integers(0, d, n) for d in dims]
+    key = cols[0] * 10**6 + cols[1] * 10**4 + cols[2] * 100 + cols[3]
+    _, first = np.unique(key, return_index=True)
+    path = tmp_path / "s.tns"
+    with open(path, "w") as f:
+        for q in sorted(first):
+            f.write(" ".join(str(int(c[q]) + 1) for c in cols) + " %.6f\n" % rng.random())
+    exe = os.path.join(os.path.dirname(A.__file__), "..", "cpd64")
+    r = subprocess.run([exe, "-i", str(path), "-r", "8", "-m", "5", "-e", "1e-5", "-l", model, "-a", "0"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert f"{label} (ALTO) on the GPU: 5 batches" in r.stdout
