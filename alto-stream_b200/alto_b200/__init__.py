@@ -39,7 +39,7 @@ FIT_REFERENCE, FIT_EXACT = 0, 1
 EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
-    "alto_tensor_device_bytes", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
+    "alto_tensor_device_bytes", "alto_tensor_restrict", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph",
@@ -218,6 +218,12 @@ class AltoTensor:
         check(lib().alto_tensor_export(self.h, p(masks), p(am), p(idx), p(vals), p(perm), p(pp), p(iv)))
         return dict(masks=masks.reshape(N, 2), alto_mask=am, idx=idx[: 2 * nnz].reshape(nnz, 2),
                     vals=vals[:nnz], perm=perm[:nnz], prtn_ptr=pp, intervals=iv.reshape(P, N, 2))
+
+    def restrict(self, begin, end, stream=None):
+        """Keep line entries [begin, end) of the ALTO order (a shard; alto_tensor_restrict)."""
+        check(lib().alto_tensor_restrict(self.h, c_uint64(int(begin)), c_uint64(int(end)), _stream_handle(stream)))
+        self._refresh()
+        return self
 
     def device_bytes(self):
         b = c_uint64()

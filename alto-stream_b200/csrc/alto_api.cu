@@ -273,6 +273,15 @@ alto_status alto_tensor_device_bytes(const alto_tensor* t, uint64_t* bytes) {
   return ALTO_OK;
 }
 
+alto_status alto_tensor_restrict(alto_tensor* t, uint64_t begin, uint64_t end, alto_cuda_stream stream) {
+  if (!t || begin > end || end > t->nnz) {
+    set_error("bad tensor or range [%llu, %llu) of %llu entries", (unsigned long long)begin,
+              (unsigned long long)end, t ? (unsigned long long)t->nnz : 0ull);
+    return ALTO_ERR_INVALID;
+  }
+  return restrict_line(t, begin, end, (cudaStream_t)stream);
+}
+
 alto_status alto_tensor_destroy(alto_tensor* t) {
   delete t;
   return ALTO_OK;

@@ -496,6 +496,77 @@ static unsigned grid_for(uint64_t n, int threads) {
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Tiles, their intervals and the reference's partitions of the line (the
+// part of encoding after the sort), for t->nnz line entries.
+static alto_status finish_layout(alto_tensor* t, int nprtn, cudaStream_t st) {
+  const int N = t->nmodes;
+  const uint64_t nnz = t->nnz;
+  const uint32_t n32 = (uint32_t)nnz;
+  const LineDecode dec = t->dec;
+  // MTTKRP tiles and their intervals.  Tiles hold 4096 nonzeros, fewer for
+  // small tensors (down to 256) so the grid still has two tiles per SM: a
+  // lane group walks tile/64 nonzeros in order, so the tile size is also the
+  // length of the kernel's latency chain.
+  {
+    static int sm_count = 0;
+    if (!sm_count) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+      if (sm_count <= 0) sm_count = 148;
+    }
+    uint32_t tile = 4096;
+    while (tile > 256 && (nnz + tile - 1) / tile < 2ull * (uint64_t)sm_count) tile >>= 1;
+    t->tile_nnz = tile;
+  }
+  t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
+  ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
+    t->sorted[m].ready = false;
+    t->tile_len_sorted[m].clear();
+  }
+  t->tuned.clear();
+  if (t->ntiles) {
+    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->line.p, dec, n32, t->tile_nnz,
+                                                    t->tile_iv.as<uint32_t>());
+    ALTO_LAUNCHED();
+    std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
+    ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+    for (int m = 0; m < N; ++m) {
+      auto& v = t->tile_len_sorted[m];
+      v.resize(t->ntiles);
+      for (uint32_t k = 0; k < t->ntiles; ++k) v[k] = iv[((size_t)k * N + m) * 2 + 1];
+      std::sort(v.begin(), v.end());
+    }
+  }
+
+  // the reference's partitions
+  t->prtn_ptr.assign(nprtn + 1, 0);
+  uint64_t per = (nnz + nprtn - 1) / nprtn;
+  for (int p = 0; p < nprtn; ++p) {
+    uint64_t e = std::min<uint64_t>((uint64_t)(p + 1) * per, nnz);
+    t->prtn_ptr[p + 1] = e;
+  }
+  ALTO_TRY(t->prtn_iv.ensure((size_t)nprtn * N * 2 * 8 + (size_t)(nprtn + 1) * 8 + N * 8));
+  uint64_t* d_iv = t->prtn_iv.as<uint64_t>();
+  uint64_t* d_ptr = d_iv + (size_t)nprtn * N * 2;
+  uint64_t* d_dims = d_ptr + nprtn + 1;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(d_ptr, t->prtn_ptr.data(), (nprtn + 1) * 8, cudaMemcpyHostToDevice, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(d_dims, t->dims, N * 8, cudaMemcpyHostToDevice, st));
+  unsigned long long* d_ivu = reinterpret_cast<unsigned long long*>(d_iv);
+  prtn_interval_init_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(d_dims, N, nprtn, d_ivu);
+  ALTO_LAUNCHED();
+  if (nnz) {
+    prtn_interval_kernel<<<(unsigned)((nnz + kPrtnChunk - 1) / kPrtnChunk), 256, 0, st>>>(
+        t->line.p, dec, nnz, per, d_ivu);
+    ALTO_LAUNCHED();
+  }
+  prtn_interval_fix_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(nprtn * N, d_ivu);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
 alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st) {
   const int N = coo->nmodes;
   const uint64_t nnz = coo->nnz;
@@ -611,69 +682,26 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
     ALTO_LAUNCHED();
   }
 
-  // MTTKRP tiles and their intervals.  Tiles hold 4096 nonzeros, fewer for
-  // small tensors (down to 256) so the grid still has two tiles per SM: a
-  // lane group walks tile/64 nonzeros in order, so the tile size is also the
-  // length of the kernel's latency chain.
-  {
-    static int sm_count = 0;
-    if (!sm_count) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
-      if (sm_count <= 0) sm_count = 148;
-    }
-    uint32_t tile = 4096;
-    while (tile > 256 && (nnz + tile - 1) / tile < 2ull * (uint64_t)sm_count) tile >>= 1;
-    t->tile_nnz = tile;
-  }
-  t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
-  ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
-  for (int m = 0; m < ALTO_MAX_MODES; ++m) {
-    t->sorted[m].ready = false;
-    t->tile_len_sorted[m].clear();
-  }
-  t->tuned.clear();
-  if (t->ntiles) {
-    tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->line.p, dec, n32, t->tile_nnz,
-                                                    t->tile_iv.as<uint32_t>());
-    ALTO_LAUNCHED();
-    std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
-    ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
-    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-    for (int m = 0; m < N; ++m) {
-      auto& v = t->tile_len_sorted[m];
-      v.resize(t->ntiles);
-      for (uint32_t k = 0; k < t->ntiles; ++k) v[k] = iv[((size_t)k * N + m) * 2 + 1];
-      std::sort(v.begin(), v.end());
-    }
-  }
-
-  // the reference's partitions
-  t->prtn_ptr.assign(nprtn + 1, 0);
-  uint64_t per = (nnz + nprtn - 1) / nprtn;
-  for (int p = 0; p < nprtn; ++p) {
-    uint64_t e = std::min<uint64_t>((uint64_t)(p + 1) * per, nnz);
-    t->prtn_ptr[p + 1] = e;
-  }
-  ALTO_TRY(t->prtn_iv.ensure((size_t)nprtn * N * 2 * 8 + (size_t)(nprtn + 1) * 8 + N * 8));
-  uint64_t* d_iv = t->prtn_iv.as<uint64_t>();
-  uint64_t* d_ptr = d_iv + (size_t)nprtn * N * 2;
-  uint64_t* d_dims = d_ptr + nprtn + 1;
-  ALTO_TRY_CUDA(cudaMemcpyAsync(d_ptr, t->prtn_ptr.data(), (nprtn + 1) * 8, cudaMemcpyHostToDevice, st));
-  ALTO_TRY_CUDA(cudaMemcpyAsync(d_dims, t->dims, N * 8, cudaMemcpyHostToDevice, st));
-unsigned long long* d_ivu = reinterpret_cast<unsigned long long*>(d_iv);
-  prtn_interval_init_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(d_dims, N, nprtn, d_ivu);
-  ALTO_LAUNCHED();
-  if (nnz) {
-    prtn_interval_kernel<<<(unsigned)((nnz + kPrtnChunk - 1) / kPrtnChunk), 256, 0, st>>>(
-        t->line.p, dec, nnz, per, d_ivu);
-    ALTO_LAUNCHED();
-  }
-  prtn_interval_fix_kernel<<<(nprtn * N + 255) / 256, 256, 0, st>>>(nprtn * N, d_ivu);
-  ALTO_LAUNCHED();
+  ALTO_TRY(finish_layout(t, nprtn, st));
   if (!coo->on_device) ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // host COO must outlive the copies
   return ALTO_OK;
+}
+
+// Keep line entries [begin, end) (a shard of the nonzeros in ALTO order),
+// then rebuild tiles, intervals and partitions for them.
+alto_status restrict_line(alto_tensor* t, uint64_t begin, uint64_t end, cudaStream_t st) {
+  const uint64_t n = end - begin;
+  const size_t rb = rec_bytes(t->dec.hi_words);
+  if (begin > 0 && n > 0) {
+    ALTO_TRY(t->scratch.ensure(n * (rb + 4)));
+    char* tmp = t->scratch.as<char>();
+    ALTO_TRY_CUDA(cudaMemcpyAsync(tmp, t->line.as<char>() + begin * rb, n * rb, cudaMemcpyDeviceToDevice, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(tmp + n * rb, t->perm.as<uint32_t>() + begin, n * 4, cudaMemcpyDeviceToDevice, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(t->line.p, tmp, n * rb, cudaMemcpyDeviceToDevice, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(t->perm.p, tmp + n * rb, n * 4, cudaMemcpyDeviceToDevice, st));
+  }
+  t->nnz = n;
+  return finish_layout(t, t->nprtn, st);
 }
 
 // ------------------------------------------------ per-mode row-sorted lines

@@ -258,6 +258,8 @@ struct alto_tensor {
 namespace alto {
 // Encode (linearise, sort, lay out, partition) a COO tensor into t.
 alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st);
+// Keep line entries [begin, end) and rebuild tiles, intervals, partitions.
+alto_status restrict_line(alto_tensor* t, uint64_t begin, uint64_t end, cudaStream_t st);
 // Host-side mask setup (setup_packed_alto).
 int setup_masks(int nmodes, const uint64_t* dims, int max_bits, Key2* masks, Key2* alto_mask,
                 int* bits);

@@ -96,6 +96,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--factor-dtype", choices=["f32", "bf16"], default="f32",
                     help="factor storage (bf16 halves gather bytes; accumulation stays f32)")
+    ap.add_argument("--shard", action="store_true",
+                    help="mttkrp under torchrun: one tensor sharded over the ranks' line ranges, each step "
+                         "the local MTTKRPs plus an NCCL all-reduce of every output (strong scaling)")
     ap.add_argument("--profile-small", action="store_true",
                     help="small tensor (for ncu captures): 20M nonzeros, 1 step")
     args = ap.parse_args()
@@ -276,8 +279,15 @@ def ours(args):
     R = args.rank
     N = len(DIMS)
 
-    cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=1234 + rank, values="lognormal", device=dev)
+    # independent tensors per rank (weak scaling), or one tensor sharded
+    seed = 1234 if args.shard else 1234 + rank
+    cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=seed, values="lognormal", device=dev)
     t = A.AltoTensor(DIMS, cidx, vals, nprtn=1)
+    total_nnz = t.nnz
+    if args.shard:
+        from alto_b200 import shard
+
+        shard.shard_tensor(t, rank, world)
     nnz = t.nnz
     del cidx, vals
     torch.cuda.empty_cache()
@@ -298,6 +308,8 @@ def ours(args):
             t.mttkrp(m, factors, R, out=outs[m], accumulate=True, stream=stream)
             if ev is not None:
                 ev[m][1].record(stream)
+            if args.shard and world > 1:
+                torch.distributed.all_reduce(outs[m])
 
     for _ in range(warmup):
         step()
@@ -330,7 +342,7 @@ def ours(args):
         x = torch.tensor([elapsed], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
         elapsed = float(x.item())
-    units = nnz * R * N * steps * world
+    units = (total_nnz if args.shard else nnz * world) * R * N * steps
     value = units / elapsed
 
     # roofline of the MTTKRP kernel (per-mode launches, CUDA events on its stream)
@@ -348,7 +360,10 @@ def ours(args):
 
     # end to end through the host-buffer C-ABI entry point
     e2e = None
-    if not args.no_e2e:
+    if args.shard:
+        e2e = {"value": None, "unit": "nnz*R/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+               "note": "not measured in shard mode (the host-buffer entry point covers one rank's shard)"}
+    elif not args.no_e2e:
         hostF = [torch.empty((d, R), dtype=torch.float64, pin_memory=True) for d in DIMS]
         for h, f in zip(hostF, factors):
             h.copy_(f.float().double().cpu())
@@ -387,10 +402,13 @@ def ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "nnz*R/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": elapsed / steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "dims": DIMS, "nnz": nnz, "rank": R, "zipf": 1.2,
+            "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dims": DIMS, "nnz": total_nnz if args.shard else nnz, "rank": R,
+                       "zipf": 1.2,
                        "values": "lognormal(0,1)", "key_bits": t.key_bits, "alto_bits": alto_bits,
-                       "factor_dtype": args.factor_dtype, "parallelism": f"independent tensor per GPU x{world}",
+                       "factor_dtype": args.factor_dtype,
+                       "parallelism": (f"one tensor, line sharded over {world} GPUs + NCCL all-reduce per mode"
+                                       if args.shard else f"independent tensor per GPU x{world}"),
                        "l2": "inputs larger than L2 (line + factors > 3 GB); no flush",
                        "line_bytes_per_nnz": line_bytes_per_nnz(alto_bits),
                        "variants": [vnames.get(v, str(v)) for v in variants],

@@ -137,6 +137,15 @@ alto_status alto_tensor_info(const alto_tensor* t, int* nmodes, uint64_t* dims, 
 /* Bytes of device memory the tensor holds. */
 alto_status alto_tensor_device_bytes(const alto_tensor* t, uint64_t* bytes);
 
+/* Keep only line entries [begin, end) of the tensor's ALTO order: one
+ * GPU's shard of a sharded MTTKRP.  The shards follow the reference's
+ * partition rule (prtn_alto, include/alto.hpp:1128-1160: partition p of P
+ * is [min(p*ceil(nnz/P), nnz), min((p+1)*ceil(nnz/P), nnz))); each GPU runs
+ * its MTTKRP into a full-size output and an all-reduce (sum) gives the
+ * tensor's MTTKRP.  Dims, masks and the key layout are unchanged; tiles,
+ * intervals and partitions are rebuilt for the kept entries. */
+alto_status alto_tensor_restrict(alto_tensor* t, uint64_t begin, uint64_t end, alto_cuda_stream stream);
+
 alto_status alto_tensor_destroy(alto_tensor* t); /* destroy_alto, include/alto.hpp:584-604 */
 
 /* --------------------------------------------------------------- MTTKRP */

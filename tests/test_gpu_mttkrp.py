@@ -247,3 +247,33 @@ def test_deterministic_accumulates_and_rejects_unsupported():
         t.mttkrp(0, Fd10, 10, variant=A.DETERMINISTIC)
     with pytest.raises(A.AltoError):
         t.mttkrp(0, [f.to(torch.bfloat16) for f in Fd], R, variant=A.DETERMINISTIC)
+
+
+# ------------------------------------------------------------ shards
+
+@pytest.mark.parametrize("nparts", [1, 3, 8])
+def test_shards_sum_to_the_whole(nparts):
+    """alto_tensor_restrict: the shards' MTTKRPs add up to the whole
+    tensor's, and each shard keeps the exact keys of its line range."""
+    import torch
+
+    from alto_b200 import shard
+
+    dims = np.array([4800000, 1800000, 1800000], np.uint64)
+    cidx, vals = synth.powerlaw_coo(dims, 100000, [1.2, 1.2, 1.2], seed=21, values="lognormal")
+    R = 32
+    rng = np.random.default_rng(7)
+    Fd = to_dev([rng.uniform(-1, 1, (int(d), R)) for d in dims], torch.float32)
+    whole = A.create_alto(dims, cidx, vals)
+    keys = whole.export()
+    parts = [shard.shard_tensor(A.create_alto(dims, cidx, vals), p, nparts) for p in range(nparts)]
+    assert sum(p.nnz for p in parts) == whole.nnz
+    off = 0
+    for p in parts:
+        k = p.export()
+        assert np.array_equal(k["idx"], keys["idx"][off:off + p.nnz])
+        off += p.nnz
+    for m in range(3):
+        ref = whole.mttkrp(m, Fd, R).cpu().numpy()
+        tot = sum(p.mttkrp(m, Fd, R, variant=v).cpu().numpy() for p in parts for v in (A.AUTO,))
+        assert rel_err(tot, ref) <= 1e-5
