@@ -274,6 +274,44 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!ok[u]) continue;
+      if constexpr (NM <= 5) {
+        // exact mode count: packed FP32x2 products, the last factor fused
+        // into the running sum (acc = p f_last, or acc += p f_last)
+        float2 p2[V / 2];
+#pragma unroll
+        for (int h = 0; h < V / 2; ++h) {
+          p2[h] = __fmul2_rn(make_float2(vals[u], vals[u]), make_float2(f[u][0][2 * h], f[u][0][2 * h + 1]));
+#pragma unroll
+          for (int j = 1; j < NM - 2; ++j)
+            p2[h] = __fmul2_rn(p2[h], make_float2(f[u][j][2 * h], f[u][j][2 * h + 1]));
+        }
+        if (rows[u] != cur) {
+          if (cur != kNoRow) {
+            if (!DET)
+              flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+            else if (nrun++ == 0)
+              det_slot<R, V, G>(a, slot0, cur, sub, acc, false);
+            else
+              det_plain<R, V, G>(a.out, cur, sub, acc);
+          }
+          cur = rows[u];
+#pragma unroll
+          for (int h = 0; h < V / 2; ++h) {
+            const float2 r2 = __fmul2_rn(p2[h], make_float2(f[u][NM - 2][2 * h], f[u][NM - 2][2 * h + 1]));
+            acc[2 * h] = r2.x;
+            acc[2 * h + 1] = r2.y;
+          }
+        } else {
+#pragma unroll
+          for (int h = 0; h < V / 2; ++h) {
+            const float2 r2 = __ffma2_rn(p2[h], make_float2(f[u][NM - 2][2 * h], f[u][NM - 2][2 * h + 1]),
+                                         make_float2(acc[2 * h], acc[2 * h + 1]));
+            acc[2 * h] = r2.x;
+            acc[2 * h + 1] = r2.y;
+          }
+        }
+        continue;
+      }
       float p[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) p[q] = vals[u];
