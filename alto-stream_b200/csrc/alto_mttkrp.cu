@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
 // bit from run to run and whatever else runs on the device.
 
 constexpr uint32_t kShortChain = 64;
-constexpr uint32_t kChainSeg = 2048;  // slots per segment of a long chain
+constexpr uint32_t kChainSeg = 256;  // slots per segment of a long chain
 
 // Workspace of the long chains (device): counters, then the chains
 // {first slot, end slot, first segment, segments}, then the segments
@@ -434,13 +434,25 @@ __global__ void __launch_bounds__(256)
   for (uint32_t i = gw; i < nslots; i += nw) {
     const uint32_t row = rows[i];
     if (i > 0 && rows[i - 1] == row) continue;  // not the head of its chain
-    uint32_t lo = i + 1, hi = nslots;           // chain end: first slot with a larger row
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (rows[mid] == row)
-        lo = mid + 1;
-      else
-        hi = mid;
+    // chain end: first slot with a larger row -- the next 32 slots in one
+    // coalesced probe, a binary search beyond them
+    const uint32_t pi = i + 1 + lane;
+    const unsigned differ = __ballot_sync(0xffffffffu, pi < nslots && rows[pi] != row);
+    uint32_t lo;
+    if (differ) {
+      lo = i + 1 + __ffs(differ) - 1;
+    } else if (i + 33 >= nslots) {
+      lo = nslots;
+    } else {
+      lo = i + 33;
+      uint32_t hi = nslots;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (rows[mid] == row)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
     }
     if (lo - i > kShortChain) {
       // long chain: register it and its segments (the order of the lists
@@ -506,22 +518,49 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// One warp per long chain: its segments' sums added in segment order, then
-// added to the chain's output row.
+// One block per long chain: thread (s, q) sums segments s, s+S, ... of rank
+// quad q, then a fixed tree over s; the result is added to the chain's row.
 __global__ void __launch_bounds__(256)
     det_fix_final_kernel(const uint32_t* __restrict__ rows, int R, float* __restrict__ out, DetLong dl) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  __shared__ float4 part[256];
+  const int Q = R / 4, S = 256 / Q;
+  const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
   const uint32_t nlong = dl.counters[0];
-  for (uint32_t c = gw; c < nlong; c += nw) {
+  for (uint32_t c = blockIdx.x; c < nlong; c += gridDim.x) {
     const uint4 ch = dl.chains[c];
-    const uint32_t row = rows[ch.x];
-    for (int r = lane; r < R; r += 32) {
-      float x = 0.f;
-      for (uint32_t k = 0; k < ch.w; ++k) x += dl.segpart[(size_t)(ch.z + k) * R + r];
-      out[(size_t)row * R + r] += x;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sidx < S)
+      for (uint32_t k = sidx; k < ch.w; k += S) {
+        const float4 v = *reinterpret_cast<const float4*>(dl.segpart + (size_t)(ch.z + k) * R + q * 4);
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
+      }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int stride = S / 2; stride >= 1; stride >>= 1) {
+      if (sidx < stride) {
+        const float4 o = part[(sidx + stride) * Q + q];
+        float4& m = part[sidx * Q + q];
+        m.x += o.x;
+        m.y += o.y;
+        m.z += o.z;
+        m.w += o.w;
+      }
+      __syncthreads();
     }
+    if (sidx == 0) {
+      float4* o = reinterpret_cast<float4*>(out + (size_t)rows[ch.x] * R + q * 4);
+      float4 x = *o;
+      const float4 p = part[q];
+      x.x += p.x;
+      x.y += p.y;
+      x.z += p.z;
+      x.w += p.w;
+      *o = x;
+    }
+    __syncthreads();
   }
 }
 
@@ -747,7 +786,7 @@ static alto_status launch_det_nm(const MttkrpArgs& a, const DetLong& dl, cudaStr
   const unsigned g1 = std::min<unsigned>((nslots + 7) / 8, (unsigned)num_sms() * 16);
   det_fix_short_kernel<<<g1, 256, 0, st>>>(a.det_rows, a.det_vals, nslots, R, a.out, dl);
   ALTO_LAUNCHED();
-  det_fix_seg_kernel<<<(unsigned)num_sms() * 2, 256, 0, st>>>(a.det_vals, R, dl);
+  det_fix_seg_kernel<<<(unsigned)num_sms() * 4, 256, 0, st>>>(a.det_vals, R, dl);
   ALTO_LAUNCHED();
   det_fix_final_kernel<<<(unsigned)num_sms(), 256, 0, st>>>(a.det_rows, R, a.out, dl);
   ALTO_LAUNCHED();

@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed steps before (mttkrp 3; cpstream 3 slices; serve 1 slice per stream)")
     ap.add_argument("--workers", type=int, default=16, help="serve: server worker threads")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="cpstream: launch every inner iteration directly (no CUDA graph; for per-kernel profiles)")
     ap.add_argument("--model", choices=["cpstream", "spcpstream"], default="cpstream",
                     help="cpstream/serve: the streaming model (spcpstream: row-sparse updates, no constraint)")
     ap.add_argument("--streams", type=int, default=64, help="serve: independent streams")
@@ -523,6 +525,7 @@ def ours_cpstream(args):
     s = A.CPStream(4, 0, R, constraint=A.NONNEG, forgetting=0.95, max_inner=50, epsilon=1e-5)
     if args.model == "spcpstream":
         s.set_model(A.SPCPSTREAM)
+    s.set_graph(not args.no_graph)
     used = 0
     lat, inner, dev_ms, nbytes, h2d = [], [], [], 0, 0
     stream = torch.cuda.current_stream()
@@ -577,7 +580,8 @@ def ours_cpstream(args):
                    "slice_nnz_mean": float(np.mean([len(b["vals"]) for b in batches[W:]])),
                    "inner_iters_mean": float(np.mean(inner)), "inner_iters_max": int(np.max(inner)),
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                   "launch": "first inner iteration direct, the rest one CUDA graph per slice",
+                   "launch": ("every inner iteration launched directly" if args.no_graph
+                              else "first inner iteration direct, the rest one CUDA graph per slice"),
                    "l2": "per-slice work streams the slice and the factors (> L2 in total over a slice); no flush"},
         "roofline": {"bound": "hbm", "achieved": nbytes / dev_total / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": nbytes / dev_total / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
