@@ -310,31 +310,31 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
             acc[2 * h + 1] = r2.y;
           }
         }
-        continue;
-      }
-      float p[V];
-#pragma unroll
-      for (int q = 0; q < V; ++q) p[q] = vals[u];
-#pragma unroll
-      for (int j = 0; j < NM - 1; ++j)
-        if ((j < a.target ? j : j + 1) < a.dec.nmodes)
-#pragma unroll
-          for (int q = 0; q < V; ++q) p[q] *= f[u][j][q];
-      if (rows[u] != cur) {
-        if (cur != kNoRow) {
-          if (!DET)
-            flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
-          else if (nrun++ == 0)
-            det_slot<R, V, G>(a, slot0, cur, sub, acc, false);
-          else
-            det_plain<R, V, G>(a.out, cur, sub, acc);
-        }
-        cur = rows[u];
-#pragma unroll
-        for (int q = 0; q < V; ++q) acc[q] = p[q];
       } else {
+        float p[V];
 #pragma unroll
-        for (int q = 0; q < V; ++q) acc[q] += p[q];
+        for (int q = 0; q < V; ++q) p[q] = vals[u];
+#pragma unroll
+        for (int j = 0; j < NM - 1; ++j)
+          if ((j < a.target ? j : j + 1) < a.dec.nmodes)
+#pragma unroll
+            for (int q = 0; q < V; ++q) p[q] *= f[u][j][q];
+        if (rows[u] != cur) {
+          if (cur != kNoRow) {
+            if (!DET)
+              flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+            else if (nrun++ == 0)
+              det_slot<R, V, G>(a, slot0, cur, sub, acc, false);
+            else
+              det_plain<R, V, G>(a.out, cur, sub, acc);
+          }
+          cur = rows[u];
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[q] = p[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[q] += p[q];
+        }
       }
     }
   }
@@ -419,7 +419,7 @@ constexpr uint32_t kChainSeg = 256;  // slots per segment of a long chain
 // {first slot, end slot, first segment, segments}, then the segments
 // {chain, index in chain}, then each segment's R partial sums.
 struct DetLong {
-  uint32_t* counters;  // [0] long chains, [1] segments
+  uint32_t* counters;  // [0] long chains, [1] segments, [2] blocks of det_fix_final done
   uint4* chains;
   uint2* segs;
   float* segpart;
@@ -525,7 +525,17 @@ __global__ void __launch_bounds__(256)
   __shared__ float4 part[256];
   const int Q = R / 4, S = 256 / Q;
   const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
-  const uint32_t nlong = dl.counters[0];
+  __shared__ uint32_t s_nlong;
+  if (threadIdx.x == 0) s_nlong = dl.counters[0];
+  __syncthreads();
+  const uint32_t nlong = s_nlong;
+  // the last block to have read the counters clears them for the next call
+  // (they start at zero when the workspace is allocated)
+  if (threadIdx.x == 0 && atomicAdd(&dl.counters[2], 1u) == gridDim.x - 1) {
+    dl.counters[0] = 0;
+    dl.counters[1] = 0;
+    dl.counters[2] = 0;
+  }
   for (uint32_t c = blockIdx.x; c < nlong; c += gridDim.x) {
     const uint4 ch = dl.chains[c];
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -782,7 +792,6 @@ static alto_status launch_det_nm(const MttkrpArgs& a, const DetLong& dl, cudaStr
   mttkrp_tile_kernel<R, float, HW, false, NM, true><<<grid, kMttkrpThreads, 0, st>>>(a);
   ALTO_LAUNCHED();
   const uint32_t nslots = a.ntiles * kMttkrpWarps * LaneWidth<R>::NPW * 2;
-  ALTO_TRY_CUDA(cudaMemsetAsync(dl.counters, 0, 2 * sizeof(uint32_t), st));
   const unsigned g1 = std::min<unsigned>((nslots + 7) / 8, (unsigned)num_sms() * 16);
   det_fix_short_kernel<<<g1, 256, 0, st>>>(a.det_rows, a.det_vals, nslots, R, a.out, dl);
   ALTO_LAUNCHED();
@@ -982,7 +991,9 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     auto up = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
     const uint64_t o_chains = 256, o_segs = o_chains + up(max_chains * sizeof(uint4)),
                    o_part = o_segs + up(max_segs * sizeof(uint2)), bytes = o_part + max_segs * rank * 4;
+    const size_t before = t->det_long.bytes;  // a new allocation starts with zero counters
     ALTO_TRY(t->det_long.ensure(bytes));
+    if (t->det_long.bytes != before) ALTO_TRY_CUDA(cudaMemsetAsync(t->det_long.p, 0, 16, st));
     a.det_rows = t->det_rows.as<uint32_t>();
     a.det_vals = t->det_vals.as<float>();
     char* base = t->det_long.as<char>();

@@ -40,8 +40,6 @@
 #include "alto_dense.cuh"
 
 namespace alto {
-alto_status convert_f64_to_f32(const double* a, uint64_t n, float* b, cudaStream_t st);
-alto_status convert_f32_to_f64(const float* a, uint64_t n, double* b, cudaStream_t st);
 
 constexpr int kAdmmThreads = 256;
 constexpr int kAdmmMaxIters = 25;
@@ -52,7 +50,7 @@ struct AdmmState {
   int converged;     // the test passed
   int chunk_start;   // sweeps done before the current chunk
   int chunk_sweeps;  // sweeps of the current chunk that stand
-  int pad;
+  unsigned ticket;   // blocks of the current pass 1 done
 };
 
 // Inner-iteration bookkeeping kept on the device.
@@ -185,16 +183,6 @@ __global__ void __launch_bounds__(kAdmmThreads)
   }
 }
 
-// The historical Gram product of mode j: A = G_t(old) * prod_{m in mask}
-// (prev_U_m^T U_m), the cross Grams cached per mode.
-__global__ void hist_product_kernel(const double* __restrict__ old_gram, const double* __restrict__ cross,
-                                    unsigned mask, int N, int RR, double* __restrict__ A) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < RR; p += gridDim.x * blockDim.x) {
-    double v = old_gram ? old_gram[p] : 1.0;
-    for (int m = 0; m < N; ++m)
-      if (mask & (1u << m)) v *= cross[(size_t)m * RR + p];
-    A[p] = v;
-  }
 }
 
 // The ADMM rows of mode j: rhs formed on the fly from prev_U_j, the MTTKRP
@@ -205,11 +193,16 @@ __global__ void __launch_bounds__(kAdmmThreads)
     admm_rows_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
                      float* __restrict__ U32, double* __restrict__ primal, double* __restrict__ aux,
                      double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
-                     uint64_t I, int R, double* __restrict__ partials, const AdmmState* __restrict__ state) {
+                     uint64_t I, int R, double* __restrict__ partials, AdmmState* __restrict__ state, double tol,
+                     cudaGraphConditionalHandle h, int in_graph) {
   constexpr int M = AdmmBatch<SLOTS>::M;
   constexpr int KR = RowMap<SEG>::kRows;
   constexpr int NW = kAdmmThreads / 32;
-  if (PASS1 ? state->stop : state->chunk_sweeps == 0) return;
+  if (PASS1 && state->stop) {  // a chunk after the stop (launched directly): nothing stands
+    if (blockIdx.x == 0 && threadIdx.x == 0) state->chunk_sweeps = 0;
+    return;
+  }
+  if (!PASS1 && state->chunk_sweeps == 0) return;
   const int start = PASS1 ? state->iters : state->chunk_start;  // sweeps done before this chunk
   const int nsweeps = PASS1 ? min(kAdmmChunk, kAdmmMaxIters - start) : state->chunk_sweeps;
   const bool first = start == 0;
@@ -321,58 +314,44 @@ __global__ void __launch_bounds__(kAdmmThreads)
       for (int w = 0; w < NW; ++w) t += wsum[w][p];
       partials[(size_t)blockIdx.x * kAdmmSums + p] = t;
     }
-  }
-}
-
-// Start of an ADMM solve: clear the state, open the chunk loop.
-__global__ void admm_begin_kernel(AdmmState* __restrict__ state, cudaGraphConditionalHandle h, int in_graph) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    state->iters = 0;
-    state->stop = 0;
-    state->converged = 0;
-    state->chunk_start = 0;
-    state->chunk_sweeps = 0;
-    set_condition(h, in_graph, true);
-  }
-}
-
-// Adds the blocks' per-sweep partials (one warp per sum: lane l takes blocks
-// l, l + 32, ... in order, then a fixed butterfly; lane 0's value stands)
-// and takes the chunk's sweep count: the first sweep whose sums pass the
-// test, else every sweep of the chunk.  Launch with kAdmmSums warps.
-__global__ void admm_decide_kernel(const double* __restrict__ partials, int nblocks, double tol,
-                                   AdmmState* __restrict__ state, cudaGraphConditionalHandle h, int in_graph) {
-  __shared__ double S[kAdmmSums];
-  const bool idle = state->stop != 0;
-  const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
-  if (!idle && p < kAdmmSums) {
-    double t = 0.0;
-    for (int b = lane; b < nblocks; b += 32) t += partials[(size_t)b * kAdmmSums + p];
-    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (lane == 0) S[p] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  if (idle) {
-    state->chunk_sweeps = 0;
-    set_condition(h, in_graph, false);
-    return;
-  }
-  const int start = state->iters;
-  const int n = min(kAdmmChunk, kAdmmMaxIters - start);
-  int k = n, conv = 0;
-  for (int j = 0; j < n; ++j)
-    if (S[j * 4 + 0] <= tol * S[j * 4 + 2] && S[j * 4 + 1] <= tol * S[j * 4 + 3]) {
-      k = j + 1;
-      conv = 1;
-      break;
+    // the last block to finish adds the blocks' sums (warp per sum, lanes
+    // over blocks in order, fixed butterfly) and takes the chunk's sweep
+    // count: the first sweep whose sums pass the test, else the whole chunk
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&state->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double S[kAdmmSums];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int p = warp; p < kAdmmSums; p += NW) {
+      double t = 0.0;
+      for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(partials + (size_t)b * kAdmmSums + p);
+      for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) S[p] = t;
     }
-  state->chunk_start = start;
-  state->chunk_sweeps = k;
-  state->iters = start + k;
-  state->converged = conv;
-  state->stop = conv || start + k >= kAdmmMaxIters;
-  set_condition(h, in_graph, !state->stop);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int n = min(kAdmmChunk, kAdmmMaxIters - start);
+      int k = n, conv = 0;
+      for (int j = 0; j < n; ++j)
+        if (S[j * 4 + 0] <= tol * S[j * 4 + 2] && S[j * 4 + 1] <= tol * S[j * 4 + 3]) {
+          k = j + 1;
+          conv = 1;
+          break;
+        }
+      state->ticket = 0;
+      state->chunk_start = start;
+      state->chunk_sweeps = k;
+      state->iters = start + k;
+      state->converged = conv;
+      state->stop = conv || start + k >= kAdmmMaxIters;
+      __threadfence();
+      set_condition(h, in_graph, !state->stop);
+    }
+  }
 }
 
 // End of an inner iteration (src/streaming_cpd.cpp:1457-1482): delta = sum
@@ -402,6 +381,56 @@ __global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, 
   it->done = k + 1;
   if (stop) it->stop = 1;
   set_condition(h, in_graph, !stop && k + 1 < max_inner);
+}
+
+// The time rows after their solve set-up, one block: s = mttkrp W (float64,
+// k order) into time64 and, rounded, into the float32 factor rows; old =
+// G_t; G_t += sum_rows s s^T (the operations of apply, convert, copy and
+// rank update, in their order).
+__global__ void __launch_bounds__(256)
+    time_update_kernel(const float* __restrict__ B32, const double* __restrict__ W, uint64_t rows, int R,
+                       double* __restrict__ time64, float* __restrict__ U32, double* __restrict__ Gt,
+                       double* __restrict__ old_gram) {
+  const int RR = R * R;
+  for (uint64_t q = threadIdx.x; q < rows * R; q += blockDim.x) {
+    const uint64_t i = q / R;
+    const int c = (int)(q % R);
+    double x = 0.0;
+    for (int k = 0; k < R; ++k) x = __fma_rn((double)B32[i * R + k], W[k * R + c], x);
+    time64[q] = x;
+    U32[q] = (float)x;
+  }
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) old_gram[p] = Gt[p];
+  __syncthreads();
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) {
+    const int a = p / R, b = p % R;
+    double sv = Gt[p];
+    for (uint64_t q = 0; q < rows; ++q) sv += time64[q * R + b] * time64[q * R + a];
+    Gt[p] = sv;
+  }
+}
+
+// Per mode before its solve: the historical product A = base *
+// prod_{m in mask} src[m] (base NULL: 1), and, for a constrained mode, the
+// ADMM state cleared and its chunk loop opened.
+__global__ void mode_prep_kernel(const double* __restrict__ base, const double* __restrict__ src, unsigned mask,
+                                 int N, int RR, double* __restrict__ A, AdmmState* __restrict__ admm,
+                                 cudaGraphConditionalHandle h, int in_graph) {
+  for (int p = threadIdx.x; p < RR; p += blockDim.x) {
+    double v = base ? base[p] : 1.0;
+    for (int m = 0; m < N; ++m)
+      if (mask & (1u << m)) v *= src[(size_t)m * RR + p];
+    A[p] = v;
+  }
+  if (admm && threadIdx.x == 0) {
+    admm->iters = 0;
+    admm->stop = 0;
+    admm->converged = 0;
+    admm->chunk_start = 0;
+    admm->chunk_sweeps = 0;
+    admm->ticket = 0;
+    set_condition(h, in_graph, true);
+  }
 }
 
 // Head of the iteration graph: run the loop only if the batch goes on.
@@ -655,16 +684,15 @@ alto_status admm_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t 
   double* aux = s->aux.as<double>();
   const double tol = (double)1e-6f;
   const cudaGraphConditionalHandle h = L.in_graph ? L.admm[mode] : cudaGraphConditionalHandle{};
-  admm_begin_kernel<<<1, 32, 0, st>>>(state, h, L.in_graph);
-  ALTO_LAUNCHED();
+  // (the state was cleared and the loop opened by mode_prep_kernel)
   auto chunk = [&](cudaStream_t cs) -> alto_status {
     admm_rows_kernel<SLOTS, SEG, true><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
-        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
-    ALTO_LAUNCHED();
-    admm_decide_kernel<<<1, 32 * kAdmmSums, 0, cs>>>(part, (int)blocks, tol, state, h, L.in_graph);
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state, tol, h,
+        L.in_graph);
     ALTO_LAUNCHED();
     admm_rows_kernel<SLOTS, SEG, false><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
-        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state);
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, R, part, state, tol, h,
+        L.in_graph);
     ALTO_LAUNCHED();
     return ALTO_OK;
   };
@@ -742,21 +770,23 @@ alto_status enqueue_iteration(alto_stream_session* s, const IterLaunch& L, cudaS
   ALTO_TRY(run_mttkrp(s->at, t, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
   ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidge, 1e-12, s->W.as<double>(),
                        s->status.as<int>(), nullptr, st));
-  ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->dims[t], R,
-                            s->time64.as<double>(), st));
-  ALTO_TRY(convert_f64_to_f32(s->time64.as<double>(), s->dims[t] * R, s->U[t].as<float>(), st));
   double* Gt = G + (size_t)t * RR;
-  ALTO_TRY(rr_op(s->old_gram.as<double>(), Gt, (int)RR, 0, 0.0, st));
-  ALTO_TRY(rank_update(Gt, s->time64.as<double>(), s->dims[t], R, st));
+  time_update_kernel<<<1, 256, 0, st>>>(s->buf32.as<float>(), s->W.as<double>(), s->dims[t], R,
+                                        s->time64.as<double>(), s->U[t].as<float>(), Gt, s->old_gram.as<double>());
+  ALTO_LAUNCHED();
 
   for (int j = 0; j < N; ++j) {
     if (j == t) continue;
     const uint64_t I = s->dims[j];
     ALTO_TRY(run_mttkrp(s->at, j, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
-    // historical term: A = G_t(old) * prod_{m != j, t} prev_U_m^T U_m
-    hist_product_kernel<<<(unsigned)((RR + 255) / 256), 256, 0, st>>>(
-        s->old_gram.as<double>(), s->cross.as<double>(), all & ~(1u << j) & ~(1u << t), N, (int)RR,
-        s->ata.as<double>());
+    // historical term: A = G_t(old) * prod_{m != j, t} prev_U_m^T U_m (and,
+    // for a constrained mode, the ADMM state cleared and its loop opened)
+    const bool admm_mode = s->con != ALTO_UNCONSTRAINED;
+    mode_prep_kernel<<<1, 256, 0, st>>>(s->old_gram.as<double>(), s->cross.as<double>(), all & ~(1u << j) & ~(1u << t),
+                                        N, (int)RR, s->ata.as<double>(),
+                                        admm_mode ? s->admm_state.as<AdmmState>() : nullptr,
+                                        admm_mode && L.in_graph ? L.admm[j] : cudaGraphConditionalHandle{},
+                                        admm_mode ? L.in_graph : 0);
     ALTO_LAUNCHED();
     if (s->con == ALTO_UNCONSTRAINED) {
       ALTO_TRY(solve_setup(G, N, all & ~(1u << j), R, kSolveRidge, 1e-12, s->W.as<double>(),
@@ -895,19 +925,17 @@ alto_status enqueue_iteration_sparse(alto_stream_session* s, const IterLaunch& L
   ALTO_TRY(run_mttkrp(s->at, t, L.fac, ALTO_F32, R, s->buf32.as<float>(), 0, L.mv, st));
   ALTO_TRY(solve_setup(G, N, all & ~(1u << t), R, kSolveRidgeKeep, 1e-12, s->W.as<double>(), s->status.as<int>(),
                        nullptr, st));
-  ALTO_TRY(apply_f32_to_f64(s->buf32.as<float>(), nullptr, s->W.as<double>(), s->nnzr[t], R, s->time64.as<double>(),
-                            st));
-  ALTO_TRY(convert_f64_to_f32(s->time64.as<double>(), s->nnzr[t] * R, s->Anz[t].as<float>(), st));
-  // h_t = G_t (old), then G_t += s s^T (= c_t)
+  // s_t rows; h_t = G_t (old), then G_t += s s^T (= c_t)
   double* Gt = G + (size_t)t * RR;
-  ALTO_TRY(rr_op(H + (size_t)t * RR, Gt, (int)RR, 0, 0.0, st));
-  ALTO_TRY(rank_update(Gt, s->time64.as<double>(), s->nnzr[t], R, st));
+  time_update_kernel<<<1, 256, 0, st>>>(s->buf32.as<float>(), s->W.as<double>(), s->nnzr[t], R,
+                                        s->time64.as<double>(), s->Anz[t].as<float>(), Gt, H + (size_t)t * RR);
+  ALTO_LAUNCHED();
   for (int m = 0; m < N; ++m) {
     if (m == t) continue;
     const uint64_t I = s->nnzr[m];
     // Q = Hadamard(h) but m; Phi = Hadamard(c) but m + 1e-12 I
-    hist_product_kernel<<<(unsigned)((RR + 255) / 256), 256, 0, st>>>(nullptr, H, all & ~(1u << m), N, (int)RR,
-                                                                       s->ata.as<double>());
+    mode_prep_kernel<<<1, 256, 0, st>>>(nullptr, H, all & ~(1u << m), N, (int)RR, s->ata.as<double>(), nullptr,
+                                        cudaGraphConditionalHandle{}, 0);
     ALTO_LAUNCHED();
     ALTO_TRY(solve_setup(G, N, all & ~(1u << m), R, kSolveRidgeKeep, 1e-12, s->W.as<double>(),
                          s->status.as<int>(), nullptr, st));
