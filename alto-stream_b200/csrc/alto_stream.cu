@@ -183,8 +183,6 @@ __global__ void __launch_bounds__(kAdmmThreads)
   }
 }
 
-}
-
 // The ADMM rows of mode j: rhs formed on the fly from prev_U_j, the MTTKRP
 // and A; the primal starts from U_j (float32) and ends in U_j; between
 // chunks it is kept in float64 (prim), with aux.
