@@ -234,6 +234,87 @@ def spcpstream(batches, stream_mode, rank, max_iters, eps, init_vals, forgetting
     return outs, lam, inner
 
 
+def slice_stream(dims, cidx, vals, stream_mode, nnz_threshold=1, timeslice_limit=1):
+    """The reference's stream slicer (StreamingSparseTensor,
+    src/streaming_sptensor.cpp:69-264), restated: sort by the stream mode and
+    then the following modes cyclically (tt_sort, src/sort.cpp:477-519),
+    relabel every other mode in first-seen order over the sorted tensor, and
+    cut batches of whole time steps (next_dynamic_batch): a batch grows by
+    one time step at a time while it holds fewer than nnz_threshold nonzeros
+    and fewer than timeslice_limit steps.  Batch time indices are local;
+    the other dims are the running maximum of index + 1.  Returns a list of
+    {dims, cidx, vals}."""
+    cidx = np.asarray(cidx, np.uint64)
+    vals = np.asarray(vals, np.float64)
+    N, nnz = cidx.shape
+    t = stream_mode
+    prio = [(t + m) % N for m in range(N)]
+    perm = np.lexsort([cidx[m] for m in reversed(prio)])
+    c = cidx[:, perm].copy()
+    v = vals[perm]
+    for m in range(N):
+        if m == t:
+            continue
+        u, first = np.unique(c[m], return_index=True)
+        lab = np.zeros(int(dims[m]) if len(dims) else 0, np.uint64)
+        lab[u[np.argsort(first)]] = np.arange(len(u), dtype=np.uint64)
+        c[m] = lab[c[m]]
+    time = c[t]
+    out, batch, ptr = [], 0, 0
+    prev = np.zeros(N, np.uint64)
+    while ptr < nnz:
+        first_batch = batch
+        start = int(np.searchsorted(time, batch, side="left")) if ptr == 0 else ptr
+        start = max(start, ptr)
+        end = start
+        local = []
+        while end - start < nnz_threshold and end < nnz:
+            e2 = int(np.searchsorted(time, batch + 1, side="left"))
+            local.extend([batch - first_batch] * (e2 - end))
+            end = e2
+            batch += 1
+            if batch - first_batch >= timeslice_limit:
+                break
+        bd = np.zeros(N, np.uint64)
+        bc = c[:, start:end].copy()
+        bc[t] = np.asarray(local, np.uint64)
+        for m in range(N):
+            if m == t:
+                bd[m] = batch - first_batch
+            else:
+                mx = int(bc[m].max()) + 1 if end > start else 0
+                bd[m] = max(mx, int(prev[m]))
+                prev[m] = bd[m]
+        out.append(dict(dims=bd, cidx=bc, vals=v[start:end].copy()))
+        ptr = end
+    return out
+
+
+def ref_slice_stream(dims, cidx, vals, stream_mode, nnz_threshold=1, timeslice_limit=1, bits=64):
+    """The compiled reference's slicer over the same tensor (see the harness)."""
+    L = ref_lib(bits)
+    dims = np.ascontiguousarray(dims, np.uint64)
+    cidx = np.ascontiguousarray(cidx, np.uint64)
+    vals = np.ascontiguousarray(vals, np.float64)
+    N, nnz = cidx.shape
+    maxb = int(dims[stream_mode]) + 1
+    bdims = np.zeros(maxb * N, np.uint64)
+    bnnz = np.zeros(maxb, np.uint64)
+    oc = np.zeros(N * nnz, np.uint64)
+    ov = np.zeros(nnz, np.float64)
+    nb = L.ref_slice_stream(c_int(N), _ptr(dims), c_uint64(nnz), _ptr(cidx), _ptr(vals), c_int(stream_mode),
+                            c_uint64(nnz_threshold), c_uint64(timeslice_limit), c_int(maxb), _ptr(bdims),
+                            _ptr(bnnz), _ptr(oc), _ptr(ov))
+    out, oi, ovv = [], 0, 0
+    for b in range(nb):
+        n = int(bnnz[b])
+        out.append(dict(dims=bdims[b * N:(b + 1) * N].copy(), cidx=oc[oi:oi + N * n].reshape(N, n).copy(),
+                        vals=ov[ovv:ovv + n].copy()))
+        oi += N * n
+        ovv += n
+    return out
+
+
 # ------------------------------------------------------ compiled reference
 
 class RefTensor:

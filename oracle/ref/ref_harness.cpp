@@ -25,6 +25,7 @@
 //     GrowKruskalModel would draw them (src/kruskal_model.cpp:101-178), so the
 //     CUDA path can start from the identical state.
 #include "streaming_cpd.cpp"
+#include "streaming_sptensor.hpp"
 
 #include <cstdint>
 #include <vector>
@@ -375,6 +376,39 @@ int ref_spcpstream(int nmodes, int stream_mode, int nbatch, const uint64_t* batc
                    double** out_U, double* out_lambda, double* slice_seconds) {
   return run_stream(nmodes, stream_mode, nbatch, batch_dims, batch_nnz, cidx, vals, rank, max_iters, epsilon, 0,
                     init_vals, n_init_vals, out_U, out_lambda, slice_seconds, true);
+}
+
+// The reference's stream slicer (StreamingSparseTensor,
+// src/streaming_sptensor.cpp:69-264): sorts the tensor (tt_sort by the
+// stream mode, then the following modes cyclically), relabels every other
+// mode in first-seen order and cuts batches with next_dynamic_batch.  The
+// batches are written one after another: per batch its nmodes dims, then
+// its nmodes x nnz indices and nnz values into the flat outputs; batch_nnz
+// gets the sizes.  Returns the batch count (at most max_batches).
+int ref_slice_stream(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx, const double* vals,
+                     int stream_mode, uint64_t nnz_threshold, uint64_t timeslice_limit, int max_batches,
+                     uint64_t* batch_dims, uint64_t* batch_nnz, uint64_t* out_cidx, double* out_vals) {
+  SparseTensor* X = make_coo(nmodes, dims, nnz, cidx, vals);
+  int nb = 0;
+  {
+    StreamingSparseTensor sst(X, stream_mode);
+    size_t off_i = 0, off_v = 0;
+    while (!sst.last_batch() && nb < max_batches) {
+      SparseTensor* b = sst.next_dynamic_batch(nnz_threshold, timeslice_limit);
+      if (!b) break;
+      for (int m = 0; m < nmodes; ++m) batch_dims[(size_t)nb * nmodes + m] = b->dims[m];
+      batch_nnz[nb] = b->nnz;
+      for (int m = 0; m < nmodes; ++m)
+        for (IType q = 0; q < b->nnz; ++q) out_cidx[off_i + (size_t)m * b->nnz + q] = b->cidx[m][q];
+      for (IType q = 0; q < b->nnz; ++q) out_vals[off_v + q] = b->vals[q];
+      off_i += (size_t)nmodes * b->nnz;
+      off_v += b->nnz;
+      DestroySparseTensor(b);
+      ++nb;
+    }
+  }
+  DestroySparseTensor(X);
+  return nb;
 }
 
 }  // extern "C"

@@ -127,9 +127,34 @@ def main(ref_root):
             "colsums": [o.sum(0).tolist() for o in outs]}
 
     out_json["spcpstream_small"] = spcpstream_golden(b, iv, ntot)
+    out_json["slicer"] = slicer_golden()
 
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out_json, f, indent=1)
+
+
+SLICER_CASES = [(0, 1, 1), (0, 300, 3), (0, 10**9, 4), (2, 1, 1), (2, 300, 3), (3, 50, 100)]
+
+
+def slicer_digest(batches):
+    h = hashlib.sha256()
+    for x in batches:
+        h.update(np.ascontiguousarray(x["dims"], np.uint64).tobytes())
+        h.update(np.ascontiguousarray(x["cidx"], np.uint64).tobytes())
+        h.update(np.ascontiguousarray(x["vals"], np.float64).tobytes())
+    return h.hexdigest()
+
+
+def slicer_golden():
+    """The reference's StreamingSparseTensor batches of a seeded 4-mode tensor."""
+    dims = np.array([12, 40, 30, 20], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 2500, seed=3)
+    out = []
+    for t, thr, lim in SLICER_CASES:
+        b = O.ref_slice_stream(dims, cidx, vals, t, thr, lim)
+        out.append({"stream_mode": t, "nnz_threshold": thr, "timeslice_limit": lim, "batches": len(b),
+                    "sha256": slicer_digest(b)})
+    return out
 
 
 def spcpstream_golden(b, iv, ntot):

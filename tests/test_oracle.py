@@ -164,3 +164,21 @@ class TestAgainstCompiledReference:
         np.testing.assert_allclose(fo, fr, rtol=1e-10)
         for a, b in zip(Ur, Uo):
             np.testing.assert_allclose(b, a, rtol=1e-8, atol=1e-10)
+
+
+def test_slicer_matches_reference(golden):
+    """The stream slicer restatement against the reference's
+    StreamingSparseTensor batches (sort order, first-seen labels, batch cuts,
+    growing dims), by digest."""
+    import sys
+    import os
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden as MG
+
+    dims = np.array([12, 40, 30, 20], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 2500, seed=3)
+    for case in golden["slicer"]:
+        b = O.slice_stream(dims, cidx, vals, case["stream_mode"], case["nnz_threshold"], case["timeslice_limit"])
+        assert len(b) == case["batches"]
+        assert MG.slicer_digest(b) == case["sha256"], case
