@@ -9,7 +9,10 @@ src/streaming_cpd.cpp) over the C ABI in ``include/alto_b200.h``:
 * ``mttkrp_alto_par`` (include/alto.hpp:902) -> :func:`mttkrp_alto_par`
   (accumulates into ``factors[target_mode]`` like the reference);
 * ``cpd_alto`` (include/cpd.hpp:47) -> :func:`cpd_alto`;
-* ``cpstream`` (src/streaming_cpd.cpp:26) -> :class:`CPStream`.
+* ``cpstream`` (src/streaming_cpd.cpp:26) -> :class:`CPStream`;
+* ``StreamingSparseTensor`` (include/streaming_sptensor.hpp:10-44) ->
+  :class:`Slicer`, whose batches :meth:`CPStream.push_batch` takes as they
+  lie in device memory.
 
 The library is the CUDA build ``libalto_b200.so`` next to this file.  There
 is no CPU fallback: importing works anywhere, but every call that needs the
@@ -44,6 +47,8 @@ EXPORTED = [
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph",
     "alto_stream_close",
+    "alto_slicer_create", "alto_slicer_next", "alto_slicer_last_batch", "alto_slicer_stream_prev",
+    "alto_slicer_iperm", "alto_slicer_destroy",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
@@ -386,6 +391,14 @@ class CPStream:
                                      byref(inner)))
         return inner.value
 
+    def push_batch(self, batch, init_vals=None):
+        """Process one :class:`SliceBatch` (device memory, no copy)."""
+        iv = np.ascontiguousarray(init_vals if init_vals is not None else np.zeros(0), dtype=np.float64)
+        inner = c_int()
+        check(lib().alto_stream_push(self.h, byref(batch.coo), iv.ctypes.data_as(c_void_p), c_uint64(len(iv)),
+                                     byref(inner)))
+        return inner.value
+
     def factor(self, mode, max_rows):
         out = np.zeros((max(max_rows, 1), self.rank), np.float64)
         rows = c_uint64()
@@ -409,6 +422,105 @@ class CPStream:
     def close(self):
         if getattr(self, "h", None) and self.h.value:
             lib().alto_stream_close(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------ stream slicer
+
+class _DeviceArray:
+    """A device pointer described for torch.as_tensor (no copy)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+class SliceBatch:
+    """One batch of a :class:`Slicer`: dims (host), nnz and an alto_coo of
+    device views that stay valid until the slicer's next call."""
+
+    def __init__(self, coo, nmodes):
+        self.coo = alto_coo(coo.nmodes, coo.dims, coo.nnz, coo.cidx, coo.index_bytes, coo.vals, coo.val_dtype,
+                            coo.on_device)
+        self.nmodes = nmodes
+        self.nnz = int(coo.nnz)
+        self.dims = np.array([coo.dims[m] for m in range(nmodes)], np.uint64)
+
+    def tensors(self):
+        """(list of uint32 index tensors, value tensor): torch views of the batch."""
+        import torch
+
+        if self.nnz == 0:
+            return ([torch.zeros(0, dtype=torch.int32, device="cuda") for _ in range(self.nmodes)],
+                    torch.zeros(0, dtype=torch.float64, device="cuda"))
+        idx = [torch.as_tensor(_DeviceArray(self.coo.cidx[m], self.nnz, "<i4"), device="cuda")
+               for m in range(self.nmodes)]
+        vt = "<f8" if self.coo.val_dtype == F64 else "<f4"
+        return idx, torch.as_tensor(_DeviceArray(self.coo.vals, self.nnz, vt), device="cuda")
+
+    def to_host(self):
+        """(cidx uint64 [nmodes, nnz], vals) as numpy arrays."""
+        import torch
+
+        torch.cuda.synchronize()
+        idx, v = self.tensors()
+        c = np.zeros((self.nmodes, self.nnz), np.uint64)
+        for m in range(self.nmodes):
+            c[m] = idx[m].cpu().numpy().view(np.uint32)
+        return c, v.cpu().numpy()
+
+
+class Slicer:
+    """The reference's StreamingSparseTensor on the device (alto_slicer_*):
+    the whole tensor sorted by the stream mode and relabelled once, then cut
+    into batches of whole time steps with :meth:`next`."""
+
+    def __init__(self, dims, cidx, vals, stream_mode, stream=None):
+        self.coo_in = _Coo(dims, cidx, vals)
+        self.nmodes = len(self.coo_in.dims)
+        self.stream_mode = stream_mode
+        h = c_void_p()
+        check(lib().alto_slicer_create(byref(self.coo_in.c), c_int(stream_mode), _stream_handle(stream), byref(h)))
+        self.h = h
+        self.coo_in = None  # the slicer keeps its own copy
+
+    def next(self, nnz_threshold=1, timeslice_limit=1):
+        """next_dynamic_batch: a :class:`SliceBatch`, or None at the end."""
+        c = alto_coo()
+        got = c_int()
+        check(lib().alto_slicer_next(self.h, c_uint64(nnz_threshold), c_uint64(timeslice_limit), byref(c),
+                                     byref(got)))
+        return SliceBatch(c, self.nmodes) if got.value else None
+
+    def last_batch(self):
+        last = c_int()
+        check(lib().alto_slicer_last_batch(self.h, byref(last)))
+        return bool(last.value)
+
+    def stream_prev(self, previous):
+        """The nonzeros of the last `previous` time steps returned (or None)."""
+        c = alto_coo()
+        got = c_int()
+        check(lib().alto_slicer_stream_prev(self.h, c_uint64(previous), byref(c), byref(got)))
+        return SliceBatch(c, self.nmodes) if got.value else None
+
+    def iperm(self, mode):
+        """Original index of every label of `mode` (numpy uint64)."""
+        n = c_uint64()
+        check(lib().alto_slicer_iperm(self.h, c_int(mode), None, byref(n)))
+        out = np.zeros(max(n.value, 1), np.uint64)
+        check(lib().alto_slicer_iperm(self.h, c_int(mode), out.ctypes.data_as(c_void_p), byref(n)))
+        return out[: n.value]
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().alto_slicer_destroy(self.h)
             self.h = c_void_p()
 
     def __del__(self):

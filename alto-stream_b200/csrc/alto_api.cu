@@ -22,7 +22,8 @@ void set_error(const char* fmt, ...) {
 
 alto_status export_keys(const alto_tensor* t, uint64_t* d_out, float* d_vals, cudaStream_t st);
 
-static alto_status check_coo(const alto_coo* coo) {
+// Shape checks only (no index is read).
+alto_status check_coo_shape(const alto_coo* coo) {
   if (!coo) {
     set_error("coo is NULL");
     return ALTO_ERR_INVALID;
@@ -57,6 +58,11 @@ static alto_status check_coo(const alto_coo* coo) {
       return ALTO_ERR_INVALID;
     }
   }
+  return ALTO_OK;
+}
+
+static alto_status check_coo(const alto_coo* coo) {
+  ALTO_TRY(check_coo_shape(coo));
   if (!coo->on_device) {  // host indices are checked against dims (the reference asserts)
     for (int m = 0; m < coo->nmodes; ++m) {
       for (uint64_t i = 0; i < coo->nnz; ++i) {

@@ -660,18 +660,7 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
     // LSD radix sort over the used bits
     int cur = 0;
-    const uint32_t ntiles = (uint32_t)tiles_sort;
-    for (int shift = 0; shift < total; shift += kRadixBits) {
-      radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], n32, shift, ntiles,
-                                                         counts);
-      ALTO_LAUNCHED();
-      ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, t->scan_scratch, st));
-      radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], pm[cur], n32, shift,
-                                                            ntiles, counts, klo[cur ^ 1],
-                                                            khi[cur ^ 1], pm[cur ^ 1]);
-      ALTO_LAUNCHED();
-      cur ^= 1;
-    }
+    ALTO_TRY(radix_sort_pairs(klo, khi, pm, n32, total, counts, t->scan_scratch, st, &cur));
 
     if (coo->val_dtype == ALTO_F64)
       layout_kernel<double><<<grid_for(nnz, 256), 256, 0, st>>>(
@@ -743,6 +732,30 @@ __global__ void gather_decode3_kernel(const void* __restrict__ line, LineDecode 
   }
 }
 
+// Stable LSD radix sort of (key, payload) pairs over the low `bits` bits of a
+// 64- or 128-bit key (khi[0] NULL for 64-bit keys), ping-ponging between
+// the two buffers of each array; *cur receives the buffer holding the
+// result.  counts holds kRadix * ceil(n / kSortTile) entries.
+alto_status radix_sort_pairs(uint64_t* klo[2], uint64_t* khi[2], uint32_t* pm[2], uint32_t n, int bits,
+                             uint32_t* counts, DevBuf& scan_scratch, cudaStream_t st, int* cur_out) {
+  int cur = 0;
+  const uint32_t ntiles = (n + kSortTile - 1) / kSortTile;
+  for (int shift = 0; shift < bits && n; shift += kRadixBits) {
+    radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], n, shift, ntiles, counts);
+    ALTO_LAUNCHED();
+    ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, scan_scratch, st));
+    radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], pm[cur], n, shift, ntiles, counts,
+                                                          klo[cur ^ 1], khi[cur ^ 1], pm[cur ^ 1]);
+    ALTO_LAUNCHED();
+    cur ^= 1;
+  }
+  *cur_out = cur;
+  return ALTO_OK;
+}
+
+uint32_t sort_tiles(uint64_t n) { return (uint32_t)((n + kSortTile - 1) / kSortTile); }
+int radix_buckets() { return kRadix; }
+
 // A copy of the line ordered by the row of `mode`, ALTO order kept among
 // equal rows (stable LSD sort over the mode's bits).  This is the device
 // form of the reference's op_sched traversal (include/alto.hpp:1708-1801,
@@ -773,16 +786,8 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
     mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, mode, n32, rk[0], pm[0]);
     ALTO_LAUNCHED();
     int cur = 0;
-    const uint32_t ntiles = (uint32_t)tiles_sort;
-    for (int shift = 0; shift < t->mode_bits[mode]; shift += kRadixBits) {
-      radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(rk[cur], nullptr, n32, shift, ntiles, counts);
-      ALTO_LAUNCHED();
-      ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, t->scan_scratch, st));
-      radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(rk[cur], nullptr, pm[cur], n32, shift, ntiles,
-                                                            counts, rk[cur ^ 1], nullptr, pm[cur ^ 1]);
-      ALTO_LAUNCHED();
-      cur ^= 1;
-    }
+    uint64_t* nohi[2] = {nullptr, nullptr};
+    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, t->mode_bits[mode], counts, t->scan_scratch, st, &cur));
     if (s.hw == kDecoded3)
       gather_decode3_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, pm[cur], n32,
                                                                  s.line.as<uint4>());

@@ -465,6 +465,14 @@ __global__ void row_list_kernel(const uint32_t* __restrict__ ridx, uint64_t dims
     if (ridx[i + 1] != ridx[i]) nz[ridx[i]] = (uint32_t)i;
 }
 
+// A device batch in the spCP-stream staging layout: uint64 indices, float64 values.
+__global__ void widen_u32_kernel(const uint32_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = in[i];
+}
+__global__ void widen_f32_kernel(const float* __restrict__ in, uint64_t n, double* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = in[i];
+}
+
 __global__ void renumber_kernel(uint64_t* __restrict__ idx, uint64_t nnz, const uint32_t* __restrict__ ridx) {
   for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < nnz; q += (uint64_t)gridDim.x * blockDim.x)
     idx[q] = ridx[idx[q]];
@@ -813,10 +821,6 @@ alto_status sparse_prepare(alto_stream_session* s, const alto_coo* b, bool first
   const size_t RR = (size_t)R * R;
   cudaStream_t st = s->st;
   const uint64_t nnz = b->nnz;
-  if (b->on_device) {
-    set_error("spCP-stream batches are host COO tensors");
-    return ALTO_ERR_UNSUPPORTED;
-  }
   ALTO_TRY(s->spg.ensure(kSpKinds * N * RR * 8));
   double* spg = s->spg.as<double>();
   auto SG = [&](int kind, int m) { return spg + ((size_t)kind * N + m) * RR; };
@@ -826,7 +830,22 @@ alto_status sparse_prepare(alto_stream_session* s, const alto_coo* b, bool first
   ALTO_TRY(s->coo_val.ensure(nnz * 8));
   uint64_t* ci = s->coo_idx.as<uint64_t>();
   std::vector<uint64_t> h64;
-  for (int m = 0; m < N; ++m) {
+  const unsigned gw = (unsigned)std::min<uint64_t>((nnz + 255) / 256 + 1, 148ull * 8);
+  for (int m = 0; m < N && b->on_device; ++m) {
+    if (b->index_bytes == 8) {
+      ALTO_TRY_CUDA(cudaMemcpyAsync(ci + (size_t)m * nnz, b->cidx[m], nnz * 8, cudaMemcpyDeviceToDevice, st));
+    } else {
+      widen_u32_kernel<<<gw, 256, 0, st>>>(static_cast<const uint32_t*>(b->cidx[m]), nnz, ci + (size_t)m * nnz);
+      ALTO_LAUNCHED();
+    }
+  }
+  if (b->on_device && b->val_dtype == ALTO_F64) {
+    ALTO_TRY_CUDA(cudaMemcpyAsync(s->coo_val.p, b->vals, nnz * 8, cudaMemcpyDeviceToDevice, st));
+  } else if (b->on_device) {
+    widen_f32_kernel<<<gw, 256, 0, st>>>(static_cast<const float*>(b->vals), nnz, s->coo_val.as<double>());
+    ALTO_LAUNCHED();
+  }
+  for (int m = 0; m < N && !b->on_device; ++m) {
     const void* src = b->cidx[m];
     if (b->index_bytes == 4) {
       h64.resize(nnz);
@@ -836,9 +855,9 @@ alto_status sparse_prepare(alto_stream_session* s, const alto_coo* b, bool first
     ALTO_TRY_CUDA(cudaMemcpyAsync(ci + (size_t)m * nnz, src, nnz * 8, cudaMemcpyHostToDevice, st));
     if (b->index_bytes == 4) ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // h64 is reused
   }
-  if (b->val_dtype == ALTO_F64) {
+  if (!b->on_device && b->val_dtype == ALTO_F64) {
     ALTO_TRY_CUDA(cudaMemcpyAsync(s->coo_val.p, b->vals, nnz * 8, cudaMemcpyHostToDevice, st));
-  } else {
+  } else if (!b->on_device) {
     std::vector<double> v(nnz);
     for (uint64_t q = 0; q < nnz; ++q) v[q] = static_cast<const float*>(b->vals)[q];
     ALTO_TRY_CUDA(cudaMemcpyAsync(s->coo_val.p, v.data(), nnz * 8, cudaMemcpyHostToDevice, st));

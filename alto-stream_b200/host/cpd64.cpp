@@ -213,69 +213,29 @@ int run_als(alto_tensor* t, const Coo& X, int R, int iters, double eps) {
   return 0;
 }
 
-// StreamingSparseTensor (src/streaming_sptensor.cpp:69-264): sort by the
-// stream mode then the following modes cyclically, relabel the non-stream
-// indices in first-seen order, and cut batches of timeslice_limit time steps
-// (or until nnz_threshold).
-int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_constraint con, bool sparse,
+// StreamingSparseTensor (src/streaming_sptensor.cpp:69-264) on the device
+// (alto_slicer_*): sort by the stream mode then the following modes
+// cyclically, relabel the non-stream indices in first-seen order, and cut
+// batches of timeslice_limit time steps (or until nnz_threshold); each batch
+// goes to the session as it lies in device memory.
+int run_cpstream(const Coo& X, int R, int iters, double eps, int tmode, alto_constraint con, bool sparse,
                  uint64_t nnz_threshold, uint64_t limit, double forgetting) {
-  Coo X = X0;
   const int N = X.nmodes;
-  std::vector<uint64_t> order(X.nnz());
-  std::iota(order.begin(), order.end(), 0);
-  std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
-    for (int k = 0; k < N; ++k) {
-      int m = (tmode + k) % N;
-      if (X.cidx[m][a] != X.cidx[m][b]) return X.cidx[m][a] < X.cidx[m][b];
-    }
-    return false;
-  });
-  Coo S = X;
-  for (int m = 0; m < N; ++m)
-    for (uint64_t i = 0; i < X.nnz(); ++i) S.cidx[m][i] = X.cidx[m][order[i]];
-  for (uint64_t i = 0; i < X.nnz(); ++i) S.vals[i] = X.vals[order[i]];
-  for (int m = 0; m < N; ++m) {
-    if (m == tmode) continue;
-    std::vector<uint64_t> perm(S.dims[m], UINT64_MAX);
-    uint64_t seen = 0;
-    for (auto& ix : S.cidx[m]) {
-      if (perm[ix] == UINT64_MAX) perm[ix] = seen++;
-      ix = perm[ix];
-    }
-  }
+  std::vector<const void*> in_ptrs;
+  alto_coo in = view(X, in_ptrs);
+  alto_slicer* sl = nullptr;
+  CHECK(alto_slicer_create(&in, tmode, nullptr, &sl));
   alto_stream_session* s = nullptr;
   CHECK(alto_stream_open(N, tmode, R, con, forgetting, iters, eps, nullptr, &s));
   if (sparse) CHECK(alto_stream_set_model(s, ALTO_MODEL_SPCPSTREAM));
-  std::vector<uint64_t> prev(N, 0);
-  uint64_t ptr = 0, batch_num = 0;
   int nb = 0;
   double t0 = now();
-  while (ptr < S.nnz()) {
-    uint64_t start = ptr, end = ptr, first_batch = batch_num;
-    while (end - start < nnz_threshold && end < S.nnz()) {
-      while (end < S.nnz() && S.cidx[tmode][end] < batch_num + 1) ++end;
-      ++batch_num;
-      if (batch_num - first_batch >= limit) break;
-    }
-    Coo B;
-    B.nmodes = N;
-    B.dims.assign(N, 0);
-    B.cidx.assign(N, {});
-    B.vals.assign(S.vals.begin() + start, S.vals.begin() + end);
-    for (int m = 0; m < N; ++m) {
-      B.cidx[m].assign(S.cidx[m].begin() + start, S.cidx[m].begin() + end);
-      if (m == tmode) {
-        for (auto& ix : B.cidx[m]) ix -= first_batch;
-        B.dims[m] = batch_num - first_batch;
-      } else {
-        uint64_t mx = 0;
-        for (auto ix : B.cidx[m]) mx = std::max(mx, ix);
-        B.dims[m] = std::max(mx + 1, prev[m]);
-        prev[m] = B.dims[m];
-      }
-    }
-    ptr = end;
-    if (B.nnz() == 0) continue;
+  for (;;) {
+    alto_coo B;
+    int got = 0;
+    CHECK(alto_slicer_next(sl, nnz_threshold, limit, &B, &got));
+    if (!got) break;
+    if (B.nnz == 0) continue;
     std::vector<double> init;
     static std::vector<uint64_t> have(ALTO_MAX_MODES, 0);
     for (int m = 0; m < N; ++m) {
@@ -283,17 +243,16 @@ int run_cpstream(const Coo& X0, int R, int iters, double eps, int tmode, alto_co
       for (uint64_t q = have[m] * R; q < d * R; ++q) init.push_back(rand_val());
       have[m] = d;
     }
-    std::vector<const void*> ptrs;
-    alto_coo c = view(B, ptrs);
     int inner = 0;
-    CHECK(alto_stream_push(s, &c, init.data(), init.size(), &inner));
+    CHECK(alto_stream_push(s, &B, init.data(), init.size(), &inner));
     ++nb;
-    fprintf(stderr, "batch %d: %llu nnz, %d inner iterations\n", nb, (unsigned long long)B.nnz(), inner);
+    fprintf(stderr, "batch %d: %llu nnz, %d inner iterations\n", nb, (unsigned long long)B.nnz, inner);
   }
   double el = now() - t0;
   printf("%s (ALTO) on the GPU: %d batches in %f s (%f s/batch)\n", sparse ? "spCPSTREAM" : "CPSTREAM", nb, el,
          nb ? el / nb : 0.0);
   alto_stream_close(s);
+  alto_slicer_destroy(sl);
   return 0;
 }
 

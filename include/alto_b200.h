@@ -266,6 +266,44 @@ alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model mode
 alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
 alto_status alto_stream_close(alto_stream_session* s);
 
+/* ---------------------------------------------------------- stream slicer */
+
+/* The reference's StreamingSparseTensor (include/streaming_sptensor.hpp:10-44)
+ * on the device.  A whole tensor is sorted by the stream mode, then the
+ * following modes cyclically (tt_sort, src/sort.cpp:477-519), and every
+ * other mode is relabelled in first-seen order; batches of whole time steps
+ * are then cut from it.  Batches are device views (index_bytes 4, the input's
+ * value type, on_device 1) that alto_stream_push takes directly. */
+typedef struct alto_slicer alto_slicer;
+
+/* StreamingSparseTensor(sp, stream_mode), src/streaming_sptensor.cpp:69-125.
+ * coo: host or device COO; dims[m] < 2^32, nmodes * (nnz + 1) < 2^32 and
+ * the bits of all dims <= 128 (ALTO_ERR_UNSUPPORTED otherwise); an index
+ * outside its mode is ALTO_ERR_INVALID.  Synchronous. */
+alto_status alto_slicer_create(const alto_coo* coo, int stream_mode, alto_cuda_stream stream,
+                               alto_slicer** out);
+/* next_dynamic_batch(nnz_threshold, timeslice_limit), :196-264: grow the
+ * batch by whole time steps while it holds fewer than nnz_threshold
+ * nonzeros and fewer than timeslice_limit steps.  *batch receives views
+ * that stay valid until the next call on s (its dims and pointer arrays
+ * are owned by s); the stream-mode indices are local to the batch.
+ * *got = 0 once every nonzero was returned (the reference returns NULL).
+ * A run of time steps without nonzeros gives a batch with nnz 0, as the
+ * reference does when built without assertions (it asserts nnz > 0). */
+alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit,
+                             alto_coo* batch, int* got);
+/* last_batch(), :266-269. */
+alto_status alto_slicer_last_batch(const alto_slicer* s, int* last);
+/* stream_prev(previous), :284-327: the nonzeros of the last `previous` time
+ * steps returned so far, time indices relative to the first of them; other
+ * dims as of the last batch.  Valid until the next stream_prev call. */
+alto_status alto_slicer_stream_prev(alto_slicer* s, uint64_t previous, alto_coo* out, int* got);
+/* The original index of every label of `mode` (the Permutation iperms the
+ * reference keeps, :92-124) to host memory; *count receives how many
+ * (host_out may be NULL to ask for the count). */
+alto_status alto_slicer_iperm(alto_slicer* s, int mode, uint64_t* host_out, uint64_t* count);
+alto_status alto_slicer_destroy(alto_slicer* s);
+
 /* -------------------------------------------------------------- serving */
 
 /* A server for many independent CP-stream tensors (the reference has none;

@@ -282,7 +282,10 @@ def slice_stream(dims, cidx, vals, stream_mode, nnz_threshold=1, timeslice_limit
             if m == t:
                 bd[m] = batch - first_batch
             else:
-                mx = int(bc[m].max()) + 1 if end > start else 0
+                # an empty batch counts as max index 0 (dim = 0 + 1): the
+                # reference asserts nnz > 0 first (:229), so this is its
+                # behaviour with assertions compiled out
+                mx = int(bc[m].max()) + 1 if end > start else 1
                 bd[m] = max(mx, int(prev[m]))
                 prev[m] = bd[m]
         out.append(dict(dims=bd, cidx=bc, vals=v[start:end].copy()))
