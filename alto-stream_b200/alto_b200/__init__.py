@@ -443,14 +443,17 @@ class _DeviceArray:
 
 class SliceBatch:
     """One batch of a :class:`Slicer`: dims (host), nnz and an alto_coo of
-    device views that stay valid until the slicer's next call."""
+    device views into the slicer's arrays, valid while the slicer lives (the
+    host-side dims and pointers are copied here)."""
 
     def __init__(self, coo, nmodes):
-        self.coo = alto_coo(coo.nmodes, coo.dims, coo.nnz, coo.cidx, coo.index_bytes, coo.vals, coo.val_dtype,
-                            coo.on_device)
         self.nmodes = nmodes
         self.nnz = int(coo.nnz)
         self.dims = np.array([coo.dims[m] for m in range(nmodes)], np.uint64)
+        self._ptrs = (c_void_p * nmodes)(*[coo.cidx[m] for m in range(nmodes)])
+        self.coo = alto_coo(coo.nmodes, self.dims.ctypes.data_as(POINTER(c_uint64)), coo.nnz,
+                            ctypes.cast(self._ptrs, POINTER(c_void_p)), coo.index_bytes, coo.vals, coo.val_dtype,
+                            coo.on_device)
 
     def tensors(self):
         """(list of uint32 index tensors, value tensor): torch views of the batch."""

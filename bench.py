@@ -46,6 +46,14 @@ Two more workloads print their own line:
                         slices/s, served under an 80 GB HBM budget; metric
                         slices/s with p50/p99 latency, against the plain path
                         (one slice at a time, each stream's session in turn).
+  --workload slice      the stream slicer (StreamingSparseTensor) over the
+                        CP-stream workload's shape as one 4-mode tensor:
+                        200 time steps with log-normal nonzero counts
+                        (median 2e5, sigma 1, clipped to [5e4, 2e6]),
+                        100,000 x 100,000 x 10,000 Zipf(1.1) coordinates,
+                        int64 indices and float64 values in HBM.  A step is
+                        the sort, the first-seen relabel and all 200
+                        single-step batches; metric nonzeros/s.
 """
 from __future__ import annotations
 
@@ -76,7 +84,7 @@ WORKLOAD = "powerlaw3d-4.8Mx1.8Mx1.8M-140Mnnz-zipf1.2-R32-allmode"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve"], default="mttkrp")
+    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve", "slice"], default="mttkrp")
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (mttkrp: all-mode MTTKRPs, default 10; cpstream: slices, default 197; "
                          "serve: slices per stream, default 7)")
@@ -102,9 +110,9 @@ def parse():
                     help="mttkrp under torchrun: one tensor sharded over the ranks' line ranges, each step "
                          "the local MTTKRPs plus an NCCL all-reduce of every output (strong scaling)")
     ap.add_argument("--profile-small", action="store_true",
-                    help="small tensor (for ncu captures): 20M nonzeros, 1 step")
+                    help="small case for ncu captures (mttkrp: 20M nonzeros; slice: a quarter of the tensor), 1 step")
     args = ap.parse_args()
-    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1)}[args.workload]
+    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1), "slice": (20, 3)}[args.workload]
     if args.steps is None:
         args.steps = defaults[0]
     if args.warmup is None:
@@ -797,8 +805,209 @@ def reference_stream_arm(args):
     return 0
 
 
+SLICE_METRIC = "stream slicer nnz/s (sort by time, first-seen relabel, every single-step batch)"
+SLICE_WORKLOAD = "c4-shape-one-tensor-200x100kx100kx10k-lognormal-steps-zipf1.1"
+SLICE_DIMS = [200, 100000, 100000, 10000]
+SLICE_SEED = 77
+SLICE_CPU_SAMPLE = 6_000_000
+
+
+def slice_counts():
+    import numpy as np
+
+    rng = np.random.default_rng(SLICE_SEED)
+    return np.clip(rng.lognormal(np.log(2e5), 1.0, SLICE_DIMS[0]), 5e4, 2e6).astype(np.int64)
+
+
+def slice_tensor(dev, scale=1.0):
+    """The slicer workload on the device: int64 index columns, float64 values
+    (scale < 1 shrinks every time step's count, for profiler captures)."""
+    import torch
+
+    from alto_b200 import synth
+
+    counts = (slice_counts() * scale).astype("int64")
+    n = int(counts.sum())
+    sp, v = synth.zipf_coo_device(SLICE_DIMS[1:], n, [1.1, 1.1, 1.1], seed=SLICE_SEED, device=dev)
+    n = sp.shape[1]
+    g = torch.Generator(device=dev)
+    g.manual_seed(SLICE_SEED + 1)
+    time_col = torch.repeat_interleave(torch.arange(SLICE_DIMS[0], device=dev),
+                                       torch.as_tensor(counts, device=dev))[:n]
+    time_col = time_col[torch.randperm(n, generator=g, device=dev)].contiguous()
+    cols = [time_col] + [sp[m].contiguous() for m in range(3)]
+    return cols, v.double()
+
+
+def ref_slice_rate(cols, vals, n):
+    """The reference's StreamingSparseTensor (oracle/_ref: tt_sort, relabel,
+    next_dynamic_batch per time step, batches copied out) on the first n
+    nonzeros (a uniform sample: the order is random); (nnz/s, threads, n)."""
+    import numpy as np
+
+    import oracle as O
+
+    L = O.ref_lib(64)
+    threads = os.cpu_count() or 1
+    L.ref_set_threads(threads)
+    c = np.stack([x[:n].cpu().numpy().astype(np.uint64) for x in cols])
+    v = vals[:n].cpu().numpy()
+    t0 = time.perf_counter()
+    with stdout_to_stderr():
+        O.ref_slice_stream(np.array(SLICE_DIMS, np.uint64), c, v, 0, 1, 1)
+    sec = time.perf_counter() - t0
+    return c.shape[1] / sec, threads, c.shape[1]
+
+
+def ours_slice(args):
+    import numpy as np
+    import torch
+
+    import alto_b200 as A
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    if args.profile_small:  # a quarter of the tensor, one warm-up and one timed step
+        args.steps, args.warmup, args.no_e2e, args.no_cpu_baseline = 1, 1, True, True
+    cols, vals = slice_tensor(dev, 0.25 if args.profile_small else 1.0)
+    nnz = cols[0].numel()
+    N = len(SLICE_DIMS)
+    stream = torch.cuda.current_stream()
+
+    def one(cidx, v):
+        sl = A.Slicer(SLICE_DIMS, cidx, v, 0)
+        first = None
+        nb = 0
+        while True:
+            b = sl.next(1, 1)
+            if b is None:
+                break
+            first = first or b
+            nb += 1
+        return sl, first, nb
+
+    for _ in range(args.warmup):
+        one(cols, vals)[0].close()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = A.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    nbs = []
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        sl, _, nb = one(cols, vals)
+        ev[k][1].record(stream)
+        nbs.append(nb)
+        sl.close()
+    torch.cuda.synchronize()
+    launches = A.kernel_launches() - launches0
+    clocks = sampler.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    step_ms = sum(ms) / len(ms)
+    value = nnz / (step_ms * 1e-3)
+
+    # end to end through the C ABI: host COO (the reference's uint64 indices
+    # and float64 values, pinned) in, every batch's indices and values back
+    # into pinned host memory
+    h_idx = torch.empty((N, nnz), dtype=torch.int64, pin_memory=True)
+    for m in range(N):
+        h_idx[m].copy_(cols[m])
+    h_val = torch.empty(nnz, dtype=torch.float64, pin_memory=True)
+    h_val.copy_(vals)
+    hc = h_idx.numpy().view(np.uint64)  # one pinned [N, nnz] block: passed without a host copy
+    hv = h_val.numpy()
+    o_idx = [torch.empty(nnz, dtype=torch.int32, pin_memory=True) for _ in range(N)]
+    o_val = torch.empty(nnz, dtype=torch.float64, pin_memory=True)
+    e2e_ms = []
+    for _ in range(0 if args.no_e2e else max(args.e2e_steps, 1) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sl, first, _ = one(hc, hv)
+        # the batches are consecutive ranges of the slicer's arrays: one copy per array
+        for m in range(N):
+            o_idx[m].copy_(torch.as_tensor(A._DeviceArray(first.coo.cidx[m], nnz, "<i4"), device="cuda"),
+                           non_blocking=True)
+        o_val.copy_(torch.as_tensor(A._DeviceArray(first.coo.vals, nnz, "<f8"), device="cuda"), non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        sl.close()
+    e2e_ms = e2e_ms[1:]
+    e2e_val = nnz / (statistics.median(e2e_ms) * 1e-3) if e2e_ms else None
+
+    peak, peak_kind = measured_peaks()
+    algo = nnz * (N * 8 + 8) + nnz * (N * 4 + 8)
+    achieved = algo / (step_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "slicer_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            t = json.load(f)
+        traffic = t["bytes_per_nnz"] * nnz
+    line = {
+        "metric": SLICE_METRIC, "value": value, "unit": "nnz/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32+u64", "data": "synthetic",
+        "config": {"workload": SLICE_WORKLOAD, "nnz": nnz, "dims": SLICE_DIMS, "stream_mode": 0,
+                   "nnz_threshold": 1, "timeslice_limit": 1, "batches": nbs[0],
+                   "step_ms_min": min(ms), "step_ms_max": max(ms),
+                   "l2": "input (%.1f GB) exceeds L2; no flush" % (nnz * 40 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "kernel": "the whole slicing (all kernels of a step)",
+                     "algorithmic_bytes": "per nonzero: 4 int64 indices + a float64 value read once, "
+                                          "4 uint32 indices + a float64 value written once (64 B)",
+                     "peak_kind": peak_kind},
+        "cpu_baseline": None,
+        "e2e": {"value": e2e_val, "unit": "nnz/s", "h2d_bytes_per_step": nnz * (N * 8 + 8),
+                "d2h_bytes_per_step": nnz * (N * 4 + 8),
+                "api": "alto_slicer_create (host COO) + alto_slicer_next per batch + batch contents to host"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            rate, threads, n = ref_slice_rate(cols, vals, args.cpu_sample if args.cpu_sample != CPU_SAMPLE_NNZ
+                                              else SLICE_CPU_SAMPLE)
+            line["cpu_baseline"] = {"value": rate, "unit": "nnz/s", "cores": threads, "kind": "reference",
+                                    "sample": f"first {n} nonzeros (uniform sample), all single-step batches"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "nnz/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+    return 0
+
+
+def reference_slice_arm(args):
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
+    try:
+        import torch
+
+        cols, vals = slice_tensor(torch.device("cuda", 0)) if torch.cuda.is_available() else (None, None)
+        if cols is None:
+            raise RuntimeError("the workload generator needs a GPU")
+        rate, threads, n = ref_slice_rate(cols, vals, SLICE_CPU_SAMPLE)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
+        return 0
+    print(json.dumps({
+        "impl": "reference", "metric": SLICE_METRIC, "value": rate, "unit": "nnz/s", "n_gpus": args.gpus,
+        "steps": 1, "warmup": 0, "ms_per_step": n / rate * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": {"workload": SLICE_WORKLOAD},
+        "cpu_baseline": {"value": rate, "unit": "nnz/s", "cores": threads, "kind": "reference",
+                         "sample": f"first {n} nonzeros (uniform sample), all single-step batches"},
+        "e2e": {"value": rate, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "slice":
+        return reference_slice_arm(args) if args.impl == "reference" else ours_slice(args)
     if args.workload != "mttkrp":
         if args.impl == "reference":
             return reference_stream_arm(args)

@@ -284,9 +284,11 @@ alto_status alto_slicer_create(const alto_coo* coo, int stream_mode, alto_cuda_s
                                alto_slicer** out);
 /* next_dynamic_batch(nnz_threshold, timeslice_limit), :196-264: grow the
  * batch by whole time steps while it holds fewer than nnz_threshold
- * nonzeros and fewer than timeslice_limit steps.  *batch receives views
- * that stay valid until the next call on s (its dims and pointer arrays
- * are owned by s); the stream-mode indices are local to the batch.
+ * nonzeros and fewer than timeslice_limit steps.  *batch receives views of
+ * s's device arrays (consecutive batches are consecutive ranges of them),
+ * valid until alto_slicer_destroy; its host dims and cidx arrays belong to
+ * s and are overwritten by the next call.  The stream-mode indices are
+ * local to the batch.
  * *got = 0 once every nonzero was returned (the reference returns NULL).
  * A run of time steps without nonzeros gives a batch with nnz 0, as the
  * reference does when built without assertions (it asserts nnz > 0). */
