@@ -10,6 +10,8 @@ src/streaming_cpd.cpp) over the C ABI in ``include/alto_b200.h``:
   (accumulates into ``factors[target_mode]`` like the reference);
 * ``cpd_alto`` (include/cpd.hpp:47) -> :func:`cpd_alto`;
 * ``cpstream`` (src/streaming_cpd.cpp:26) -> :class:`CPStream`;
+* ``ImportSparseTensor`` / ``ExportSparseTensor`` (src/sptensor.cpp:22-249)
+  -> :func:`read_tensor` (parsed on the device) / :func:`write_tensor`;
 * ``StreamingSparseTensor`` (include/streaming_sptensor.hpp:10-44) ->
   :class:`Slicer`, whose batches :meth:`CPStream.push_batch` takes as they
   lie in device memory.
@@ -47,6 +49,7 @@ EXPORTED = [
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph",
     "alto_stream_close",
+    "alto_read_tensor", "alto_dcoo_view", "alto_dcoo_stats", "alto_dcoo_to_host", "alto_dcoo_destroy", "alto_write_tensor",
     "alto_slicer_create", "alto_slicer_next", "alto_slicer_last_batch", "alto_slicer_stream_prev",
     "alto_slicer_iperm", "alto_slicer_destroy",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
@@ -429,6 +432,69 @@ class CPStream:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------- tensor files
+
+TEXT, BINARY = 0, 1  # the reference's FileFormat
+
+
+class DeviceCoo:
+    """A tensor read from a file into device memory (alto_read_tensor):
+    uint64 indices and float64 values, the reference's IType and FType."""
+
+    def __init__(self, path, binary=False, zero_based=False, stream=None):
+        h = c_void_p()
+        check(lib().alto_read_tensor(str(path).encode(), c_int(BINARY if binary else TEXT),
+                                     c_int(1 if zero_based else 0), _stream_handle(stream), byref(h)))
+        self.h = h
+        self.coo = alto_coo()
+        check(lib().alto_dcoo_view(self.h, byref(self.coo)))
+        self.nmodes = int(self.coo.nmodes)
+        self.nnz = int(self.coo.nnz)
+        self.dims = np.array([self.coo.dims[m] for m in range(self.nmodes)], np.uint64)
+
+    def tensors(self):
+        """(list of int64 index tensors, float64 value tensor): torch views."""
+        import torch
+
+        idx = [torch.as_tensor(_DeviceArray(self.coo.cidx[m], self.nnz, "<i8"), device="cuda")
+               for m in range(self.nmodes)]
+        return idx, torch.as_tensor(_DeviceArray(self.coo.vals, self.nnz, "<f8"), device="cuda")
+
+    def to_host(self):
+        """(cidx uint64 [nmodes, nnz], vals float64) as numpy arrays (alto_dcoo_to_host)."""
+        c = np.zeros((self.nmodes, self.nnz), np.uint64)
+        v = np.zeros(self.nnz)
+        check(lib().alto_dcoo_to_host(self.h, c.ctypes.data_as(c_void_p), v.ctypes.data_as(c_void_p)))
+        return c, v
+
+    def stats(self):
+        r, p, fb, hv = c_double(), c_double(), c_uint64(), c_uint64()
+        check(lib().alto_dcoo_stats(self.h, byref(r), byref(p), byref(fb), byref(hv)))
+        return {"read_ms": r.value, "parse_ms": p.value, "file_bytes": fb.value, "host_values": hv.value}
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().alto_dcoo_destroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_tensor(path, binary=False, zero_based=False, stream=None):
+    """ImportSparseTensor into device memory: a :class:`DeviceCoo`."""
+    return DeviceCoo(path, binary, zero_based, stream)
+
+
+def write_tensor(path, dims, cidx, vals, binary=False):
+    """ExportSparseTensor of a host (numpy) or device (torch) COO tensor."""
+    coo = _Coo(dims, cidx, vals)
+    check(lib().alto_write_tensor(str(path).encode(), c_int(BINARY if binary else TEXT), byref(coo.c)))
 
 
 # ------------------------------------------------------------ stream slicer

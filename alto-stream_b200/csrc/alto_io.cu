@@ -1,0 +1,753 @@
+// Tensor files (the reference's ImportSparseTensor / ExportSparseTensor,
+// src/sptensor.cpp:22-249), with the parse on the device.
+//
+// Text (.tns) import.  The file is streamed through two pinned staging
+// buffers into HBM; then, all on the device:
+//   1. per 16 KiB tile, the newlines that start a line (tns_count_kernel),
+//      an exclusive scan over the tiles, and the start of every line
+//      (tns_starts_kernel);
+//   2. per line, getline's validity rule (more than one byte read, not a
+//      '#' comment) and the first valid line (tns_valid_kernel), and an
+//      exclusive scan giving every valid line its nonzero slot;
+//   3. per valid line, the reference's own parse (tns_parse_kernel): nmodes
+//      strtoull calls (exact, including sign, overflow and no-digit cases)
+//      and one strtod.  Decimal values whose significand fits 19 digits and
+//      whose value is exact in Clinger's fast path (significand <= 2^53,
+//      power of ten <= 10^22, so one correctly rounded IEEE multiply or
+//      divide) are converted on the device; any other value text
+//      (hexadecimal, inf/nan, long significands, large exponents) is
+//      listed and converted on the host with the C library's strtod from
+//      the file itself, so every value equals the reference's bit for bit.
+// The mode count comes from the first valid line, split on space and tab as
+// the reference's strtok does (the newline stays in the last token).
+//
+// Binary import streams the file's index and value arrays straight into one
+// device buffer.  Export formats on the host with all cores ("%llu " of index
+// + 1, "%g\n" of the value; integral values below 1e6 are written digit by
+// digit, which is what %g prints for them) and writes in order.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+
+#include "alto_internal.cuh"
+
+namespace alto {
+alto_status check_coo_shape(const alto_coo* coo);
+}
+
+using namespace alto;
+
+struct alto_dcoo {
+  int nmodes = 0;
+  uint64_t nnz = 0;
+  uint64_t dims[ALTO_MAX_MODES] = {};
+  DevBuf raw;  // [nmodes][nnz] uint64 indices, then [nnz] float64 values
+  const void* ptrs[ALTO_MAX_MODES] = {};
+  double read_ms = 0, parse_ms = 0;
+  uint64_t file_bytes = 0, host_lines = 0;
+};
+
+namespace {
+
+constexpr int kIoThreads = 256;
+constexpr int kIoBytesPerThread = 64;
+constexpr uint64_t kIoTile = (uint64_t)kIoThreads * kIoBytesPerThread;  // 16 KiB
+constexpr size_t kStage = 64ull << 20;                                   // pinned staging buffer
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t ws[kIoThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  uint32_t pre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kIoThreads / 32; ++w) {
+    if (w < warp) pre += ws[w];
+    tot += ws[w];
+  }
+  __syncthreads();
+  *total = tot;
+  return pre + x - v;
+}
+
+// Newlines at positions < size - 1 in this thread's 64 bytes (the buffer is
+// zero-padded to a whole tile, so the 16-byte loads stay inside it).
+__device__ __forceinline__ uint32_t count_nl(const uint4* __restrict__ buf, uint64_t base, uint64_t size) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < kIoBytesPerThread / 16; ++k) {
+    const uint4 w = buf[base / 16 + k];
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const uint64_t p = base + k * 16 + j * 4 + b;
+        c += (((ws[j] >> (8 * b)) & 0xffu) == '\n' && p + 1 < size) ? 1u : 0u;
+      }
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(kIoThreads)
+    tns_count_kernel(const uint4* __restrict__ buf, uint64_t size, uint32_t* __restrict__ tile_nl) {
+  const uint64_t base = blockIdx.x * kIoTile + threadIdx.x * (uint64_t)kIoBytesPerThread;
+  uint32_t tot;
+  block_excl_scan(count_nl(buf, base, size), &tot);
+  if (threadIdx.x == 0) tile_nl[blockIdx.x] = tot;
+}
+
+// starts[0] = 0; starts[1 + k] = position after the k-th line-starting newline.
+__global__ void __launch_bounds__(kIoThreads)
+    tns_starts_kernel(const uint4* __restrict__ buf, uint64_t size, const uint32_t* __restrict__ tile_base,
+                      uint64_t* __restrict__ starts) {
+  const uint64_t base = blockIdx.x * kIoTile + threadIdx.x * (uint64_t)kIoBytesPerThread;
+  uint32_t tot;
+  uint32_t r = tile_base[blockIdx.x] + block_excl_scan(count_nl(buf, base, size), &tot);
+  if (blockIdx.x == 0 && threadIdx.x == 0) starts[0] = 0;
+  const unsigned char* b8 = reinterpret_cast<const unsigned char*>(buf);
+  for (int k = 0; k < kIoBytesPerThread; ++k) {
+    const uint64_t p = base + k;
+    if (b8[p] == '\n' && p + 1 < size) starts[1 + r++] = p + 1;
+  }
+}
+
+// valid[l] = getline read more than one byte and the line is not a comment.
+__global__ void tns_valid_kernel(const unsigned char* __restrict__ buf, uint64_t size,
+                                 const uint64_t* __restrict__ starts, uint32_t nlines, uint32_t* __restrict__ valid,
+                                 uint32_t* __restrict__ first_valid) {
+  for (uint64_t l = blockIdx.x * blockDim.x + threadIdx.x; l <= nlines; l += gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+    if (l < nlines) {
+      const uint64_t s = starts[l], e = l + 1 < nlines ? starts[l + 1] : size;
+      v = (e - s > 1 && buf[s] != '#') ? 1u : 0u;
+      if (v) atomicMin(first_valid, (uint32_t)l);
+    }
+    valid[l] = v;
+  }
+}
+
+// 10^0 .. 10^22, every one exact in float64.
+__constant__ double c_p10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                 1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+__device__ __forceinline__ bool is_space(unsigned c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
+}
+
+// strtoull(p, &end, 10) within [p, e) (a NUL ends the string as in C).
+__device__ uint64_t dev_strtoull(const unsigned char* __restrict__ buf, uint64_t& p, uint64_t e) {
+  uint64_t q = p;
+  while (q < e && buf[q] && is_space(buf[q])) ++q;
+  bool neg = false;
+  if (q < e && (buf[q] == '+' || buf[q] == '-')) {
+    neg = buf[q] == '-';
+    ++q;
+  }
+  uint64_t v = 0;
+  bool any = false, over = false;
+  while (q < e && buf[q] >= '0' && buf[q] <= '9') {
+    const uint64_t d = buf[q] - '0';
+    if (v > (~0ull - d) / 10) over = true;
+    v = v * 10 + d;
+    any = true;
+    ++q;
+  }
+  if (!any) return 0;  // no conversion: the end pointer stays at p
+  p = q;
+  if (over) return ~0ull;
+  return neg ? (uint64_t)(0 - v) : v;
+}
+
+// strtod's decimal fast path; false when the host must convert the text.
+__device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, uint64_t e, double& out) {
+  uint64_t q = p;
+  while (q < e && buf[q] && is_space(buf[q])) ++q;
+  bool neg = false;
+  if (q < e && (buf[q] == '+' || buf[q] == '-')) {
+    neg = buf[q] == '-';
+    ++q;
+  }
+  if (q < e) {  // hexadecimal, inf, nan: the host converts
+    const unsigned c = buf[q] | 0x20u;
+    if (c == 'i' || c == 'n') return false;
+    if (buf[q] == '0' && q + 1 < e && (buf[q + 1] | 0x20u) == 'x') return false;
+  }
+  uint64_t w = 0;
+  int nd = 0, ex = 0;
+  bool any = false;
+  while (q < e && buf[q] >= '0' && buf[q] <= '9') {
+    const unsigned d = buf[q] - '0';
+    any = true;
+    if (w != 0 || d != 0) {  // (leading zeros carry no digit)
+      if (nd == 19) return false;
+      w = w * 10 + d;
+      ++nd;
+    }
+    ++q;
+  }
+  if (q < e && buf[q] == '.') {
+    ++q;
+    while (q < e && buf[q] >= '0' && buf[q] <= '9') {
+      const unsigned d = buf[q] - '0';
+      any = true;
+      if (w != 0 || d != 0) {
+        if (nd == 19) return false;
+        w = w * 10 + d;
+        ++nd;
+      }
+      --ex;
+      ++q;
+    }
+  }
+  if (!any) {  // no conversion
+    out = 0.0;
+    return true;
+  }
+  if (q < e && (buf[q] | 0x20u) == 'e') {
+    uint64_t r = q + 1;
+    bool eneg = false;
+    if (r < e && (buf[r] == '+' || buf[r] == '-')) {
+      eneg = buf[r] == '-';
+      ++r;
+    }
+    if (r < e && buf[r] >= '0' && buf[r] <= '9') {
+      int x = 0;
+      while (r < e && buf[r] >= '0' && buf[r] <= '9') {
+        if (x < 100000) x = x * 10 + (buf[r] - '0');
+        ++r;
+      }
+      ex += eneg ? -x : x;
+    }
+  }
+  if (w == 0) {
+    out = neg ? -0.0 : 0.0;
+    return true;
+  }
+  constexpr uint64_t k2p53 = 1ull << 53;
+  if (w > k2p53) return false;
+  double v;
+  if (ex >= 0 && ex <= 22) {
+    v = __dmul_rn((double)w, c_p10[ex]);
+  } else if (ex < 0 && ex >= -22) {
+    v = __ddiv_rn((double)w, c_p10[-ex]);
+  } else if (ex > 22 && ex <= 22 + 16) {  // move powers into the significand while it stays exact
+    uint64_t ww = w;
+    for (int k = 22; k < ex; ++k) {
+      if (ww > k2p53 / 10) return false;
+      ww *= 10;
+    }
+    v = __dmul_rn((double)ww, c_p10[22]);
+  } else {
+    return false;
+  }
+  out = neg ? -v : v;
+  return true;
+}
+
+__global__ void tns_parse_kernel(const unsigned char* __restrict__ buf, uint64_t size,
+                                 const uint64_t* __restrict__ starts, const uint32_t* __restrict__ slot,
+                                 uint32_t nlines, int nmodes, uint64_t zero_based, uint64_t nnz,
+                                 uint64_t* __restrict__ idx, double* __restrict__ vals,
+                                 unsigned long long* __restrict__ dims, uint32_t* __restrict__ host_list,
+                                 uint32_t* __restrict__ host_count) {
+  uint64_t dmax[ALTO_MAX_MODES];
+  for (int m = 0; m < ALTO_MAX_MODES; ++m) dmax[m] = 0;
+  const uint64_t one_based = zero_based ? 0 : 1;
+  for (uint64_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nlines; l += gridDim.x * blockDim.x) {
+    const uint32_t k = slot[l];
+    if (slot[l + 1] == k) continue;  // not a valid line
+    const uint64_t s = starts[l], e = l + 1 < nlines ? starts[l + 1] : size;
+    uint64_t p = s;
+    for (int m = 0; m < nmodes; ++m) {
+      const uint64_t x = dev_strtoull(buf, p, e);
+      dmax[m] = max(dmax[m], x + zero_based);
+      idx[(uint64_t)m * nnz + k] = x - one_based;
+    }
+    double v = 0.0;
+    if (!dev_strtod(buf, p, e, v)) {
+      const uint32_t h = atomicAdd(host_count, 1u);
+      host_list[2 * (uint64_t)h] = (uint32_t)l;
+      host_list[2 * (uint64_t)h + 1] = (uint32_t)p - (uint32_t)s;  // value offset within the line
+    }
+    vals[k] = v;
+  }
+  for (int m = 0; m < nmodes; ++m) atomicMax(dims + m, (unsigned long long)dmax[m]);
+}
+
+// For each listed line: its start, end and nonzero slot (one copy to the host).
+__global__ void host_lines_kernel(const uint32_t* __restrict__ list, uint32_t n, const uint64_t* __restrict__ starts,
+                                  const uint32_t* __restrict__ slot, uint32_t nlines, uint64_t size,
+                                  uint64_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t l = list[2 * (uint64_t)i];
+    out[3 * (uint64_t)i] = starts[l];
+    out[3 * (uint64_t)i + 1] = l + 1 < nlines ? starts[l + 1] : size;
+    out[3 * (uint64_t)i + 2] = slot[l];
+  }
+}
+
+__global__ void scatter_vals_kernel(const uint32_t* __restrict__ at, const double* __restrict__ v, uint32_t n,
+                                    double* __restrict__ vals) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vals[at[i]] = v[i];
+}
+
+unsigned grid_io(uint64_t n, int threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b > 148ull * 16) b = 148ull * 16;
+  return (unsigned)(b ? b : 1);
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Pinned {
+  void* p[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  ~Pinned() {
+    for (int i = 0; i < 2; ++i) {
+      if (ev[i]) {
+        cudaEventSynchronize(ev[i]);
+        cudaEventDestroy(ev[i]);
+      }
+      if (p[i]) cudaFreeHost(p[i]);
+    }
+  }
+  alto_status init() {
+    for (int i = 0; i < 2; ++i) {
+      ALTO_TRY_CUDA(cudaHostAlloc(&p[i], kStage, cudaHostAllocDefault));
+      ALTO_TRY_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    }
+    return ALTO_OK;
+  }
+};
+
+// Read bytes [off, off + n) of fd into device memory dst, through the pinned buffers.
+alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst, Pinned& pin, cudaStream_t st) {
+  int cur = 0;
+  bool used[2] = {false, false};
+  for (uint64_t done = 0; done < n;) {
+    const size_t want = (size_t)std::min<uint64_t>(kStage, n - done);
+    if (used[cur]) ALTO_TRY_CUDA(cudaEventSynchronize(pin.ev[cur]));
+    size_t got = 0;
+    while (got < want) {
+      const ssize_t r = pread(fd, static_cast<char*>(pin.p[cur]) + got, want - got, (off_t)(off + done + got));
+      if (r <= 0) {
+        set_error("file ended early or could not be read");
+        return ALTO_ERR_INVALID;
+      }
+      got += (size_t)r;
+    }
+    ALTO_TRY_CUDA(cudaMemcpyAsync(dst + done, pin.p[cur], want, cudaMemcpyHostToDevice, st));
+    ALTO_TRY_CUDA(cudaEventRecord(pin.ev[cur], st));
+    used[cur] = true;
+    done += want;
+    cur ^= 1;
+  }
+  return ALTO_OK;
+}
+
+// The reference's strtok count on the first valid line, minus one.
+int count_modes(std::string line) {
+  line = line.substr(0, strnlen(line.c_str(), line.size()));
+  int n = 0;
+  bool in = false;
+  for (char c : line) {
+    const bool delim = c == ' ' || c == '\t';
+    if (!delim && !in) ++n;
+    in = !delim;
+  }
+  return n - 1;
+}
+
+alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t st, alto_dcoo* d) {
+  Pinned pin;
+  ALTO_TRY(pin.init());
+  const uint64_t ntiles = (size + kIoTile - 1) / kIoTile;
+  DevBuf file, tiles, starts, valid, scan_scratch, misc;
+  ALTO_TRY(file.ensure(ntiles * kIoTile + 16));
+  const double t0 = now_ms();
+  ALTO_TRY_CUDA(cudaMemsetAsync(file.as<char>() + size, 0, ntiles * kIoTile + 16 - size, st));
+  ALTO_TRY(stream_file(fd, 0, size, file.as<char>(), pin, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  d->read_ms = now_ms() - t0;
+
+  cudaEvent_t e0, e1;
+  ALTO_TRY_CUDA(cudaEventCreate(&e0));
+  ALTO_TRY_CUDA(cudaEventCreate(&e1));
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } evg{e0, e1};
+  ALTO_TRY_CUDA(cudaEventRecord(e0, st));
+  ALTO_TRY(tiles.ensure((ntiles + 1) * 4));
+  tns_count_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>());
+  ALTO_LAUNCHED();
+  ALTO_TRY_CUDA(cudaMemsetAsync(tiles.as<uint32_t>() + ntiles, 0, 4, st));
+  ALTO_TRY(exclusive_scan_u32(tiles.as<uint32_t>(), ntiles + 1, scan_scratch, st));
+  uint32_t nl = 0;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&nl, tiles.as<uint32_t>() + ntiles, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  if ((uint64_t)nl + 1 >= (1ull << 32) - 1) {
+    set_error("more than 2^32 - 2 lines");
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  const uint32_t nlines = nl + 1;
+  ALTO_TRY(starts.ensure((uint64_t)nlines * 8));
+  tns_starts_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>(),
+                                                              starts.as<uint64_t>());
+  ALTO_LAUNCHED();
+  ALTO_TRY(valid.ensure(((uint64_t)nlines + 1) * 4));
+  ALTO_TRY(misc.ensure(64 + 8 * ALTO_MAX_MODES));
+  uint32_t* first_valid = misc.as<uint32_t>();
+  uint32_t* host_count = first_valid + 1;
+  unsigned long long* ddims = reinterpret_cast<unsigned long long*>(misc.as<char>() + 64);
+  ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(first_valid, 0xff, 4, st));
+  tns_valid_kernel<<<grid_io((uint64_t)nlines + 1, 256), 256, 0, st>>>(
+      file.as<unsigned char>(), size, starts.as<uint64_t>(), nlines, valid.as<uint32_t>(), first_valid);
+  ALTO_LAUNCHED();
+  ALTO_TRY(exclusive_scan_u32(valid.as<uint32_t>(), (uint64_t)nlines + 1, scan_scratch, st));
+  uint32_t hv[2] = {0, 0};
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&hv[0], valid.as<uint32_t>() + nlines, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&hv[1], first_valid, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  const uint64_t nnz = hv[0];
+  if (nnz == 0) {
+    set_error("no nonzero lines in the file (the reference asserts)");
+    return ALTO_ERR_INVALID;
+  }
+  // the first valid line, on the host, for the mode count
+  uint64_t fl[2] = {0, size};
+  ALTO_TRY_CUDA(cudaMemcpyAsync(fl, starts.as<uint64_t>() + hv[1], hv[1] + 1 < nlines ? 16 : 8,
+                                cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  std::string first(fl[1] - fl[0], '\0');
+  if (pread(fd, &first[0], first.size(), (off_t)fl[0]) != (ssize_t)first.size()) {
+    set_error("could not re-read the first line");
+    return ALTO_ERR_INVALID;
+  }
+  const int N = count_modes(first);
+  if (N < 1 || N > ALTO_MAX_MODES) {
+    set_error("the first line gives %d modes (1..%d supported)", N, ALTO_MAX_MODES);
+    return N < 1 ? ALTO_ERR_INVALID : ALTO_ERR_UNSUPPORTED;
+  }
+  ALTO_TRY(d->raw.ensure((uint64_t)(N + 1) * nnz * 8));
+  uint64_t* idx = d->raw.as<uint64_t>();
+  double* vals = reinterpret_cast<double*>(idx + (uint64_t)N * nnz);
+  DevBuf hl;
+  ALTO_TRY(hl.ensure(nnz * 8));
+  tns_parse_kernel<<<grid_io(nlines, 256), 256, 0, st>>>(file.as<unsigned char>(), size, starts.as<uint64_t>(),
+                                                         valid.as<uint32_t>(), nlines, N, zero_based, nnz, idx,
+                                                         vals, ddims, hl.as<uint32_t>(), host_count);
+  ALTO_LAUNCHED();
+  ALTO_TRY_CUDA(cudaEventRecord(e1, st));
+  uint32_t nhost = 0;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(d->dims, ddims, 8 * N, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&nhost, host_count, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  float pm = 0;
+  cudaEventElapsedTime(&pm, e0, e1);
+  d->parse_ms = pm;
+  d->host_lines = nhost;
+  if (nhost) {  // values the device left to the C library
+    std::vector<uint32_t> list(2 * (size_t)nhost), at(nhost);
+    std::vector<uint64_t> ses(3 * (size_t)nhost);
+    std::vector<double> v(nhost);
+    DevBuf sesd;
+    ALTO_TRY(sesd.ensure((size_t)nhost * 24));
+    host_lines_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(hl.as<uint32_t>(), nhost, starts.as<uint64_t>(),
+                                                           valid.as<uint32_t>(), nlines, size, sesd.as<uint64_t>());
+    ALTO_LAUNCHED();
+    ALTO_TRY_CUDA(cudaMemcpyAsync(list.data(), hl.p, list.size() * 4, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(ses.data(), sesd.p, ses.size() * 8, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+    std::string line;
+    for (uint32_t i = 0; i < nhost; ++i) {
+      line.assign(ses[3 * (size_t)i + 1] - ses[3 * (size_t)i], '\0');
+      if (pread(fd, &line[0], line.size(), (off_t)ses[3 * (size_t)i]) != (ssize_t)line.size()) {
+        set_error("could not re-read a line");
+        return ALTO_ERR_INVALID;
+      }
+      at[i] = (uint32_t)ses[3 * (size_t)i + 2];
+      v[i] = strtod(line.c_str() + list[2 * (size_t)i + 1], nullptr);
+    }
+    DevBuf hb;
+    ALTO_TRY(hb.ensure((size_t)nhost * 12));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(hb.p, v.data(), (size_t)nhost * 8, cudaMemcpyHostToDevice, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(hb.as<char>() + (size_t)nhost * 8, at.data(), (size_t)nhost * 4,
+                                  cudaMemcpyHostToDevice, st));
+    scatter_vals_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(
+        reinterpret_cast<const uint32_t*>(hb.as<char>() + (size_t)nhost * 8), hb.as<double>(), nhost, vals);
+    ALTO_LAUNCHED();
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  }
+  d->nmodes = N;
+  d->nnz = nnz;
+  return ALTO_OK;
+}
+
+alto_status read_binary(int fd, uint64_t size, cudaStream_t st, alto_dcoo* d) {
+  uint64_t nm = 0;
+  if (size >= 8 && pread(fd, &nm, 8, 0) == 8 && (nm >> 32) && (nm & 0xffffffffull) <= ALTO_MAX_MODES)
+    nm &= 0xffffffffull;  // the reference writes its int nmodes as 8 bytes (src/sptensor.cpp:59): the
+                          // upper half is whatever followed the int in memory
+  if (size < 8 || nm < 1 || nm > ALTO_MAX_MODES) {
+    set_error("binary header: bad mode count");
+    return ALTO_ERR_INVALID;
+  }
+  uint64_t head[ALTO_MAX_MODES + 1];
+  if (pread(fd, head, 8 * (nm + 1), 8) != (ssize_t)(8 * (nm + 1))) {
+    set_error("binary header is short");
+    return ALTO_ERR_INVALID;
+  }
+  const uint64_t nnz = head[nm];
+  const uint64_t body = 8 * (nm + 2);
+  if (nnz == 0 || nnz >= (1ull << 32) || size < body + (nm + 1) * nnz * 8) {
+    set_error("binary file: nnz %llu does not match the file size", (unsigned long long)nnz);
+    return nnz >= (1ull << 32) ? ALTO_ERR_UNSUPPORTED : ALTO_ERR_INVALID;
+  }
+  Pinned pin;
+  ALTO_TRY(pin.init());
+  ALTO_TRY(d->raw.ensure((nm + 1) * nnz * 8));
+  const double t0 = now_ms();
+  ALTO_TRY(stream_file(fd, body, (nm + 1) * nnz * 8, d->raw.as<char>(), pin, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  d->read_ms = now_ms() - t0;
+  d->nmodes = (int)nm;
+  d->nnz = nnz;
+  for (uint64_t m = 0; m < nm; ++m) d->dims[m] = head[m];
+  return ALTO_OK;
+}
+
+// "%g" of v as glibc prints it.
+void put_g(std::string& out, double v) {
+  if (std::isfinite(v) && v == std::floor(v) && std::fabs(v) < 1e6) {
+    if (v == 0) {
+      out += std::signbit(v) ? "-0" : "0";
+      return;
+    }
+    long long i = (long long)v;
+    char b[24];
+    int n = 0;
+    const bool neg = i < 0;
+    unsigned long long u = neg ? (unsigned long long)(-i) : (unsigned long long)i;
+    while (u) {
+      b[n++] = (char)('0' + u % 10);
+      u /= 10;
+    }
+    if (neg) out += '-';
+    while (n) out += b[--n];
+    return;
+  }
+  char b[64];
+  snprintf(b, sizeof(b), "%g", v);
+  out += b;
+}
+
+void put_u64(std::string& out, uint64_t u) {
+  char b[24];
+  int n = 0;
+  do {
+    b[n++] = (char)('0' + u % 10);
+    u /= 10;
+  } while (u);
+  while (n) out += b[--n];
+}
+
+}  // namespace
+
+extern "C" {
+
+alto_status alto_read_tensor(const char* path, alto_file_format format, int zero_based, alto_cuda_stream stream,
+                             alto_dcoo** out) {
+  if (!path || !out || (format != ALTO_FILE_TEXT && format != ALTO_FILE_BINARY)) {
+    set_error("bad path, format or out");
+    return ALTO_ERR_INVALID;
+  }
+  *out = nullptr;
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) {
+    set_error("cannot open %s", path);
+    return ALTO_ERR_INVALID;
+  }
+  struct stat sb;
+  if (fstat(fd, &sb) != 0 || sb.st_size == 0) {
+    close(fd);
+    set_error("%s is empty or cannot be read", path);
+    return ALTO_ERR_INVALID;
+  }
+  alto_dcoo* d = new (std::nothrow) alto_dcoo();
+  if (!d) {
+    close(fd);
+    set_error("host allocation failed");
+    return ALTO_ERR_NOMEM;
+  }
+  d->file_bytes = (uint64_t)sb.st_size;
+  cudaStream_t st = (cudaStream_t)stream;
+  alto_status r = format == ALTO_FILE_TEXT ? read_text(fd, (uint64_t)sb.st_size, zero_based ? 1 : 0, st, d)
+                                           : read_binary(fd, (uint64_t)sb.st_size, st, d);
+  close(fd);
+  if (r != ALTO_OK) {
+    cudaStreamSynchronize(st);
+    delete d;
+    return r;
+  }
+  for (int m = 0; m < d->nmodes; ++m) d->ptrs[m] = d->raw.as<uint64_t>() + (uint64_t)m * d->nnz;
+  *out = d;
+  return ALTO_OK;
+}
+
+alto_status alto_dcoo_view(const alto_dcoo* d, alto_coo* view) {
+  if (!d || !view) {
+    set_error("tensor or view is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  view->nmodes = d->nmodes;
+  view->dims = d->dims;
+  view->nnz = d->nnz;
+  view->cidx = d->ptrs;
+  view->index_bytes = 8;
+  view->vals = d->raw.as<uint64_t>() + (uint64_t)d->nmodes * d->nnz;
+  view->val_dtype = ALTO_F64;
+  view->on_device = 1;
+  return ALTO_OK;
+}
+
+alto_status alto_dcoo_stats(const alto_dcoo* d, double* read_ms, double* parse_ms, uint64_t* file_bytes,
+                            uint64_t* host_values) {
+  if (!d) {
+    set_error("tensor is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  if (read_ms) *read_ms = d->read_ms;
+  if (parse_ms) *parse_ms = d->parse_ms;
+  if (file_bytes) *file_bytes = d->file_bytes;
+  if (host_values) *host_values = d->host_lines;
+  return ALTO_OK;
+}
+
+alto_status alto_dcoo_to_host(const alto_dcoo* d, uint64_t* cidx, double* vals) {
+  if (!d) {
+    set_error("tensor is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  const uint64_t n = d->nnz, N = (uint64_t)d->nmodes;
+  if (cidx) ALTO_TRY_CUDA(cudaMemcpy(cidx, d->raw.p, N * n * 8, cudaMemcpyDeviceToHost));
+  if (vals) ALTO_TRY_CUDA(cudaMemcpy(vals, d->raw.as<uint64_t>() + N * n, n * 8, cudaMemcpyDeviceToHost));
+  return ALTO_OK;
+}
+
+alto_status alto_dcoo_destroy(alto_dcoo* d) {
+  delete d;
+  return ALTO_OK;
+}
+
+alto_status alto_write_tensor(const char* path, alto_file_format format, const alto_coo* coo) {
+  if (!path || (format != ALTO_FILE_TEXT && format != ALTO_FILE_BINARY)) {
+    set_error("bad path or format");
+    return ALTO_ERR_INVALID;
+  }
+  ALTO_TRY(check_coo_shape(coo));
+  if (coo->nnz == 0) {
+    set_error("empty tensor (the reference asserts nnz > 0)");
+    return ALTO_ERR_INVALID;
+  }
+  const int N = coo->nmodes;
+  const uint64_t nnz = coo->nnz;
+  // host copies: uint64 indices, float64 values
+  std::vector<std::vector<uint64_t>> ci(N, std::vector<uint64_t>(nnz));
+  std::vector<double> v(nnz);
+  for (int m = 0; m < N; ++m) {
+    if (coo->index_bytes == 8 && coo->on_device) {
+      ALTO_TRY_CUDA(cudaMemcpy(ci[m].data(), coo->cidx[m], nnz * 8, cudaMemcpyDeviceToHost));
+    } else if (coo->index_bytes == 8) {
+      memcpy(ci[m].data(), coo->cidx[m], nnz * 8);
+    } else {
+      std::vector<uint32_t> t(nnz);
+      if (coo->on_device)
+        ALTO_TRY_CUDA(cudaMemcpy(t.data(), coo->cidx[m], nnz * 4, cudaMemcpyDeviceToHost));
+      else
+        memcpy(t.data(), coo->cidx[m], nnz * 4);
+      for (uint64_t i = 0; i < nnz; ++i) ci[m][i] = t[i];
+    }
+  }
+  if (coo->val_dtype == ALTO_F64) {
+    if (coo->on_device)
+      ALTO_TRY_CUDA(cudaMemcpy(v.data(), coo->vals, nnz * 8, cudaMemcpyDeviceToHost));
+    else
+      memcpy(v.data(), coo->vals, nnz * 8);
+  } else {
+    std::vector<float> t(nnz);
+    if (coo->on_device)
+      ALTO_TRY_CUDA(cudaMemcpy(t.data(), coo->vals, nnz * 4, cudaMemcpyDeviceToHost));
+    else
+      memcpy(t.data(), coo->vals, nnz * 4);
+    for (uint64_t i = 0; i < nnz; ++i) v[i] = t[i];
+  }
+  FILE* f = fopen(path, "wb");
+  if (!f) {
+    set_error("cannot create %s", path);
+    return ALTO_ERR_INVALID;
+  }
+  bool ok = true;
+  if (format == ALTO_FILE_BINARY) {
+    const uint64_t nm = (uint64_t)N;
+    ok = fwrite(&nm, 8, 1, f) == 1 && fwrite(coo->dims, 8, N, f) == (size_t)N && fwrite(&nnz, 8, 1, f) == 1;
+    for (int m = 0; m < N && ok; ++m) ok = fwrite(ci[m].data(), 8, nnz, f) == nnz;
+    ok = ok && fwrite(v.data(), 8, nnz, f) == nnz;
+  } else {
+    // format blocks of lines on all cores, write them in order
+    const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const uint64_t block = 1 << 20;
+    for (uint64_t b0 = 0; b0 < nnz && ok; b0 += block * nt) {
+      std::vector<std::string> parts(nt);
+      std::vector<std::thread> th;
+      for (unsigned k = 0; k < nt; ++k) {
+        const uint64_t lo = b0 + k * block, hi = std::min(nnz, lo + block);
+        if (lo >= hi) break;
+        th.emplace_back([&, k, lo, hi] {
+          std::string& s = parts[k];
+          s.reserve((hi - lo) * (8 * N + 12));
+          for (uint64_t i = lo; i < hi; ++i) {
+            for (int m = 0; m < N; ++m) {
+              put_u64(s, ci[m][i] + 1);
+              s += ' ';
+            }
+            put_g(s, v[i]);
+            s += '\n';
+          }
+        });
+      }
+      for (auto& t : th) t.join();
+      for (auto& s : parts) ok = ok && fwrite(s.data(), 1, s.size(), f) == s.size();
+    }
+  }
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) {
+    set_error("writing %s failed", path);
+    return ALTO_ERR_INVALID;
+  }
+  return ALTO_OK;
+}
+
+}  // extern "C"

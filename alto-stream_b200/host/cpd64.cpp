@@ -33,12 +33,14 @@
 
 namespace {
 
+// The tensor's shape, and (for --check only) a host copy of its nonzeros.
 struct Coo {
   int nmodes = 0;
+  uint64_t count = 0;
   std::vector<uint64_t> dims;
   std::vector<std::vector<uint64_t>> cidx;
   std::vector<double> vals;
-  uint64_t nnz() const { return vals.size(); }
+  uint64_t nnz() const { return count; }
 };
 
 [[noreturn]] void die(const char* what, alto_status s) {
@@ -51,80 +53,6 @@ struct Coo {
     alto_status s_ = (call);          \
     if (s_ != ALTO_OK) die(#call, s_); \
   } while (0)
-
-// Text format (src/sptensor.cpp:74-158): whitespace-separated indices then a
-// value per line, '#' comments, dims = max index.
-bool read_tns(const char* path, bool zero_based, Coo& X) {
-  FILE* f = fopen(path, "r");
-  if (!f) return false;
-  char* line = nullptr;
-  size_t cap = 0;
-  ssize_t n;
-  while ((n = getline(&line, &cap, f)) != -1) {
-    if (n <= 1 || line[0] == '#') continue;
-    std::vector<double> tok;
-    char* p = line;
-    char* end;
-    while (true) {
-      double v = strtod(p, &end);
-      if (end == p) break;
-      tok.push_back(v);
-      p = end;
-    }
-    if (tok.size() < 2) continue;
-    if (X.nmodes == 0) {
-      X.nmodes = (int)tok.size() - 1;
-      X.cidx.assign(X.nmodes, {});
-      X.dims.assign(X.nmodes, 0);
-    }
-    for (int m = 0; m < X.nmodes; ++m) {
-      uint64_t ix = (uint64_t)tok[m] - (zero_based ? 0 : 1);
-      X.cidx[m].push_back(ix);
-      X.dims[m] = std::max(X.dims[m], ix + 1);
-    }
-    X.vals.push_back(tok[X.nmodes]);
-  }
-  free(line);
-  fclose(f);
-  return X.nmodes > 0;
-}
-
-// Binary format (src/sptensor.cpp:206-242): u64 nmodes, u64 dims[n], u64 nnz,
-// u64 cidx[n][nnz] (0-based), f64 vals[nnz].
-bool read_bin(const char* path, Coo& X) {
-  FILE* f = fopen(path, "rb");
-  if (!f) return false;
-  uint64_t nm = 0, nnz = 0;
-  bool ok = fread(&nm, 8, 1, f) == 1 && nm >= 1 && nm <= ALTO_MAX_MODES;
-  if (ok) {
-    X.nmodes = (int)nm;
-    X.dims.resize(nm);
-    ok = fread(X.dims.data(), 8, nm, f) == nm && fread(&nnz, 8, 1, f) == 1;
-  }
-  if (ok) {
-    X.cidx.assign(nm, std::vector<uint64_t>(nnz));
-    for (uint64_t m = 0; m < nm && ok; ++m) ok = fread(X.cidx[m].data(), 8, nnz, f) == nnz;
-    X.vals.resize(nnz);
-    ok = ok && fread(X.vals.data(), 8, nnz, f) == nnz;
-  }
-  fclose(f);
-  return ok;
-}
-
-alto_coo view(const Coo& X, std::vector<const void*>& ptrs) {
-  ptrs.resize(X.nmodes);
-  for (int m = 0; m < X.nmodes; ++m) ptrs[m] = X.cidx[m].data();
-  alto_coo c;
-  c.nmodes = X.nmodes;
-  c.dims = X.dims.data();
-  c.nnz = X.nnz();
-  c.cidx = ptrs.data();
-  c.index_bytes = 8;
-  c.vals = X.vals.data();
-  c.val_dtype = ALTO_F64;
-  c.on_device = 0;
-  return c;
-}
 
 // rand_val of the reference (src/util.cpp:28-35).
 double rand_val() {
@@ -218,11 +146,9 @@ int run_als(alto_tensor* t, const Coo& X, int R, int iters, double eps) {
 // cyclically, relabel the non-stream indices in first-seen order, and cut
 // batches of timeslice_limit time steps (or until nnz_threshold); each batch
 // goes to the session as it lies in device memory.
-int run_cpstream(const Coo& X, int R, int iters, double eps, int tmode, alto_constraint con, bool sparse,
+int run_cpstream(const alto_coo& in, int R, int iters, double eps, int tmode, alto_constraint con, bool sparse,
                  uint64_t nnz_threshold, uint64_t limit, double forgetting) {
-  const int N = X.nmodes;
-  std::vector<const void*> in_ptrs;
-  alto_coo in = view(X, in_ptrs);
+  const int N = in.nmodes;
   alto_slicer* sl = nullptr;
   CHECK(alto_slicer_create(&in, tmode, nullptr, &sl));
   alto_stream_session* s = nullptr;
@@ -301,27 +227,41 @@ int main(int argc, char** argv) {
       default: usage(argv[0]); return 1;
     }
   }
-  Coo X;
-  if (!bin.empty()) {
-    if (!read_bin(bin.c_str(), X)) { fprintf(stderr, "cannot read %s\n", bin.c_str()); return 1; }
-  } else if (!text.empty()) {
-    if (!read_tns(text.c_str(), zero, X)) { fprintf(stderr, "cannot read %s\n", text.c_str()); return 1; }
-  } else {
+  // ImportSparseTensor (src/sptensor.cpp:160-249), parsed on the device
+  if (bin.empty() && text.empty()) {
     usage(argv[0]);
     return 1;
+  }
+  const std::string& path = bin.empty() ? text : bin;
+  alto_dcoo* D = nullptr;
+  if (alto_read_tensor(path.c_str(), bin.empty() ? ALTO_FILE_TEXT : ALTO_FILE_BINARY, zero ? 1 : 0, nullptr, &D) !=
+      ALTO_OK) {
+    fprintf(stderr, "cannot read %s: %s\n", path.c_str(), alto_last_error());
+    return 1;
+  }
+  alto_coo coo;
+  CHECK(alto_dcoo_view(D, &coo));
+  Coo X;
+  X.nmodes = coo.nmodes;
+  X.count = coo.nnz;
+  X.dims.assign(coo.dims, coo.dims + coo.nmodes);
+  if (check) {  // host copy for the COO ground truth
+    std::vector<uint64_t> flat((size_t)X.nmodes * X.count);
+    X.vals.resize(X.count);
+    CHECK(alto_dcoo_to_host(D, flat.data(), X.vals.data()));
+    for (int m = 0; m < X.nmodes; ++m)
+      X.cidx.emplace_back(flat.begin() + (size_t)m * X.count, flat.begin() + (size_t)(m + 1) * X.count);
   }
   if (R < 1 || target >= X.nmodes) { usage(argv[0]); return 1; }
   printf("tensor: %d modes, %llu nonzeros, rank %d\n", X.nmodes, (unsigned long long)X.nnz(), R);
   if (model == "cpstream_alto" || model == "CPSTREAM_ALTO") {
     if (tmode < 0 || tmode >= X.nmodes) { fprintf(stderr, "need -a streaming mode\n"); return 1; }
-    return run_cpstream(X, R, iters, eps, tmode, con, false, nnz_threshold, limit ? limit : 1, forgetting);
+    return run_cpstream(coo, R, iters, eps, tmode, con, false, nnz_threshold, limit ? limit : 1, forgetting);
   }
   if (model == "spcpstream_alto" || model == "SPCPSTREAM_ALTO") {
     if (tmode < 0 || tmode >= X.nmodes) { fprintf(stderr, "need -a streaming mode\n"); return 1; }
-    return run_cpstream(X, R, iters, eps, tmode, con, true, nnz_threshold, limit ? limit : 1, forgetting);
+    return run_cpstream(coo, R, iters, eps, tmode, con, true, nnz_threshold, limit ? limit : 1, forgetting);
   }
-  std::vector<const void*> ptrs;
-  alto_coo coo = view(X, ptrs);
   alto_tensor* t = nullptr;
   double t0 = now();
   CHECK(alto_tensor_create(&coo, 0, 1, -1, nullptr, &t));
@@ -331,5 +271,6 @@ int main(int argc, char** argv) {
   else if (bench) rc = run_bench(t, X, R, target, iters);
   else rc = run_als(t, X, R, iters, eps);
   alto_tensor_destroy(t);
+  alto_dcoo_destroy(D);
   return rc;
 }

@@ -54,6 +54,12 @@ Two more workloads print their own line:
                         int64 indices and float64 values in HBM.  A step is
                         the sort, the first-seen relabel and all 200
                         single-step batches; metric nonzeros/s.
+  --workload tns        reading the MTTKRP workload's tensor (140M nonzeros,
+                        3 modes) from a .tns text file (written once with
+                        the library's writer, "%g" values) into device
+                        memory; metric nonzeros/s: `value` the device parse
+                        with the file's bytes in HBM, `e2e` the whole
+                        alto_read_tensor call from a file in the page cache.
 """
 from __future__ import annotations
 
@@ -84,7 +90,7 @@ WORKLOAD = "powerlaw3d-4.8Mx1.8Mx1.8M-140Mnnz-zipf1.2-R32-allmode"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve", "slice"], default="mttkrp")
+    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve", "slice", "tns"], default="mttkrp")
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (mttkrp: all-mode MTTKRPs, default 10; cpstream: slices, default 197; "
                          "serve: slices per stream, default 7)")
@@ -109,10 +115,11 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="mttkrp under torchrun: one tensor sharded over the ranks' line ranges, each step "
                          "the local MTTKRPs plus an NCCL all-reduce of every output (strong scaling)")
+    ap.add_argument("--tns-path", default=None, help="tns: where the text file is written (default: a temp dir)")
     ap.add_argument("--profile-small", action="store_true",
                     help="small case for ncu captures (mttkrp: 20M nonzeros; slice: a quarter of the tensor), 1 step")
     args = ap.parse_args()
-    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1), "slice": (20, 3)}[args.workload]
+    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1), "slice": (20, 3), "tns": (3, 1)}[args.workload]
     if args.steps is None:
         args.steps = defaults[0]
     if args.warmup is None:
@@ -1004,8 +1011,161 @@ def reference_slice_arm(args):
     return 0
 
 
+TNS_METRIC = "tensor file import nnz/s (.tns text into device memory)"
+TNS_WORKLOAD = "tns-" + WORKLOAD.split("-R32")[0]
+TNS_CPU_SAMPLE = 4_000_000
+
+
+def tns_file(args, dev):
+    """Write the MTTKRP workload's tensor as a .tns text file (once)."""
+    import tempfile
+
+    import torch
+
+    import alto_b200 as A
+    from alto_b200 import synth
+
+    nnz = 20_000_000 if args.profile_small else args.nnz
+    path = args.tns_path or os.path.join(tempfile.gettempdir(), f"alto_bench_{nnz}.tns")
+    cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=1234, values="lognormal", device=dev)
+    n = cidx.shape[1]
+    A.write_tensor(path, DIMS, [cidx[m] for m in range(3)], vals.double())
+    del cidx, vals
+    torch.cuda.empty_cache()
+    return path, n
+
+
+def ref_import_rate(path, n_sample):
+    """The reference's ImportSparseTensor (oracle/_ref, one host thread: the
+    reader is serial) on the file's first n_sample lines."""
+    import tempfile
+
+    import oracle as O
+
+    sample = os.path.join(tempfile.gettempdir(), "alto_bench_sample.tns")
+    with open(path, "rb") as f, open(sample, "wb") as g:
+        for _ in range(n_sample):
+            line = f.readline()
+            if not line:
+                break
+            g.write(line)
+    L = O.ref_lib(64)
+    import ctypes
+
+    nm, nnz = ctypes.c_uint64(), ctypes.c_uint64()
+    import numpy as np
+
+    dims = np.zeros(16, np.uint64)
+    t0 = time.perf_counter()
+    L.ref_import_info(sample.encode(), 0, ctypes.c_uint64(0), ctypes.byref(nm),
+                      dims.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nnz))
+    sec = time.perf_counter() - t0
+    size = os.path.getsize(sample)
+    os.remove(sample)
+    return nnz.value / sec, nnz.value, size
+
+
+def ours_tns(args):
+    import torch
+
+    import alto_b200 as A
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    if args.profile_small:
+        args.steps, args.warmup, args.no_cpu_baseline = 1, 1, True
+    path, nnz = tns_file(args, dev)
+    size = os.path.getsize(path)
+    for _ in range(args.warmup):
+        A.read_tensor(path).close()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = A.kernel_launches()
+    walls, parses, reads, hostv = [], [], [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t = A.read_tensor(path)
+        walls.append((time.perf_counter() - t0) * 1e3)
+        st = t.stats()
+        parses.append(st["parse_ms"])
+        reads.append(st["read_ms"])
+        hostv.append(st["host_values"])
+        n_read, dims = t.nnz, [int(x) for x in t.dims]
+        t.close()
+    launches = A.kernel_launches() - launches0
+    clocks = sampler.stop()
+    parse_ms = statistics.median(parses)
+    wall_ms = statistics.median(walls)
+    peak, peak_kind = measured_peaks()
+    algo = size + n_read * 4 * 8
+    achieved = algo / (parse_ms * 1e-3) / 1e9
+    line = {
+        "metric": TNS_METRIC, "value": n_read / (parse_ms * 1e-3), "unit": "nnz/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": parse_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": TNS_WORKLOAD, "nnz": n_read, "file_bytes": size, "dims": dims,
+                   "wall_ms": wall_ms, "host_read_ms": statistics.median(reads),
+                   "values_left_to_host_strtod": hostv[0],
+                   "l2": "file (%.1f GB) exceeds L2; no flush" % (size / 1e9),
+                   "timing": "value: CUDA events around the device parse (file bytes in HBM); "
+                             "e2e: host clock around alto_read_tensor, file in the page cache"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "the device parse (all kernels after the file is in HBM)",
+                     "algorithmic_bytes": "the file once, plus 3 uint64 indices and a float64 value per nonzero",
+                     "peak_kind": peak_kind},
+        "cpu_baseline": None,
+        "e2e": {"value": n_read / (wall_ms * 1e-3), "unit": "nnz/s", "h2d_bytes_per_step": size,
+                "d2h_bytes_per_step": 8 * len(dims), "api": "alto_read_tensor (text file -> device COO)"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            rate, n, sbytes = ref_import_rate(path, TNS_CPU_SAMPLE)
+            line["cpu_baseline"] = {"value": rate, "unit": "nnz/s", "cores": 1, "kind": "reference",
+                                    "sample": f"first {n} lines ({sbytes} bytes) of the same file"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "nnz/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if not args.tns_path:
+        os.remove(path)
+    print(json.dumps(line))
+    return 0
+
+
+def reference_tns_arm(args):
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("the workload generator needs a GPU")
+        args.nnz = min(args.nnz, 10_000_000)  # only the sample is read
+        path, _ = tns_file(args, torch.device("cuda", 0))
+        rate, n, sbytes = ref_import_rate(path, TNS_CPU_SAMPLE)
+        os.remove(path)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
+        return 0
+    print(json.dumps({
+        "impl": "reference", "metric": TNS_METRIC, "value": rate, "unit": "nnz/s", "n_gpus": args.gpus,
+        "steps": 1, "warmup": 0, "ms_per_step": n / rate * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": {"workload": TNS_WORKLOAD},
+        "cpu_baseline": {"value": rate, "unit": "nnz/s", "cores": 1, "kind": "reference",
+                         "sample": f"first {n} lines ({sbytes} bytes) of the workload's file"},
+        "e2e": {"value": rate, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "tns":
+        return reference_tns_arm(args) if args.impl == "reference" else ours_tns(args)
     if args.workload == "slice":
         return reference_slice_arm(args) if args.impl == "reference" else ours_slice(args)
     if args.workload != "mttkrp":

@@ -266,6 +266,46 @@ alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model mode
 alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
 alto_status alto_stream_close(alto_stream_session* s);
 
+/* ---------------------------------------------------------- tensor files */
+
+/* The reference's FileFormat (include/sptensor.hpp:29-32). */
+typedef enum { ALTO_FILE_TEXT = 0, ALTO_FILE_BINARY = 1 } alto_file_format;
+
+/* A COO tensor read from a file into device memory (uint64 indices,
+ * float64 values: the reference's IType and FType). */
+typedef struct alto_dcoo alto_dcoo;
+
+/* ImportSparseTensor(path, format, &X, zero_based), src/sptensor.cpp:160-249.
+ * Text (.tns): whitespace-separated indices then a value per line, '#'
+ * comments, 1-based unless zero_based; the mode count is the first line's
+ * token count minus one and dims[m] the largest index (+1 when zero_based),
+ * exactly as the reference reads them (src/sptensor.cpp:74-158).  The file
+ * is streamed into HBM and parsed there; values equal the C library's
+ * strtod bit for bit.  Binary: uint64 nmodes, dims[nmodes], nnz, the index
+ * arrays mode by mode, float64 values.  An unreadable file, a file without
+ * nonzeros or a short binary file is ALTO_ERR_INVALID.  Synchronous. */
+alto_status alto_read_tensor(const char* path, alto_file_format format, int zero_based,
+                             alto_cuda_stream stream, alto_dcoo** out);
+/* A device view of the tensor (on_device 1, index_bytes 8, ALTO_F64), valid
+ * until alto_dcoo_destroy; it can be given to alto_tensor_create,
+ * alto_slicer_create and alto_stream_push. */
+alto_status alto_dcoo_view(const alto_dcoo* d, alto_coo* view);
+/* Timings of the read: host file reading and copies (read_ms), device
+ * parse (parse_ms, text only); the file's size; how many values the device
+ * left to the C library's strtod.  Any pointer may be NULL. */
+alto_status alto_dcoo_stats(const alto_dcoo* d, double* read_ms, double* parse_ms, uint64_t* file_bytes,
+                            uint64_t* host_values);
+/* The tensor in host memory, as ImportSparseTensor leaves it: cidx
+ * [nmodes][nnz] uint64, vals [nnz] float64 (either may be NULL).  Synchronous. */
+alto_status alto_dcoo_to_host(const alto_dcoo* d, uint64_t* cidx, double* vals);
+alto_status alto_dcoo_destroy(alto_dcoo* d);
+
+/* ExportSparseTensor(path, format, X), src/sptensor.cpp:22-72, from a host
+ * or device COO: text lines of "%llu " (index + 1) per mode and "%g\n" of
+ * the value, formatted on all host cores; or the binary layout above.
+ * Synchronous. */
+alto_status alto_write_tensor(const char* path, alto_file_format format, const alto_coo* coo);
+
 /* ---------------------------------------------------------- stream slicer */
 
 /* The reference's StreamingSparseTensor (include/streaming_sptensor.hpp:10-44)

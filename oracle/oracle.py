@@ -318,6 +318,162 @@ def ref_slice_stream(dims, cidx, vals, stream_mode, nnz_threshold=1, timeslice_l
     return out
 
 
+# ------------------------------------------------------------- tensor files
+
+_SPACE = b" \t\n\v\f\r"
+_U64 = (1 << 64) - 1
+
+
+def _strtoull(line, p):
+    """C strtoull(line + p, &end, 10) on one NUL-terminated line: (value, end)."""
+    q = p
+    n = len(line)
+    while q < n and line[q] in _SPACE:
+        q += 1
+    neg = False
+    if q < n and line[q] in b"+-":
+        neg = line[q] == ord("-")
+        q += 1
+    s = q
+    while q < n and 48 <= line[q] <= 57:
+        q += 1
+    if q == s:
+        return 0, p  # no conversion: end = start
+    v = int(line[s:q])
+    if v > _U64:
+        return _U64, q
+    return ((-v) & _U64 if neg else v), q
+
+
+def _strtod(line, p):
+    """C strtod(line + p, &end) on one line: decimal, hexadecimal, inf and nan
+    forms (the shortest-round-trip decimal conversion is correctly rounded
+    in both C and Python)."""
+    import re
+
+    q = p
+    n = len(line)
+    while q < n and line[q] in _SPACE:
+        q += 1
+    rest = line[q:].decode("latin-1")
+    m = re.match(r"[+-]?0[xX](?:[0-9a-fA-F]+\.?[0-9a-fA-F]*|\.[0-9a-fA-F]+)(?:[pP][+-]?[0-9]+)?", rest)
+    if m:
+        txt = m.group(0)
+        sign = -1.0 if txt[0] == "-" else 1.0
+        body = txt.lstrip("+-")
+        if not re.search(r"[pP]", body):
+            body += "p0"
+        return sign * float.fromhex(body), q + len(txt)
+    m = re.match(r"[+-]?(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:[eE][+-]?[0-9]+)?", rest)
+    if m:
+        return float(m.group(0)), q + len(m.group(0))
+    m = re.match(r"[+-]?(?:inf(?:inity)?|nan(?:\([0-9A-Za-z_]*\))?)", rest, re.IGNORECASE)
+    if m:
+        txt = m.group(0)
+        neg = txt[0] == "-"
+        body = txt.lstrip("+-").lower()
+        v = float("inf") if body.startswith("inf") else float("nan")
+        return (-v if neg else v), q + len(txt)
+    return 0.0, p
+
+
+def _tns_lines(data):
+    """getline over the file: each line with its newline; the valid ones
+    (more than one byte read and not starting with '#')."""
+    out = []
+    pos = 0
+    n = len(data)
+    while pos < n:
+        e = data.find(b"\n", pos)
+        e = n if e < 0 else e + 1
+        line = data[pos:e]
+        if len(line) > 1 and line[0] != ord("#"):
+            out.append(line)
+        pos = e
+    return out
+
+
+def read_tns(data, zero_based=0):
+    """ImportSparseTensor(TEXT_FORMAT) (src/sptensor.cpp:74-158), restated on
+    the file's bytes: the mode count is the first valid line's token count
+    (strtok on space and tab) minus one; every valid line gives a nonzero
+    from nmodes strtoull calls and one strtod; dims[m] is the maximum of
+    index + zero_based, and the stored index is index - (1 - zero_based),
+    all in uint64 arithmetic.  Returns (dims, cidx [nmodes, nnz], vals)."""
+    import re
+
+    lines = _tns_lines(data)
+    if not lines:
+        return np.zeros(0, np.uint64), np.zeros((0, 0), np.uint64), np.zeros(0)
+    first = lines[0].split(b"\0")[0]
+    nmodes = len([t for t in re.split(rb"[ \t]+", first) if t]) - 1
+    one_based = 0 if zero_based else 1
+    dims = [0] * nmodes
+    cidx = np.zeros((max(nmodes, 0), len(lines)), np.uint64)
+    vals = np.zeros(len(lines))
+    for k, line in enumerate(lines):
+        line = line.split(b"\0")[0]
+        p = 0
+        for m in range(nmodes):
+            v, p = _strtoull(line, p)
+            dims[m] = max(dims[m], (v + zero_based) & _U64)
+            cidx[m, k] = (v - one_based) & _U64
+        vals[k], p = _strtod(line, p)
+    return np.array(dims, np.uint64), cidx, vals
+
+
+def _fmt_g(v):
+    """printf("%g") as glibc writes it."""
+    import math
+
+    if math.isnan(v):
+        return "-nan" if math.copysign(1.0, v) < 0 else "nan"
+    return "%g" % v
+
+
+def write_tns(cidx, vals):
+    """ExportSparseTensor(TEXT_FORMAT) (src/sptensor.cpp:48-56): per nonzero
+    "%llu " of index + 1 for every mode, then "%g\n" of the value."""
+    cidx = np.asarray(cidx, np.uint64)
+    out = []
+    for k in range(len(vals)):
+        out.append("".join("%d " % ((int(cidx[m, k]) + 1) & _U64) for m in range(cidx.shape[0]))
+                   + _fmt_g(float(vals[k])) + "\n")
+    return "".join(out).encode()
+
+
+def write_bin(dims, cidx, vals):
+    """ExportSparseTensor(BINARY_FORMAT) (src/sptensor.cpp:57-69): uint64
+    nmodes, dims, nnz, the index arrays mode by mode, float64 values."""
+    cidx = np.asarray(cidx, np.uint64)
+    head = np.array([cidx.shape[0]] + [int(d) for d in dims] + [cidx.shape[1]], np.uint64)
+    return head.tobytes() + np.ascontiguousarray(cidx).tobytes() + np.asarray(vals, np.float64).tobytes()
+
+
+def ref_import(path, fmt=0, zero_based=0):
+    """The compiled reference's ImportSparseTensor of `path`."""
+    L = ref_lib(64)
+    nm, nnz = c_uint64(), c_uint64()
+    dims = np.zeros(16, np.uint64)
+    p = str(path).encode()
+    if L.ref_import_info(p, c_int(fmt), c_uint64(zero_based), ctypes.byref(nm), _ptr(dims), ctypes.byref(nnz)):
+        raise FileNotFoundError(path)
+    c = np.zeros((nm.value, nnz.value), np.uint64)
+    v = np.zeros(nnz.value)
+    L.ref_import_data(p, c_int(fmt), c_uint64(zero_based), _ptr(c), _ptr(v))
+    return dims[: nm.value].copy(), c, v
+
+
+def ref_export(path, fmt, dims, cidx, vals):
+    """The compiled reference's ExportSparseTensor to `path`."""
+    L = ref_lib(64)
+    dims = np.ascontiguousarray(dims, np.uint64)
+    cidx = np.ascontiguousarray(cidx, np.uint64)
+    vals = np.ascontiguousarray(vals, np.float64)
+    L.ref_export(str(path).encode(), c_int(fmt), c_int(cidx.shape[0]), _ptr(dims), c_uint64(cidx.shape[1]),
+                 _ptr(cidx), _ptr(vals))
+
+
 # ------------------------------------------------------ compiled reference
 
 class RefTensor:

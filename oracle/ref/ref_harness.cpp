@@ -411,4 +411,38 @@ int ref_slice_stream(int nmodes, const uint64_t* dims, uint64_t nnz, const uint6
   return nb;
 }
 
+// ImportSparseTensor (src/sptensor.cpp:160-249): shape of the file's tensor.
+// Returns 0, or -1 when the file cannot be opened (the reference asserts).
+int ref_import_info(const char* path, int format, uint64_t zero_based, uint64_t* nmodes, uint64_t* dims,
+                    uint64_t* nnz) {
+  FILE* f = fopen(path, "r");
+  if (!f) return -1;
+  fclose(f);
+  SparseTensor* X = nullptr;
+  ImportSparseTensor(path, format == 1 ? BINARY_FORMAT : TEXT_FORMAT, &X, zero_based);
+  *nmodes = X->nmodes;
+  for (IType m = 0; m < X->nmodes; ++m) dims[m] = X->dims[m];
+  *nnz = X->nnz;
+  DestroySparseTensor(X);
+  return 0;
+}
+
+// The same import's indices ([nmodes][nnz]) and values.
+int ref_import_data(const char* path, int format, uint64_t zero_based, uint64_t* cidx, double* vals) {
+  SparseTensor* X = nullptr;
+  ImportSparseTensor(path, format == 1 ? BINARY_FORMAT : TEXT_FORMAT, &X, zero_based);
+  for (IType m = 0; m < X->nmodes; ++m) memcpy(cidx + m * X->nnz, X->cidx[m], X->nnz * sizeof(IType));
+  memcpy(vals, X->vals, X->nnz * sizeof(FType));
+  DestroySparseTensor(X);
+  return 0;
+}
+
+// ExportSparseTensor (src/sptensor.cpp:22-72) of a COO tensor to `path`.
+void ref_export(const char* path, int format, int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                const double* vals) {
+  SparseTensor* X = make_coo(nmodes, dims, nnz, cidx, vals);
+  ExportSparseTensor(path, format == 1 ? BINARY_FORMAT : TEXT_FORMAT, X);
+  DestroySparseTensor(X);
+}
+
 }  // extern "C"

@@ -128,6 +128,8 @@ def main(ref_root):
 
     out_json["spcpstream_small"] = spcpstream_golden(b, iv, ntot)
     out_json["slicer"] = slicer_golden()
+    out_json["tns"] = tns_golden()
+    out_json["tns_export"] = export_golden()
 
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out_json, f, indent=1)
@@ -164,5 +166,113 @@ def spcpstream_golden(b, iv, ntot):
             "norms": [float(np.linalg.norm(o)) for o in outs], "colsums": [o.sum(0).tolist() for o in outs]}
 
 
+def _fmt_val(rng):
+    r = rng.random()
+    if r < 0.6:
+        return "%g" % (rng.random() * 10.0 ** int(rng.integers(-6, 7)))
+    if r < 0.8:
+        return "%d" % rng.integers(0, 100)
+    if r < 0.9:
+        return "%.10e" % rng.normal()
+    return "%.17g" % rng.normal()
+
+
+def tns_cases():
+    """Text tensor files covering the reader's edge cases, as bytes."""
+    cases = {
+        "basic": b"1 1 1 1.5\n2 3 1 2\n3 2 4 -0.25\n",
+        "comments_blank": b"# header\n\n1 2 3 4\n#mid\n\n2 2 2 5e-1\n   \n3 1 1 7\n",
+        "crlf_tabs": b"1\t2\t3\t1.25\r\n 4  5 6   2.5\r\n7 8 9 3\r\n",
+        "trailing_space_first": b"1 2 3 4.5 \n2 3 4 5.5\n3 1 1 6.25\n",
+        "no_final_newline": b"1 2 3 4\n5 6 7 8",
+        "single_char_last": b"1 2 3 4\n2 2 2 9\n5",
+        "index_forms": (b"+3 2 1 1\n-1 2 2 2\n18446744073709551615 1 1 3\n18446744073709551616 1 1 4\n"
+                        b"0 1 1 5\nabc 1 2 3\n4 5 6\n"),
+    }
+    forms = ["1e-3", "2.5E+02", "-0.0", "+7", ".5", "5.", "1e", "0x1.8p1", "inf", "-INF", "nan",
+             "1.7976931348623157e308", "4.9e-324", "123456789012345678901234567890", "0.1",
+             "3.14159265358979323846", "1e400", "1e-400", "007", "9007199254740993", "12345678901234567e-5",
+             "1.0000000000000000000000001", "0e5", "1e22", "1e23", "123e20", "5e-22", "0x", "-.5e+1", "1.e2",
+             "9007199254740992", "0.000000000000000000000000000001234", "1E+0010"]
+    cases["value_forms"] = "".join("%d %d %d %s\n" % (k + 1, k % 5 + 1, k % 3 + 1, f)
+                                   for k, f in enumerate(forms)).encode()
+    rng = np.random.default_rng(21)
+    cases["five_modes"] = "".join(" ".join(str(int(x)) for x in rng.integers(1, 40, 5)) + " " + _fmt_val(rng) + "\n"
+                                  for _ in range(300)).encode()
+    lines = []
+    for k in range(20000):
+        if k % 997 == 0:
+            lines.append("# block %d\n" % k)
+        sep = " " if k % 7 else "\t"
+        lines.append(sep.join(str(int(x)) for x in rng.integers(1, 1000, 3)) + sep + _fmt_val(rng) + "\n")
+    cases["random_mixed"] = "".join(lines).encode()
+    return cases
+
+
+def tns_digest(dims, cidx, vals):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(dims, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(cidx, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(vals, np.float64).tobytes())
+    return h.hexdigest()
+
+
+def tns_golden():
+    """The reference's ImportSparseTensor of every case, 1- and 0-based, by digest."""
+    import tempfile
+
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, data in tns_cases().items():
+            path = os.path.join(d, name + ".tns")
+            with open(path, "wb") as f:
+                f.write(data)
+            for zb in (0, 1):
+                dims, c, v = O.ref_import(path, 0, zb)
+                out[f"{name}_zb{zb}"] = {"nmodes": len(dims), "nnz": int(c.shape[1]), "dims": [int(x) for x in dims],
+                                         "sha256": tns_digest(dims, c, v)}
+    return out
+
+
+def export_tensor():
+    """A seeded tensor whose values exercise %g (signed zero, 1e6, tiny, inf, nan)."""
+    rng = np.random.default_rng(31)
+    dims = np.array([50, 60, 70], np.uint64)
+    c = np.stack([rng.integers(0, d, 1000).astype(np.uint64) for d in dims])
+    v = np.concatenate([rng.random(500) * 10, rng.integers(-5, 5, 500).astype(float)])
+    v[3:11] = [-0.0, 1e6, 123456.0, 1e-5, np.inf, -np.nan, 0.0, 999999.0]
+    return dims, c, v
+
+
+def export_golden():
+    """SHA-256 of the reference's ExportSparseTensor output, text and binary.
+    The binary header's first word is written from the struct's int nmodes
+    with sizeof(IType) = 8 bytes (src/sptensor.cpp:59), so its upper four
+    bytes are whatever follows the int in memory; they are zeroed before
+    hashing."""
+    import tempfile
+
+    dims, c, v = export_tensor()
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for fmt, name in ((0, "text"), (1, "binary")):
+            path = os.path.join(d, "x")
+            O.ref_export(path, fmt, dims, c, v)
+            with open(path, "rb") as f:
+                data = bytearray(f.read())
+            if fmt == 1:
+                data[4:8] = bytes(4)
+            out[name] = hashlib.sha256(bytes(data)).hexdigest()
+    return out
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1 and sys.argv[1] == "tns":  # refresh only the tensor-file cases
+        with open(os.path.join(HERE, "golden.json")) as f:
+            g = json.load(f)
+        g["tns"] = tns_golden()
+        g["tns_export"] = export_golden()
+        with open(os.path.join(HERE, "golden.json"), "w") as f:
+            json.dump(g, f, indent=1)
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
