@@ -47,11 +47,11 @@ EXPORTED = [
     "alto_tensor_device_bytes", "alto_tensor_restrict", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
-    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph",
+    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph", "alto_stream_error",
     "alto_stream_close",
     "alto_read_tensor", "alto_dcoo_view", "alto_dcoo_stats", "alto_dcoo_to_host", "alto_dcoo_destroy", "alto_write_tensor",
     "alto_slicer_create", "alto_slicer_next", "alto_slicer_last_batch", "alto_slicer_stream_prev",
-    "alto_slicer_iperm", "alto_slicer_destroy",
+    "alto_slicer_iperm", "alto_slicer_tensor", "alto_slicer_destroy",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
@@ -417,6 +417,15 @@ class CPStream:
         launched one by one (alto_stream_set_graph)."""
         check(lib().alto_stream_set_graph(self.h, c_int(1 if enable else 0)))
 
+    def error(self, X):
+        """cpd_error of the current model against X: a :class:`SliceBatch`
+        (e.g. :meth:`Slicer.tensor` or :meth:`Slicer.stream_prev`) or a
+        (dims, cidx, vals) tuple in the session's indexing."""
+        coo = X if isinstance(X, SliceBatch) else _Coo(*X)
+        err = c_double()
+        check(lib().alto_stream_error(self.h, byref(coo.coo if isinstance(X, SliceBatch) else coo.c), byref(err)))
+        return err.value
+
     def lam(self):
         out = np.zeros(self.rank, np.float64)
         check(lib().alto_stream_lambda(self.h, out.ctypes.data_as(c_void_p)))
@@ -578,6 +587,12 @@ class Slicer:
         got = c_int()
         check(lib().alto_slicer_stream_prev(self.h, c_uint64(previous), byref(c), byref(got)))
         return SliceBatch(c, self.nmodes) if got.value else None
+
+    def tensor(self):
+        """The whole sorted, relabelled tensor with global time indices."""
+        c = alto_coo()
+        check(lib().alto_slicer_tensor(self.h, byref(c)))
+        return SliceBatch(c, self.nmodes)
 
     def iperm(self, mode):
         """Original index of every label of `mode` (numpy uint64)."""

@@ -219,6 +219,8 @@ struct alto_slicer {
   uint64_t bdims[ALTO_MAX_MODES] = {}, pdims[ALTO_MAX_MODES] = {};
   const void* bptr[ALTO_MAX_MODES] = {};
   const void* pptr[ALTO_MAX_MODES] = {};
+  uint64_t tdims[ALTO_MAX_MODES] = {};  // the whole tensor's view
+  const void* tptr[ALTO_MAX_MODES] = {};
 };
 
 namespace {
@@ -474,6 +476,17 @@ alto_status alto_slicer_stream_prev(alto_slicer* s, uint64_t previous, alto_coo*
   for (int m = 0; m < s->N; ++m) s->pdims[m] = m == s->t ? s->step - start_time : s->prev_dim[m];
   fill_view(s, start, start + n, s->pdims, s->pptr, s->ptime.as<uint32_t>(), out);
   *got = 1;
+  return ALTO_OK;
+}
+
+alto_status alto_slicer_tensor(const alto_slicer* s, alto_coo* out) {
+  if (!s || !out) {
+    set_error("slicer or out is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  alto_slicer* w = const_cast<alto_slicer*>(s);
+  for (int m = 0; m < s->N; ++m) w->tdims[m] = s->dims[m];
+  fill_view(s, 0, s->nnz, w->tdims, w->tptr, s->gtime.as<uint32_t>(), out);
   return ALTO_OK;
 }
 

@@ -1212,6 +1212,173 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   return ALTO_OK;
 }
 
+// ------------------------------------------------- model error (cpd_error)
+
+struct ErrArgs {
+  const void* cidx[ALTO_MAX_MODES];
+  const float* U[ALTO_MAX_MODES];
+  uint64_t rows[ALTO_MAX_MODES];  // model rows (the time mode: X's time steps)
+  uint64_t xdims[ALTO_MAX_MODES];
+};
+
+constexpr int kErrThreads = 256;
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Per block: sum_k v_k * sum_r prod_m F_m[i_m(k), r] and sum_k v_k^2, in a
+// fixed order (cpd_error's inner product, as a per-nonzero model value
+// instead of an MTTKRP of one mode; the two sums are equal).  Model rows
+// past the session's dims are zero; an index outside X's dims sets *bad.
+template <int IB, typename VT>
+__global__ void __launch_bounds__(kErrThreads)
+    model_inner_kernel(ErrArgs a, int N, int t, int R, const double* __restrict__ trow, const VT* __restrict__ vals,
+                       uint64_t nnz, double* __restrict__ partial, int* __restrict__ bad) {
+  double inner = 0, xx = 0;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += (uint64_t)gridDim.x * blockDim.x) {
+    const double v = (double)vals[k];
+    xx += v * v;
+    uint64_t ix[ALTO_MAX_MODES];
+    bool zero = false;
+    for (int m = 0; m < N; ++m) {
+      ix[m] = IB == 8 ? ((const uint64_t*)a.cidx[m])[k] : ((const uint32_t*)a.cidx[m])[k];
+      if (ix[m] >= a.xdims[m]) {
+        atomicOr(bad, 1);
+        zero = true;
+      } else if (ix[m] >= a.rows[m]) {
+        zero = true;
+      }
+    }
+    if (zero) continue;
+    double sum = 0;
+    for (int r = 0; r < R; ++r) {
+      double p = trow[ix[t] * R + r];
+      for (int m = 0; m < N; ++m)
+        if (m != t) p *= (double)a.U[m][ix[m] * R + r];
+      sum += p;
+    }
+    inner += v * sum;
+  }
+  __shared__ double sh[2][kErrThreads / 32];
+  for (int o = 16; o; o >>= 1) {
+    inner += __shfl_xor_sync(0xffffffffu, inner, o);
+    xx += __shfl_xor_sync(0xffffffffu, xx, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[0][warp] = inner;
+    sh[1][warp] = xx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a0 = 0, a1 = 0;
+    for (int w = 0; w < kErrThreads / 32; ++w) {
+      a0 += sh[0][w];
+      a1 += sh[1][w];
+    }
+    partial[2 * blockIdx.x] = a0;
+    partial[2 * blockIdx.x + 1] = a1;
+  }
+}
+
+alto_status model_error(alto_stream_session* s, const alto_coo* X, double* err) {
+  const int N = s->N, t = s->t, R = s->R;
+  cudaStream_t st = s->st;
+  const uint64_t nnz = X->nnz, T = X->dims[t];
+  const uint64_t have = s->time_rows.size() / R;
+  if (T > have) {
+    set_error("the tensor has %llu time steps, the model %llu", (unsigned long long)T, (unsigned long long)have);
+    return ALTO_ERR_INVALID;
+  }
+  // the last T time rows (get_prev_kruskal, src/kruskal_model.cpp:445-478)
+  const double* trow_h = s->time_rows.data() + (have - T) * R;
+  const int vb = X->val_dtype == ALTO_F64 ? 8 : 4;
+  const unsigned nb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((nnz + kErrThreads - 1) / kErrThreads,
+                                                                         148ull * 8));
+  size_t off = 0;
+  const size_t o_t = off;
+  off += align256(std::max<uint64_t>(T, 1) * R * 8);
+  const size_t o_p = off;
+  off += align256((size_t)nb * 16);
+  const size_t o_b = off;
+  off += 256;
+  const size_t o_g = off;
+  off += align256((size_t)N * R * R * 8);
+  const size_t o_x = off;
+  if (!X->on_device) off += align256(nnz * ((size_t)N * X->index_bytes + vb));
+  DevBuf buf;
+  ALTO_TRY(buf.ensure(off));
+  char* b = buf.as<char>();
+  ErrArgs a{};
+  const void* vals = X->vals;
+  for (int m = 0; m < N; ++m) {
+    a.cidx[m] = X->cidx[m];
+    a.U[m] = m == t ? nullptr : s->U[m].as<float>();
+    a.rows[m] = m == t ? T : s->dims[m];
+    a.xdims[m] = X->dims[m];
+  }
+  if (!X->on_device && nnz) {  // host tensor: copy it in
+    for (int m = 0; m < N; ++m) {
+      char* dst = b + o_x + (size_t)m * nnz * X->index_bytes;
+      ALTO_TRY_CUDA(cudaMemcpyAsync(dst, X->cidx[m], nnz * X->index_bytes, cudaMemcpyHostToDevice, st));
+      a.cidx[m] = dst;
+    }
+    char* vd = b + o_x + (size_t)N * nnz * X->index_bytes;
+    ALTO_TRY_CUDA(cudaMemcpyAsync(vd, X->vals, nnz * vb, cudaMemcpyHostToDevice, st));
+    vals = vd;
+  }
+  if (T) ALTO_TRY_CUDA(cudaMemcpyAsync(b + o_t, trow_h, T * R * 8, cudaMemcpyHostToDevice, st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(b + o_b, 0, 4, st));
+  const double* trow = reinterpret_cast<const double*>(b + o_t);
+  double* part = reinterpret_cast<double*>(b + o_p);
+  int* bad = reinterpret_cast<int*>(b + o_b);
+  if (X->index_bytes == 8 && X->val_dtype == ALTO_F64)
+    model_inner_kernel<8, double><<<nb, kErrThreads, 0, st>>>(a, N, t, R, trow, (const double*)vals, nnz, part, bad);
+  else if (X->index_bytes == 8)
+    model_inner_kernel<8, float><<<nb, kErrThreads, 0, st>>>(a, N, t, R, trow, (const float*)vals, nnz, part, bad);
+  else if (X->val_dtype == ALTO_F64)
+    model_inner_kernel<4, double><<<nb, kErrThreads, 0, st>>>(a, N, t, R, trow, (const double*)vals, nnz, part, bad);
+  else
+    model_inner_kernel<4, float><<<nb, kErrThreads, 0, st>>>(a, N, t, R, trow, (const float*)vals, nnz, part, bad);
+  ALTO_LAUNCHED();
+  // Grams of the non-stream factors (kruskal_norm, src/kruskal_model.cpp:400-443)
+  double* G = reinterpret_cast<double*>(b + o_g);
+  for (int m = 0; m < N; ++m)
+    if (m != t) ALTO_TRY(gram(s->U[m].as<float>(), s->dims[m], R, G + (size_t)m * R * R, s->gscr, st));
+  std::vector<double> hp(2 * (size_t)nb), hg((size_t)N * R * R);
+  int hbad = 0;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * 8, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(hg.data(), G, hg.size() * 8, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  if (hbad) {
+    set_error("an index of the tensor is outside its dims");
+    return ALTO_ERR_INVALID;
+  }
+  double inner = 0, xx = 0;
+  for (unsigned k = 0; k < nb; ++k) {
+    inner += hp[2 * (size_t)k];
+    xx += hp[2 * (size_t)k + 1];
+  }
+  // the time factor's Gram on the host (T x R, small)
+  double* Gt = hg.data() + (size_t)t * R * R;
+  for (int i = 0; i < R * R; ++i) Gt[i] = 0;
+  for (uint64_t q = 0; q < T; ++q)
+    for (int i = 0; i < R; ++i)
+      for (int j = 0; j < R; ++j) Gt[i * R + j] += trow_h[q * R + i] * trow_h[q * R + j];
+  // weights^T (Hadamard of the Grams) weights with unit weights: cpd_error
+  // sets lambda to 1 before kruskal_norm (src/streaming_cpd.cpp:432)
+  double z = 0;
+  for (int i = 0; i < R; ++i)
+    for (int j = 0; j < R; ++j) {
+      double p = 1;
+      for (int m = 0; m < N; ++m) p *= hg[(size_t)m * R * R + (size_t)i * R + j];
+      z += p;
+    }
+  z = std::fabs(z);
+  *err = std::sqrt(xx + z - 2 * inner) / std::sqrt(xx);
+  return ALTO_OK;
+}
+
 }  // namespace
 
 namespace alto {
@@ -1320,6 +1487,19 @@ alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_ou
   ALTO_TRY_CUDA(cudaStreamSynchronize(s->st));
   for (uint64_t q = 0; q < n; ++q) host_out[q] = tmp[q];
   return ALTO_OK;
+}
+
+alto_status alto_stream_error(alto_stream_session* s, const alto_coo* X, double* err) {
+  if (!s || !X || !err || X->nmodes != s->N || !X->dims || (X->nnz && (!X->cidx || !X->vals)) ||
+      (X->index_bytes != 4 && X->index_bytes != 8) || (X->val_dtype != ALTO_F64 && X->val_dtype != ALTO_F32)) {
+    set_error("bad session, tensor or output");
+    return ALTO_ERR_INVALID;
+  }
+  if (s->batches == 0) {
+    set_error("the model is empty (no batch pushed)");
+    return ALTO_ERR_INVALID;
+  }
+  return model_error(s, X, err);
 }
 
 alto_status alto_stream_lambda(alto_stream_session* s, double* host_out) {

@@ -177,6 +177,12 @@ int run_cpstream(const alto_coo& in, int R, int iters, double eps, int tmode, al
   double el = now() - t0;
   printf("%s (ALTO) on the GPU: %d batches in %f s (%f s/batch)\n", sparse ? "spCPSTREAM" : "CPSTREAM", nb, el,
          nb ? el / nb : 0.0);
+  // cpd_error of the final model against the whole (relabelled) tensor, as
+  // the reference reports it (src/streaming_cpd.cpp:311-345)
+  alto_coo whole;
+  double err = 0;
+  CHECK(alto_slicer_tensor(sl, &whole));
+  if (nb && alto_stream_error(s, &whole, &err) == ALTO_OK) printf("final fit error: %f\n", err * err);
   alto_stream_close(s);
   alto_slicer_destroy(sl);
   return 0;

@@ -264,6 +264,16 @@ alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model mode
  * inner iteration.  Both issue the same kernels in the same order and give
  * identical results. */
 alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
+/* cpd_error(X, M), src/streaming_cpd.cpp:368-464: the relative residual
+ * ||X - M|| / ||X|| of the session's current model (unit weights, as
+ * cpd_error sets them) against a COO tensor X in the session's indexing
+ * (host or device).  X's time indices address the last X->dims[t] rows of
+ * the model's time factor: the whole factor for the whole tensor (the
+ * reference's final "fit error" is err^2), the last `previous` rows for
+ * alto_slicer_stream_prev(previous) as compute_errorsq does
+ * (src/streaming_cpd.cpp:1521-1532).  Model rows past the session's dims
+ * are zero.  Synchronous. */
+alto_status alto_stream_error(alto_stream_session* s, const alto_coo* X, double* err);
 alto_status alto_stream_close(alto_stream_session* s);
 
 /* ---------------------------------------------------------- tensor files */
@@ -340,6 +350,10 @@ alto_status alto_slicer_last_batch(const alto_slicer* s, int* last);
  * steps returned so far, time indices relative to the first of them; other
  * dims as of the last batch.  Valid until the next stream_prev call. */
 alto_status alto_slicer_stream_prev(alto_slicer* s, uint64_t previous, alto_coo* out, int* got);
+/* The whole tensor as the reference's StreamingSparseTensor holds it after
+ * construction: sorted, relabelled, global time indices, the input dims
+ * (device view, valid until alto_slicer_destroy; for alto_stream_error). */
+alto_status alto_slicer_tensor(const alto_slicer* s, alto_coo* out);
 /* The original index of every label of `mode` (the Permutation iperms the
  * reference keeps, :92-124) to host memory; *count receives how many
  * (host_out may be NULL to ask for the count). */

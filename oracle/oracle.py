@@ -318,6 +318,41 @@ def ref_slice_stream(dims, cidx, vals, stream_mode, nnz_threshold=1, timeslice_l
     return out
 
 
+def cpd_error(cidx, vals, factors):
+    """cpd_error (src/streaming_cpd.cpp:368-464), restated: with unit
+    weights, inner = sum_k v_k sum_r prod_m U_m[i_m(k), r] (the reference
+    forms it as an MTTKRP of the shortest mode followed by a dot product),
+    ||X||^2 = sum v^2, ||M||^2 = sum_ij prod_m (U_m^T U_m)_ij
+    (kruskal_norm, src/kruskal_model.cpp:400-443); the result is
+    sqrt(||X||^2 + ||M||^2 - 2 inner) / ||X||."""
+    cidx = np.asarray(cidx, np.int64)
+    vals = np.asarray(vals, np.float64)
+    R = factors[0].shape[1]
+    prod = np.ones((len(vals), R))
+    for m, U in enumerate(factors):
+        prod *= U[cidx[m]]
+    inner = float(vals @ prod.sum(1))
+    xx = float(vals @ vals)
+    G = np.ones((R, R))
+    for U in factors:
+        G *= U.T @ U
+    z = abs(float(G.sum()))
+    return float(np.sqrt(xx + z - 2 * inner) / np.sqrt(xx))
+
+
+def ref_cpd_error(dims, cidx, vals, factors):
+    """The compiled reference's cpd_error of the given model against the tensor."""
+    L = ref_lib(64)
+    L.ref_cpd_error.restype = c_double
+    dims = np.ascontiguousarray(dims, np.uint64)
+    cidx = np.ascontiguousarray(cidx, np.uint64)
+    vals = np.ascontiguousarray(vals, np.float64)
+    F = [np.ascontiguousarray(f, np.float64) for f in factors]
+    ptrs = (c_void_p * len(F))(*[f.ctypes.data for f in F])
+    return L.ref_cpd_error(c_int(len(F)), _ptr(dims), c_uint64(cidx.shape[1]), _ptr(cidx), _ptr(vals), ptrs,
+                           c_int(F[0].shape[1]))
+
+
 # ------------------------------------------------------------- tensor files
 
 _SPACE = b" \t\n\v\f\r"

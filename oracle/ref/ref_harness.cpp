@@ -411,6 +411,21 @@ int ref_slice_stream(int nmodes, const uint64_t* dims, uint64_t nnz, const uint6
   return nb;
 }
 
+// cpd_error (src/streaming_cpd.cpp:368-464) of a model whose factors
+// (factors[m]: dims[m] x rank, row-major) are given, against a COO tensor.
+double ref_cpd_error(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx, const double* vals,
+                     double** factors, int rank) {
+  SparseTensor* X = make_coo(nmodes, dims, nnz, cidx, vals);
+  KruskalModel* M = nullptr;
+  CreateKruskalModel(nmodes, X->dims, rank, &M);
+  for (int m = 0; m < nmodes; ++m) memcpy(M->U[m], factors[m], dims[m] * rank * sizeof(FType));
+  for (int r = 0; r < rank; ++r) M->lambda[r] = 1.0;
+  const double e = cpd_error(X, M);
+  DestroyKruskalModel(M);
+  DestroySparseTensor(X);
+  return e;
+}
+
 // ImportSparseTensor (src/sptensor.cpp:160-249): shape of the file's tensor.
 // Returns 0, or -1 when the file cannot be opened (the reference asserts).
 int ref_import_info(const char* path, int format, uint64_t zero_based, uint64_t* nmodes, uint64_t* dims,

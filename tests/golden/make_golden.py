@@ -4,6 +4,7 @@ Run here, where the reference sources exist (the GPU box has no copy):
 
     make -C oracle ref         # oracle/_ref/libaltoref{64,128}.so
     python tests/golden/make_golden.py [path-to-reference]
+    python tests/golden/make_golden.py only tns tns_export cpd_error   # refresh some parts
 
 Inputs are the reference's own fixture tensors (tests/tensors/*.tns in the
 reference project, 1-based text format, src/sptensor.cpp:74-158) plus seeded
@@ -130,6 +131,7 @@ def main(ref_root):
     out_json["slicer"] = slicer_golden()
     out_json["tns"] = tns_golden()
     out_json["tns_export"] = export_golden()
+    out_json["cpd_error"] = cpd_error_golden()
 
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out_json, f, indent=1)
@@ -266,12 +268,29 @@ def export_golden():
     return out
 
 
+def cpd_error_case():
+    """A seeded tensor and model for cpd_error."""
+    rng = np.random.default_rng(41)
+    dims = np.array([30, 40, 20, 10], np.uint64)
+    c = np.stack([rng.integers(0, d, 2000).astype(np.uint64) for d in dims])
+    v = rng.random(2000)
+    F = [rng.random((int(d), 8)) * 0.3 for d in dims]
+    return dims, c, v, F
+
+
+def cpd_error_golden():
+    dims, c, v, F = cpd_error_case()
+    return {"err": O.ref_cpd_error(dims, c, v, F)}
+
+
+PARTS = {"tns": tns_golden, "tns_export": export_golden, "cpd_error": cpd_error_golden}
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "tns":  # refresh only the tensor-file cases
+    if len(sys.argv) > 2 and sys.argv[1] == "only":  # refresh the named parts of golden.json
         with open(os.path.join(HERE, "golden.json")) as f:
             g = json.load(f)
-        g["tns"] = tns_golden()
-        g["tns_export"] = export_golden()
+        for part in sys.argv[2:]:
+            g[part] = PARTS[part]()
         with open(os.path.join(HERE, "golden.json"), "w") as f:
             json.dump(g, f, indent=1)
     else:

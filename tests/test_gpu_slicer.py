@@ -175,3 +175,39 @@ def test_cpstream_fed_by_device_slicer_matches_host_batches(model):
     b = run(dev)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("model", [A.CPSTREAM, A.SPCPSTREAM])
+def test_stream_error_matches_reference(model):
+    """cpd_error of the streamed model against the whole tensor and against
+    stream_prev's last steps (compute_errorsq), on the device, against the
+    oracle and the compiled reference fed the same factor values."""
+    dims = np.array([12, 40, 30, 20], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 2500, seed=3)
+    R, t = 8, 0
+    iv = np.random.default_rng(4).random(4096 * R)
+    s = A.CPStream(4, t, R, constraint=A.NONNEG, max_inner=10, epsilon=1e-5)
+    s.set_model(model)
+    sl = A.Slicer(dims, cidx, vals, t)
+    prev, used = np.zeros(4, np.int64), 0
+    while (b := sl.next(300, 3)) is not None:
+        d = b.dims.astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * R
+        s.push_batch(b, iv[used:used + need])
+        used += need
+        prev = np.maximum(prev, d)
+    F = [s.factor(0, 12)] + [np.vstack([s.factor(m, int(prev[m])), np.zeros((int(dims[m] - prev[m]), R))])
+                             for m in (1, 2, 3)]
+    X = sl.tensor()
+    c, v = X.to_host()
+    err = s.error(X)
+    want = O.cpd_error(c, v, F)
+    assert abs(err - want) <= 1e-10 * max(1.0, want)
+    assert abs(O.ref_cpd_error(dims, c, v, F) - want) <= 1e-12 * max(1.0, want)
+    P = sl.stream_prev(3)  # the last three time steps against the last three time rows
+    pc, pv = P.to_host()
+    e3 = s.error(P)
+    want3 = O.cpd_error(pc, pv, [F[0][-3:]] + F[1:])
+    assert abs(e3 - want3) <= 1e-10 * max(1.0, want3)
+    s.close()
+    sl.close()

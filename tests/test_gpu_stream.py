@@ -174,3 +174,4 @@ def test_cpd64_streaming_models(tmp_path, model, label):
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[-2000:]
     assert f"{label} (ALTO) on the GPU: 5 batches" in r.stdout
+    assert "final fit error: " in r.stdout

@@ -46,3 +46,8 @@ def test_writer_uint32_float32_inputs(tmp_path):
     v = (rng.random(500) * 100).astype(np.float32)
     A.write_tensor(tmp_path / "n.tns", dims, c, v)
     assert (tmp_path / "n.tns").read_bytes() == O.write_tns(c.astype(np.uint64), v.astype(np.float64))
+
+
+def test_cpd_error_restatement_matches_reference(golden):
+    dims, c, v, F = MG.cpd_error_case()
+    assert abs(O.cpd_error(c, v, F) - golden["cpd_error"]["err"]) <= 1e-13
