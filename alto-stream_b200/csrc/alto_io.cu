@@ -1,8 +1,8 @@
 // Tensor files (the reference's ImportSparseTensor / ExportSparseTensor,
 // src/sptensor.cpp:22-249), with the parse on the device.
 //
-// Text (.tns) import.  The file is streamed through two pinned staging
-// buffers into HBM; then, all on the device:
+// Text (.tns) import.  The file is streamed into HBM by eight reader
+// threads through pinned staging buffers; then, all on the device:
 //   1. per 16 KiB tile, the newlines that start a line (tns_count_kernel),
 //      an exclusive scan over the tiles, and the start of every line
 //      (tns_starts_kernel);
@@ -34,6 +34,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -61,7 +63,7 @@ namespace {
 constexpr int kIoThreads = 256;
 constexpr int kIoBytesPerThread = 64;
 constexpr uint64_t kIoTile = (uint64_t)kIoThreads * kIoBytesPerThread;  // 16 KiB
-constexpr size_t kStage = 64ull << 20;                                   // pinned staging buffer
+constexpr size_t kStage = 16ull << 20;                                   // pinned staging buffer
 
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
   __shared__ uint32_t ws[kIoThreads / 32];
@@ -317,48 +319,104 @@ double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-struct Pinned {
-  void* p[2] = {nullptr, nullptr};
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  ~Pinned() {
-    for (int i = 0; i < 2; ++i) {
-      if (ev[i]) {
-        cudaEventSynchronize(ev[i]);
-        cudaEventDestroy(ev[i]);
-      }
-      if (p[i]) cudaFreeHost(p[i]);
-    }
-  }
+// Pinned staging for file reads, kept per device for the life of the
+// process (pinning is slow; a read should not pay for it): kReaders reader
+// threads, each with two buffers and its own non-blocking stream.
+constexpr int kReaders = 8;
+
+struct Staging {
+  std::mutex mu;  // one read at a time per device
+  void* buf[kReaders][2] = {};
+  cudaEvent_t ev[kReaders][2] = {};
+  cudaStream_t st[kReaders] = {};
+  bool ready = false;
   alto_status init() {
-    for (int i = 0; i < 2; ++i) {
-      ALTO_TRY_CUDA(cudaHostAlloc(&p[i], kStage, cudaHostAllocDefault));
-      ALTO_TRY_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    if (ready) return ALTO_OK;
+    for (int r = 0; r < kReaders; ++r) {
+      ALTO_TRY_CUDA(cudaStreamCreateWithFlags(&st[r], cudaStreamNonBlocking));
+      for (int i = 0; i < 2; ++i) {
+        ALTO_TRY_CUDA(cudaHostAlloc(&buf[r][i], kStage, cudaHostAllocDefault));
+        ALTO_TRY_CUDA(cudaEventCreateWithFlags(&ev[r][i], cudaEventDisableTiming));
+      }
     }
+    ready = true;
     return ALTO_OK;
   }
 };
 
-// Read bytes [off, off + n) of fd into device memory dst, through the pinned buffers.
-alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst, Pinned& pin, cudaStream_t st) {
-  int cur = 0;
-  bool used[2] = {false, false};
-  for (uint64_t done = 0; done < n;) {
-    const size_t want = (size_t)std::min<uint64_t>(kStage, n - done);
-    if (used[cur]) ALTO_TRY_CUDA(cudaEventSynchronize(pin.ev[cur]));
-    size_t got = 0;
-    while (got < want) {
-      const ssize_t r = pread(fd, static_cast<char*>(pin.p[cur]) + got, want - got, (off_t)(off + done + got));
-      if (r <= 0) {
-        set_error("file ended early or could not be read");
-        return ALTO_ERR_INVALID;
+Staging* staging_for_device() {
+  static std::mutex mu;
+  static Staging* per[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (!per[dev]) per[dev] = new Staging();
+  return per[dev];
+}
+
+// Read bytes [off, off + n) of fd into device memory dst: chunk c goes to
+// reader c % kReaders, which reads it into one of its pinned buffers and
+// copies it on its own stream, so file reads and copies overlap.  Every copy
+// is complete on return (work that follows on any stream sees the bytes).
+alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst) {
+  Staging* sg = staging_for_device();
+  if (!sg) {
+    set_error("no current CUDA device");
+    return ALTO_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(sg->mu);
+  ALTO_TRY(sg->init());
+  const uint64_t nchunks = (n + kStage - 1) / kStage;
+  const int nr = (int)std::min<uint64_t>(kReaders, std::max<uint64_t>(nchunks, 1));
+  std::atomic<int> failed{0};
+  std::vector<std::string> errs(nr);
+  auto reader = [&](int r) {
+    int slot = 0;
+    bool used[2] = {false, false};
+    for (uint64_t c = r; c < nchunks && !failed.load(); c += nr) {
+      const uint64_t at = c * kStage;
+      const size_t want = (size_t)std::min<uint64_t>(kStage, n - at);
+      if (used[slot] && cudaEventSynchronize(sg->ev[r][slot]) != cudaSuccess) {
+        errs[r] = "staging copy failed";
+        failed = 1;
+        break;
       }
-      got += (size_t)r;
+      size_t got = 0;
+      while (got < want) {
+        const ssize_t k = pread(fd, static_cast<char*>(sg->buf[r][slot]) + got, want - got, (off_t)(off + at + got));
+        if (k <= 0) break;
+        got += (size_t)k;
+      }
+      if (got < want) {
+        errs[r] = "file ended early or could not be read";
+        failed = 1;
+        break;
+      }
+      if (cudaMemcpyAsync(dst + at, sg->buf[r][slot], want, cudaMemcpyHostToDevice, sg->st[r]) != cudaSuccess ||
+          cudaEventRecord(sg->ev[r][slot], sg->st[r]) != cudaSuccess) {
+        errs[r] = "staging copy failed";
+        failed = 1;
+        break;
+      }
+      used[slot] = true;
+      slot ^= 1;
     }
-    ALTO_TRY_CUDA(cudaMemcpyAsync(dst + done, pin.p[cur], want, cudaMemcpyHostToDevice, st));
-    ALTO_TRY_CUDA(cudaEventRecord(pin.ev[cur], st));
-    used[cur] = true;
-    done += want;
-    cur ^= 1;
+    if (cudaStreamSynchronize(sg->st[r]) != cudaSuccess && errs[r].empty()) {
+      errs[r] = "staging copy failed";
+      failed = 1;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int r = 1; r < nr; ++r) th.emplace_back(reader, r);
+  reader(0);
+  for (auto& x : th) x.join();
+  if (failed) {
+    for (auto& e : errs)
+      if (!e.empty()) {
+        set_error("%s", e.c_str());
+        break;
+      }
+    return ALTO_ERR_INVALID;
   }
   return ALTO_OK;
 }
@@ -377,15 +435,13 @@ int count_modes(std::string line) {
 }
 
 alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t st, alto_dcoo* d) {
-  Pinned pin;
-  ALTO_TRY(pin.init());
   const uint64_t ntiles = (size + kIoTile - 1) / kIoTile;
   DevBuf file, tiles, starts, valid, scan_scratch, misc;
   ALTO_TRY(file.ensure(ntiles * kIoTile + 16));
   const double t0 = now_ms();
   ALTO_TRY_CUDA(cudaMemsetAsync(file.as<char>() + size, 0, ntiles * kIoTile + 16 - size, st));
-  ALTO_TRY(stream_file(fd, 0, size, file.as<char>(), pin, st));
-  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // the padding is cleared before the readers copy
+  ALTO_TRY(stream_file(fd, 0, size, file.as<char>()));
   d->read_ms = now_ms() - t0;
 
   cudaEvent_t e0, e1;
@@ -526,12 +582,9 @@ alto_status read_binary(int fd, uint64_t size, cudaStream_t st, alto_dcoo* d) {
     set_error("binary file: nnz %llu does not match the file size", (unsigned long long)nnz);
     return nnz >= (1ull << 32) ? ALTO_ERR_UNSUPPORTED : ALTO_ERR_INVALID;
   }
-  Pinned pin;
-  ALTO_TRY(pin.init());
   ALTO_TRY(d->raw.ensure((nm + 1) * nnz * 8));
   const double t0 = now_ms();
-  ALTO_TRY(stream_file(fd, body, (nm + 1) * nnz * 8, d->raw.as<char>(), pin, st));
-  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  ALTO_TRY(stream_file(fd, body, (nm + 1) * nnz * 8, d->raw.as<char>()));
   d->read_ms = now_ms() - t0;
   d->nmodes = (int)nm;
   d->nnz = nnz;
