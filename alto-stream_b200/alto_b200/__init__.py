@@ -50,7 +50,7 @@ EXPORTED = [
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph", "alto_stream_error",
     "alto_stream_close",
     "alto_read_tensor", "alto_dcoo_view", "alto_dcoo_stats", "alto_dcoo_to_host", "alto_dcoo_destroy", "alto_write_tensor",
-    "alto_slicer_create", "alto_slicer_next", "alto_slicer_last_batch", "alto_slicer_stream_prev",
+    "alto_slicer_create", "alto_slicer_next", "alto_slicer_cut_all", "alto_slicer_batch", "alto_slicer_last_batch", "alto_slicer_stream_prev",
     "alto_slicer_iperm", "alto_slicer_tensor", "alto_slicer_destroy",
     "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
@@ -575,6 +575,19 @@ class Slicer:
         check(lib().alto_slicer_next(self.h, c_uint64(nnz_threshold), c_uint64(timeslice_limit), byref(c),
                                      byref(got)))
         return SliceBatch(c, self.nmodes) if got.value else None
+
+    def cut_all(self, nnz_threshold=1, timeslice_limit=1):
+        """Every remaining batch at once (alto_slicer_cut_all); returns the
+        count, and :meth:`batch` gives each one."""
+        n = c_uint64()
+        check(lib().alto_slicer_cut_all(self.h, c_uint64(nnz_threshold), c_uint64(timeslice_limit), byref(n)))
+        return n.value
+
+    def batch(self, b):
+        """Batch b of the last :meth:`cut_all`."""
+        c = alto_coo()
+        check(lib().alto_slicer_batch(self.h, c_uint64(b), byref(c)))
+        return SliceBatch(c, self.nmodes)
 
     def last_batch(self):
         last = c_int()

@@ -219,6 +219,8 @@ struct alto_slicer {
   uint64_t bdims[ALTO_MAX_MODES] = {}, pdims[ALTO_MAX_MODES] = {};
   const void* bptr[ALTO_MAX_MODES] = {};
   const void* pptr[ALTO_MAX_MODES] = {};
+  std::vector<uint64_t> cut_start, cut_end, cut_dims;  // alto_slicer_cut_all's batches
+  DevBuf steptab;                                     // each time step's batch first step
   uint64_t tdims[ALTO_MAX_MODES] = {};  // the whole tensor's view
   const void* tptr[ALTO_MAX_MODES] = {};
 };
@@ -410,14 +412,15 @@ alto_status alto_slicer_create(const alto_coo* coo, int stream_mode, alto_cuda_s
   return ALTO_OK;
 }
 
-alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit, alto_coo* batch,
-                             int* got) {
-  if (!s || !batch || !got) {
-    set_error("slicer, batch or got is NULL");
-    return ALTO_ERR_INVALID;
-  }
-  *got = 0;
-  if (s->ptr == s->nnz) return ALTO_OK;  // the reference returns NULL
+}  // extern "C"
+
+namespace {
+
+// One next_dynamic_batch cut (src/streaming_sptensor.cpp:196-264) on the
+// host tables: advances the position and the step, sets s->bdims and
+// s->prev_dim; [start, end) and the batch's first step are returned.
+void cut_batch(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit, uint64_t* start_out,
+               uint64_t* end_out, uint64_t* first_out) {
   const uint64_t first = s->step;
   const uint64_t start = std::max<uint64_t>(s->ptr, s->off[std::min(s->step, s->T)]);
   uint64_t end = start;
@@ -435,6 +438,40 @@ alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t ti
       s->prev_dim[m] = s->bdims[m];
     }
   }
+  s->ptr = end;
+  *start_out = start;
+  *end_out = end;
+  *first_out = first;
+}
+
+}  // namespace
+
+namespace alto {
+namespace {
+// out[i] = time[begin + i] - first_of[time[begin + i]], i < n: every
+// position's batch-local time, given each time step's batch first step.
+__global__ void slice_local_time_all_kernel(const uint32_t* __restrict__ gtime, uint64_t begin, uint64_t n,
+                                            const uint32_t* __restrict__ first_of, uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t tt = gtime[begin + i];
+    out[begin + i] = tt - first_of[tt];
+  }
+}
+}  // namespace
+}  // namespace alto
+
+extern "C" {
+
+alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit, alto_coo* batch,
+                             int* got) {
+  if (!s || !batch || !got) {
+    set_error("slicer, batch or got is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  *got = 0;
+  if (s->ptr == s->nnz) return ALTO_OK;  // the reference returns NULL
+  uint64_t start, end, first;
+  cut_batch(s, nnz_threshold, timeslice_limit, &start, &end, &first);
   uint32_t* time = s->idx.as<uint32_t>() + (size_t)s->t * s->nnz + start;
   if (end > start) {
     slice_local_time_kernel<<<grid_n(end - start, 256), 256, 0, s->st>>>(
@@ -442,8 +479,49 @@ alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t ti
     ALTO_LAUNCHED();
   }
   fill_view(s, start, end, s->bdims, s->bptr, time, batch);
-  s->ptr = end;
   *got = 1;
+  return ALTO_OK;
+}
+
+alto_status alto_slicer_cut_all(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit,
+                                uint64_t* nbatches) {
+  if (!s || !nbatches) {
+    set_error("slicer or nbatches is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  const int N = s->N;
+  s->cut_start.clear();
+  s->cut_end.clear();
+  s->cut_dims.clear();
+  const uint64_t p0 = s->ptr;
+  std::vector<uint32_t> first_of(s->T + 1, 0);
+  while (s->ptr < s->nnz) {
+    uint64_t start, end, first;
+    cut_batch(s, nnz_threshold, timeslice_limit, &start, &end, &first);
+    for (uint64_t b = first; b < std::min(s->step, s->T); ++b) first_of[b] = (uint32_t)first;
+    s->cut_start.push_back(start);
+    s->cut_end.push_back(end);
+    for (int m = 0; m < N; ++m) s->cut_dims.push_back(s->bdims[m]);
+  }
+  if (s->nnz > p0) {
+    ALTO_TRY(s->steptab.ensure((s->T + 1) * 4));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(s->steptab.p, first_of.data(), (s->T + 1) * 4, cudaMemcpyHostToDevice, s->st));
+    slice_local_time_all_kernel<<<grid_n(s->nnz - p0, 256), 256, 0, s->st>>>(
+        s->gtime.as<uint32_t>(), p0, s->nnz - p0, s->steptab.as<uint32_t>(), s->idx.as<uint32_t>() + (size_t)s->t * s->nnz);
+    ALTO_LAUNCHED();
+  }
+  *nbatches = s->cut_start.size();
+  return ALTO_OK;
+}
+
+alto_status alto_slicer_batch(alto_slicer* s, uint64_t b, alto_coo* out) {
+  if (!s || !out || b >= s->cut_start.size()) {
+    set_error("bad slicer, batch number or out");
+    return ALTO_ERR_INVALID;
+  }
+  const uint64_t start = s->cut_start[b];
+  fill_view(s, start, s->cut_end[b], s->cut_dims.data() + b * s->N, s->bptr,
+            s->idx.as<uint32_t>() + (size_t)s->t * s->nnz + start, out);
   return ALTO_OK;
 }
 

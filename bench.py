@@ -53,7 +53,9 @@ Two more workloads print their own line:
                         100,000 x 100,000 x 10,000 Zipf(1.1) coordinates,
                         int64 indices and float64 values in HBM.  A step is
                         the sort, the first-seen relabel and all 200
-                        single-step batches; metric nonzeros/s.
+                        single-step batches (alto_slicer_cut_all: the cuts
+                        of repeated next_dynamic_batch calls, one kernel for
+                        the batch-local times); metric nonzeros/s.
   --workload tns        reading the MTTKRP workload's tensor (140M nonzeros,
                         3 modes) from a .tns text file (written once with
                         the library's writer, "%g" values) into device
@@ -881,17 +883,10 @@ def ours_slice(args):
     N = len(SLICE_DIMS)
     stream = torch.cuda.current_stream()
 
-    def one(cidx, v):
+    def one(cidx, v):  # construction, then every single-step batch in one call
         sl = A.Slicer(SLICE_DIMS, cidx, v, 0)
-        first = None
-        nb = 0
-        while True:
-            b = sl.next(1, 1)
-            if b is None:
-                break
-            first = first or b
-            nb += 1
-        return sl, first, nb
+        nb = sl.cut_all(1, 1)
+        return sl, (sl.batch(0) if nb else None), nb
 
     for _ in range(args.warmup):
         one(cols, vals)[0].close()
@@ -970,7 +965,7 @@ def ours_slice(args):
         "cpu_baseline": None,
         "e2e": {"value": e2e_val, "unit": "nnz/s", "h2d_bytes_per_step": nnz * (N * 8 + 8),
                 "d2h_bytes_per_step": nnz * (N * 4 + 8),
-                "api": "alto_slicer_create (host COO) + alto_slicer_next per batch + batch contents to host"},
+                "api": "alto_slicer_create (host COO) + alto_slicer_cut_all + batch contents to host"},
         "clocks": clocks,
         "gpu_launches": launches,
     }

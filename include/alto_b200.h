@@ -344,6 +344,15 @@ alto_status alto_slicer_create(const alto_coo* coo, int stream_mode, alto_cuda_s
  * reference does when built without assertions (it asserts nnz > 0). */
 alto_status alto_slicer_next(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit,
                              alto_coo* batch, int* got);
+/* Every remaining batch at once: the cuts repeated alto_slicer_next calls
+ * would make, with the batch-local time indices of all of them written by
+ * one kernel (no counterpart in the reference, whose slicer only iterates).
+ * *nbatches receives the count; alto_slicer_batch then gives each view. */
+alto_status alto_slicer_cut_all(alto_slicer* s, uint64_t nnz_threshold, uint64_t timeslice_limit,
+                                uint64_t* nbatches);
+/* Batch b of the last alto_slicer_cut_all, as alto_slicer_next returns it
+ * (its cidx array is overwritten by the next call on s). */
+alto_status alto_slicer_batch(alto_slicer* s, uint64_t b, alto_coo* out);
 /* last_batch(), :266-269. */
 alto_status alto_slicer_last_batch(const alto_slicer* s, int* last);
 /* stream_prev(previous), :284-327: the nonzeros of the last `previous` time

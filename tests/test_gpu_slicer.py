@@ -211,3 +211,28 @@ def test_stream_error_matches_reference(model):
     assert abs(e3 - want3) <= 1e-10 * max(1.0, want3)
     s.close()
     sl.close()
+
+
+def test_cut_all_equals_repeated_next():
+    """alto_slicer_cut_all makes the cuts repeated next() calls make, with the
+    same batch contents, including empty time steps; stream_prev and the end
+    state follow."""
+    rng = np.random.default_rng(12)
+    dims = np.array([40, 30, 20, 10], np.uint64)
+    n = 3000
+    steps = rng.choice(np.array([0, 1, 4, 5, 6, 9, 17, 30, 31, 39], np.uint64), n)
+    cidx = np.stack([steps] + [rng.integers(0, int(d), n).astype(np.uint64) for d in dims[1:]])
+    vals = rng.random(n)
+    for thr, lim in [(1, 1), (200, 3), (10**9, 7)]:
+        want, _ = gpu_batches(dims, cidx, vals, 0, thr, lim)
+        sl = A.Slicer(dims, cidx, vals, 0)
+        nb = sl.cut_all(thr, lim)
+        assert nb == len(want) and sl.last_batch() and sl.next(thr, lim) is None
+        for k in range(nb):
+            b = sl.batch(k)
+            c, v = b.to_host()
+            assert np.array_equal(b.dims, want[k]["dims"]) and np.array_equal(c, want[k]["cidx"])
+            assert np.array_equal(v, want[k]["vals"])
+        p = sl.stream_prev(5)
+        assert p is not None and p.dims[0] == 5
+        sl.close()
