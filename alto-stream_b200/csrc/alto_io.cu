@@ -3,13 +3,13 @@
 //
 // Text (.tns) import.  The file is streamed into HBM by eight reader
 // threads through pinned staging buffers; then, all on the device:
-//   1. per 16 KiB tile, the newlines that start a line (tns_count_kernel),
-//      an exclusive scan over the tiles, and the start of every line
-//      (tns_starts_kernel);
-//   2. per line, getline's validity rule (more than one byte read, not a
-//      '#' comment) and the first valid line (tns_valid_kernel), and an
-//      exclusive scan giving every valid line its nonzero slot;
-//   3. per valid line, the reference's own parse (tns_parse_kernel): nmodes
+//   1. per 16 KiB tile, the line starts that getline's rule keeps (more
+//      than one byte read, no leading '#'), counted from 16-byte loads
+//      (tns_count_kernel); an exclusive scan over the tiles gives each kept
+//      line its nonzero slot, and the same tiles again write every kept
+//      line's start at its slot (tns_starts_kernel);
+//   2. per kept line, the reference's own parse (tns_parse_kernel, a
+//      block's 256 lines staged in shared memory): nmodes
 //      strtoull calls (exact, including sign, overflow and no-digit cases)
 //      and one strtod.  Decimal values whose significand fits 19 digits and
 //      whose value is exact in Clinger's fast path (significand <= 2^53,
@@ -87,10 +87,16 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
   return pre + x - v;
 }
 
-// Newlines at positions < size - 1 in this thread's 64 bytes (the buffer is
-// zero-padded to a whole tile, so the 16-byte loads stay inside it).
-__device__ __forceinline__ uint32_t count_nl(const uint4* __restrict__ buf, uint64_t base, uint64_t size) {
-  uint32_t c = 0;
+// The valid line starts in this thread's 64 bytes [base, base + 64): a
+// position q starts a line when q == 0 or byte q - 1 is a newline, and the
+// line is one getline reads with more than one byte and without a leading
+// '#' exactly when q + 1 < size and byte q is neither '\n' nor '#'.  The
+// bytes come from four 16-byte loads (the buffer is zero-padded to a whole
+// tile, so they stay inside it).  Calls f(q) for each, in order.
+template <typename F>
+__device__ __forceinline__ void valid_starts(const uint4* __restrict__ buf, uint64_t base, uint64_t size, F f) {
+  const unsigned char* b8 = reinterpret_cast<const unsigned char*>(buf);
+  unsigned prev = base ? b8[base - 1] : (unsigned)'\n';
 #pragma unroll
   for (int k = 0; k < kIoBytesPerThread / 16; ++k) {
     const uint4 w = buf[base / 16 + k];
@@ -99,49 +105,32 @@ __device__ __forceinline__ uint32_t count_nl(const uint4* __restrict__ buf, uint
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        const uint64_t p = base + k * 16 + j * 4 + b;
-        c += (((ws[j] >> (8 * b)) & 0xffu) == '\n' && p + 1 < size) ? 1u : 0u;
+        const unsigned c = (ws[j] >> (8 * b)) & 0xffu;
+        const uint64_t q = base + k * 16 + j * 4 + b;
+        if (prev == '\n' && q + 1 < size && c != '\n' && c != '#') f(q);
+        prev = c;
       }
   }
-  return c;
 }
 
 __global__ void __launch_bounds__(kIoThreads)
-    tns_count_kernel(const uint4* __restrict__ buf, uint64_t size, uint32_t* __restrict__ tile_nl) {
+    tns_count_kernel(const uint4* __restrict__ buf, uint64_t size, uint32_t* __restrict__ tile_lines) {
   const uint64_t base = blockIdx.x * kIoTile + threadIdx.x * (uint64_t)kIoBytesPerThread;
-  uint32_t tot;
-  block_excl_scan(count_nl(buf, base, size), &tot);
-  if (threadIdx.x == 0) tile_nl[blockIdx.x] = tot;
+  uint32_t c = 0, tot;
+  valid_starts(buf, base, size, [&](uint64_t) { ++c; });
+  block_excl_scan(c, &tot);
+  if (threadIdx.x == 0) tile_lines[blockIdx.x] = tot;
 }
 
-// starts[0] = 0; starts[1 + k] = position after the k-th line-starting newline.
+// starts[k] = the start of the k-th valid line (its nonzero slot is k).
 __global__ void __launch_bounds__(kIoThreads)
     tns_starts_kernel(const uint4* __restrict__ buf, uint64_t size, const uint32_t* __restrict__ tile_base,
                       uint64_t* __restrict__ starts) {
   const uint64_t base = blockIdx.x * kIoTile + threadIdx.x * (uint64_t)kIoBytesPerThread;
-  uint32_t tot;
-  uint32_t r = tile_base[blockIdx.x] + block_excl_scan(count_nl(buf, base, size), &tot);
-  if (blockIdx.x == 0 && threadIdx.x == 0) starts[0] = 0;
-  const unsigned char* b8 = reinterpret_cast<const unsigned char*>(buf);
-  for (int k = 0; k < kIoBytesPerThread; ++k) {
-    const uint64_t p = base + k;
-    if (b8[p] == '\n' && p + 1 < size) starts[1 + r++] = p + 1;
-  }
-}
-
-// valid[l] = getline read more than one byte and the line is not a comment.
-__global__ void tns_valid_kernel(const unsigned char* __restrict__ buf, uint64_t size,
-                                 const uint64_t* __restrict__ starts, uint32_t nlines, uint32_t* __restrict__ valid,
-                                 uint32_t* __restrict__ first_valid) {
-  for (uint64_t l = blockIdx.x * blockDim.x + threadIdx.x; l <= nlines; l += gridDim.x * blockDim.x) {
-    uint32_t v = 0;
-    if (l < nlines) {
-      const uint64_t s = starts[l], e = l + 1 < nlines ? starts[l + 1] : size;
-      v = (e - s > 1 && buf[s] != '#') ? 1u : 0u;
-      if (v) atomicMin(first_valid, (uint32_t)l);
-    }
-    valid[l] = v;
-  }
+  uint32_t c = 0, tot;
+  valid_starts(buf, base, size, [&](uint64_t) { ++c; });
+  uint32_t r = tile_base[blockIdx.x] + block_excl_scan(c, &tot);
+  valid_starts(buf, base, size, [&](uint64_t q) { starts[r++] = q; });
 }
 
 // 10^0 .. 10^22, every one exact in float64.
@@ -152,10 +141,13 @@ __device__ __forceinline__ bool is_space(unsigned c) {
   return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
 }
 
-// strtoull(p, &end, 10) within [p, e) (a NUL ends the string as in C).
+// strtoull(p, &end, 10) on the line at p: the line ends at its newline, a
+// NUL or e (the reference parses one getline buffer, so nothing after the
+// newline is reached: skipping whitespace stops there as it stops at the
+// buffer's terminating NUL).
 __device__ uint64_t dev_strtoull(const unsigned char* __restrict__ buf, uint64_t& p, uint64_t e) {
   uint64_t q = p;
-  while (q < e && buf[q] && is_space(buf[q])) ++q;
+  while (q < e && buf[q] && buf[q] != '\n' && is_space(buf[q])) ++q;
   bool neg = false;
   if (q < e && (buf[q] == '+' || buf[q] == '-')) {
     neg = buf[q] == '-';
@@ -179,7 +171,7 @@ __device__ uint64_t dev_strtoull(const unsigned char* __restrict__ buf, uint64_t
 // strtod's decimal fast path; false when the host must convert the text.
 __device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, uint64_t e, double& out) {
   uint64_t q = p;
-  while (q < e && buf[q] && is_space(buf[q])) ++q;
+  while (q < e && buf[q] && buf[q] != '\n' && is_space(buf[q])) ++q;
   bool neg = false;
   if (q < e && (buf[q] == '+' || buf[q] == '-')) {
     neg = buf[q] == '-';
@@ -262,46 +254,61 @@ __device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, ui
   return true;
 }
 
-__global__ void tns_parse_kernel(const unsigned char* __restrict__ buf, uint64_t size,
-                                 const uint64_t* __restrict__ starts, const uint32_t* __restrict__ slot,
-                                 uint32_t nlines, int nmodes, uint64_t zero_based, uint64_t nnz,
-                                 uint64_t* __restrict__ idx, double* __restrict__ vals,
-                                 unsigned long long* __restrict__ dims, uint32_t* __restrict__ host_list,
-                                 uint32_t* __restrict__ host_count) {
+constexpr int kStageBytes = 24 << 10;  // a block's lines staged in shared memory
+
+// One thread per valid line.  A block takes 256 consecutive lines; when
+// their bytes fit kStageBytes they are staged in shared memory with 16-byte
+// loads and parsed from there, else parsed from global memory.
+__global__ void __launch_bounds__(kIoThreads)
+    tns_parse_kernel(const unsigned char* __restrict__ buf, uint64_t size, const uint64_t* __restrict__ starts,
+                     uint64_t nnz, int nmodes, uint64_t zero_based, uint64_t* __restrict__ idx,
+                     double* __restrict__ vals, unsigned long long* __restrict__ dims,
+                     uint64_t* __restrict__ host_list, uint32_t host_cap, uint32_t* __restrict__ host_count) {
+  __shared__ __align__(16) unsigned char sm[kStageBytes];
   uint64_t dmax[ALTO_MAX_MODES];
   for (int m = 0; m < ALTO_MAX_MODES; ++m) dmax[m] = 0;
   const uint64_t one_based = zero_based ? 0 : 1;
-  for (uint64_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nlines; l += gridDim.x * blockDim.x) {
-    const uint32_t k = slot[l];
-    if (slot[l + 1] == k) continue;  // not a valid line
-    const uint64_t s = starts[l], e = l + 1 < nlines ? starts[l + 1] : size;
-    uint64_t p = s;
-    for (int m = 0; m < nmodes; ++m) {
-      const uint64_t x = dev_strtoull(buf, p, e);
-      dmax[m] = max(dmax[m], x + zero_based);
-      idx[(uint64_t)m * nnz + k] = x - one_based;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * kIoThreads; k0 < nnz; k0 += (uint64_t)gridDim.x * kIoThreads) {
+    const uint64_t k1 = min(k0 + kIoThreads, nnz);
+    const uint64_t lo = starts[k0], hi = k1 < nnz ? starts[k1] : size;
+    const uint64_t alo = lo & ~15ull, span = hi - alo;
+    const bool staged = span <= (uint64_t)kStageBytes;
+    if (staged) {
+      const uint4* src = reinterpret_cast<const uint4*>(buf + alo);
+      for (uint64_t o = threadIdx.x; o * 16 < span; o += kIoThreads) reinterpret_cast<uint4*>(sm)[o] = src[o];
     }
-    double v = 0.0;
-    if (!dev_strtod(buf, p, e, v)) {
-      const uint32_t h = atomicAdd(host_count, 1u);
-      host_list[2 * (uint64_t)h] = (uint32_t)l;
-      host_list[2 * (uint64_t)h + 1] = (uint32_t)p - (uint32_t)s;  // value offset within the line
+    __syncthreads();
+    const uint64_t k = k0 + threadIdx.x;
+    if (k < k1) {
+      const unsigned char* b = staged ? sm : buf;
+      const uint64_t off = staged ? alo : 0;
+      const uint64_t s = starts[k] - off, e = hi - off;
+      uint64_t p = s;
+      for (int m = 0; m < nmodes; ++m) {
+        const uint64_t x = dev_strtoull(b, p, e);
+        dmax[m] = max(dmax[m], x + zero_based);
+        idx[(uint64_t)m * nnz + k] = x - one_based;
+      }
+      double v = 0.0;
+      if (!dev_strtod(b, p, e, v)) {  // the host converts this value (line start + value offset)
+        const uint32_t h = atomicAdd(host_count, 1u);
+        if (h < host_cap) {  // (past the capacity the count still grows; the host then reruns)
+          host_list[2 * (uint64_t)h] = k;
+          host_list[2 * (uint64_t)h + 1] = p - s;
+        }
+      }
+      vals[k] = v;
     }
-    vals[k] = v;
+    __syncthreads();
   }
   for (int m = 0; m < nmodes; ++m) atomicMax(dims + m, (unsigned long long)dmax[m]);
 }
 
-// For each listed line: its start, end and nonzero slot (one copy to the host).
-__global__ void host_lines_kernel(const uint32_t* __restrict__ list, uint32_t n, const uint64_t* __restrict__ starts,
-                                  const uint32_t* __restrict__ slot, uint32_t nlines, uint64_t size,
+// For each listed line: its start in the file (one copy to the host).
+__global__ void host_lines_kernel(const uint64_t* __restrict__ list, uint32_t n, const uint64_t* __restrict__ starts,
                                   uint64_t* __restrict__ out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t l = list[2 * (uint64_t)i];
-    out[3 * (uint64_t)i] = starts[l];
-    out[3 * (uint64_t)i + 1] = l + 1 < nlines ? starts[l + 1] : size;
-    out[3 * (uint64_t)i + 2] = slot[l];
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = starts[list[2 * (uint64_t)i]];
 }
 
 __global__ void scatter_vals_kernel(const uint32_t* __restrict__ at, const double* __restrict__ v, uint32_t n,
@@ -421,6 +428,29 @@ alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst) {
   return ALTO_OK;
 }
 
+// The line of the file starting at `start`, up to and including its newline
+// (or to the end of the file), as getline returns it.
+alto_status read_line(int fd, uint64_t start, uint64_t size, std::string* out) {
+  out->clear();
+  char chunk[4096];
+  for (uint64_t at = start; at < size;) {
+    const size_t want = (size_t)std::min<uint64_t>(sizeof(chunk), size - at);
+    const ssize_t r = pread(fd, chunk, want, (off_t)at);
+    if (r <= 0) {
+      set_error("could not re-read a line of the file");
+      return ALTO_ERR_INVALID;
+    }
+    const char* nl = static_cast<const char*>(memchr(chunk, '\n', (size_t)r));
+    if (nl) {
+      out->append(chunk, (size_t)(nl - chunk) + 1);
+      return ALTO_OK;
+    }
+    out->append(chunk, (size_t)r);
+    at += (uint64_t)r;
+  }
+  return ALTO_OK;
+}
+
 // The reference's strtok count on the first valid line, minus one.
 int count_modes(std::string line) {
   line = line.substr(0, strnlen(line.c_str(), line.size()));
@@ -435,8 +465,12 @@ int count_modes(std::string line) {
 }
 
 alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t st, alto_dcoo* d) {
+  if (size >= (1ull << 33)) {  // (line slots are counted in 32 bits: a valid line has two bytes or more)
+    set_error("text files of 8 GiB or more are not supported");
+    return ALTO_ERR_UNSUPPORTED;
+  }
   const uint64_t ntiles = (size + kIoTile - 1) / kIoTile;
-  DevBuf file, tiles, starts, valid, scan_scratch, misc;
+  DevBuf file, tiles, starts, scan_scratch, misc;
   ALTO_TRY(file.ensure(ntiles * kIoTile + 16));
   const double t0 = now_ms();
   ALTO_TRY_CUDA(cudaMemsetAsync(file.as<char>() + size, 0, ntiles * kIoTile + 16 - size, st));
@@ -444,108 +478,104 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
   ALTO_TRY(stream_file(fd, 0, size, file.as<char>()));
   d->read_ms = now_ms() - t0;
 
-  cudaEvent_t e0, e1;
-  ALTO_TRY_CUDA(cudaEventCreate(&e0));
-  ALTO_TRY_CUDA(cudaEventCreate(&e1));
+  // device time of the parse: the kernels' spans, without the host work and
+  // allocations between them
+  cudaEvent_t ev[6] = {};
   struct EvGuard {
-    cudaEvent_t a, b;
+    cudaEvent_t* e;
     ~EvGuard() {
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
+      for (int i = 0; i < 6; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
     }
-  } evg{e0, e1};
-  ALTO_TRY_CUDA(cudaEventRecord(e0, st));
+  } evg{ev};
+  for (int i = 0; i < 6; ++i) ALTO_TRY_CUDA(cudaEventCreate(&ev[i]));
+  ALTO_TRY_CUDA(cudaEventRecord(ev[0], st));
   ALTO_TRY(tiles.ensure((ntiles + 1) * 4));
   tns_count_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>());
   ALTO_LAUNCHED();
   ALTO_TRY_CUDA(cudaMemsetAsync(tiles.as<uint32_t>() + ntiles, 0, 4, st));
   ALTO_TRY(exclusive_scan_u32(tiles.as<uint32_t>(), ntiles + 1, scan_scratch, st));
+  ALTO_TRY_CUDA(cudaEventRecord(ev[1], st));
   uint32_t nl = 0;
   ALTO_TRY_CUDA(cudaMemcpyAsync(&nl, tiles.as<uint32_t>() + ntiles, 4, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  if ((uint64_t)nl + 1 >= (1ull << 32) - 1) {
-    set_error("more than 2^32 - 2 lines");
-    return ALTO_ERR_UNSUPPORTED;
-  }
-  const uint32_t nlines = nl + 1;
-  ALTO_TRY(starts.ensure((uint64_t)nlines * 8));
-  tns_starts_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>(),
-                                                              starts.as<uint64_t>());
-  ALTO_LAUNCHED();
-  ALTO_TRY(valid.ensure(((uint64_t)nlines + 1) * 4));
-  ALTO_TRY(misc.ensure(64 + 8 * ALTO_MAX_MODES));
-  uint32_t* first_valid = misc.as<uint32_t>();
-  uint32_t* host_count = first_valid + 1;
-  unsigned long long* ddims = reinterpret_cast<unsigned long long*>(misc.as<char>() + 64);
-  ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
-  ALTO_TRY_CUDA(cudaMemsetAsync(first_valid, 0xff, 4, st));
-  tns_valid_kernel<<<grid_io((uint64_t)nlines + 1, 256), 256, 0, st>>>(
-      file.as<unsigned char>(), size, starts.as<uint64_t>(), nlines, valid.as<uint32_t>(), first_valid);
-  ALTO_LAUNCHED();
-  ALTO_TRY(exclusive_scan_u32(valid.as<uint32_t>(), (uint64_t)nlines + 1, scan_scratch, st));
-  uint32_t hv[2] = {0, 0};
-  ALTO_TRY_CUDA(cudaMemcpyAsync(&hv[0], valid.as<uint32_t>() + nlines, 4, cudaMemcpyDeviceToHost, st));
-  ALTO_TRY_CUDA(cudaMemcpyAsync(&hv[1], first_valid, 4, cudaMemcpyDeviceToHost, st));
-  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  const uint64_t nnz = hv[0];
+  const uint64_t nnz = nl;
   if (nnz == 0) {
     set_error("no nonzero lines in the file (the reference asserts)");
     return ALTO_ERR_INVALID;
   }
+  ALTO_TRY(starts.ensure(nnz * 8));
+  ALTO_TRY_CUDA(cudaEventRecord(ev[2], st));
+  tns_starts_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>(),
+                                                              starts.as<uint64_t>());
+  ALTO_LAUNCHED();
+  ALTO_TRY_CUDA(cudaEventRecord(ev[3], st));
   // the first valid line, on the host, for the mode count
-  uint64_t fl[2] = {0, size};
-  ALTO_TRY_CUDA(cudaMemcpyAsync(fl, starts.as<uint64_t>() + hv[1], hv[1] + 1 < nlines ? 16 : 8,
-                                cudaMemcpyDeviceToHost, st));
+  uint64_t s0 = 0;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&s0, starts.p, 8, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  std::string first(fl[1] - fl[0], '\0');
-  if (pread(fd, &first[0], first.size(), (off_t)fl[0]) != (ssize_t)first.size()) {
-    set_error("could not re-read the first line");
-    return ALTO_ERR_INVALID;
-  }
+  std::string first;
+  ALTO_TRY(read_line(fd, s0, size, &first));
   const int N = count_modes(first);
   if (N < 1 || N > ALTO_MAX_MODES) {
     set_error("the first line gives %d modes (1..%d supported)", N, ALTO_MAX_MODES);
     return N < 1 ? ALTO_ERR_INVALID : ALTO_ERR_UNSUPPORTED;
   }
+  ALTO_TRY(misc.ensure(64 + 8 * ALTO_MAX_MODES));
+  uint32_t* host_count = misc.as<uint32_t>();
+  unsigned long long* ddims = reinterpret_cast<unsigned long long*>(misc.as<char>() + 64);
+  ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
   ALTO_TRY(d->raw.ensure((uint64_t)(N + 1) * nnz * 8));
   uint64_t* idx = d->raw.as<uint64_t>();
   double* vals = reinterpret_cast<double*>(idx + (uint64_t)N * nnz);
+  // lines whose value the host converts: room for 2^20, a rerun with room
+  // for every line when more turn up
+  uint32_t cap = (uint32_t)std::min<uint64_t>(nnz, 1u << 20);
   DevBuf hl;
-  ALTO_TRY(hl.ensure(nnz * 8));
-  tns_parse_kernel<<<grid_io(nlines, 256), 256, 0, st>>>(file.as<unsigned char>(), size, starts.as<uint64_t>(),
-                                                         valid.as<uint32_t>(), nlines, N, zero_based, nnz, idx,
-                                                         vals, ddims, hl.as<uint32_t>(), host_count);
+  ALTO_TRY(hl.ensure((uint64_t)cap * 16));
+  ALTO_TRY_CUDA(cudaEventRecord(ev[4], st));
+  tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
+                                                                    starts.as<uint64_t>(), nnz, N, zero_based, idx,
+                                                                    vals, ddims, hl.as<uint64_t>(), cap, host_count);
   ALTO_LAUNCHED();
-  ALTO_TRY_CUDA(cudaEventRecord(e1, st));
+  ALTO_TRY_CUDA(cudaEventRecord(ev[5], st));
   uint32_t nhost = 0;
   ALTO_TRY_CUDA(cudaMemcpyAsync(d->dims, ddims, 8 * N, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaMemcpyAsync(&nhost, host_count, 4, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  float pm = 0;
-  cudaEventElapsedTime(&pm, e0, e1);
-  d->parse_ms = pm;
+  float pm[3] = {0, 0, 0};
+  for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&pm[i], ev[2 * i], ev[2 * i + 1]);
+  d->parse_ms = (double)pm[0] + pm[1] + pm[2];
+  if (nhost > cap) {  // every listed line again, with room for all
+    cap = (uint32_t)nnz;
+    ALTO_TRY(hl.ensure((uint64_t)cap * 16));
+    ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
+    tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
+                                                                      starts.as<uint64_t>(), nnz, N, zero_based, idx,
+                                                                      vals, ddims, hl.as<uint64_t>(), cap, host_count);
+    ALTO_LAUNCHED();
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&nhost, host_count, 4, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  }
   d->host_lines = nhost;
   if (nhost) {  // values the device left to the C library
-    std::vector<uint32_t> list(2 * (size_t)nhost), at(nhost);
-    std::vector<uint64_t> ses(3 * (size_t)nhost);
+    std::vector<uint64_t> list(2 * (size_t)nhost), ls(nhost);
+    std::vector<uint32_t> at(nhost);
     std::vector<double> v(nhost);
-    DevBuf sesd;
-    ALTO_TRY(sesd.ensure((size_t)nhost * 24));
-    host_lines_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(hl.as<uint32_t>(), nhost, starts.as<uint64_t>(),
-                                                           valid.as<uint32_t>(), nlines, size, sesd.as<uint64_t>());
+    DevBuf lsd;
+    ALTO_TRY(lsd.ensure((size_t)nhost * 8));
+    host_lines_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(hl.as<uint64_t>(), nhost, starts.as<uint64_t>(),
+                                                           lsd.as<uint64_t>());
     ALTO_LAUNCHED();
-    ALTO_TRY_CUDA(cudaMemcpyAsync(list.data(), hl.p, list.size() * 4, cudaMemcpyDeviceToHost, st));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(ses.data(), sesd.p, ses.size() * 8, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(list.data(), hl.p, list.size() * 8, cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(ls.data(), lsd.p, ls.size() * 8, cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
     std::string line;
     for (uint32_t i = 0; i < nhost; ++i) {
-      line.assign(ses[3 * (size_t)i + 1] - ses[3 * (size_t)i], '\0');
-      if (pread(fd, &line[0], line.size(), (off_t)ses[3 * (size_t)i]) != (ssize_t)line.size()) {
-        set_error("could not re-read a line");
-        return ALTO_ERR_INVALID;
-      }
-      at[i] = (uint32_t)ses[3 * (size_t)i + 2];
-      v[i] = strtod(line.c_str() + list[2 * (size_t)i + 1], nullptr);
+      ALTO_TRY(read_line(fd, ls[i], size, &line));
+      at[i] = (uint32_t)list[2 * (size_t)i];
+      const size_t o = (size_t)list[2 * (size_t)i + 1];
+      v[i] = o <= line.size() ? strtod(line.c_str() + o, nullptr) : 0.0;
     }
     DevBuf hb;
     ALTO_TRY(hb.ensure((size_t)nhost * 12));

@@ -155,3 +155,22 @@ def test_cpd64_reads_files(tmp_path, binary):
     assert r.returncode == 0, r.stderr[-2000:]
     assert "tensor: 3 modes, 5000 nonzeros" in r.stdout
     assert r.stdout.count("correct") == 3 and "INCORRECT" not in r.stdout
+
+
+def test_many_values_left_to_host(tmp_path):
+    """More than 2^20 values outside the device's fast path (17 significant
+    digits): the listed lines overflow their first buffer and are listed
+    again; every value still equals the C library's conversion."""
+    rng = np.random.default_rng(10)
+    n = (1 << 20) + 5000
+    c = np.stack([rng.integers(1, 500, n), rng.integers(1, 400, n), rng.integers(1, 300, n)])
+    v = rng.normal(size=n) * 1e-3
+    text = "".join("%d %d %d %.17g\n" % (a, b, d, x) for a, b, d, x in zip(c[0], c[1], c[2], v))
+    (tmp_path / "long.tns").write_text(text)
+    t = A.read_tensor(tmp_path / "long.tns")
+    got_c, got_v = t.to_host()
+    assert t.stats()["host_values"] > (1 << 20)
+    assert np.array_equal(got_c, (c - 1).astype(np.uint64))
+    want = np.array([float(ln.rsplit(" ", 1)[1]) for ln in text.splitlines()])
+    assert np.array_equal(got_v, want)
+    t.close()
