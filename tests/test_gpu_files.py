@@ -162,7 +162,7 @@ def test_many_values_left_to_host(tmp_path):
     digits): the listed lines overflow their first buffer and are listed
     again; every value still equals the C library's conversion."""
     rng = np.random.default_rng(10)
-    n = (1 << 20) + 5000
+    n = 1_300_000  # (about 9 in 10 of these values need all 17 digits)
     c = np.stack([rng.integers(1, 500, n), rng.integers(1, 400, n), rng.integers(1, 300, n)])
     v = rng.normal(size=n) * 1e-3
     text = "".join("%d %d %d %.17g\n" % (a, b, d, x) for a, b, d, x in zip(c[0], c[1], c[2], v))
