@@ -3,6 +3,7 @@
 // every entry point validates its arguments and returns an alto_status.
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "alto_internal.cuh"
@@ -12,6 +13,26 @@ namespace alto {
 std::atomic<uint64_t> g_kernel_launches{0};
 thread_local cudaStream_t tls_alloc_stream = nullptr;
 static thread_local char g_err[512] = "";
+
+cudaMemPool_t transient_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;  // keep freed memory for the next call
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
 
 void set_error(const char* fmt, ...) {
   va_list ap;

@@ -90,6 +90,49 @@ struct DevBuf {
   }
 };
 
+// Transient device memory from a stream-ordered pool the library owns, one
+// per device, which keeps what is freed for the next allocation (its memory
+// stays reserved until the process exits).  For buffers that live within
+// one call and are several GB: cudaMalloc / cudaFree of such sizes cost
+// milliseconds each and cudaFree synchronises the device.  Freed in stream
+// order on the stream given to ensure(); any other stream that used the
+// buffer must be complete before release.
+cudaMemPool_t transient_pool();
+struct PoolBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  PoolBuf() = default;
+  PoolBuf(const PoolBuf&) = delete;
+  PoolBuf& operator=(const PoolBuf&) = delete;
+  ~PoolBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    bytes = 0;
+  }
+  // At least n bytes on stream s; contents are not preserved on growth.
+  alto_status ensure(size_t n, cudaStream_t s) {
+    if (n <= bytes && p && s == st) return ALTO_OK;
+    release();
+    cudaMemPool_t pool = transient_pool();
+    if (!pool) return cuda_status(cudaErrorInvalidDevice, "transient pool", __FILE__, __LINE__);
+    st = s;
+    const size_t want = n < 256 ? 256 : n;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_status(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+    }
+    bytes = want;
+    return ALTO_OK;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 // ------------------------------------------------------------- ALTO keys
 
 struct Key2 {

@@ -470,8 +470,9 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
     return ALTO_ERR_UNSUPPORTED;
   }
   const uint64_t ntiles = (size + kIoTile - 1) / kIoTile;
-  DevBuf file, tiles, starts, scan_scratch, misc;
-  ALTO_TRY(file.ensure(ntiles * kIoTile + 16));
+  PoolBuf file, starts;  // (transient: the library pool keeps them for the next read)
+  DevBuf tiles, scan_scratch, misc;
+  ALTO_TRY(file.ensure(ntiles * kIoTile + 16, st));
   const double t0 = now_ms();
   ALTO_TRY_CUDA(cudaMemsetAsync(file.as<char>() + size, 0, ntiles * kIoTile + 16 - size, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // the padding is cleared before the readers copy
@@ -504,7 +505,7 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
     set_error("no nonzero lines in the file (the reference asserts)");
     return ALTO_ERR_INVALID;
   }
-  ALTO_TRY(starts.ensure(nnz * 8));
+  ALTO_TRY(starts.ensure(nnz * 8, st));
   ALTO_TRY_CUDA(cudaEventRecord(ev[2], st));
   tns_starts_kernel<<<(unsigned)ntiles, kIoThreads, 0, st>>>(file.as<uint4>(), size, tiles.as<uint32_t>(),
                                                               starts.as<uint64_t>());
@@ -531,8 +532,8 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
   // lines whose value the host converts: room for 2^20, a rerun with room
   // for every line when more turn up
   uint32_t cap = (uint32_t)std::min<uint64_t>(nnz, 1u << 20);
-  DevBuf hl;
-  ALTO_TRY(hl.ensure((uint64_t)cap * 16));
+  PoolBuf hl;
+  ALTO_TRY(hl.ensure((uint64_t)cap * 16, st));
   ALTO_TRY_CUDA(cudaEventRecord(ev[4], st));
   tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
                                                                     starts.as<uint64_t>(), nnz, N, zero_based, idx,
@@ -548,7 +549,7 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
   d->parse_ms = (double)pm[0] + pm[1] + pm[2];
   if (nhost > cap) {  // every listed line again, with room for all
     cap = (uint32_t)nnz;
-    ALTO_TRY(hl.ensure((uint64_t)cap * 16));
+    ALTO_TRY(hl.ensure((uint64_t)cap * 16, st));
     ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
     tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
                                                                       starts.as<uint64_t>(), nnz, N, zero_based, idx,

@@ -206,11 +206,13 @@ struct alto_slicer {
   uint64_t dims[ALTO_MAX_MODES] = {};
   alto_dtype vdt = ALTO_F64;
   cudaStream_t st = nullptr;
-  DevBuf idx;    // [N][nnz] uint32: labels; the stream mode's row holds batch-local time
-  DevBuf gtime;  // [nnz] uint32: time step of each sorted position
-  DevBuf vals;   // [nnz] values in sorted order, input dtype
-  DevBuf ptime;  // stream_prev's time indices
-  DevBuf iperm;  // per non-stream mode, original index of each label
+  // (from the library's pool, on st; alto_slicer_destroy waits for the
+  // whole device before they return to it, as cudaFree would)
+  PoolBuf idx;    // [N][nnz] uint32: labels; the stream mode's row holds batch-local time
+  PoolBuf gtime;  // [nnz] uint32: time step of each sorted position
+  PoolBuf vals;   // [nnz] values in sorted order, input dtype
+  PoolBuf ptime;  // stream_prev's time indices
+  PoolBuf iperm;  // per non-stream mode, original index of each label
   uint64_t iperm_off[ALTO_MAX_MODES] = {};
   std::vector<uint32_t> off;  // [T + 1]
   std::vector<uint32_t> cnt;  // [N][T + 1]
@@ -220,7 +222,7 @@ struct alto_slicer {
   const void* bptr[ALTO_MAX_MODES] = {};
   const void* pptr[ALTO_MAX_MODES] = {};
   std::vector<uint64_t> cut_start, cut_end, cut_dims;  // alto_slicer_cut_all's batches
-  DevBuf steptab;                                     // each time step's batch first step
+  PoolBuf steptab;                                    // each time step's batch first step
   uint64_t tdims[ALTO_MAX_MODES] = {};  // the whole tensor's view
   const void* tptr[ALTO_MAX_MODES] = {};
 };
@@ -260,12 +262,13 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   const size_t cap = std::max<uint64_t>(nnz, 1);
   const size_t tiles = std::max<uint32_t>(sort_tiles(nnz), 1);
   const size_t nflag = (size_t)N * (nnz + 1);
-  ALTO_TRY(s->idx.ensure((size_t)N * cap * 4));
-  ALTO_TRY(s->gtime.ensure(cap * 4));
-  ALTO_TRY(s->vals.ensure(cap * vbytes));
-  ALTO_TRY(s->iperm.ensure(std::max<uint64_t>(nfirst, 1) * 4));
+  ALTO_TRY(s->idx.ensure((size_t)N * cap * 4, st));
+  ALTO_TRY(s->gtime.ensure(cap * 4, st));
+  ALTO_TRY(s->vals.ensure(cap * vbytes, st));
+  ALTO_TRY(s->iperm.ensure(std::max<uint64_t>(nfirst, 1) * 4, st));
 
-  DevBuf scratch, scan_scratch;
+  PoolBuf scratch;  // (transient: the library pool keeps it for the next slicer)
+  DevBuf scan_scratch;
   size_t o = 0;
   const size_t o_lo0 = o; o = align256(o + cap * 8);
   const size_t o_lo1 = o; o = align256(o + cap * 8);
@@ -280,7 +283,7 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   const size_t o_err = o; o = align256(o + 4);
   const size_t o_vin = o; o = align256(o + (coo->on_device ? 0 : cap * vbytes));
   const size_t o_cin = o; o = align256(o + (coo->on_device ? 0 : (size_t)N * cap * coo->index_bytes));
-  ALTO_TRY(scratch.ensure(o));
+  ALTO_TRY(scratch.ensure(o, st));
   char* sb = scratch.as<char>();
   uint64_t* klo[2] = {(uint64_t*)(sb + o_lo0), (uint64_t*)(sb + o_lo1)};
   uint64_t* khi[2] = {two_words ? (uint64_t*)(sb + o_hi0) : nullptr, two_words ? (uint64_t*)(sb + o_hi1) : nullptr};
@@ -504,7 +507,7 @@ alto_status alto_slicer_cut_all(alto_slicer* s, uint64_t nnz_threshold, uint64_t
     for (int m = 0; m < N; ++m) s->cut_dims.push_back(s->bdims[m]);
   }
   if (s->nnz > p0) {
-    ALTO_TRY(s->steptab.ensure((s->T + 1) * 4));
+    ALTO_TRY(s->steptab.ensure((s->T + 1) * 4, s->st));
     ALTO_TRY_CUDA(cudaMemcpyAsync(s->steptab.p, first_of.data(), (s->T + 1) * 4, cudaMemcpyHostToDevice, s->st));
     slice_local_time_all_kernel<<<grid_n(s->nnz - p0, 256), 256, 0, s->st>>>(
         s->gtime.as<uint32_t>(), p0, s->nnz - p0, s->steptab.as<uint32_t>(), s->idx.as<uint32_t>() + (size_t)s->t * s->nnz);
@@ -544,7 +547,7 @@ alto_status alto_slicer_stream_prev(alto_slicer* s, uint64_t previous, alto_coo*
   const uint64_t start_time = previous < s->step ? s->step - previous : 0;
   const uint64_t start = s->off[std::min(start_time, s->T)], end = s->ptr;
   const uint64_t n = end > start ? end - start : 0;
-  ALTO_TRY(s->ptime.ensure(std::max<uint64_t>(n, 1) * 4));
+  ALTO_TRY(s->ptime.ensure(std::max<uint64_t>(n, 1) * 4, s->st));
   if (n) {
     slice_local_time_kernel<<<grid_n(n, 256), 256, 0, s->st>>>(s->gtime.as<uint32_t>(), (uint32_t)start,
                                                                 (uint32_t)n, (uint32_t)start_time,
@@ -591,7 +594,7 @@ alto_status alto_slicer_iperm(alto_slicer* s, int mode, uint64_t* host_out, uint
 
 alto_status alto_slicer_destroy(alto_slicer* s) {
   if (s) {
-    cudaStreamSynchronize(s->st);
+    cudaDeviceSynchronize();  // batches may be in use on any stream
     delete s;
   }
   return ALTO_OK;

@@ -293,7 +293,10 @@ typedef struct alto_dcoo alto_dcoo;
  * is streamed into HBM and parsed there; values equal the C library's
  * strtod bit for bit.  Binary: uint64 nmodes, dims[nmodes], nnz, the index
  * arrays mode by mode, float64 values.  An unreadable file, a file without
- * nonzeros or a short binary file is ALTO_ERR_INVALID.  Synchronous. */
+ * nonzeros or a short binary file is ALTO_ERR_INVALID.  The read's working
+ * buffers (about the file's size plus 8 bytes per line) come from a device
+ * memory pool the library keeps for later reads and slicers until the
+ * process exits.  Synchronous. */
 alto_status alto_read_tensor(const char* path, alto_file_format format, int zero_based,
                              alto_cuda_stream stream, alto_dcoo** out);
 /* A device view of the tensor (on_device 1, index_bytes 8, ALTO_F64), valid
@@ -329,7 +332,9 @@ typedef struct alto_slicer alto_slicer;
 /* StreamingSparseTensor(sp, stream_mode), src/streaming_sptensor.cpp:69-125.
  * coo: host or device COO; dims[m] < 2^32, nmodes * (nnz + 1) < 2^32 and
  * the bits of all dims <= 128 (ALTO_ERR_UNSUPPORTED otherwise); an index
- * outside its mode is ALTO_ERR_INVALID.  Synchronous. */
+ * outside its mode is ALTO_ERR_INVALID.  Construction's working buffers
+ * (about 60 bytes per nonzero) come from the library's device memory pool
+ * (kept for later calls, as alto_read_tensor's).  Synchronous. */
 alto_status alto_slicer_create(const alto_coo* coo, int stream_mode, alto_cuda_stream stream,
                                alto_slicer** out);
 /* next_dynamic_batch(nnz_threshold, timeslice_limit), :196-264: grow the
