@@ -1097,6 +1097,11 @@ def ours_tns(args):
     peak, peak_kind = measured_peaks()
     algo = size + n_read * 4 * 8
     achieved = algo / (parse_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "tns_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f)["bytes_per_line"] * n_read
     line = {
         "metric": TNS_METRIC, "value": n_read / (parse_ms * 1e-3), "unit": "nnz/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": parse_ms, "higher_is_better": True,
@@ -1108,7 +1113,7 @@ def ours_tns(args):
                    "timing": "value: CUDA events around the device parse (file bytes in HBM); "
                              "e2e: host clock around alto_read_tensor, file in the page cache"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "the device parse (all kernels after the file is in HBM)",
+                     "traffic": traffic, "kernel": "the device parse (all kernels after the file is in HBM)",
                      "algorithmic_bytes": "the file once, plus 3 uint64 indices and a float64 value per nonzero",
                      "peak_kind": peak_kind},
         "cpu_baseline": None,
