@@ -1,8 +1,9 @@
 // Tensor files (the reference's ImportSparseTensor / ExportSparseTensor,
 // src/sptensor.cpp:22-249), with the parse on the device.
 //
-// Text (.tns) import.  The file is streamed into HBM by eight reader
-// threads through pinned staging buffers; then, all on the device:
+// Text (.tns) import.  The file is streamed into HBM by reader threads (one
+// per host hardware thread, 4 to 16) through pinned staging buffers; then,
+// all on the device:
 //   1. per 16 KiB tile, the line starts that getline's rule keeps (more
 //      than one byte read, no leading '#'), counted from 16-byte loads
 //      (tns_count_kernel); an exclusive scan over the tiles gives each kept
@@ -327,9 +328,15 @@ double now_ms() {
 }
 
 // Pinned staging for file reads, kept per device for the life of the
-// process (pinning is slow; a read should not pay for it): kReaders reader
+// process (pinning is slow; a read should not pay for it): up to kReaders
+// reader
 // threads, each with two buffers and its own non-blocking stream.
-constexpr int kReaders = 8;
+constexpr int kReaders = 16;  // (used: the host's hardware threads, 4 .. 16)
+
+int reader_count() {
+  static const int n = (int)std::min(16u, std::max(4u, std::thread::hardware_concurrency()));
+  return n;
+}
 
 struct Staging {
   std::mutex mu;  // one read at a time per device
@@ -339,7 +346,7 @@ struct Staging {
   bool ready = false;
   alto_status init() {
     if (ready) return ALTO_OK;
-    for (int r = 0; r < kReaders; ++r) {
+    for (int r = 0; r < reader_count(); ++r) {
       ALTO_TRY_CUDA(cudaStreamCreateWithFlags(&st[r], cudaStreamNonBlocking));
       for (int i = 0; i < 2; ++i) {
         ALTO_TRY_CUDA(cudaHostAlloc(&buf[r][i], kStage, cudaHostAllocDefault));
@@ -362,7 +369,7 @@ Staging* staging_for_device() {
 }
 
 // Read bytes [off, off + n) of fd into device memory dst: chunk c goes to
-// reader c % kReaders, which reads it into one of its pinned buffers and
+// reader c % (reader count), which reads it into one of its pinned buffers and
 // copies it on its own stream, so file reads and copies overlap.  Every copy
 // is complete on return (work that follows on any stream sees the bytes).
 alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst) {
@@ -374,7 +381,7 @@ alto_status stream_file(int fd, uint64_t off, uint64_t n, char* dst) {
   std::lock_guard<std::mutex> lock(sg->mu);
   ALTO_TRY(sg->init());
   const uint64_t nchunks = (n + kStage - 1) / kStage;
-  const int nr = (int)std::min<uint64_t>(kReaders, std::max<uint64_t>(nchunks, 1));
+  const int nr = (int)std::min<uint64_t>(reader_count(), std::max<uint64_t>(nchunks, 1));
   std::atomic<int> failed{0};
   std::vector<std::string> errs(nr);
   auto reader = [&](int r) {
