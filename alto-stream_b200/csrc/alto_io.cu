@@ -142,26 +142,43 @@ __device__ __forceinline__ bool is_space(unsigned c) {
   return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
 }
 
+// Byte sources for the parse: at(q) is byte q of the line's buffer, 0 (the
+// C string's terminator) at or past the end.  Shared memory with 32-bit
+// offsets for staged lines, global memory otherwise.
+struct SmemBytes {
+  const unsigned char* b;
+  uint32_t e;
+  __device__ __forceinline__ unsigned at(uint32_t q) const { return q < e ? (unsigned)b[q] : 0u; }
+};
+struct GlobalBytes {
+  const unsigned char* b;
+  uint64_t e;
+  __device__ __forceinline__ unsigned at(uint64_t q) const { return q < e ? (unsigned)__ldg(b + q) : 0u; }
+};
+
 // strtoull(p, &end, 10) on the line at p: the line ends at its newline, a
-// NUL or e (the reference parses one getline buffer, so nothing after the
-// newline is reached: skipping whitespace stops there as it stops at the
-// buffer's terminating NUL).
-__device__ uint64_t dev_strtoull(const unsigned char* __restrict__ buf, uint64_t& p, uint64_t e) {
-  uint64_t q = p;
-  while (q < e && buf[q] && buf[q] != '\n' && is_space(buf[q])) ++q;
+// NUL or the buffer's end (the reference parses one getline buffer, so
+// nothing after the newline is reached: skipping whitespace stops there as
+// it stops at the buffer's terminating NUL).
+template <typename Src, typename Pos>
+__device__ __forceinline__ uint64_t dev_strtoull(const Src& s, Pos& p) {
+  Pos q = p;
+  unsigned c = s.at(q);
+  while (c != 0u && c != '\n' && is_space(c)) c = s.at(++q);
   bool neg = false;
-  if (q < e && (buf[q] == '+' || buf[q] == '-')) {
-    neg = buf[q] == '-';
-    ++q;
+  if (c == '+' || c == '-') {
+    neg = c == '-';
+    c = s.at(++q);
   }
   uint64_t v = 0;
   bool any = false, over = false;
-  while (q < e && buf[q] >= '0' && buf[q] <= '9') {
-    const uint64_t d = buf[q] - '0';
-    if (v > (~0ull - d) / 10) over = true;
+  constexpr uint64_t kMax10 = 1844674407370955161ull;  // (2^64 - 1) / 10, remainder 5
+  while (c - '0' < 10u) {
+    const unsigned d = c - '0';
+    if (v > kMax10 || (v == kMax10 && d > 5)) over = true;
     v = v * 10 + d;
     any = true;
-    ++q;
+    c = s.at(++q);
   }
   if (!any) return 0;  // no conversion: the end pointer stays at p
   p = q;
@@ -170,36 +187,38 @@ __device__ uint64_t dev_strtoull(const unsigned char* __restrict__ buf, uint64_t
 }
 
 // strtod's decimal fast path; false when the host must convert the text.
-__device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, uint64_t e, double& out) {
-  uint64_t q = p;
-  while (q < e && buf[q] && buf[q] != '\n' && is_space(buf[q])) ++q;
+template <typename Src, typename Pos>
+__device__ __forceinline__ bool dev_strtod(const Src& s, Pos p, double& out) {
+  Pos q = p;
+  unsigned c = s.at(q);
+  while (c != 0u && c != '\n' && is_space(c)) c = s.at(++q);
   bool neg = false;
-  if (q < e && (buf[q] == '+' || buf[q] == '-')) {
-    neg = buf[q] == '-';
-    ++q;
+  if (c == '+' || c == '-') {
+    neg = c == '-';
+    c = s.at(++q);
   }
-  if (q < e) {  // hexadecimal, inf, nan: the host converts
-    const unsigned c = buf[q] | 0x20u;
-    if (c == 'i' || c == 'n') return false;
-    if (buf[q] == '0' && q + 1 < e && (buf[q + 1] | 0x20u) == 'x') return false;
+  {  // hexadecimal, inf, nan: the host converts
+    const unsigned lc = c | 0x20u;
+    if (lc == 'i' || lc == 'n') return false;
+    if (c == '0' && (s.at(q + 1) | 0x20u) == 'x') return false;
   }
   uint64_t w = 0;
   int nd = 0, ex = 0;
   bool any = false;
-  while (q < e && buf[q] >= '0' && buf[q] <= '9') {
-    const unsigned d = buf[q] - '0';
+  while (c - '0' < 10u) {
+    const unsigned d = c - '0';
     any = true;
     if (w != 0 || d != 0) {  // (leading zeros carry no digit)
       if (nd == 19) return false;
       w = w * 10 + d;
       ++nd;
     }
-    ++q;
+    c = s.at(++q);
   }
-  if (q < e && buf[q] == '.') {
-    ++q;
-    while (q < e && buf[q] >= '0' && buf[q] <= '9') {
-      const unsigned d = buf[q] - '0';
+  if (c == '.') {
+    c = s.at(++q);
+    while (c - '0' < 10u) {
+      const unsigned d = c - '0';
       any = true;
       if (w != 0 || d != 0) {
         if (nd == 19) return false;
@@ -207,25 +226,26 @@ __device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, ui
         ++nd;
       }
       --ex;
-      ++q;
+      c = s.at(++q);
     }
   }
   if (!any) {  // no conversion
     out = 0.0;
     return true;
   }
-  if (q < e && (buf[q] | 0x20u) == 'e') {
-    uint64_t r = q + 1;
+  if ((c | 0x20u) == 'e') {
+    Pos r = q + 1;
+    unsigned ce = s.at(r);
     bool eneg = false;
-    if (r < e && (buf[r] == '+' || buf[r] == '-')) {
-      eneg = buf[r] == '-';
-      ++r;
+    if (ce == '+' || ce == '-') {
+      eneg = ce == '-';
+      ce = s.at(++r);
     }
-    if (r < e && buf[r] >= '0' && buf[r] <= '9') {
+    if (ce - '0' < 10u) {
       int x = 0;
-      while (r < e && buf[r] >= '0' && buf[r] <= '9') {
-        if (x < 100000) x = x * 10 + (buf[r] - '0');
-        ++r;
+      while (ce - '0' < 10u) {
+        if (x < 100000) x = x * 10 + (int)(ce - '0');
+        ce = s.at(++r);
       }
       ex += eneg ? -x : x;
     }
@@ -255,11 +275,39 @@ __device__ bool dev_strtod(const unsigned char* __restrict__ buf, uint64_t p, ui
   return true;
 }
 
+// One line: nmodes indices and the value (its slot k, the line's start s).
+// NM > 0: the mode count at compile time (the loop unrolls and dmax stays in
+// registers); NM = 0: nmodes at run time.
+template <int NM, typename Src, typename Pos>
+__device__ __forceinline__ void parse_line(const Src& src, Pos s, uint64_t k, int nmodes, uint64_t zero_based,
+                                           uint64_t nnz, uint64_t* __restrict__ idx, double* __restrict__ vals,
+                                           uint64_t (&dmax)[ALTO_MAX_MODES], uint64_t* __restrict__ host_list,
+                                           uint32_t host_cap, uint32_t* __restrict__ host_count) {
+  const uint64_t one_based = zero_based ? 0 : 1;
+  Pos p = s;
+#pragma unroll
+  for (int m = 0; m < (NM ? NM : nmodes); ++m) {
+    const uint64_t x = dev_strtoull(src, p);
+    dmax[m] = max(dmax[m], x + zero_based);
+    idx[(uint64_t)m * nnz + k] = x - one_based;
+  }
+  double v = 0.0;
+  if (!dev_strtod(src, p, v)) {  // the host converts this value (line start + value offset)
+    const uint32_t h = atomicAdd(host_count, 1u);
+    if (h < host_cap) {  // (past the capacity the count still grows; the host then reruns)
+      host_list[2 * (uint64_t)h] = k;
+      host_list[2 * (uint64_t)h + 1] = (uint64_t)(p - s);
+    }
+  }
+  vals[k] = v;
+}
+
 constexpr int kStageBytes = 24 << 10;  // a block's lines staged in shared memory
 
 // One thread per valid line.  A block takes 256 consecutive lines; when
 // their bytes fit kStageBytes they are staged in shared memory with 16-byte
 // loads and parsed from there, else parsed from global memory.
+template <int NM>
 __global__ void __launch_bounds__(kIoThreads)
     tns_parse_kernel(const unsigned char* __restrict__ buf, uint64_t size, const uint64_t* __restrict__ starts,
                      uint64_t nnz, int nmodes, uint64_t zero_based, uint64_t* __restrict__ idx,
@@ -268,7 +316,6 @@ __global__ void __launch_bounds__(kIoThreads)
   __shared__ __align__(16) unsigned char sm[kStageBytes];
   uint64_t dmax[ALTO_MAX_MODES];
   for (int m = 0; m < ALTO_MAX_MODES; ++m) dmax[m] = 0;
-  const uint64_t one_based = zero_based ? 0 : 1;
   for (uint64_t k0 = (uint64_t)blockIdx.x * kIoThreads; k0 < nnz; k0 += (uint64_t)gridDim.x * kIoThreads) {
     const uint64_t k1 = min(k0 + kIoThreads, nnz);
     const uint64_t lo = starts[k0], hi = k1 < nnz ? starts[k1] : size;
@@ -281,28 +328,35 @@ __global__ void __launch_bounds__(kIoThreads)
     __syncthreads();
     const uint64_t k = k0 + threadIdx.x;
     if (k < k1) {
-      const unsigned char* b = staged ? sm : buf;
-      const uint64_t off = staged ? alo : 0;
-      const uint64_t s = starts[k] - off, e = hi - off;
-      uint64_t p = s;
-      for (int m = 0; m < nmodes; ++m) {
-        const uint64_t x = dev_strtoull(b, p, e);
-        dmax[m] = max(dmax[m], x + zero_based);
-        idx[(uint64_t)m * nnz + k] = x - one_based;
-      }
-      double v = 0.0;
-      if (!dev_strtod(b, p, e, v)) {  // the host converts this value (line start + value offset)
-        const uint32_t h = atomicAdd(host_count, 1u);
-        if (h < host_cap) {  // (past the capacity the count still grows; the host then reruns)
-          host_list[2 * (uint64_t)h] = k;
-          host_list[2 * (uint64_t)h + 1] = p - s;
-        }
-      }
-      vals[k] = v;
+      if (staged)
+        parse_line<NM>(SmemBytes{sm, (uint32_t)span}, (uint32_t)(starts[k] - alo), k, nmodes, zero_based, nnz,
+                       idx, vals, dmax, host_list, host_cap, host_count);
+      else
+        parse_line<NM>(GlobalBytes{buf, hi}, starts[k], k, nmodes, zero_based, nnz, idx, vals, dmax, host_list,
+                       host_cap, host_count);
     }
     __syncthreads();
   }
-  for (int m = 0; m < nmodes; ++m) atomicMax(dims + m, (unsigned long long)dmax[m]);
+#pragma unroll
+  for (int m = 0; m < (NM ? NM : nmodes); ++m) atomicMax(dims + m, (unsigned long long)dmax[m]);
+}
+
+// The parse for nmodes modes (3 and 4 compiled for their count).
+alto_status launch_parse(unsigned grid, cudaStream_t st, const unsigned char* buf, uint64_t size,
+                         const uint64_t* starts, uint64_t nnz, int nmodes, uint64_t zero_based, uint64_t* idx,
+                         double* vals, unsigned long long* dims, uint64_t* host_list, uint32_t host_cap,
+                         uint32_t* host_count) {
+  if (nmodes == 3)
+    tns_parse_kernel<3><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
+                                                     host_list, host_cap, host_count);
+  else if (nmodes == 4)
+    tns_parse_kernel<4><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
+                                                     host_list, host_cap, host_count);
+  else
+    tns_parse_kernel<0><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
+                                                     host_list, host_cap, host_count);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
 }
 
 // For each listed line: its start in the file (one copy to the host).
@@ -542,10 +596,8 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
   PoolBuf hl;
   ALTO_TRY(hl.ensure((uint64_t)cap * 16, st));
   ALTO_TRY_CUDA(cudaEventRecord(ev[4], st));
-  tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
-                                                                    starts.as<uint64_t>(), nnz, N, zero_based, idx,
-                                                                    vals, ddims, hl.as<uint64_t>(), cap, host_count);
-  ALTO_LAUNCHED();
+  ALTO_TRY(launch_parse(grid_io(nnz, kIoThreads), st, file.as<unsigned char>(), size, starts.as<uint64_t>(), nnz, N,
+                        zero_based, idx, vals, ddims, hl.as<uint64_t>(), cap, host_count));
   ALTO_TRY_CUDA(cudaEventRecord(ev[5], st));
   uint32_t nhost = 0;
   ALTO_TRY_CUDA(cudaMemcpyAsync(d->dims, ddims, 8 * N, cudaMemcpyDeviceToHost, st));
@@ -558,10 +610,8 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
     cap = (uint32_t)nnz;
     ALTO_TRY(hl.ensure((uint64_t)cap * 16, st));
     ALTO_TRY_CUDA(cudaMemsetAsync(misc.p, 0, 64 + 8 * ALTO_MAX_MODES, st));
-    tns_parse_kernel<<<grid_io(nnz, kIoThreads), kIoThreads, 0, st>>>(file.as<unsigned char>(), size,
-                                                                      starts.as<uint64_t>(), nnz, N, zero_based, idx,
-                                                                      vals, ddims, hl.as<uint64_t>(), cap, host_count);
-    ALTO_LAUNCHED();
+    ALTO_TRY(launch_parse(grid_io(nnz, kIoThreads), st, file.as<unsigned char>(), size, starts.as<uint64_t>(), nnz,
+                          N, zero_based, idx, vals, ddims, hl.as<uint64_t>(), cap, host_count));
     ALTO_TRY_CUDA(cudaMemcpyAsync(&nhost, host_count, 4, cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
   }
