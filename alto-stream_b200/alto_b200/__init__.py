@@ -52,7 +52,7 @@ EXPORTED = [
     "alto_read_tensor", "alto_dcoo_view", "alto_dcoo_stats", "alto_dcoo_to_host", "alto_dcoo_destroy", "alto_write_tensor",
     "alto_slicer_create", "alto_slicer_next", "alto_slicer_cut_all", "alto_slicer_batch", "alto_slicer_last_batch", "alto_slicer_stream_prev",
     "alto_slicer_iperm", "alto_slicer_tensor", "alto_slicer_destroy",
-    "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait",
+    "alto_server_create", "alto_server_open", "alto_server_submit", "alto_server_wait", "alto_server_poll",
     "alto_server_drain", "alto_server_stats", "alto_server_factor", "alto_server_close", "alto_server_destroy",
 ]
 
@@ -673,6 +673,12 @@ class Server:
         inner, lat = c_int(), c_double()
         check(lib().alto_server_wait(self.h, c_uint64(ticket), byref(inner), byref(lat)))
         return inner.value, lat.value
+
+    def poll(self, ticket):
+        """None while the slice is queued or running, else (inner iterations, latency ms)."""
+        done, inner, lat = c_int(), c_int(), c_double()
+        check(lib().alto_server_poll(self.h, c_uint64(ticket), byref(done), byref(inner), byref(lat)))
+        return (inner.value, lat.value) if done.value else None
 
     def drain(self):
         check(lib().alto_server_drain(self.h))

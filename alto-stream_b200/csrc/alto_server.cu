@@ -326,6 +326,24 @@ alto_status alto_server_wait(alto_server* s, uint64_t ticket, int* inner_iters, 
   return ti.status;
 }
 
+alto_status alto_server_poll(alto_server* s, uint64_t ticket, int* done, int* inner_iters, double* latency_ms) {
+  if (!s || !done) {
+    set_error("server or done is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) {
+    set_error("unknown ticket %llu", (unsigned long long)ticket);
+    return ALTO_ERR_INVALID;
+  }
+  *done = it->second.done ? 1 : 0;
+  if (!it->second.done) return ALTO_OK;
+  if (inner_iters) *inner_iters = it->second.inner;
+  if (latency_ms) *latency_ms = it->second.latency_ms;
+  return it->second.status;
+}
+
 alto_status alto_server_drain(alto_server* s) {
   if (!s) {
     set_error("server is NULL");

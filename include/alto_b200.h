@@ -416,6 +416,9 @@ alto_status alto_server_submit(alto_server* s, int sid, const alto_coo* batch, c
                                uint64_t n_init, uint64_t* ticket);
 /* Wait for one slice; its status, inner iterations and latency. */
 alto_status alto_server_wait(alto_server* s, uint64_t ticket, int* inner_iters, double* latency_ms);
+/* The same without waiting: *done = 0 while the slice is queued or running
+ * (ALTO_OK), else 1 with alto_server_wait's outputs and status. */
+alto_status alto_server_poll(alto_server* s, uint64_t ticket, int* done, int* inner_iters, double* latency_ms);
 /* Wait until every admitted stream has processed all its slices. */
 alto_status alto_server_drain(alto_server* s);
 alto_status alto_server_stats(alto_server* s, alto_serving_stats* out);

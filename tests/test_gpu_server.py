@@ -89,8 +89,10 @@ def test_admission_waits_for_budget():
     submit_all(srv, s1, b1, iv1, 8)
     srv.drain()
     assert srv.stats()["completed"] == 3  # only the admitted stream ran
+    assert srv.poll(t2[-1]) is None  # queued behind the budget
     srv.close(s1)
-    srv.wait(t2[-1])
+    got = srv.wait(t2[-1])
     assert srv.stats()["completed"] == 6
+    assert srv.poll(t2[-1]) == got
     srv.close(s2)
     srv.destroy()
