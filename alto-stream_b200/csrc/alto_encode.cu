@@ -168,8 +168,14 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 // Stable scatter of one tile: elements are ranked in index order, round by
-// round (round r holds elements base + r*256 + thread), with per-warp
-// digit counts combined in warp order and a running per-digit count.
+// round (round r holds elements base + r*256 + thread), with per-warp digit
+// counts combined in warp order and a running per-digit count.  The ranked
+// tile is then reordered by digit in shared memory and written out in that
+// order, so consecutive threads write consecutive addresses of a digit's
+// run (writing each element straight to its destination spreads a warp's
+// stores over up to 32 buckets).  Dynamic shared memory: the tile's keys
+// (one or two words) and payloads.
+static_assert(kRadix == kSortThreads, "one digit per thread in the tile's digit scan");
 __global__ void __launch_bounds__(kSortThreads)
     radix_scatter_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
                          const uint32_t* __restrict__ pin, uint32_t n, int shift,
@@ -180,53 +186,96 @@ __global__ void __launch_bounds__(kSortThreads)
   __shared__ uint32_t warp_cnt[kWarps][kRadix];
   __shared__ uint32_t running[kRadix];
   __shared__ uint32_t gbase[kRadix];
+  __shared__ uint32_t lstart[kRadix];
+  __shared__ uint32_t wsum[kWarps];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  uint64_t* s_lo = reinterpret_cast<uint64_t*>(dsm);
+  uint64_t* s_hi = s_lo + kSortTile;
+  uint32_t* s_p = reinterpret_cast<uint32_t*>(khi ? s_hi + kSortTile : s_lo + kSortTile);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int d = tid; d < kRadix; d += kSortThreads) {
-    running[d] = 0;
-    gbase[d] = offsets[(size_t)d * ntiles + blockIdx.x];
-  }
-  uint32_t base = blockIdx.x * kSortTile;
-  for (int r = 0; r < kSortItems; ++r) {
-    for (int d = tid; d < kRadix; d += kSortThreads)
+  running[tid] = 0;
+  gbase[tid] = offsets[(size_t)tid * ntiles + blockIdx.x];
+  const uint32_t base = blockIdx.x * kSortTile;
+  uint64_t vlo[kSortItems], vhi[kSortItems];
+  uint32_t vp[kSortItems], dg[kSortItems], rk[kSortItems];
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) warp_cnt[w][d] = 0;
+  for (int r = 0; r < kSortItems; ++r) {
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) warp_cnt[w][tid] = 0;
     __syncthreads();
-    uint32_t i = base + r * kSortThreads + tid;
-    bool valid = i < n;
-    uint32_t d = 0, lane_rank = 0;
-    uint64_t vlo = 0, vhi = 0;
-    uint32_t vp = 0;
-    unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    const uint32_t i = base + r * kSortThreads + tid;
+    const bool valid = i < n;
+    uint32_t lane_rank = 0;
+    vlo[r] = 0;
+    vhi[r] = 0;
+    vp[r] = 0;
+    dg[r] = 0;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      vlo = klo[i];
-      vhi = khi ? khi[i] : 0;
-      vp = pin[i];
-      d = (uint32_t)((shift >= 64 ? vhi : vlo) >> (shift & 63)) & (kRadix - 1);
-      unsigned peers = __match_any_sync(vmask, d);
+      vlo[r] = klo[i];
+      vhi[r] = khi ? khi[i] : 0;
+      vp[r] = pin[i];
+      dg[r] = (uint32_t)((shift >= 64 ? vhi[r] : vlo[r]) >> (shift & 63)) & (kRadix - 1);
+      const unsigned peers = __match_any_sync(vmask, dg[r]);
       lane_rank = __popc(peers & ((1u << lane) - 1));
-      if (lane_rank == 0) warp_cnt[warp][d] = __popc(peers);
+      if (lane_rank == 0) warp_cnt[warp][dg[r]] = __popc(peers);
     }
     __syncthreads();
-    for (int dd = tid; dd < kRadix; dd += kSortThreads) {
-      uint32_t run = running[dd];
+    {  // digit tid: warps' counts in warp order after the running count
+      uint32_t run = running[tid];
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) {
-        uint32_t c = warp_cnt[w][dd];
-        warp_cnt[w][dd] = run;
+        const uint32_t c = warp_cnt[w][tid];
+        warp_cnt[w][tid] = run;
         run += c;
       }
-      running[dd] = run;
+      running[tid] = run;
     }
     __syncthreads();
-    if (valid) {
-      uint32_t dst = gbase[d] + warp_cnt[warp][d] + lane_rank;
-      olo[dst] = vlo;
-      if (ohi) ohi[dst] = vhi;
-      pout[dst] = vp;
+    rk[r] = valid ? warp_cnt[warp][dg[r]] + lane_rank : 0;  // rank among the tile's digit-d elements
+    __syncthreads();  // (the next round clears warp_cnt)
+  }
+  // the tile's digit starts: exclusive scan of its digit counts
+  {
+    const uint32_t v = running[tid];
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
+    uint32_t pre = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w)
+      if (w < warp) pre += wsum[w];
+    lstart[tid] = pre + x - v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    if (base + r * kSortThreads + tid < n) {
+      const uint32_t at = lstart[dg[r]] + rk[r];
+      s_lo[at] = vlo[r];
+      if (khi) s_hi[at] = vhi[r];
+      s_p[at] = vp[r];
+    }
+  }
+  __syncthreads();
+  const uint32_t tile_n = min((uint32_t)kSortTile, n - base);
+  for (uint32_t j = tid; j < tile_n; j += kSortThreads) {
+    const uint64_t lo = s_lo[j], hi = khi ? s_hi[j] : 0;
+    const uint32_t d = (uint32_t)((shift >= 64 ? hi : lo) >> (shift & 63)) & (kRadix - 1);
+    const uint32_t dst = gbase[d] + (j - lstart[d]);
+    olo[dst] = lo;
+    if (ohi) ohi[dst] = hi;
+    pout[dst] = s_p[j];
   }
 }
+
+// Dynamic shared memory of radix_scatter_kernel for one- or two-word keys.
+size_t scatter_smem(bool two_words) { return (size_t)kSortTile * ((two_words ? 16 : 8) + 4); }
 
 // Sorted interleaved keys -> line records (mode-contiguous key + value), the
 // value gathered by input position (float64 or float32 input, stored float32).
@@ -740,12 +789,20 @@ alto_status radix_sort_pairs(uint64_t* klo[2], uint64_t* khi[2], uint32_t* pm[2]
                              uint32_t* counts, DevBuf& scan_scratch, cudaStream_t st, int* cur_out) {
   int cur = 0;
   const uint32_t ntiles = (n + kSortTile - 1) / kSortTile;
+  static std::atomic<bool> raised[64];  // per device
+  int dev = 0;
+  ALTO_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !raised[dev].load()) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)scatter_smem(true)));
+    if (dev >= 0 && dev < 64) raised[dev] = true;
+  }
   for (int shift = 0; shift < bits && n; shift += kRadixBits) {
     radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], n, shift, ntiles, counts);
     ALTO_LAUNCHED();
     ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, scan_scratch, st));
-    radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], pm[cur], n, shift, ntiles, counts,
-                                                          klo[cur ^ 1], khi[cur ^ 1], pm[cur ^ 1]);
+    radix_scatter_kernel<<<ntiles, kSortThreads, scatter_smem(khi[cur] != nullptr), st>>>(
+        klo[cur], khi[cur], pm[cur], n, shift, ntiles, counts, klo[cur ^ 1], khi[cur ^ 1], pm[cur ^ 1]);
     ALTO_LAUNCHED();
     cur ^= 1;
   }
