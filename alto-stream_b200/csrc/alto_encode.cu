@@ -167,15 +167,17 @@ __global__ void __launch_bounds__(kSortThreads)
     counts[(size_t)d * ntiles + blockIdx.x] = hist[d];
 }
 
-// Stable scatter of one tile: elements are ranked in index order, round by
-// round (round r holds elements base + r*256 + thread), with per-warp digit
-// counts combined in warp order and a running per-digit count.  The ranked
-// tile is then reordered by digit in shared memory and written out in that
-// order, so consecutive threads write consecutive addresses of a digit's
-// run (writing each element straight to its destination spreads a warp's
-// stores over up to 32 buckets).  Dynamic shared memory: the tile's keys
-// (one or two words) and payloads.
+// Stable scatter of one tile.  Warp w owns the tile's elements
+// [w*256, w*256 + 256) and ranks them in index order, 32 at a time, with its
+// own per-digit counters (the lanes of one digit found with match_any; no
+// block barrier while ranking).  One pass over the digits turns the warps'
+// counts into each warp's start within the digit, and a scan of the tile's
+// digit counts gives each digit's start in the tile.  The ranked tile is
+// then reordered by digit in shared memory and written out in that order,
+// so consecutive threads write consecutive addresses of a digit's run.
+// Dynamic shared memory: the tile's keys (one or two words) and payloads.
 static_assert(kRadix == kSortThreads, "one digit per thread in the tile's digit scan");
+static_assert(kSortTile / (kSortThreads / 32) == kSortItems * 32, "each warp ranks kSortItems rounds of 32");
 __global__ void __launch_bounds__(kSortThreads)
     radix_scatter_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
                          const uint32_t* __restrict__ pin, uint32_t n, int shift,
@@ -183,8 +185,8 @@ __global__ void __launch_bounds__(kSortThreads)
                          uint64_t* __restrict__ olo, uint64_t* __restrict__ ohi,
                          uint32_t* __restrict__ pout) {
   constexpr int kWarps = kSortThreads / 32;
-  __shared__ uint32_t warp_cnt[kWarps][kRadix];
-  __shared__ uint32_t running[kRadix];
+  constexpr int kPerWarp = kSortTile / kWarps;  // 256 elements, kPerWarp / 32 = kSortItems rounds
+  __shared__ uint32_t wrun[kWarps][kRadix];      // per warp: digit counts, then the warp's start in the digit
   __shared__ uint32_t gbase[kRadix];
   __shared__ uint32_t lstart[kRadix];
   __shared__ uint32_t wsum[kWarps];
@@ -193,52 +195,60 @@ __global__ void __launch_bounds__(kSortThreads)
   uint64_t* s_hi = s_lo + kSortTile;
   uint32_t* s_p = reinterpret_cast<uint32_t*>(khi ? s_hi + kSortTile : s_lo + kSortTile);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  running[tid] = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) wrun[w][tid] = 0;
   gbase[tid] = offsets[(size_t)tid * ntiles + blockIdx.x];
+  __syncthreads();
   const uint32_t base = blockIdx.x * kSortTile;
   uint64_t vlo[kSortItems], vhi[kSortItems];
   uint32_t vp[kSortItems], dg[kSortItems], rk[kSortItems];
 #pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) warp_cnt[w][tid] = 0;
-    __syncthreads();
-    const uint32_t i = base + r * kSortThreads + tid;
-    const bool valid = i < n;
-    uint32_t lane_rank = 0;
+  for (int r = 0; r < kSortItems; ++r) {  // every round's loads first, all in flight together
+    const uint32_t i = base + warp * kPerWarp + r * 32 + lane;
     vlo[r] = 0;
     vhi[r] = 0;
     vp[r] = 0;
+    if (i < n) {
+      vlo[r] = klo[i];
+      if (khi) vhi[r] = khi[i];
+      vp[r] = pin[i];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint32_t i = base + warp * kPerWarp + r * 32 + lane;
+    const bool valid = i < n;
     dg[r] = 0;
+    rk[r] = 0;
     const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      vlo[r] = klo[i];
-      vhi[r] = khi ? khi[i] : 0;
-      vp[r] = pin[i];
       dg[r] = (uint32_t)((shift >= 64 ? vhi[r] : vlo[r]) >> (shift & 63)) & (kRadix - 1);
       const unsigned peers = __match_any_sync(vmask, dg[r]);
-      lane_rank = __popc(peers & ((1u << lane) - 1));
-      if (lane_rank == 0) warp_cnt[warp][dg[r]] = __popc(peers);
-    }
-    __syncthreads();
-    {  // digit tid: warps' counts in warp order after the running count
-      uint32_t run = running[tid];
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        const uint32_t c = warp_cnt[w][tid];
-        warp_cnt[w][tid] = run;
-        run += c;
+      const int leader = __ffs(peers) - 1;
+      uint32_t before = 0;
+      if (lane == leader) {
+        before = wrun[warp][dg[r]];
+        wrun[warp][dg[r]] = before + __popc(peers);
       }
-      running[tid] = run;
+      before = __shfl_sync(peers, before, leader);
+      rk[r] = before + __popc(peers & ((1u << lane) - 1));  // rank among the warp's digit-d elements
     }
-    __syncthreads();
-    rk[r] = valid ? warp_cnt[warp][dg[r]] + lane_rank : 0;  // rank among the tile's digit-d elements
-    __syncthreads();  // (the next round clears warp_cnt)
+    __syncwarp();
   }
-  // the tile's digit starts: exclusive scan of its digit counts
-  {
-    const uint32_t v = running[tid];
-    uint32_t x = v;
+  __syncthreads();
+  uint32_t cnt;
+  {  // digit tid: each warp's start within the digit, in warp order; the tile's count
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = wrun[w][tid];
+      wrun[w][tid] = run;
+      run += c;
+    }
+    cnt = run;
+  }
+  {  // the tile's digit starts: exclusive scan of its digit counts
+    uint32_t x = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -250,13 +260,13 @@ __global__ void __launch_bounds__(kSortThreads)
 #pragma unroll
     for (int w = 0; w < kWarps; ++w)
       if (w < warp) pre += wsum[w];
-    lstart[tid] = pre + x - v;
+    lstart[tid] = pre + x - cnt;
   }
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
-    if (base + r * kSortThreads + tid < n) {
-      const uint32_t at = lstart[dg[r]] + rk[r];
+    if (base + warp * kPerWarp + r * 32 + lane < n) {
+      const uint32_t at = lstart[dg[r]] + wrun[warp][dg[r]] + rk[r];
       s_lo[at] = vlo[r];
       if (khi) s_hi[at] = vhi[r];
       s_p[at] = vp[r];

@@ -954,7 +954,8 @@ def ours_slice(args):
         "vs_baseline": None, "dtype": "u32+u64", "data": "synthetic",
         "config": {"workload": SLICE_WORKLOAD, "nnz": nnz, "dims": SLICE_DIMS, "stream_mode": 0,
                    "nnz_threshold": 1, "timeslice_limit": 1, "batches": nbs[0],
-                   "step_ms_min": min(ms), "step_ms_max": max(ms),
+                   "step_ms_min": min(ms), "step_ms_max": max(ms), "step_ms_median": statistics.median(ms),
+                   "step_ms": [round(x, 2) for x in ms],
                    "l2": "input (%.1f GB) exceeds L2; no flush" % (nnz * 40 / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
