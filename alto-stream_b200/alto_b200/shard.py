@@ -7,6 +7,10 @@ all-reduce (sum) over the ranks gives the tensor's MTTKRP.  Output rows of
 different ranks overlap only where their line ranges share rows, but the
 collective is a plain all-reduce of the I_n x R float32 output (NCCL over
 NVLink on GPUs, gloo on CPUs).  The factors are replicated on every rank.
+
+CP-stream serving shards differently: independent streams go to different
+GPUs whole (streams_for_rank), each GPU running its own server, and no data
+crosses GPUs (one slice's update is too small to split).
 """
 from __future__ import annotations
 
@@ -19,6 +23,14 @@ def partition_range(nnz, part, nparts):
         raise ValueError("part outside 0..nparts-1")
     per = (int(nnz) + nparts - 1) // nparts
     return min(part * per, int(nnz)), min((part + 1) * per, int(nnz))
+
+
+def streams_for_rank(nstreams, rank, world):
+    """The serving streams rank `rank` of `world` serves: stream k on rank
+    k mod world (round robin, so ranks differ by at most one stream)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank outside 0..world-1")
+    return list(range(rank, int(nstreams), world))
 
 
 def shard_tensor(tensor, rank, world, stream=None):

@@ -46,6 +46,9 @@ Two more workloads print their own line:
                         slices/s, served under an 80 GB HBM budget; metric
                         slices/s with p50/p99 latency, against the plain path
                         (one slice at a time, each stream's session in turn).
+                        Under torchrun the streams are sharded round robin
+                        over the GPUs, one server each, with no collective
+                        on the data path (strong scaling: 64 streams in all).
   --workload slice      the stream slicer (StreamingSparseTensor) over the
                         CP-stream workload's shape as one 4-mode tensor:
                         200 time steps with log-normal nonzero counts
@@ -644,23 +647,44 @@ def ours_serve(args):
 
     import alto_b200 as A
 
-    torch.cuda.set_device(0)
+    from alto_b200 import shard
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:  # streams sharded over the GPUs, one server each; no data crosses GPUs
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     streams, pool, offs, need, order, arrive = serve_setup(args)
+    mine = shard.streams_for_rank(len(streams), rank, world)
+    keep = np.isin(order, mine)
+    order, arrive = order[keep], arrive[keep]
     W, K = args.warmup, args.steps
     cons = {0: A.UNCONSTRAINED, 1: A.NONNEG}
+
+    def across_ranks(x, op):  # max / sum / min of a host number over the ranks
+        if world == 1:
+            return x
+        import torch.distributed as dist
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op={"max": dist.ReduceOp.MAX, "sum": dist.ReduceOp.SUM, "min": dist.ReduceOp.MIN}[op])
+        return t.item()
 
     def init_for(k, j):  # initial values with the first slice only
         return pool[offs[k]:offs[k] + need[k]] if j == 0 else None
 
     # plain path: one session per stream, one slice at a time, arrival order
     model = A.SPCPSTREAM if args.model == "spcpstream" else A.CPSTREAM
-    sess = [A.CPStream(4, 0, st["rank"], constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10,
-                       epsilon=1e-5) for st in streams]
-    for x in sess:
+    sess = {k: A.CPStream(4, 0, streams[k]["rank"], constraint=cons[streams[k]["constraint"]], forgetting=0.99,
+                          max_inner=10, epsilon=1e-5) for k in mine}
+    for x in sess.values():
         x.set_model(model)
     for j in range(W):
-        for k, st in enumerate(streams):
-            b = st["slices"][j]
+        for k in mine:
+            b = streams[k]["slices"][j]
             sess[k].push(b["dims"], b["cidx"], b["vals"], init_for(k, j))
     torch.cuda.synchronize()
     nxt = [W] * len(streams)
@@ -673,25 +697,27 @@ def ours_serve(args):
         iso.append((time.perf_counter() - ts) * 1e3)
         nxt[k] += 1
     plain_s = time.perf_counter() - t0
-    check = list(range(min(8, len(streams))))
+    check = mine[:8]
     plain_out = {k: [sess[k].factor(m, int(streams[k]["dims"][m]) + 1) for m in (1, 2, 3)] for k in check}
-    for x in sess:
+    for x in sess.values():
         x.close()
     del sess
     torch.cuda.synchronize()
 
     # server: warm-up slices, then the timed slices at their arrival times
     srv = A.Server(80 << 30, workers=args.workers)
-    sids = [srv.open(4, 0, st["rank"], st["dims"], max(len(b["vals"]) for b in st["slices"]),
-                     constraint=cons[st["constraint"]], forgetting=0.99, max_inner=10, epsilon=1e-5, model=model)
-            for st in streams]
+    sids = {k: srv.open(4, 0, streams[k]["rank"], streams[k]["dims"], max(len(b["vals"]) for b in streams[k]["slices"]),
+                        constraint=cons[streams[k]["constraint"]], forgetting=0.99, max_inner=10, epsilon=1e-5,
+                        model=model) for k in mine}
     for j in range(W):
-        for k, st in enumerate(streams):
-            b = st["slices"][j]
+        for k in mine:
+            b = streams[k]["slices"][j]
             srv.submit(sids[k], b["dims"], b["cidx"], b["vals"], init_for(k, j))
     srv.drain()
     st0 = srv.stats()
-    sampler = ClockSampler(0)
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
     launches0 = A.kernel_launches()
@@ -716,23 +742,43 @@ def ours_serve(args):
                for i, m in enumerate((1, 2, 3)))
     srv.destroy()
 
-    n = len(order)
+    # whole job: every rank's slices over the slowest rank's time
+    n_local = len(order)
+    n = int(across_ranks(n_local, "sum"))
+    served_s = across_ranks(served_s, "max")
+    plain_s = across_ranks(plain_s, "max")
+    same = bool(across_ranks(1 if same else 0, "min"))
+    launches = int(across_ranks(launches, "sum"))
+    h2d = int(across_ranks(h2d, "sum"))
+    if world > 1:
+        import torch.distributed as dist
+
+        parts = [None] * world
+        dist.all_gather_object(parts, (lat, iso))
+        lat = [x for p in parts for x in p[0]]
+        iso = [x for p in parts for x in p[1]]
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     value = n / served_s
     plain_rate = n / plain_s
     p99_iso = float(np.percentile(iso, 99))
     line = {
         "metric": SERVE_METRIC + (" [spCP-stream model]" if args.model == "spcpstream" else ""),
-        "value": value, "unit": "slices/s", "n_gpus": 1, "steps": n, "warmup": W * len(streams),
-        "ms_per_step": served_s / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": value, "unit": "slices/s", "n_gpus": world, "steps": n, "warmup": W * len(streams),
+        "ms_per_step": served_s / n * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "model": args.model, "streams": len(streams), "slices_per_stream": W + K,
+                   "parallelism": ("streams sharded round robin over %d GPUs, one server each, no collective" % world
+                                   if world > 1 else "one GPU"),
                    "workers": args.workers, "arrival_rate": args.rate, "hbm_budget_bytes": 80 << 30,
                    "max_inner": 10, "epsilon": 1e-5,
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                    "plain_slices_per_s": plain_rate, "speedup_vs_plain": value / plain_rate,
                    "isolated_p50_ms": float(np.percentile(iso, 50)), "isolated_p99_ms": p99_iso,
                    "p99_vs_isolated_p99": float(np.percentile(lat, 99)) / p99_iso,
-                   "results_identical_to_plain": bool(same), "checked_streams": len(check),
+                   "results_identical_to_plain": bool(same), "checked_streams": len(check) * world,
                    "reserved_bytes": st1["reserved_bytes"], "admitted_streams": st1["admitted_streams"],
                    "warmup_completed": st0["completed"],
                    "timing": "host clock from the first timed arrival to the drained server",

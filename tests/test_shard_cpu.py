@@ -82,3 +82,13 @@ def test_two_rank_sharded_mttkrp_equals_whole():
     (_, r0, e0), (_, r1, e1) = res
     assert r0[0] == 0 and r0[1] == r1[0] and r1[1] > r1[0]
     assert max(e0 + e1) <= 1e-12
+
+
+def test_streams_for_rank_cover_every_stream_once():
+    from alto_b200 import shard
+
+    for world in (1, 2, 3, 8):
+        got = sorted(k for r in range(world) for k in shard.streams_for_rank(64, r, world))
+        assert got == list(range(64))
+        sizes = [len(shard.streams_for_rank(64, r, world)) for r in range(world)]
+        assert max(sizes) - min(sizes) <= 1
