@@ -95,3 +95,32 @@ def test_stream_batches_follow_the_reference_slicer():
         for m in (1, 2, 3):
             assert int(x["cidx"][m].max()) < int(x["dims"][m])
         prev = x["dims"]
+
+
+def test_new_entry_points_reject_bad_arguments_without_device_work(tmp_path):
+    """Argument checks of the slicer, tensor-file, error and poll entry
+    points (each fails before any device work)."""
+    L = A.lib()
+    c = ctypes.c_int()
+    u = ctypes.c_uint64()
+    coo = A.alto_coo()
+    assert L.alto_slicer_next(None, ctypes.c_uint64(1), ctypes.c_uint64(1), ctypes.byref(coo), ctypes.byref(c)) \
+        == A.ERR_INVALID
+    assert L.alto_slicer_cut_all(None, ctypes.c_uint64(1), ctypes.c_uint64(1), ctypes.byref(u)) == A.ERR_INVALID
+    assert L.alto_slicer_batch(None, ctypes.c_uint64(0), ctypes.byref(coo)) == A.ERR_INVALID
+    assert L.alto_slicer_last_batch(None, ctypes.byref(c)) == A.ERR_INVALID
+    assert L.alto_slicer_tensor(None, ctypes.byref(coo)) == A.ERR_INVALID
+    assert L.alto_slicer_destroy(None) == A.OK
+    h = ctypes.c_void_p()
+    assert L.alto_read_tensor(str(tmp_path / "missing.tns").encode(), 0, 0, None, ctypes.byref(h)) == A.ERR_INVALID
+    (tmp_path / "empty.tns").write_bytes(b"")
+    assert L.alto_read_tensor(str(tmp_path / "empty.tns").encode(), 0, 0, None, ctypes.byref(h)) == A.ERR_INVALID
+    assert L.alto_read_tensor(str(tmp_path / "x.tns").encode(), 7, 0, None, ctypes.byref(h)) == A.ERR_INVALID
+    assert L.alto_dcoo_view(None, ctypes.byref(coo)) == A.ERR_INVALID
+    assert L.alto_dcoo_destroy(None) == A.OK
+    assert L.alto_server_poll(None, ctypes.c_uint64(0), ctypes.byref(c), None, None) == A.ERR_INVALID
+    assert L.alto_stream_error(None, ctypes.byref(coo), None) == A.ERR_INVALID
+    dims = np.array([3, 3], np.uint64)
+    with pytest.raises(A.AltoError) as e:  # the reference asserts nnz > 0 on export
+        A.write_tensor(tmp_path / "e.tns", dims, np.zeros((2, 0), np.uint64), np.zeros(0))
+    assert e.value.status == A.ERR_INVALID
