@@ -20,7 +20,14 @@ fixtures pin both the C restatement in oracle/ and the CUDA path:
   16 sampled rows;
 * CP-ALS: fits of 8 iterations on med.tns at rank 8;
 * CP-stream: final factor norms of a small seeded stream, unconstrained and
-  non-negative.
+  non-negative; spCP-stream on the same stream;
+* the stream slicer (StreamingSparseTensor): digests of the batches of a
+  seeded 4-mode tensor for six (stream mode, nnz_threshold, timeslice_limit)
+  cases;
+* tensor files: digests of ImportSparseTensor's reads of ten edge-case
+  .tns files (1- and 0-based) and of ExportSparseTensor's text and binary
+  output;
+* cpd_error of a seeded model against a seeded tensor.
 """
 from __future__ import annotations
 
