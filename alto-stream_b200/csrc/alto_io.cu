@@ -17,8 +17,9 @@
 //      power of ten <= 10^22, so one correctly rounded IEEE multiply or
 //      divide) are converted on the device; any other value text
 //      (hexadecimal, inf/nan, long significands, large exponents) is
-//      listed and converted on the host with the C library's strtod from
-//      the file itself, so every value equals the reference's bit for bit.
+//      listed; its text is copied back in bulk and converted with the C
+//      library's strtod on all host cores, so every value equals the
+//      reference's bit for bit.
 // The mode count comes from the first valid line, split on space and tab as
 // the reference's strtok does (the newline stays in the last token).
 //
@@ -359,11 +360,23 @@ alto_status launch_parse(unsigned grid, cudaStream_t st, const unsigned char* bu
   return ALTO_OK;
 }
 
-// For each listed line: its start in the file (one copy to the host).
-__global__ void host_lines_kernel(const uint64_t* __restrict__ list, uint32_t n, const uint64_t* __restrict__ starts,
-                                  uint64_t* __restrict__ out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = starts[list[2 * (uint64_t)i]];
+// Listed entries [i0, i0 + n): each value's text, from its offset to the
+// line's newline, a NUL or the file's end, NUL-terminated in a kValText-byte
+// slot; a text that does not fit ends with byte 1 in the slot's last byte
+// (the host then re-reads that line from the file).
+constexpr int kValText = 64;
+__global__ void value_text_kernel(const uint64_t* __restrict__ list, uint64_t i0, uint32_t n,
+                                  const uint64_t* __restrict__ starts, const unsigned char* __restrict__ buf,
+                                  uint64_t size, char* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t k = list[2 * (i0 + i)], off = list[2 * (i0 + i) + 1];
+    uint64_t q = starts[k] + off;
+    char* o = out + (uint64_t)i * kValText;
+    int c = 0;
+    while (c < kValText - 1 && q < size && buf[q] != '\n' && buf[q] != 0) o[c++] = (char)buf[q++];
+    o[c] = 0;
+    o[kValText - 1] = (c == kValText - 1 && q < size && buf[q] != '\n' && buf[q] != 0) ? 1 : 0;
+  }
 }
 
 __global__ void scatter_vals_kernel(const uint32_t* __restrict__ at, const double* __restrict__ v, uint32_t n,
@@ -616,34 +629,55 @@ alto_status read_text(int fd, uint64_t size, uint64_t zero_based, cudaStream_t s
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
   }
   d->host_lines = nhost;
-  if (nhost) {  // values the device left to the C library
-    std::vector<uint64_t> list(2 * (size_t)nhost), ls(nhost);
-    std::vector<uint32_t> at(nhost);
-    std::vector<double> v(nhost);
-    DevBuf lsd;
-    ALTO_TRY(lsd.ensure((size_t)nhost * 8));
-    host_lines_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(hl.as<uint64_t>(), nhost, starts.as<uint64_t>(),
-                                                           lsd.as<uint64_t>());
-    ALTO_LAUNCHED();
-    ALTO_TRY_CUDA(cudaMemcpyAsync(list.data(), hl.p, list.size() * 8, cudaMemcpyDeviceToHost, st));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(ls.data(), lsd.p, ls.size() * 8, cudaMemcpyDeviceToHost, st));
-    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-    std::string line;
-    for (uint32_t i = 0; i < nhost; ++i) {
-      ALTO_TRY(read_line(fd, ls[i], size, &line));
-      at[i] = (uint32_t)list[2 * (size_t)i];
-      const size_t o = (size_t)list[2 * (size_t)i + 1];
-      v[i] = o <= line.size() ? strtod(line.c_str() + o, nullptr) : 0.0;
+  if (nhost) {  // values the device left to the C library, in chunks of up to 4M
+    const uint32_t chunk = std::min<uint32_t>(nhost, 1u << 22);
+    PoolBuf txt, hb;
+    ALTO_TRY(txt.ensure((size_t)chunk * kValText, st));
+    ALTO_TRY(hb.ensure((size_t)chunk * 12, st));
+    std::vector<char> htxt((size_t)chunk * kValText);
+    std::vector<uint64_t> list(2 * (size_t)chunk);
+    std::vector<uint32_t> at(chunk);
+    std::vector<double> v(chunk);
+    const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    for (uint32_t i0 = 0; i0 < nhost; i0 += chunk) {
+      const uint32_t n = std::min(chunk, nhost - i0);
+      value_text_kernel<<<grid_io(n, 256), 256, 0, st>>>(hl.as<uint64_t>(), i0, n, starts.as<uint64_t>(),
+                                                         file.as<unsigned char>(), size, txt.as<char>());
+      ALTO_LAUNCHED();
+      ALTO_TRY_CUDA(cudaMemcpyAsync(htxt.data(), txt.p, (size_t)n * kValText, cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaMemcpyAsync(list.data(), hl.as<uint64_t>() + 2 * (size_t)i0, (size_t)n * 16,
+                                    cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+      // the C library's strtod on every listed text, on all host cores
+      std::vector<std::thread> th;
+      for (unsigned r = 0; r < nt; ++r)
+        th.emplace_back([&, r] {
+          for (uint32_t i = r; i < n; i += nt) {
+            at[i] = (uint32_t)list[2 * (size_t)i];
+            const char* tx = htxt.data() + (size_t)i * kValText;
+            v[i] = tx[kValText - 1] ? 0.0 : strtod(tx, nullptr);
+          }
+        });
+      for (auto& x : th) x.join();
+      // texts longer than a slot: the whole line again from the file
+      std::string line;
+      for (uint32_t i = 0; i < n; ++i) {
+        if (!htxt[(size_t)i * kValText + kValText - 1]) continue;
+        uint64_t ls = 0;
+        ALTO_TRY_CUDA(cudaMemcpyAsync(&ls, starts.as<uint64_t>() + at[i], 8, cudaMemcpyDeviceToHost, st));
+        ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+        ALTO_TRY(read_line(fd, ls, size, &line));
+        const size_t o = (size_t)list[2 * (size_t)i + 1];
+        v[i] = o <= line.size() ? strtod(line.c_str() + o, nullptr) : 0.0;
+      }
+      ALTO_TRY_CUDA(cudaMemcpyAsync(hb.p, v.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st));
+      ALTO_TRY_CUDA(cudaMemcpyAsync(hb.as<char>() + (size_t)chunk * 8, at.data(), (size_t)n * 4,
+                                    cudaMemcpyHostToDevice, st));
+      scatter_vals_kernel<<<grid_io(n, 256), 256, 0, st>>>(
+          reinterpret_cast<const uint32_t*>(hb.as<char>() + (size_t)chunk * 8), hb.as<double>(), n, vals);
+      ALTO_LAUNCHED();
+      ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // (v and at are refilled by the next chunk)
     }
-    DevBuf hb;
-    ALTO_TRY(hb.ensure((size_t)nhost * 12));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(hb.p, v.data(), (size_t)nhost * 8, cudaMemcpyHostToDevice, st));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(hb.as<char>() + (size_t)nhost * 8, at.data(), (size_t)nhost * 4,
-                                  cudaMemcpyHostToDevice, st));
-    scatter_vals_kernel<<<grid_io(nhost, 256), 256, 0, st>>>(
-        reinterpret_cast<const uint32_t*>(hb.as<char>() + (size_t)nhost * 8), hb.as<double>(), nhost, vals);
-    ALTO_LAUNCHED();
-    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
   }
   d->nmodes = N;
   d->nnz = nnz;

@@ -174,3 +174,23 @@ def test_many_values_left_to_host(tmp_path):
     want = np.array([float(ln.rsplit(" ", 1)[1]) for ln in text.splitlines()])
     assert np.array_equal(got_v, want)
     t.close()
+
+
+def test_host_values_long_texts_and_numpy_style(tmp_path):
+    """Values in numpy's savetxt style (%.18e: every one converted on the
+    host from the text copied back) and value texts longer than the 64-byte
+    copy (re-read from the file): each equals the C library's conversion."""
+    rng = np.random.default_rng(14)
+    n = 50_000
+    v = rng.normal(size=n) * 10.0 ** rng.integers(-8, 8, n)
+    vt = ["%.18e" % x for x in v]
+    for k in range(0, n, 997):  # texts past the 64-byte copy
+        vt[k] = "0." + "0" * (70 + k % 9) + "123456789012345678901234"
+    lines = ["%d %d %d %s\n" % (k % 100 + 1, k % 37 + 1, k % 11 + 1, t) for k, t in enumerate(vt)]
+    (tmp_path / "np.tns").write_text("".join(lines))
+    t = A.read_tensor(tmp_path / "np.tns")
+    _, got = t.to_host()
+    assert t.stats()["host_values"] == n
+    want = np.array([float(x) for x in vt])
+    assert np.array_equal(got, want)
+    t.close()
