@@ -342,7 +342,8 @@ __global__ void __launch_bounds__(kIoThreads)
   for (int m = 0; m < (NM ? NM : nmodes); ++m) atomicMax(dims + m, (unsigned long long)dmax[m]);
 }
 
-// The parse for nmodes modes (3 and 4 compiled for their count).
+// The parse for nmodes modes (3, 4 and 5, the reference's specialised mode
+// counts, compiled for their count).
 alto_status launch_parse(unsigned grid, cudaStream_t st, const unsigned char* buf, uint64_t size,
                          const uint64_t* starts, uint64_t nnz, int nmodes, uint64_t zero_based, uint64_t* idx,
                          double* vals, unsigned long long* dims, uint64_t* host_list, uint32_t host_cap,
@@ -352,6 +353,9 @@ alto_status launch_parse(unsigned grid, cudaStream_t st, const unsigned char* bu
                                                      host_list, host_cap, host_count);
   else if (nmodes == 4)
     tns_parse_kernel<4><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
+                                                     host_list, host_cap, host_count);
+  else if (nmodes == 5)
+    tns_parse_kernel<5><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
                                                      host_list, host_cap, host_count);
   else
     tns_parse_kernel<0><<<grid, kIoThreads, 0, st>>>(buf, size, starts, nnz, nmodes, zero_based, idx, vals, dims,
