@@ -899,7 +899,9 @@ std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
 
 // Device address of the scratch array on the current device, resolved once
-// per device (the array's name in host code is only a stand-in).
+// per device (the array's name in host code is only a stand-in).  The
+// address is kept for the process's life: a cudaDeviceReset of the device
+// would leave it stale, which the header rules out for callers.
 alto_status noalloc_scratch(double** out) {
   int dev = 0;
   ALTO_TRY_CUDA(cudaGetDevice(&dev));

@@ -84,14 +84,29 @@ struct alto_server {
   std::deque<int> pending;  // streams waiting for admission
   std::vector<std::thread> workers;
   bool stop = false;
+  // tickets not yet handed back as done by wait/poll (erased then, so the
+  // map holds only outstanding work)
   std::unordered_map<uint64_t, TicketInfo> tickets;
+  // latencies of the last kLatencyWindow completed slices (a ring)
   std::vector<double> lat_ms;
+  size_t lat_next = 0;
   uint64_t submitted = 0, completed = 0;
   double t_first = 0, t_last = 0;
   int busy_workers = 0;
 };
 
 namespace {
+
+constexpr size_t kLatencyWindow = size_t(1) << 20;
+
+void record_latency(alto_server* s, double ms) {  // caller holds s->mu
+  if (s->lat_ms.size() < kLatencyWindow) {
+    s->lat_ms.push_back(ms);
+  } else {
+    s->lat_ms[s->lat_next] = ms;
+    s->lat_next = (s->lat_next + 1) % kLatencyWindow;
+  }
+}
 
 // Device footprint estimate of a stream: model, previous model and duals
 // (with growth headroom), the float64 solve buffers, the encoded slice, its
@@ -176,7 +191,7 @@ void worker_main(alto_server* s) {
     ti.status = st;
     ti.latency_ms = (t_end - q->t_submit) * 1e3;
     if (st != ALTO_OK) r->err = st;
-    s->lat_ms.push_back(ti.latency_ms);
+    record_latency(s, ti.latency_ms);
     s->completed++;
     s->t_last = t_end;
     r->done++;
@@ -319,8 +334,17 @@ alto_status alto_server_wait(alto_server* s, uint64_t ticket, int* inner_iters, 
     set_error("unknown ticket %llu", (unsigned long long)ticket);
     return ALTO_ERR_INVALID;
   }
-  s->cv_done.wait(lk, [&] { return s->tickets[ticket].done; });
-  const TicketInfo ti = s->tickets[ticket];
+  s->cv_done.wait(lk, [&] {
+    auto jt = s->tickets.find(ticket);
+    return jt == s->tickets.end() || jt->second.done;
+  });
+  it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) {  // another waiter took it first
+    set_error("ticket %llu was already handed back", (unsigned long long)ticket);
+    return ALTO_ERR_INVALID;
+  }
+  const TicketInfo ti = it->second;
+  s->tickets.erase(it);
   if (inner_iters) *inner_iters = ti.inner;
   if (latency_ms) *latency_ms = ti.latency_ms;
   return ti.status;
@@ -339,9 +363,11 @@ alto_status alto_server_poll(alto_server* s, uint64_t ticket, int* done, int* in
   }
   *done = it->second.done ? 1 : 0;
   if (!it->second.done) return ALTO_OK;
-  if (inner_iters) *inner_iters = it->second.inner;
-  if (latency_ms) *latency_ms = it->second.latency_ms;
-  return it->second.status;
+  const TicketInfo ti = it->second;
+  s->tickets.erase(it);
+  if (inner_iters) *inner_iters = ti.inner;
+  if (latency_ms) *latency_ms = ti.latency_ms;
+  return ti.status;
 }
 
 alto_status alto_server_drain(alto_server* s) {
@@ -416,7 +442,15 @@ alto_status alto_server_close(alto_server* s, int sid) {
   }
   StreamRec* r = it->second;
   s->cv_done.wait(lk, [&] { return !r->busy && (r->q.empty() || !r->admitted); });
-  for (SliceReq* q : r->q) delete q;  // never-admitted work is dropped
+  // never-admitted work is dropped: its tickets finish with an error so that
+  // waiters (already blocked or later) return
+  for (SliceReq* q : r->q) {
+    TicketInfo& ti = s->tickets[q->ticket];
+    ti.done = true;
+    ti.status = ALTO_ERR_INVALID;
+    delete q;
+  }
+  const bool dropped = !r->q.empty();
   r->q.clear();
   s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), sid), s->pending.end());
   if (r->admitted) s->reserved -= r->reserve;
@@ -425,6 +459,7 @@ alto_status alto_server_close(alto_server* s, int sid) {
   const alto_status err = r->err;
   delete r;
   admit_pending(s);
+  if (dropped) s->cv_done.notify_all();
   lk.unlock();
   if (sess) alto_stream_close(sess);
   return err;

@@ -9,7 +9,15 @@
 //   -p        MTTKRP benchmark (BenchmarkAlto)          -c       check MTTKRP against COO
 //   -l MODEL  als | cpstream_alto                       -z CON   nonneg | lasso
 //   -a MODE   streaming mode                            -g L     time slices per batch (1)
-//   -k T      nonzero threshold per batch               -f F     forgetting factor (0.99)
+//   -k T      nonzero threshold per batch               -f N     save to file (0): N != 0
+//                                                                writes a text input back as
+//                                                                binary, a binary input as text
+//   -o FILE   output file: the tensor read, as text (the reference parses -o but
+//             its only use is commented out, src/main.cpp:152-153, 355)
+//   -d/-s     dims / sparsity of a generated tensor: parsed, then refused (the
+//             reference's Poisson generator is not part of this library)
+//   --forgetting F   CP-stream forgetting factor (0.99; the reference fixes it
+//                    at compile time, src/streaming_cpd.cpp:18); long form only
 //   -h / -v   help / version
 //
 // The initial model uses the C library's rand() after srand(seed), drawing
@@ -77,7 +85,8 @@ double now() {
 void usage(const char* argv0) {
   fprintf(stderr,
           "usage: %s (-i FILE | -b FILE) [-r R] [-m K] [-x SEED] [-t MODE] [-e EPS] [-u]\n"
-          "          [-p | -c | -l als|cpstream_alto] [-z nonneg|lasso] [-a MODE] [-g L] [-k T] [-f F]\n",
+          "          [-p | -c | -l als|cpstream_alto|spcpstream_alto] [-z nonneg|lasso] [-a MODE]\n"
+          "          [-g L] [-k T] [-f N] [-o FILE] [--forgetting F]\n",
           argv0);
 }
 
@@ -188,6 +197,10 @@ int run_cpstream(const alto_coo& in, int R, int iters, double eps, int tmode, al
   return 0;
 }
 
+// getopt code of the long-only --forgetting option (no short letter: -f is
+// the reference's --file)
+constexpr int kForgettingOpt = 0x100;
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -198,16 +211,19 @@ int main(int argc, char** argv) {
       {"target-mode", 1, nullptr, 't'}, {"epsilon", 1, nullptr, 'e'}, {"zero-based", 0, nullptr, 'u'},
       {"check", 0, nullptr, 'c'}, {"bench", 0, nullptr, 'p'}, {"streaming-mode", 1, nullptr, 'a'},
       {"timeslice-limit", 1, nullptr, 'g'}, {"nnz-threshold", 1, nullptr, 'k'},
-      {"forgetting", 1, nullptr, 'f'}, {nullptr, 0, nullptr, 0}};
-  std::string text, bin, model = "als";
-  int R = 16, iters = 10, target = -1, tmode = -1;
+      {"file", 1, nullptr, 'f'}, {"output", 1, nullptr, 'o'}, {"dims", 1, nullptr, 'd'},
+      {"sparsity", 1, nullptr, 's'}, {"forgetting", 1, nullptr, kForgettingOpt}, {nullptr, 0, nullptr, 0}};
+  std::string text, bin, out_file, model = "als";
+  int R = 16, iters = 10, target = -1, tmode = -1, save_to_file = 0;
+  bool generate = false;
   double eps = 5e-2, forgetting = 0.99;
   bool zero = false, check = false, bench = false;
   alto_constraint con = ALTO_UNCONSTRAINED;
   uint64_t nnz_threshold = UINT64_MAX, limit = 1;
   srand((unsigned)time(nullptr));
   int c;
-  while ((c = getopt_long(argc, argv, "hvi:b:l:z:r:m:x:t:e:ucpa:g:k:f:", long_opt, nullptr)) != -1) {
+  // the reference's short options (src/main.cpp:93)
+  while ((c = getopt_long(argc, argv, "hvi:o:b:l:z:r:m:x:d:t:s:e:f:ucpa:g:k:", long_opt, nullptr)) != -1) {
     switch (c) {
       case 'h': usage(argv[0]); return 0;
       case 'v': printf("cpd64 (B200) %d\n", alto_version()); return 0;
@@ -229,9 +245,20 @@ int main(int argc, char** argv) {
       case 'a': tmode = atoi(optarg); break;
       case 'g': limit = strtoull(optarg, nullptr, 10); break;
       case 'k': nnz_threshold = strtoull(optarg, nullptr, 10); break;
-      case 'f': forgetting = atof(optarg); break;
+      case 'f':
+        save_to_file = atoi(optarg);
+        if (save_to_file < 0) fprintf(stderr, "Invalid -file: %s.\n", optarg);
+        break;
+      case 'o': out_file = optarg; break;
+      case 'd':
+      case 's': generate = true; break;
+      case kForgettingOpt: forgetting = atof(optarg); break;
       default: usage(argv[0]); return 1;
     }
+  }
+  if (generate && bin.empty() && text.empty()) {
+    fprintf(stderr, "cpd64: generated tensors (-d/-s) are not supported here; pass -i or -b\n");
+    return 1;
   }
   // ImportSparseTensor (src/sptensor.cpp:160-249), parsed on the device
   if (bin.empty() && text.empty()) {
@@ -247,6 +274,19 @@ int main(int argc, char** argv) {
   }
   alto_coo coo;
   CHECK(alto_dcoo_view(D, &coo));
+  // -f: the reference writes the tensor back in the other format under its
+  // own file name (src/main.cpp:268-289, ExportSparseTensor with path NULL,
+  // src/sptensor.cpp:33-45)
+  if (save_to_file) {
+    const bool to_text = !bin.empty();
+    char fn[64];
+    snprintf(fn, sizeof fn, "%lluD_%llu.%s", (unsigned long long)coo.nmodes, (unsigned long long)coo.nnz,
+             to_text ? "tns" : "bin");
+    double tw = now();
+    CHECK(alto_write_tensor(fn, to_text ? ALTO_FILE_TEXT : ALTO_FILE_BINARY, &coo));
+    printf("Writing to %s file: %f\n", to_text ? "text" : "binary", now() - tw);
+  }
+  if (!out_file.empty()) CHECK(alto_write_tensor(out_file.c_str(), ALTO_FILE_TEXT, &coo));
   Coo X;
   X.nmodes = coo.nmodes;
   X.count = coo.nnz;

@@ -201,7 +201,10 @@ alto_status alto_gram(const float* U, uint64_t rows, int rank, double* G, alto_c
  * allocation: the partial sums live in a fixed 2 MiB device array inside
  * this library, present on every GPU that loads it until the process
  * exits.  The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * (cudaGetSymbolAddress) and keeps it for the life of the process, so make
+ * that call before any stream capture, and do not call this entry point on
+ * a device after cudaDeviceReset of it (the kept address would be stale;
+ * the rest of the library has the same rule for its cached buffers).  All calls
  * share the array: calls that may overlap on the GPU (different streams or
  * host threads without ordering) race and must be serialised by the caller. */
 alto_status alto_gram_noalloc(const float* U, uint64_t rows, int rank, double* G,
@@ -400,7 +403,8 @@ typedef struct {
 
 typedef struct {
   uint64_t submitted, completed;
-  double p50_ms, p99_ms, max_ms;  /* slice latency, submission to completion */
+  double p50_ms, p99_ms, max_ms;  /* slice latency, submission to completion, over
+                                     the last 2^20 completed slices */
   double slices_per_s;            /* completed slices over first submission .. last completion */
   uint64_t reserved_bytes;
   int admitted_streams, pending_streams;
@@ -414,17 +418,24 @@ alto_status alto_server_open(alto_server* s, const alto_stream_config* cfg, cons
 /* Queue one time batch (copied; host memory).  init_vals as alto_stream_push. */
 alto_status alto_server_submit(alto_server* s, int sid, const alto_coo* batch, const double* init_vals,
                                uint64_t n_init, uint64_t* ticket);
-/* Wait for one slice; its status, inner iterations and latency. */
+/* Wait for one slice; its status, inner iterations and latency.  A ticket is
+ * handed back once: after wait (or a poll that reports it done) returns it,
+ * the server forgets it and a second wait or poll is ALTO_ERR_INVALID.  A
+ * slice dropped by alto_server_close before its stream was admitted ends
+ * with ALTO_ERR_INVALID. */
 alto_status alto_server_wait(alto_server* s, uint64_t ticket, int* inner_iters, double* latency_ms);
 /* The same without waiting: *done = 0 while the slice is queued or running
- * (ALTO_OK), else 1 with alto_server_wait's outputs and status. */
+ * (ALTO_OK), else 1 with alto_server_wait's outputs and status (and the
+ * ticket is handed back, as by wait). */
 alto_status alto_server_poll(alto_server* s, uint64_t ticket, int* done, int* inner_iters, double* latency_ms);
 /* Wait until every admitted stream has processed all its slices. */
 alto_status alto_server_drain(alto_server* s);
 alto_status alto_server_stats(alto_server* s, alto_serving_stats* out);
 /* A stream's factor (as alto_stream_factor) once its queued slices are done. */
 alto_status alto_server_factor(alto_server* s, int sid, int mode, double* host_out, uint64_t* rows);
-/* Finish a stream's queued slices, free its device state, admit waiting streams. */
+/* Finish a stream's queued slices, free its device state, admit waiting
+ * streams.  A stream not yet admitted has its queued slices dropped: their
+ * tickets finish with ALTO_ERR_INVALID, waking any waiter. */
 alto_status alto_server_close(alto_server* s, int sid);
 alto_status alto_server_destroy(alto_server* s);
 

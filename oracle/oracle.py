@@ -68,7 +68,7 @@ def ref_lib(bits=64):
     if bits not in _REF:
         path = os.path.join(HERE, "_ref", f"libaltoref{bits}.so")
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference sources exist")
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref REF=<reference dir>` where the reference sources exist")
         L = ctypes.CDLL(path)
         L.ref_alto_create.restype = c_void_p
         L.ref_alto_destroy.argtypes = [c_void_p]

@@ -2,7 +2,7 @@
 
 Run here, where the reference sources exist (the GPU box has no copy):
 
-    make -C oracle ref         # oracle/_ref/libaltoref{64,128}.so
+    make -C oracle ref REF=<reference dir>   # oracle/_ref/libaltoref{64,128}.so
     python tests/golden/make_golden.py [path-to-reference]
     python tests/golden/make_golden.py only tns tns_export cpd_error   # refresh some parts
 
@@ -301,4 +301,6 @@ if __name__ == "__main__":
         with open(os.path.join(HERE, "golden.json"), "w") as f:
             json.dump(g, f, indent=1)
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+        default = os.environ.get("ALTO_REFERENCE",
+                                 os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference"))
+        main(sys.argv[1] if len(sys.argv) > 1 else default)

@@ -157,6 +157,36 @@ def test_cpd64_reads_files(tmp_path, binary):
     assert r.stdout.count("correct") == 3 and "INCORRECT" not in r.stdout
 
 
+@pytest.mark.parametrize("binary", [False, True])
+def test_cpd64_takes_the_reference_flags(tmp_path, binary):
+    """The reference's own flag strings, unchanged: -f 1 writes the tensor back
+    in the other format as <N>D_<nnz>.bin / .tns in the working directory
+    (src/main.cpp:268-289), -o names an output file, -x seeds, -e and -m set
+    epsilon and iterations, and -l als runs CP-ALS."""
+    import subprocess
+
+    rng = np.random.default_rng(16)
+    dims = np.array([60, 50, 40], np.uint64)
+    c = np.stack([rng.integers(0, d, 3000).astype(np.uint64) for d in dims])
+    key = (c[0] * 50 + c[1]) * 40 + c[2]
+    _, first = np.unique(key, return_index=True)
+    c = c[:, np.sort(first)]
+    v = rng.integers(1, 9, c.shape[1]).astype(np.float64)  # (exact in %g)
+    nnz = c.shape[1]
+    path = tmp_path / ("t.bin" if binary else "t.tns")
+    path.write_bytes(O.write_bin(dims, c, v) if binary else O.write_tns(c, v))
+    exe = os.path.abspath(os.path.join(os.path.dirname(A.__file__), "..", "cpd64"))
+    args = [exe, "-b" if binary else "-i", str(path), "-r", "4", "-m", "3", "-x", "5", "-e", "1e-5", "-f", "1",
+            "-o", str(tmp_path / "out.tns"), "-l", "als"]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=120, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "it: 2" in r.stdout
+    back = tmp_path / ("3D_%d.%s" % (nnz, "tns" if binary else "bin"))
+    read_dims = dims if binary else c.max(axis=1) + 1  # (text files: largest index + 1)
+    assert back.read_bytes() == (O.write_tns(c, v) if binary else O.write_bin(read_dims, c, v))
+    assert (tmp_path / "out.tns").read_bytes() == O.write_tns(c, v)
+
+
 def test_many_values_left_to_host(tmp_path):
     """More than 2^20 values outside the device's fast path (17 significant
     digits): the listed lines overflow their first buffer and are listed

@@ -3,6 +3,9 @@ and in a mix with other streams -- bit for bit, since CP-stream sessions use
 the deterministic MTTKRP and fixed-order reductions throughout (the stated
 bound is 1e-4) --, slices of one stream keep their order, admission respects
 the HBM budget, and the alone result matches the FP64 oracle within 1e-4."""
+import threading
+import time
+
 import numpy as np
 import pytest
 
@@ -93,6 +96,42 @@ def test_admission_waits_for_budget():
     srv.close(s1)
     got = srv.wait(t2[-1])
     assert srv.stats()["completed"] == 6
-    assert srv.poll(t2[-1]) == got
+    assert got[0] >= 1
+    with pytest.raises(A.AltoError):  # a ticket is handed back once
+        srv.poll(t2[-1])
     srv.close(s2)
+    srv.destroy()
+
+
+def test_close_of_pending_stream_wakes_its_waiters():
+    srv = A.Server(1, workers=1)  # room for one stream at a time
+    b1, iv1 = make_stream(31, [100, 100, 20], 2, 8)
+    b2, iv2 = make_stream(32, [100, 100, 20], 2, 8)
+    s1 = srv.open(4, 0, 8, [3, 200, 200, 40], 1000)
+    s2 = srv.open(4, 0, 8, [3, 200, 200, 40], 1000)
+    assert srv.stats()["pending_streams"] == 1
+    t2 = submit_all(srv, s2, b2, iv2, 8)
+    out = {}
+
+    def waiter():
+        try:
+            srv.wait(t2[0])
+            out["status"] = "ok"
+        except A.AltoError as e:
+            out["status"] = e.status
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    time.sleep(0.2)
+    assert th.is_alive()  # blocked: s2 is not admitted
+    srv.close(s2)  # drops s2's queued slices
+    th.join(timeout=30)
+    assert not th.is_alive(), "waiter still blocked after close"
+    assert out["status"] == A.ERR_INVALID
+    with pytest.raises(A.AltoError) as e:
+        srv.poll(t2[1])
+    assert e.value.status == A.ERR_INVALID
+    submit_all(srv, s1, b1, iv1, 8)
+    srv.drain()
+    srv.close(s1)
     srv.destroy()

@@ -51,3 +51,20 @@ def test_writer_uint32_float32_inputs(tmp_path):
 def test_cpd_error_restatement_matches_reference(golden):
     dims, c, v, F = MG.cpd_error_case()
     assert abs(O.cpd_error(c, v, F) - golden["cpd_error"]["err"]) <= 1e-13
+
+
+def test_cpd64_parses_the_reference_flags_without_a_gpu():
+    """cpd64's option string is the reference's (src/main.cpp:93): -h prints
+    the usage, -f takes the reference's integer (not a forgetting factor),
+    and a generated tensor (-d/-s) is refused with a clear message before
+    any device work."""
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(A.__file__), "..", "cpd64")
+    r = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "-f N" in r.stderr and "--forgetting" in r.stderr
+    r = subprocess.run([exe, "-d", "10,10,10", "-s", "0.1", "-r", "4", "-f", "1"], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 1 and "-d/-s" in r.stderr
+    r = subprocess.run([exe, "-q"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1

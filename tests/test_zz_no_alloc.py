@@ -30,13 +30,25 @@ def _call(fn, U, G, stream):
               ctypes.c_void_p(G.data_ptr()), ctypes.c_void_p(stream))
 
 
-def test_noalloc_gram_matches_alto_gram_on_two_calls():
+# Pairs of calls in a row; the second is smaller than the first.  The cases
+# cover the 64-block cap (100000 rows at rank 64), the per-thread share of
+# 16 used for a share-of-8 need (rank 40), a single row and rank 1, and zero
+# rows, where G is cleared without a kernel.
+CALL_PAIRS = [
+    [(100000, 64), (3000, 16)],
+    [(50000, 40), (1, 1)],
+    [(20000, 8), (0, 8)],
+]
+
+
+@pytest.mark.parametrize("calls", CALL_PAIRS, ids=["cap-then-small", "rank40-then-one-row", "then-empty"])
+def test_noalloc_gram_matches_alto_gram_on_two_calls(calls):
     import torch
 
     L = A.lib()
     stream = torch.cuda.current_stream().cuda_stream
     rng = np.random.default_rng(7)
-    for rows, rank in [(100000, 64), (3000, 16)]:
+    for rows, rank in calls:
         U = torch.tensor(rng.uniform(-1, 1, (rows, rank)).astype(np.float32), device="cuda")
         G_ref = torch.empty((rank, rank), dtype=torch.float64, device="cuda")
         G_new = torch.full((rank, rank), float("nan"), dtype=torch.float64, device="cuda")
