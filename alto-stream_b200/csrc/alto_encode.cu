@@ -755,13 +755,21 @@ alto_status restrict_line(alto_tensor* t, uint64_t begin, uint64_t end, cudaStre
 // ------------------------------------------------ per-mode row-sorted lines
 
 // Row index of every line entry for one mode, and the identity payload.
-__global__ void mode_rows_kernel(const void* __restrict__ line, LineDecode dec, int mode, uint32_t nnz,
-                                 uint64_t* __restrict__ rows, uint32_t* __restrict__ pos) {
+// Sort key of each line entry for a row-sorted copy: the row of `mode`,
+// followed (when fiber_mode >= 0) by the row of fiber_mode in the low
+// fiber_bits bits, so that a stable sort groups each output row's nonzeros
+// by their fiber_mode row as well.
+__global__ void mode_rows_kernel(const void* __restrict__ line, LineDecode dec, int mode, int fiber_mode,
+                                 int fiber_bits, uint32_t nnz, uint64_t* __restrict__ rows,
+                                 uint32_t* __restrict__ pos) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
     uint64_t lo, hi;
     float v;
     rec_read(line, dec.hi_words, i, lo, hi, v);
-    rows[i] = line_field(lo, hi, dec.pos[mode], dec.mask[mode]);
+    uint64_t k = line_field(lo, hi, dec.pos[mode], dec.mask[mode]);
+    if (fiber_mode >= 0)
+      k = (k << fiber_bits) | line_field(lo, hi, dec.pos[fiber_mode], dec.mask[fiber_mode]);
+    rows[i] = k;
     pos[i] = i;
   }
 }
@@ -834,6 +842,20 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   const int hw = t->dec.hi_words;
   // 3-mode copies store the rows decoded (same 16 bytes per record)
   s.hw = t->nmodes == 3 ? kDecoded3 : hw;
+  // 3-mode copies are ordered by (row, fiber row, ALTO order): among one
+  // output row's nonzeros, those sharing the row of the fiber mode (the
+  // shorter other mode) are adjacent, so the MTTKRP gathers that factor row
+  // once per fiber instead of once per nonzero.  Within a fiber the ALTO
+  // order is ascending in the third mode's row (the other two are fixed).
+  s.fiber_mode = -1;
+  if (s.hw == kDecoded3) {
+    int a = -1;
+    for (int m = 0; m < 3; ++m)
+      if (m != mode && (a < 0 || t->dims[m] < t->dims[a])) a = m;
+    if (t->mode_bits[mode] + t->mode_bits[a] <= 64) s.fiber_mode = a;
+  }
+  const int sort_bits =
+      t->mode_bits[mode] + (s.fiber_mode >= 0 ? t->mode_bits[s.fiber_mode] : 0);
   ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(s.hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
   const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
@@ -850,11 +872,13 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   uint32_t* counts = (uint32_t*)(sb + o_cnt);
   const uint32_t n32 = (uint32_t)nnz;
   if (nnz) {
-    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, mode, n32, rk[0], pm[0]);
+    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(
+        t->line.p, t->dec, mode, s.fiber_mode, s.fiber_mode >= 0 ? t->mode_bits[s.fiber_mode] : 0, n32, rk[0],
+        pm[0]);
     ALTO_LAUNCHED();
     int cur = 0;
     uint64_t* nohi[2] = {nullptr, nullptr};
-    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, t->mode_bits[mode], counts, t->scan_scratch, st, &cur));
+    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, sort_bits, counts, t->scan_scratch, st, &cur));
     if (s.hw == kDecoded3)
       gather_decode3_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, pm[cur], n32,
                                                                  s.line.as<uint4>());

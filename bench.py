@@ -11,8 +11,12 @@ the whole job.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU (torchrun, one rank per GPU): every rank owns its own tensor of the
-same size (independent tensors, weak scaling); no data-path collective.
+Multi-GPU (torchrun, one rank per GPU): the one tensor is sharded by output
+rows -- per mode, contiguous row blocks of equal nonzero count, each rank
+encoding only its block's nonzeros -- and after each mode's MTTKRP the ranks'
+row blocks are all-gathered (NCCL broadcasts); strong scaling, the whole
+job's nnz*R over the slowest rank's time.  --independent gives every rank a
+tensor of its own instead (weak scaling, no collective).
 
 The JSON line carries: value (device-timed, inputs resident in HBM; the
 tensor is larger than L2, so no flush is needed), e2e (the same metric
@@ -85,9 +89,10 @@ DIMS = [4800000, 1800000, 1800000]
 NNZ = 140_000_000
 ZIPF = [1.2, 1.2, 1.2]
 RANK = 32
-# bounded CPU sample: every mode keeps nnz/dims <= 4, so the reference runs
-# its atomic variant (no per-thread da_mem buffers of whole-mode size)
-CPU_SAMPLE_NNZ = 7_000_000
+# bounded CPU sample: 24M nonzeros keep nnz/dims above 4 in every mode (5,
+# 13, 13), so the reference runs the same variant (da_mem_pull,
+# include/alto.hpp:1544-1634) as on the whole tensor
+CPU_SAMPLE_NNZ = 24_000_000
 METRIC = "MTTKRP nnz*R/s (all-mode, rank 32)"
 WORKLOAD = "powerlaw3d-4.8Mx1.8Mx1.8M-140Mnnz-zipf1.2-R32-allmode"
 
@@ -95,7 +100,10 @@ WORKLOAD = "powerlaw3d-4.8Mx1.8Mx1.8M-140Mnnz-zipf1.2-R32-allmode"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve", "slice", "tns"], default="mttkrp")
+    ap.add_argument("--workload", choices=["mttkrp", "cpstream", "serve", "slice", "tns", "cpals3d", "cpals5d"],
+                    default="mttkrp")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="mttkrp: leave out the other configurations' sub-objects of the default line")
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (mttkrp: all-mode MTTKRPs, default 10; cpstream: slices, default 197; "
                          "serve: slices per stream, default 7)")
@@ -117,14 +125,15 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--factor-dtype", choices=["f32", "bf16"], default="f32",
                     help="factor storage (bf16 halves gather bytes; accumulation stays f32)")
-    ap.add_argument("--shard", action="store_true",
-                    help="mttkrp under torchrun: one tensor sharded over the ranks' line ranges, each step "
-                         "the local MTTKRPs plus an NCCL all-reduce of every output (strong scaling)")
+    ap.add_argument("--independent", action="store_true",
+                    help="mttkrp under torchrun: an independent tensor per rank (weak scaling, no collective) "
+                         "instead of the one tensor sharded by output-row blocks")
     ap.add_argument("--tns-path", default=None, help="tns: where the text file is written (default: a temp dir)")
     ap.add_argument("--profile-small", action="store_true",
                     help="small case for ncu captures (mttkrp: 20M nonzeros; slice: a quarter of the tensor), 1 step")
     args = ap.parse_args()
-    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1), "slice": (20, 3), "tns": (3, 1)}[args.workload]
+    defaults = {"mttkrp": (10, 3), "cpstream": (197, 3), "serve": (7, 1), "slice": (20, 3), "tns": (3, 1),
+                "cpals3d": (20, 1), "cpals5d": (5, 1)}[args.workload]
     if args.steps is None:
         args.steps = defaults[0]
     if args.warmup is None:
@@ -140,7 +149,9 @@ def dist_env():
 
 
 def line_bytes_per_nnz(alto_bits):
-    key = 8 if alto_bits <= 64 else (12 if alto_bits <= 96 else 16)
+    """Algorithmic line bytes per nonzero: the reference's key (8 bytes for a
+    64-bit ALTO mask, 16 for a 128-bit one) plus a float32 value."""
+    key = 8 if alto_bits <= 64 else 16
     return key + 4
 
 
@@ -221,42 +232,101 @@ def recorded_traffic():
     return None
 
 
-def cpu_sample(n, rank, seed=2024):
-    """The bounded host sample of the workload's distribution."""
+def host_tensor(n, seed):
+    """n nonzeros of the workload's distribution as host arrays (uint64
+    indices [3, n], float64 values): drawn on cuda:0 by the same generator as
+    the timed tensor (seed 1234 gives exactly rank 0's timed tensor), else on
+    the host with numpy when no GPU is visible."""
     import numpy as np
 
     from alto_b200 import synth
 
-    cidx, vals = synth.powerlaw_coo(DIMS, n, ZIPF, seed=seed, values="lognormal")
-    rng = np.random.default_rng(seed + 1)
-    F = [rng.uniform(-1.0, 1.0, (d, rank)) for d in DIMS]
-    return cidx, vals, F
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            c, v = synth.zipf_coo_device(DIMS, n, ZIPF, seed=seed, values="lognormal", device="cuda:0")
+            cidx = c.cpu().numpy().astype(np.uint64)
+            vals = v.double().cpu().numpy()
+            del c, v
+            torch.cuda.empty_cache()
+            return cidx, vals
+    except ImportError:
+        pass
+    return synth.powerlaw_coo(DIMS, n, ZIPF, seed=seed, values="lognormal")
 
 
-def time_reference_cpu(n, rank, reps):
-    """Seconds per all-mode step of the reference's mttkrp_alto_par (OpenMP,
-    all host threads) on an n-nonzero sample; returns (sec, threads, nnz)."""
-    import numpy as np  # noqa: F401
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def reference_threads(nnz, rank, threads):
+    """Threads (= the reference's partitions) whose per-thread da_mem buffers
+    fit the host: each holds a whole-mode output block (the power-law
+    intervals span nearly every row), max(dims) x rank float64, beside about
+    120 bytes per nonzero of COO, ALTO and sort buffers and the factors."""
+    avail = host_mem_available()
+    base = nnz * 120 + sum(DIMS) * rank * 8 * 2
+    per = max(DIMS) * rank * 8
+    fit = int((avail * 0.85 - base) // per) if avail else threads
+    return max(0, min(threads, fit)), avail
+
+
+def time_reference_cpu(n, rank, reps, seed=2024):
+    """Seconds per all-mode step of the reference's mttkrp_alto_par (OpenMP)
+    on n nonzeros of the workload distribution; returns (sec, threads, nnz,
+    host bytes available).  Threads: all host threads, fewer if the
+    reference's per-thread buffers would not fit host memory."""
+    import numpy as np
 
     import oracle as O
 
     L = O.ref_lib(128)
-    threads = os.cpu_count() or 1
+    threads, avail = reference_threads(n, rank, os.cpu_count() or 1)
+    if threads < 1:
+        raise MemoryError(f"{n} nonzeros need more than the {avail / 2**30:.0f} GiB of host memory available")
     L.ref_set_threads(threads)
-    cidx, vals, F = cpu_sample(n, rank)
-    t = O.RefTensor(DIMS, cidx, vals, threads, bits=128)
-    sec = t.mttkrp_time(-1, F, rank, reps)
+    cidx, vals = host_tensor(n, seed)
+    rng = np.random.default_rng(seed + 1)
+    F = [rng.uniform(-1.0, 1.0, (d, rank)) for d in DIMS]
+    with stdout_to_stderr():
+        t = O.RefTensor(DIMS, cidx, vals, threads, bits=128)
+        del cidx, vals
+        sec = t.mttkrp_time(-1, F, rank, reps)
     nnz = t.nnz
     t.close()
-    return sec, threads, nnz
+    return sec, threads, nnz, avail
+
+
+def reference_variants(nnz):
+    """The variant the reference's dispatcher picks per mode
+    (include/alto.hpp:835-846): atomic when dims > 512 and nnz/dims <= 4,
+    else da_mem_pull."""
+    return ["atomic" if d > 512 and nnz // d <= 4 else "da_mem_pull" for d in DIMS]
 
 
 def reference_arm(args):
+    """The reference's own OpenMP MTTKRP (oracle/_ref, mttkrp_alto_par) on the
+    whole workload tensor -- the very tensor rank 0 of the GPU arm times
+    (same generator and seed) -- when its buffers fit host memory, else on
+    the 24M-nonzero sample that keeps the same variant; steps = repetitions
+    of the all-mode MTTKRP after one untimed one."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    n, seed, same = args.nnz, 1234, True
+    threads, avail = reference_threads(n, args.rank, os.cpu_count() or 1)
+    if threads < max(1, (os.cpu_count() or 1) // 4):
+        n, seed, same = args.cpu_sample, 2024, False
     try:
-        sec, threads, nnz = time_reference_cpu(args.cpu_sample, args.rank, max(args.steps, 1))
+        sec, threads, nnz, avail = time_reference_cpu(n, args.rank, max(args.steps, 1), seed=seed)
     except Exception as e:  # the checker library is missing or failed to load
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
         return 0
@@ -266,15 +336,51 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "nnz*R/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_nnz": nnz, "dims": DIMS, "rank": args.rank,
-                   "note": "bounded sample of the same distribution (full tensor does not fit the "
-                           "reference's per-thread buffers on this host)"},
+        "config": {"workload": WORKLOAD, "nnz": nnz, "dims": DIMS, "rank": args.rank, "same_config": same,
+                   "threads": threads, "host_mem_available_gib": round(avail / 2**30, 1),
+                   "variants": reference_variants(nnz),
+                   "note": ("the whole tensor the GPU arm times (same generator and seed)" if same else
+                            "24M-nonzero sample of the same distribution: the whole tensor's per-thread "
+                            "buffers do not fit this host's memory")},
         "cpu_baseline": {"value": value, "unit": "nnz*R/s", "cores": threads, "kind": "reference",
-                         "sample": f"{nnz} nonzeros of the workload distribution, all-mode MTTKRP"},
+                         "sample": f"{nnz} nonzeros, all-mode MTTKRP, {max(args.steps, 1)} reps"},
         "e2e": {"value": value, "unit": "nnz*R/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def sampled_rows_error(cidx, vals, factors, outs, R, nrows=4096, seed=5):
+    """Max relative (normwise) error of each mode's MTTKRP output against
+    float64 sums recomputed on the host from the COO: 4096 rows drawn
+    uniformly among the rows that hold nonzeros, plus the heaviest row.
+    cidx/vals: the generated COO on the device; factors: the float32 inputs
+    (their values widened exactly); outs: the device outputs."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(seed)
+    F64 = [f.double().cpu() for f in factors]
+    errs, picked = [], []
+    for m in range(cidx.shape[0]):
+        present = torch.unique(cidx[m])
+        take = torch.from_numpy(rng.choice(present.numel(), min(nrows, present.numel()), replace=False))
+        heavy = torch.bincount(cidx[m]).argmax().view(1)
+        rows = torch.unique(torch.cat([present[take.to(present.device)], heavy]))
+        sel = torch.isin(cidx[m], rows)
+        idx = cidx[:, sel].cpu()
+        v = vals[sel].double().cpu()
+        prod = v[:, None].expand(-1, R).clone()
+        for o in range(cidx.shape[0]):
+            if o != m:
+                prod *= F64[o].index_select(0, idx[o])
+        rows_h = rows.cpu()
+        pos = torch.searchsorted(rows_h, idx[m])
+        ref = torch.zeros((rows_h.numel(), R), dtype=torch.float64).index_add_(0, pos, prod)
+        got = outs[m].index_select(0, rows).double().cpu()
+        errs.append(float((got - ref).abs().max() / ref.abs().max().clamp_min(1e-300)))
+        picked.append(int(sel.sum()))
+    return errs, picked
 
 
 def ours(args):
@@ -301,17 +407,31 @@ def ours(args):
     R = args.rank
     N = len(DIMS)
 
-    # independent tensors per rank (weak scaling), or one tensor sharded
-    seed = 1234 if args.shard else 1234 + rank
-    cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=seed, values="lognormal", device=dev)
-    t = A.AltoTensor(DIMS, cidx, vals, nprtn=1)
-    total_nnz = t.nnz
-    if args.shard:
-        from alto_b200 import shard
+    # Under torchrun: the one tensor sharded by output-row blocks (strong
+    # scaling; every rank draws the same tensor and encodes, per mode, only
+    # the nonzeros of its block of that mode's rows), or with --independent
+    # a tensor of its own per rank (weak scaling, no collective).
+    from alto_b200 import shard
 
-        shard.shard_tensor(t, rank, world)
+    sharded = world > 1 and not args.independent
+    seed = 1234 if (sharded or world == 1) else 1234 + rank
+    cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=seed, values="lognormal", device=dev)
+    total_nnz = int(cidx.shape[1])
+    bounds = None
+    if sharded:
+        tens, bounds = [], []
+        for m in range(N):
+            b = shard.row_blocks(torch.bincount(cidx[m], minlength=DIMS[m]), world)
+            c_r, v_r = shard.select_block(cidx, vals, m, b[rank], b[rank + 1])
+            tens.append(A.AltoTensor(DIMS, c_r, v_r, nprtn=1))
+            bounds.append(b)
+            del c_r, v_r
+        del cidx, vals
+        t = tens[0]
+    else:
+        t = A.AltoTensor(DIMS, cidx, vals, nprtn=1)
+        tens = [t] * N
     nnz = t.nnz
-    del cidx, vals
     torch.cuda.empty_cache()
     g = torch.Generator(device=dev)
     g.manual_seed(99 + rank)
@@ -319,7 +439,27 @@ def ours(args):
     factors = [(torch.rand((d, R), generator=g, device=dev) * 2 - 1).to(fdt).contiguous() for d in DIMS]
     outs = [torch.empty((d, R), device=dev, dtype=torch.float32) for d in DIMS]
     stream = torch.cuda.current_stream()
-    variants = t.autotune(factors, R)  # project autotuner: fastest kernel variant per mode
+
+    def timed(fn, reps=1):  # ms per call of fn, CUDA events on the stream
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # the row-sorted copies (built on first use): build time = first call - a later call
+    bytes0 = sum(x.device_bytes() for x in set(tens))
+    sorted_build_ms = []
+    for m in range(N):
+        first = timed(lambda: tens[m].mttkrp(m, factors, R, out=outs[m], variant=A.SORTED, stream=stream))
+        again = timed(lambda: tens[m].mttkrp(m, factors, R, out=outs[m], variant=A.SORTED, stream=stream))
+        sorted_build_ms.append(round(first - again, 2))
+    sorted_bytes = sum(x.device_bytes() for x in set(tens)) - bytes0
+    # project autotuner: fastest kernel variant per mode (of each mode's tensor)
+    tuned = {id(x): x.autotune(factors, R) for x in set(tens)}
+    variants = [tuned[id(tens[m])][m] for m in range(N)]
     vnames = {A.ATOMIC: "atomic", A.STAGED: "staged", A.STREAM: "stream", A.SORTED: "sorted"}
 
     def step(ev=None):
@@ -327,11 +467,11 @@ def ours(args):
             outs[m].zero_()
             if ev is not None:
                 ev[m][0].record(stream)
-            t.mttkrp(m, factors, R, out=outs[m], accumulate=True, stream=stream)
+            tens[m].mttkrp(m, factors, R, out=outs[m], accumulate=True, stream=stream)
             if ev is not None:
                 ev[m][1].record(stream)
-            if args.shard and world > 1:
-                torch.distributed.all_reduce(outs[m])
+            if sharded:
+                shard.allgather_rows(outs[m], bounds[m])
 
     for _ in range(warmup):
         step()
@@ -364,7 +504,7 @@ def ours(args):
         x = torch.tensor([elapsed], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
         elapsed = float(x.item())
-    units = (total_nnz if args.shard else nnz * world) * R * N * steps
+    units = (total_nnz if sharded else nnz * world) * R * N * steps
     value = units / elapsed
 
     # roofline of the MTTKRP kernel (per-mode launches, CUDA events on its stream)
@@ -372,7 +512,7 @@ def ours(args):
     per_mode = []
     for m in range(N):
         dt = statistics.mean(events[k][m][0].elapsed_time(events[k][m][1]) / 1e3 for k in range(steps))
-        b = mttkrp_bytes(DIMS, nnz, R, m, alto_bits, fbytes=2 if args.factor_dtype == "bf16" else 4)
+        b = mttkrp_bytes(DIMS, tens[m].nnz, R, m, alto_bits, fbytes=2 if args.factor_dtype == "bf16" else 4)
         per_mode.append((m, dt, b))
     bytes_launch = sum(b for _, _, b in per_mode) / N
     dt_launch = sum(dt for _, dt, _ in per_mode) / N
@@ -380,11 +520,30 @@ def ours(args):
     peak, peak_kind = measured_peaks()
     traffic = recorded_traffic()
 
+    # the ALTO line itself (vector atomics, no row-sorted copy), per mode
+    line_ms = [round(timed(lambda: tens[m].mttkrp(m, factors, R, out=outs[m], variant=A.ATOMIC, stream=stream), 3),
+                     4) for m in range(N)]
+    # error against float64 sums from the generated COO, on the last timed step's outputs
+    err = None
+    if not sharded:
+        for m in range(N):
+            outs[m].zero_()
+            t.mttkrp(m, factors, R, out=outs[m], accumulate=True, stream=stream)
+        torch.cuda.synchronize()
+        errs, picked = sampled_rows_error(cidx, vals, factors, outs, R)
+        err = {"max_rel_err": max(errs), "per_mode": errs, "bound": 1e-5,
+               "method": "normwise max |gpu - fp64| / max |fp64| over 4096 uniformly drawn rows with "
+                         "nonzeros plus the heaviest row of each mode; float64 sums on the host from the "
+                         "generated COO and the float32 factor values",
+               "nonzeros_checked": picked}
+        del cidx, vals
+        torch.cuda.empty_cache()
+
     # end to end through the host-buffer C-ABI entry point
     e2e = None
-    if args.shard:
+    if sharded:
         e2e = {"value": None, "unit": "nnz*R/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
-               "note": "not measured in shard mode (the host-buffer entry point covers one rank's shard)"}
+               "note": "not measured when sharded (the host-buffer entry point covers one rank's tensors)"}
     elif not args.no_e2e:
         hostF = [torch.empty((d, R), dtype=torch.float64, pin_memory=True) for d in DIMS]
         for h, f in zip(hostF, factors):
@@ -413,9 +572,11 @@ def ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_small:
         try:
-            sec, threads, snnz = time_reference_cpu(args.cpu_sample, R, 3)
+            sec, threads, snnz, _ = time_reference_cpu(args.cpu_sample, R, 3)
             cpu = {"value": snnz * R * N / sec, "unit": "nnz*R/s", "cores": threads, "kind": "reference",
-                   "sample": f"{snnz} nonzeros of the same distribution, all-mode MTTKRP, 3 reps"}
+                   "sample": f"{snnz} nonzeros of the same distribution, all-mode MTTKRP, 3 reps; the "
+                             f"reference's variants per mode: {reference_variants(snnz)} (as on the whole "
+                             f"tensor: {reference_variants(nnz)})"}
         except Exception as e:
             cpu = {"value": None, "unit": "nnz*R/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -424,17 +585,25 @@ def ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "nnz*R/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": elapsed / steps * 1e3, "higher_is_better": True,
-            "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "dims": DIMS, "nnz": total_nnz if args.shard else nnz, "rank": R,
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dims": DIMS, "nnz": total_nnz if sharded else nnz, "rank": R,
                        "zipf": 1.2,
                        "values": "lognormal(0,1)", "key_bits": t.key_bits, "alto_bits": alto_bits,
                        "factor_dtype": args.factor_dtype,
-                       "parallelism": (f"one tensor, line sharded over {world} GPUs + NCCL all-reduce per mode"
-                                       if args.shard else f"independent tensor per GPU x{world}"),
+                       "parallelism": (f"one tensor; per mode, equal-nnz output-row blocks on {world} GPUs, each "
+                                       f"encoding its own nonzeros, + a row all-gather (NCCL broadcast per block) "
+                                       f"per mode" if sharded else
+                                       (f"independent tensor per GPU x{world}" if world > 1 else "one GPU")),
                        "l2": "inputs larger than L2 (line + factors > 3 GB); no flush",
                        "line_bytes_per_nnz": line_bytes_per_nnz(alto_bits),
                        "variants": [vnames.get(v, str(v)) for v in variants],
-                       "device_bytes": t.device_bytes()},
+                       "row_sorted_copies": {
+                           "bytes": sorted_bytes, "build_ms_per_mode": sorted_build_ms,
+                           "order": "per mode: output row, then the row of the shorter other mode, then "
+                                    "ALTO order; built once, outside the timed region"},
+                       "alto_line_atomic_ms_per_mode": line_ms,
+                       "device_bytes": sum(x.device_bytes() for x in set(tens))},
+            "error_vs_fp64": err,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic.get("bytes_per_launch") if traffic else None,
@@ -445,12 +614,12 @@ def ours(args):
             "clocks": clocks,
             "gpu_launches": launches,
         }
-        print(json.dumps(line))
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    t.close()
-    return 0
+    for x in set(tens):
+        x.close()
+    return line if rank == 0 else None
 
 
 # ----------------------------------------------------------------- CP-stream
@@ -612,8 +781,7 @@ def ours_cpstream(args):
         "clocks": clocks,
         "gpu_launches": launches,
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 # ------------------------------------------------------------------- serving
@@ -760,7 +928,7 @@ def ours_serve(args):
         dist.barrier()
         dist.destroy_process_group()
         if rank != 0:
-            return 0
+            return None
     value = n / served_s
     plain_rate = n / plain_s
     p99_iso = float(np.percentile(iso, 99))
@@ -792,8 +960,7 @@ def ours_serve(args):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = serve_reference_sample(streams, pool, offs, need, model=args.model)
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def serve_reference_sample(streams, pool, offs, need, nstreams=6, nslices=3, model="cpstream"):
@@ -1209,19 +1376,312 @@ def reference_tns_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ CP-ALS
+
+CPALS3_DIMS = [1000, 1000, 1000]
+CPALS3_NNZ = 1_000_000
+CPALS5_DIMS = [100000, 100000, 10000, 1000, 100]
+CPALS5_NNZ = 50_000_000
+CPALS5_ZIPF = [1.1, 1.1, None, None, None]
+
+
+def init_model(dims, R, seed):
+    """Initial factors in [-3, 3] with random sign (the reference's rand_val range)."""
+    from alto_b200 import synth
+
+    init = synth.init_values(int(sum(dims)) * R, seed=seed)
+    U0, off = [], 0
+    for d in dims:
+        U0.append(init[off:off + int(d) * R].reshape(int(d), R).copy())
+        off += int(d) * R
+    return U0
+
+
+def flush_l2(buf):
+    buf.add_(1.0)  # writes 256 MB, twice the L2
+
+
+def ours_cpals3d(args):
+    """CP-ALS on 1000^3 with 1,000,000 uniform distinct nonzeros (values
+    U(0,1)), rank 16, a 64-bit ALTO mask, 20 iterations, plus 100 standalone
+    mode-0 MTTKRPs; fits, factors and the MTTKRP checked against the FP64
+    oracle (single-threaded restatement, fed the original float64 values and
+    initial model).  The tensor is L2-resident (12 MB), so L2 is flushed
+    before every timed MTTKRP."""
+    import numpy as np
+    import torch
+
+    import alto_b200 as A
+    import oracle as O
+    from alto_b200 import synth
+
+    torch.cuda.set_device(0)
+    R, iters = 16, 20
+    dims = np.array(CPALS3_DIMS, np.uint64)
+    cidx, vals = synth.uniform_coo(dims, CPALS3_NNZ, seed=55)
+    nnz = cidx.shape[1]
+    t = A.create_alto(dims, cidx, vals)
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(5)
+    F = [rng.uniform(-1, 1, (int(d), R)).astype(np.float32) for d in dims]
+    Fd = [torch.tensor(f, device="cuda") for f in F]
+    out = torch.empty((int(dims[0]), R), device="cuda", dtype=torch.float32)
+    junk = torch.empty(64 << 20, device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        t.mttkrp(0, Fd, R, out=out, stream=stream)
+    launches0 = A.kernel_launches()
+    ms = []
+    for _ in range(100):
+        flush_l2(junk)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t.mttkrp(0, Fd, R, out=out, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = A.kernel_launches() - launches0
+    mt_ms = float(np.mean(ms))
+    enc = O.build(dims, cidx, vals)
+    fo64 = [f.astype(np.float64) for f in F]
+    fo64[0][:] = 0
+    ref = O.mttkrp(enc, 0, fo64, R)[0]
+    got = out.cpu().numpy()
+    mt_err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    U0 = init_model(dims, R, 55)
+    A.cpd_alto(t, U0, np.ones(R), R, 1, 1e-12)  # warm
+    ts = time.perf_counter()
+    U, lam, fits, it = A.cpd_alto(t, U0, np.ones(R), R, iters, 1e-12)
+    cpd_s = time.perf_counter() - ts
+    Uo, lo, fo, ito = O.cpd_als(enc, U0, np.ones(R), R, iters, 1e-12)
+    fit_err = float(np.max(np.abs(np.asarray(fits) - fo) / np.abs(fo)))
+    fac_err = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(U, Uo))
+    t_bits = t.alto_bits
+    t.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            L = O.ref_lib(64)
+            threads = os.cpu_count() or 1
+            L.ref_set_threads(threads)
+            rt = O.RefTensor(dims, cidx, vals, threads, bits=64)
+            Fr = [f.astype(np.float64) for f in F]
+            sec = rt.mttkrp_time(0, Fr, R, 100)
+            with stdout_to_stderr():
+                ts = time.perf_counter()
+                rt.cpd_als(U0, np.ones(R), R, iters, 1e-12)
+                ref_cpd = time.perf_counter() - ts
+            rt.close()
+            cpu = {"value": nnz * R / sec, "unit": "nnz*R/s", "cores": threads, "kind": "reference",
+                   "sample": "the whole tensor: 100 mode-0 mttkrp_alto_par calls",
+                   "cpals_ms_per_iter": ref_cpd / iters * 1e3}
+        except Exception as e:
+            cpu = {"value": None, "unit": "nnz*R/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+    peak, peak_kind = measured_peaks()
+    b = mttkrp_bytes(CPALS3_DIMS, nnz, R, 0, t_bits)
+    return {
+        "metric": "CP-ALS ms/iteration; mode-0 MTTKRP nnz*R/s (rank 16)", "value": nnz * R / (mt_ms / 1e3),
+        "unit": "nnz*R/s", "n_gpus": 1, "steps": 100, "warmup": 3, "ms_per_step": mt_ms, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "cpals3d-1000^3-1Mnnz-uniform-R16-it20", "dims": CPALS3_DIMS, "nnz": nnz, "rank": R,
+                   "alto_bits": t_bits, "l2": "L2 flushed (256 MB write) before every timed MTTKRP"},
+        "cpals": {"ms_per_iter": cpd_s / iters * 1e3, "iters": it, "final_fit": float(fits[-1]),
+                  "api": "alto_cpd_als (float64 host model in and out)"},
+        "error_vs_fp64": {"fit_max_rel_err": fit_err, "fit_bound": 1e-5, "factor_max_rel_err": fac_err,
+                          "mttkrp_max_rel_err": mt_err, "mttkrp_bound": 1e-5,
+                          "method": "the oracle's CP-ALS (float64) from the original values and initial model; "
+                                    "MTTKRP against the oracle's with the same float32 factor values"},
+        "roofline": {"bound": "hbm", "achieved": b / (mt_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": b / (mt_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+    }
+
+
+def ours_cpals5d(args):
+    """Rank-64 CP-ALS on the 5-mode tensor 100k x 100k x 10k x 1k x 100 with
+    50,000,000 distinct nonzeros (modes 0-1 Zipf(1.1) with permuted labels,
+    modes 2-4 uniform, values U(0,1)), generated on the device; once with
+    float32 and once with bfloat16 factor storage (float32 accumulation,
+    float64 Grams and Cholesky).  Per-mode MTTKRP GB/s for both storages,
+    their error against float64 sums of sampled rows (bfloat16 against the
+    float32 factor values before rounding), fits and time per iteration."""
+    import numpy as np
+    import torch
+
+    import alto_b200 as A
+    from alto_b200 import synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    R, iters = 64, args.steps if args.workload == "cpals5d" else 5
+    N = len(CPALS5_DIMS)
+    cidx, vals = synth.zipf_coo_device(CPALS5_DIMS, CPALS5_NNZ, CPALS5_ZIPF, seed=9, values="uniform", device=dev)
+    t = A.AltoTensor(CPALS5_DIMS, cidx, vals, nprtn=1)
+    nnz = t.nnz
+    stream = torch.cuda.current_stream()
+    g = torch.Generator(device=dev)
+    g.manual_seed(17)
+    F32 = [(torch.rand((d, R), generator=g, device=dev) * 2 - 1).contiguous() for d in CPALS5_DIMS]
+    FB = [f.to(torch.bfloat16).contiguous() for f in F32]
+    outs = [torch.empty((d, R), device=dev, dtype=torch.float32) for d in CPALS5_DIMS]
+    peak, peak_kind = measured_peaks()
+    launches0 = A.kernel_launches()
+    res = {}
+    for name, F, fb in (("f32", F32, 4), ("bf16", FB, 2)):
+        t.autotune(F, R)
+        per = []
+        for m in range(N):
+            for _ in range(2):
+                t.mttkrp(m, F, R, out=outs[m], stream=stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(3):
+                t.mttkrp(m, F, R, out=outs[m], stream=stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / 3
+            b = mttkrp_bytes(CPALS5_DIMS, nnz, R, m, t.alto_bits, fbytes=fb)
+            per.append({"ms": round(ms, 4), "gbs": round(b / (ms / 1e3) / 1e9, 1),
+                        "frac": round(b / (ms / 1e3) / 1e9 / peak, 4),
+                        "variant": {A.ATOMIC: "atomic", A.STAGED: "staged", A.SORTED: "sorted"}.get(
+                            t.choose_variant(m, R, A.BF16 if fb == 2 else A.F32), "other")})
+        torch.cuda.synchronize()
+        errs, _ = sampled_rows_error(cidx, vals, F32, outs, R, nrows=2048)
+        res[name] = {"per_mode": per, "mttkrp_max_rel_err": max(errs), "mttkrp_err_per_mode": errs}
+    launches = A.kernel_launches() - launches0
+    del cidx, vals, F32, FB, outs
+    torch.cuda.empty_cache()
+    U0 = init_model(CPALS5_DIMS, R, 3)
+    for name, storage in (("f32", A.F32), ("bf16", A.BF16)):
+        A.cpd_alto(t, U0, np.ones(R), R, 1, 1e-12, storage=storage)  # warm
+        ts = time.perf_counter()
+        _, _, fits, it = A.cpd_alto(t, U0, np.ones(R), R, iters, 1e-12, storage=storage)
+        res[name]["cpals_ms_per_iter"] = (time.perf_counter() - ts) / iters * 1e3
+        res[name]["fits"] = [float(x) for x in fits]
+    t.close()
+    flops = nnz * R * N
+    ms_all = sum(p["ms"] for p in res["f32"]["per_mode"])
+    b_all = sum(mttkrp_bytes(CPALS5_DIMS, nnz, R, m, 65) for m in range(N))
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s of FP32 FMA on CUDA cores at max clock
+    return {
+        "metric": "CP-ALS rank 64, per-mode MTTKRP GB/s (float32 and bfloat16 factor storage)",
+        "value": b_all / (ms_all / 1e3) / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": iters, "warmup": 1,
+        "ms_per_step": res["f32"]["cpals_ms_per_iter"], "higher_is_better": True, "dtype": "f32/bf16+f64",
+        "data": "synthetic",
+        "config": {"workload": "cpals5d-100kx100kx10kx1kx100-50Mnnz-zipf1.1-R64", "dims": CPALS5_DIMS, "nnz": nnz,
+                   "rank": R, "alto_bits": t.alto_bits, "iters": iters,
+                   "l2": "line (1 GB) and factors exceed L2; no flush"},
+        "storage": res,
+        "error_vs_fp64": {"mttkrp_max_rel_err_f32": res["f32"]["mttkrp_max_rel_err"],
+                          "mttkrp_max_rel_err_bf16": res["bf16"]["mttkrp_max_rel_err"],
+                          "fit_rel_diff_bf16_vs_f32": abs(res["bf16"]["fits"][-1] - res["f32"]["fits"][-1])
+                          / abs(res["f32"]["fits"][-1]),
+                          "method": "sampled rows (2048 per mode + the heaviest) in float64 from the COO; "
+                                    "bfloat16 against the float32 factor values before rounding. The CP-ALS "
+                                    "fit against the FP64 oracle is tested at 2M nonzeros (tests/test_gpu_configs.py)"},
+        "roofline": {"bound": "hbm", "achieved": b_all / (ms_all / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": b_all / (ms_all / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "fp32_fma": {"achieved_tflops": flops * N / (ms_all / 1e3) / 1e12,
+                                  "peak_tflops_nominal": fp32_peak}},
+        "cpu_baseline": None,
+        "gpu_launches": launches,
+    }
+
+
+def reference_cpals_arm(args):
+    """--impl reference for cpals3d: the reference's CP-ALS (oracle/_ref,
+    all host threads) on the same tensor; cpals5d: not run (its per-thread
+    buffers at rank 64 and 50M nonzeros are outside a bounded run)."""
+    import numpy as np
+
+    import oracle as O
+    from alto_b200 import synth
+
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
+    if args.workload == "cpals5d":
+        print(json.dumps({"impl": "reference", "unavailable": "cpals5d is not timed on the reference (bounded runs only)"}))
+        return 0
+    try:
+        dims = np.array(CPALS3_DIMS, np.uint64)
+        cidx, vals = synth.uniform_coo(dims, CPALS3_NNZ, seed=55)
+        R = 16
+        L = O.ref_lib(64)
+        threads = os.cpu_count() or 1
+        L.ref_set_threads(threads)
+        rt = O.RefTensor(dims, cidx, vals, threads, bits=64)
+        rng = np.random.default_rng(5)
+        F = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+        sec = rt.mttkrp_time(0, F, R, max(args.steps, 1) * 5)
+        rt.close()
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
+        return 0
+    value = cidx.shape[1] * R / sec
+    print(json.dumps({
+        "impl": "reference", "metric": "CP-ALS ms/iteration; mode-0 MTTKRP nnz*R/s (rank 16)", "value": value,
+        "unit": "nnz*R/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 1, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "cpals3d-1000^3-1Mnnz-uniform-R16-it20"},
+        "cpu_baseline": {"value": value, "unit": "nnz*R/s", "cores": threads, "kind": "reference",
+                         "sample": "the whole tensor, mode-0 mttkrp_alto_par"},
+        "e2e": {"value": value, "unit": "nnz*R/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def config_lines(args):
+    """The other workload configurations, one sub-object each, for the
+    default one-GPU line: CP-ALS on 1000^3 (1M nonzeros, rank 16, 20
+    iterations), rank-64 CP-ALS on the 5-mode tensor (50M nonzeros, float32
+    and bfloat16 factor storage), CP-stream (the first 40 slices) and serving
+    (64 streams)."""
+    out = {}
+    for name, fn, steps, warmup in (("cpals_1000cubed_1M_r16", ours_cpals3d, None, None),
+                                    ("cpals_5mode_50M_r64", ours_cpals5d, None, None),
+                                    ("cpstream", ours_cpstream, 37, 3),
+                                    ("serve", ours_serve, 4, 1)):
+        sub = argparse.Namespace(**vars(args))
+        sub.workload = name
+        if steps is not None:
+            sub.steps, sub.warmup = steps, warmup
+        try:
+            out[name] = fn(sub)
+        except Exception as e:  # one configuration failing must not hide the others
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        import torch
+
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     if args.workload == "tns":
         return reference_tns_arm(args) if args.impl == "reference" else ours_tns(args)
     if args.workload == "slice":
         return reference_slice_arm(args) if args.impl == "reference" else ours_slice(args)
+    if args.workload in ("cpals3d", "cpals5d"):
+        if args.impl == "reference":
+            return reference_cpals_arm(args)
+        line = ours_cpals3d(args) if args.workload == "cpals3d" else ours_cpals5d(args)
+        print(json.dumps(line))
+        return 0
     if args.workload != "mttkrp":
         if args.impl == "reference":
             return reference_stream_arm(args)
-        return ours_cpstream(args) if args.workload == "cpstream" else ours_serve(args)
+        line = ours_cpstream(args) if args.workload == "cpstream" else ours_serve(args)
+        if line is not None:
+            print(json.dumps(line))
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
-    return ours(args)
+    line = ours(args)
+    if line is not None:
+        if line["n_gpus"] == 1 and not (args.profile_small or args.no_configs):
+            line["configs"] = config_lines(args)
+        print(json.dumps(line))
+    return 0
 
 
 if __name__ == "__main__":
