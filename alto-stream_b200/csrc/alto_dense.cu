@@ -19,6 +19,7 @@
 #include <mutex>
 
 #include "alto_dense.cuh"
+#include "alto_group.cuh"
 
 namespace alto {
 
@@ -158,9 +159,9 @@ static alto_status gram_launch(const TA* A, const TB* B, uint64_t I, int R, doub
 // Gram and change statistics of a freshly updated factor), layout
 // [block][2 R^2 + 3].
 template <int PPT>
-__global__ void __launch_bounds__(kGramThreads)
-    gram_cross_partial_kernel(const float* __restrict__ P, const float* __restrict__ U, uint64_t I, int R,
-                              uint64_t rows_per_block, double* __restrict__ partials) {
+__device__ __forceinline__ void gram_cross_partial_body(const float* __restrict__ P, const float* __restrict__ U,
+                                                        uint64_t I, int R, uint64_t rows_per_block,
+                                                        double* __restrict__ partials, uint32_t block) {
   extern __shared__ double sm[];
   double* sp = sm;
   double* su = sm + kGramRows * R;
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kGramThreads)
 #pragma unroll
   for (int k = 0; k < PPT; ++k) g[k] = c[k] = 0.0;
   double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-  const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_block;
+  const uint64_t r0 = (uint64_t)block * rows_per_block;
   const uint64_t r1 = min(r0 + rows_per_block, I);
   const int RR = R * R;
   for (uint64_t t0 = r0; t0 < r1; t0 += kGramRows) {
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(kGramThreads)
     }
     __syncthreads();
   }
-  double* out = partials + (size_t)blockIdx.x * (2 * RR + 3);
+  double* out = partials + (size_t)block * (2 * RR + 3);
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     const int p = threadIdx.x + k * kGramThreads;
@@ -226,16 +227,24 @@ __global__ void __launch_bounds__(kGramThreads)
     for (int w = 0; w < kGramThreads / 32; ++w) t += wq[threadIdx.x][w];
     out[2 * RR + threadIdx.x] = t;
   }
+  __syncthreads();
+}
+
+template <int PPT>
+__global__ void __launch_bounds__(kGramThreads)
+    gram_cross_partial_kernel(const float* __restrict__ P, const float* __restrict__ U, uint64_t I, int R,
+                              uint64_t rows_per_block, double* __restrict__ partials) {
+  gram_cross_partial_body<PPT>(P, U, I, R, rows_per_block, partials, blockIdx.x);
 }
 
 // reduce_partials_kernel with the result split over three outputs:
 // [0, n1) -> o1, [n1, 2 n1) -> o2, the rest -> o3.
-__global__ void __launch_bounds__(kReduceThreads)
-    reduce_split_kernel(const double* __restrict__ partials, int nblocks, int n1, int n, double* __restrict__ o1,
-                        double* __restrict__ o2, double* __restrict__ o3) {
+__device__ __forceinline__ void reduce_split_body(const double* __restrict__ partials, int nblocks, int n1, int n,
+                                                  double* __restrict__ o1, double* __restrict__ o2,
+                                                  double* __restrict__ o3, uint32_t block) {
   __shared__ double s[kReduceThreads / 32][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int p = blockIdx.x * 32 + lane;
+  const int p = block * 32 + lane;
   double acc = 0.0;
   if (p < n)
     for (int b = w; b < nblocks; b += kReduceThreads / 32) acc += partials[(size_t)b * n + p];
@@ -251,6 +260,99 @@ __global__ void __launch_bounds__(kReduceThreads)
     else if (o3)
       o3[p - 2 * n1] = t;
   }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kReduceThreads)
+    reduce_split_kernel(const double* __restrict__ partials, int nblocks, int n1, int n, double* __restrict__ o1,
+                        double* __restrict__ o2, double* __restrict__ o3) {
+  reduce_split_body(partials, nblocks, n1, n, o1, o2, o3, blockIdx.x);
+}
+
+// Grouped gram_cross_stats: partial blocks over all items (block_off
+// prefix sums of the items' nb), then reduction blocks (red_off).
+template <int PPT>
+__global__ void __launch_bounds__(kGramThreads)
+    gram_group_partial_kernel(Strided<GramItem> items, const uint32_t* __restrict__ block_off, int R) {
+  const int K = *items.count;
+  const uint32_t total = K > 0 ? block_off[K] : 0;
+  for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
+    int lo = 0, hi = K;  // the last s with block_off[s] <= v
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (block_off[mid] <= v)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const GramItem& it = items[lo];
+    if (it.active && !*it.active) continue;
+    gram_cross_partial_body<PPT>(it.P, it.U, it.I, R, it.rpb, it.part, v - block_off[lo]);
+  }
+}
+
+__global__ void __launch_bounds__(kReduceThreads)
+    gram_group_reduce_kernel(Strided<GramItem> items, const uint32_t* __restrict__ red_off, int R) {
+  const int K = *items.count;
+  const uint32_t total = K > 0 ? red_off[K] : 0;
+  const int RR = R * R, n = 2 * RR + 3;
+  for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
+    int lo = 0, hi = K;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (red_off[mid] <= v)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const GramItem& it = items[lo];
+    if (it.active && !*it.active) continue;
+    reduce_split_body(it.part, (int)it.nb, RR, n, it.G, it.C, it.stats3, v - red_off[lo]);
+  }
+}
+
+// At least 64 rows per block, at most 4 blocks per SM.
+void gram_split(uint64_t I, uint32_t* nb_out, uint64_t* rpb_out) {
+  uint64_t nb = std::min<uint64_t>((I + 63) / 64, (uint64_t)sms() * 4);
+  if (nb < 1) nb = 1;
+  const uint64_t rpb = (I + nb - 1) / nb;
+  nb = I ? (I + rpb - 1) / rpb : 1;
+  *nb_out = (uint32_t)nb;
+  *rpb_out = rpb;
+}
+
+uint32_t gram_reduce_blocks(int R) { return reduce_grid(2 * R * R + 3); }
+
+alto_status gram_group_launch(Strided<GramItem> items, const uint32_t* block_off, const uint32_t* red_off,
+                              int max_items, int R, cudaStream_t st) {
+  const int RR = R * R;
+  const int ppt = (RR + kGramThreads - 1) / kGramThreads;
+  const size_t smem = 2 * kGramRows * R * sizeof(double);
+  const unsigned grid = (unsigned)sms() * 4;
+#define GG_CASE(PP)                                                                                   \
+  case PP: {                                                                                          \
+    static size_t raised = 0;                                                                         \
+    if (smem > 48 * 1024 && smem > raised) {                                                          \
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(gram_group_partial_kernel<PP>,                               \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+      raised = smem;                                                                                  \
+    }                                                                                                 \
+    gram_group_partial_kernel<PP><<<grid, kGramThreads, smem, st>>>(items, block_off, R);             \
+    break;                                                                                            \
+  }
+  switch (ppt <= 1 ? 1 : ppt <= 2 ? 2 : ppt <= 4 ? 4 : ppt <= 16 ? 16 : 64) {
+    GG_CASE(1)
+    GG_CASE(2)
+    GG_CASE(4)
+    GG_CASE(16)
+    GG_CASE(64)
+  }
+#undef GG_CASE
+  ALTO_LAUNCHED();
+  const unsigned rgrid = (unsigned)std::max(1, std::min(max_items * (int)gram_reduce_blocks(R), (int)sms() * 8));
+  gram_group_reduce_kernel<<<rgrid, kReduceThreads, 0, st>>>(items, red_off, R);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
 }
 
 alto_status gram_cross_stats(const float* P, const float* U, uint64_t I, int R, double* G, double* C,
@@ -258,11 +360,10 @@ alto_status gram_cross_stats(const float* P, const float* U, uint64_t I, int R, 
   const int RR = R * R;
   const int n = 2 * RR + 3;
   const int ppt = (RR + kGramThreads - 1) / kGramThreads;
-  // at least 64 rows per block, at most 4 blocks per SM
-  uint64_t nb = std::min<uint64_t>((I + 63) / 64, (uint64_t)sms() * 4);
-  if (nb < 1) nb = 1;
-  const uint64_t rpb = (I + nb - 1) / nb;
-  nb = I ? (I + rpb - 1) / rpb : 1;
+  uint32_t nb32 = 1;
+  uint64_t rpb = 1;
+  gram_split(I, &nb32, &rpb);
+  uint64_t nb = nb32;
   ALTO_TRY(scratch.ensure(nb * n * sizeof(double)));
   double* part = scratch.as<double>();
   const size_t smem = 2 * kGramRows * R * sizeof(double);
@@ -420,10 +521,9 @@ __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes,
 // steps and operation order (so identical results), with the loops bounded
 // by RMAX and unrolled so the dot products' shared-memory loads overlap.
 template <int RMAX>
-__global__ void __launch_bounds__(32)
-    solve_setup_small_kernel(const double* __restrict__ grams, int nmodes, unsigned mask, int R, int kind,
-                             double ridge, double* __restrict__ W, int* __restrict__ status,
-                             double* __restrict__ rho_out) {
+__device__ __forceinline__ void solve_setup_small_body(const double* __restrict__ grams, int nmodes, unsigned mask,
+                                                       int R, int kind, double ridge, double* __restrict__ W,
+                                                       int* __restrict__ status, double* __restrict__ rho_out) {
   __shared__ double A[RMAX * RMAX];
   __shared__ double s_rho;
   __shared__ int s_info;
@@ -524,6 +624,42 @@ __global__ void __launch_bounds__(32)
     status[0] = info;
     if (rho_out) rho_out[0] = s_rho;
   }
+  __syncwarp();
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(32)
+    solve_setup_small_kernel(const double* __restrict__ grams, int nmodes, unsigned mask, int R, int kind,
+                             double ridge, double* __restrict__ W, int* __restrict__ status,
+                             double* __restrict__ rho_out) {
+  solve_setup_small_body<RMAX>(grams, nmodes, mask, R, kind, ridge, W, status, rho_out);
+}
+
+// One warp-sized CTA per item in turn (R <= 32).
+template <int RMAX>
+__global__ void __launch_bounds__(32) setup_group_kernel(Strided<SetupItem> items, int R) {
+  const int K = *items.count;
+  for (int s = blockIdx.x; s < K; s += gridDim.x) {
+    const SetupItem& it = items[s];
+    if (it.active && !*it.active) continue;
+    solve_setup_small_body<RMAX>(it.grams, it.nmodes, it.mask, R, it.kind, it.ridge, it.W, it.status, it.rho);
+  }
+}
+
+alto_status setup_group_launch(Strided<SetupItem> items, int max_items, int R, cudaStream_t st) {
+  const unsigned grid = (unsigned)std::max(1, std::min(max_items, 1024));
+  if (R <= 8)
+    setup_group_kernel<8><<<grid, 32, 0, st>>>(items, R);
+  else if (R <= 16)
+    setup_group_kernel<16><<<grid, 32, 0, st>>>(items, R);
+  else if (R <= 32)
+    setup_group_kernel<32><<<grid, 32, 0, st>>>(items, R);
+  else {
+    set_error("grouped solve set-up takes rank <= 32 (got %d)", R);
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  ALTO_LAUNCHED();
+  return ALTO_OK;
 }
 
 alto_status solve_setup(const double* grams, int nmodes, unsigned mask, int R, int kind,

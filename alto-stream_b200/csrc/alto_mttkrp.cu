@@ -30,7 +30,7 @@
 // measured one, else a rule on the tile intervals and the mode's reuse.
 #include <algorithm>
 
-#include "alto_internal.cuh"
+#include "alto_group.cuh"
 
 namespace alto {
 
@@ -38,34 +38,6 @@ constexpr uint32_t kNoRow = 0xffffffffu;
 constexpr int kMttkrpThreads = 256;
 constexpr int kMttkrpWarps = kMttkrpThreads / 32;
 constexpr int kStageBytes = 96 * 1024;
-
-struct FactorSet {
-  const void* f[ALTO_MAX_MODES];
-};
-
-struct MttkrpArgs {
-  const void* line;  // line records (LineRec16 / LineRec32)
-  // DETERMINISTIC: per lane-group sub-range, its first and last run (slots
-  // 2s and 2s+1: output row and R partial sums)
-  uint32_t* det_rows;
-  float* det_vals;
-  const uint32_t* tile_iv;
-  uint32_t nnz;
-  uint32_t tile_nnz;
-  uint32_t ntiles;
-  int target;
-  int stage_rows;  // rows of the shared staging buffer (0: never stage)
-  // (3-mode row-sorted copies) the mode whose row is the copy's second sort
-  // key: consecutive nonzeros often share it, and its factor row is then
-  // gathered once for the run (-1: no such order)
-  int fiber_mode;
-  // L2 prefetch of the factor rows of nonzeros this far ahead in a lane
-  // group's walk (0: none; 16-byte records only)
-  uint32_t pf_dist;
-  LineDecode dec;
-  FactorSet fac;
-  float* out;
-};
 
 template <typename FT>
 __device__ __forceinline__ float4 load4(const void* base, size_t off);
@@ -513,15 +485,55 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
 constexpr uint32_t kShortChain = 64;
 constexpr uint32_t kChainSeg = 256;  // slots per segment of a long chain
 
-// Workspace of the long chains (device): counters, then the chains
-// {first slot, end slot, first segment, segments}, then the segments
-// {chain, index in chain}, then each segment's R partial sums.
-struct DetLong {
-  uint32_t* counters;  // [0] long chains, [1] segments, [2] blocks of det_fix_final done
-  uint4* chains;
-  uint2* segs;
-  float* segpart;
-};
+// Chain starting at slot i (one warp; lanes cooperate): a short chain is
+// summed in slot order into its row; a long one registers itself and its
+// segments for det_fix_seg / det_fix_final.
+__device__ __forceinline__ void det_short_chain(const uint32_t* __restrict__ rows, const float* __restrict__ vals,
+                                                uint32_t nslots, int R, float* __restrict__ out, const DetLong& dl,
+                                                uint32_t i, int lane) {
+  const uint32_t row = rows[i];
+  if (i > 0 && rows[i - 1] == row) return;  // not the head of its chain
+  // chain end: first slot with a larger row -- the next 32 slots in one
+  // coalesced probe, a binary search beyond them
+  const uint32_t pi = i + 1 + lane;
+  const unsigned differ = __ballot_sync(0xffffffffu, pi < nslots && rows[pi] != row);
+  uint32_t lo;
+  if (differ) {
+    lo = i + 1 + __ffs(differ) - 1;
+  } else if (i + 33 >= nslots) {
+    lo = nslots;
+  } else {
+    lo = i + 33;
+    uint32_t hi = nslots;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (rows[mid] == row)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+  }
+  if (lo - i > kShortChain) {
+    // long chain: register it and its segments (the order of the lists
+    // varies from run to run; what each entry sums does not)
+    const uint32_t nseg = (lo - i + kChainSeg - 1) / kChainSeg;
+    uint32_t c = 0, base = 0;
+    if (lane == 0) {
+      c = atomicAdd(&dl.counters[0], 1u);
+      base = atomicAdd(&dl.counters[1], nseg);
+      dl.chains[c] = make_uint4(i, lo, base, nseg);
+    }
+    c = __shfl_sync(0xffffffffu, c, 0);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t k = lane; k < nseg; k += 32) dl.segs[base + k] = make_uint2(c, k);
+    return;
+  }
+  for (int r = lane; r < R; r += 32) {
+    float x = 0.f;
+    for (uint32_t k = i; k < lo; ++k) x += vals[(size_t)k * R + r];
+    out[(size_t)row * R + r] += x;
+  }
+}
 
 __global__ void __launch_bounds__(256)
     det_fix_short_kernel(const uint32_t* __restrict__ rows, const float* __restrict__ vals, uint32_t nslots,
@@ -529,146 +541,210 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t i = gw; i < nslots; i += nw) {
-    const uint32_t row = rows[i];
-    if (i > 0 && rows[i - 1] == row) continue;  // not the head of its chain
-    // chain end: first slot with a larger row -- the next 32 slots in one
-    // coalesced probe, a binary search beyond them
-    const uint32_t pi = i + 1 + lane;
-    const unsigned differ = __ballot_sync(0xffffffffu, pi < nslots && rows[pi] != row);
-    uint32_t lo;
-    if (differ) {
-      lo = i + 1 + __ffs(differ) - 1;
-    } else if (i + 33 >= nslots) {
-      lo = nslots;
-    } else {
-      lo = i + 33;
-      uint32_t hi = nslots;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (rows[mid] == row)
-          lo = mid + 1;
-        else
-          hi = mid;
-      }
-    }
-    if (lo - i > kShortChain) {
-      // long chain: register it and its segments (the order of the lists
-      // varies from run to run; what each entry sums does not)
-      const uint32_t nseg = (lo - i + kChainSeg - 1) / kChainSeg;
-      uint32_t c = 0, base = 0;
-      if (lane == 0) {
-        c = atomicAdd(&dl.counters[0], 1u);
-        base = atomicAdd(&dl.counters[1], nseg);
-        dl.chains[c] = make_uint4(i, lo, base, nseg);
-      }
-      c = __shfl_sync(0xffffffffu, c, 0);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      for (uint32_t k = lane; k < nseg; k += 32) dl.segs[base + k] = make_uint2(c, k);
-      continue;
-    }
-    for (int r = lane; r < R; r += 32) {
-      float x = 0.f;
-      for (uint32_t k = i; k < lo; ++k) x += vals[(size_t)k * R + r];
-      out[(size_t)row * R + r] += x;
-    }
-  }
+  for (uint32_t i = gw; i < nslots; i += nw) det_short_chain(rows, vals, nslots, R, out, dl, i, lane);
 }
 
-// One block per segment of a long chain: thread (s, q) sums slots
+// One segment g of a long chain (one block): thread (s, q) sums slots
 // start+s, start+s+S, ... of rank quad q (S = 256 / (R/4)), then a fixed tree
 // over s; the segment's R sums go to segpart.
+__device__ __forceinline__ void det_segment(const float* __restrict__ vals, int R, const DetLong& dl, uint32_t g,
+                                            float4* part) {
+  const int Q = R / 4, S = 256 / Q;
+  const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
+  const uint2 sg = dl.segs[g];
+  const uint4 ch = dl.chains[sg.x];
+  const uint32_t s0 = ch.x + sg.y * kChainSeg;
+  const uint32_t s1 = min(s0 + kChainSeg, ch.y);
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sidx < S)
+    for (uint32_t k = s0 + sidx; k < s1; k += S) {
+      const float4 v = *reinterpret_cast<const float4*>(vals + (size_t)k * R + q * 4);
+      acc.x += v.x;
+      acc.y += v.y;
+      acc.z += v.z;
+      acc.w += v.w;
+    }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int stride = S / 2; stride >= 1; stride >>= 1) {
+    if (sidx < stride) {
+      const float4 o = part[(sidx + stride) * Q + q];
+      float4& m = part[sidx * Q + q];
+      m.x += o.x;
+      m.y += o.y;
+      m.z += o.z;
+      m.w += o.w;
+    }
+    __syncthreads();
+  }
+  if (sidx == 0) *reinterpret_cast<float4*>(dl.segpart + (size_t)(ch.z + sg.y) * R + q * 4) = part[q];
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256)
     det_fix_seg_kernel(const float* __restrict__ vals, int R, DetLong dl) {
   __shared__ float4 part[256];
-  const int Q = R / 4, S = 256 / Q;
-  const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
   const uint32_t nseg = dl.counters[1];
-  for (uint32_t g = blockIdx.x; g < nseg; g += gridDim.x) {
-    const uint2 sg = dl.segs[g];
-    const uint4 ch = dl.chains[sg.x];
-    const uint32_t s0 = ch.x + sg.y * kChainSeg;
-    const uint32_t s1 = min(s0 + kChainSeg, ch.y);
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (sidx < S)
-      for (uint32_t k = s0 + sidx; k < s1; k += S) {
-        const float4 v = *reinterpret_cast<const float4*>(vals + (size_t)k * R + q * 4);
-        acc.x += v.x;
-        acc.y += v.y;
-        acc.z += v.z;
-        acc.w += v.w;
-      }
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    for (int stride = S / 2; stride >= 1; stride >>= 1) {
-      if (sidx < stride) {
-        const float4 o = part[(sidx + stride) * Q + q];
-        float4& m = part[sidx * Q + q];
-        m.x += o.x;
-        m.y += o.y;
-        m.z += o.z;
-        m.w += o.w;
-      }
-      __syncthreads();
-    }
-    if (sidx == 0) *reinterpret_cast<float4*>(dl.segpart + (size_t)(ch.z + sg.y) * R + q * 4) = part[q];
-    __syncthreads();
-  }
+  for (uint32_t g = blockIdx.x; g < nseg; g += gridDim.x) det_segment(vals, R, dl, g, part);
 }
 
-// One block per long chain: thread (s, q) sums segments s, s+S, ... of rank
-// quad q, then a fixed tree over s; the result is added to the chain's row.
-__global__ void __launch_bounds__(256)
-    det_fix_final_kernel(const uint32_t* __restrict__ rows, int R, float* __restrict__ out, DetLong dl) {
-  __shared__ float4 part[256];
+// One long chain c (one block): thread (s, q) sums segments s, s+S, ... of
+// rank quad q, then a fixed tree over s; the result is added to the chain's
+// row.
+__device__ __forceinline__ void det_chain_final(const uint32_t* __restrict__ rows, int R, float* __restrict__ out,
+                                                const DetLong& dl, uint32_t c, float4* part) {
   const int Q = R / 4, S = 256 / Q;
   const int sidx = threadIdx.x / Q, q = threadIdx.x % Q;
-  __shared__ uint32_t s_nlong;
-  if (threadIdx.x == 0) s_nlong = dl.counters[0];
+  const uint4 ch = dl.chains[c];
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sidx < S)
+    for (uint32_t k = sidx; k < ch.w; k += S) {
+      const float4 v = *reinterpret_cast<const float4*>(dl.segpart + (size_t)(ch.z + k) * R + q * 4);
+      acc.x += v.x;
+      acc.y += v.y;
+      acc.z += v.z;
+      acc.w += v.w;
+    }
+  part[threadIdx.x] = acc;
   __syncthreads();
-  const uint32_t nlong = s_nlong;
-  // the last block to have read the counters clears them for the next call
-  // (they start at zero when the workspace is allocated)
+  for (int stride = S / 2; stride >= 1; stride >>= 1) {
+    if (sidx < stride) {
+      const float4 o = part[(sidx + stride) * Q + q];
+      float4& m = part[sidx * Q + q];
+      m.x += o.x;
+      m.y += o.y;
+      m.z += o.z;
+      m.w += o.w;
+    }
+    __syncthreads();
+  }
+  if (sidx == 0) {
+    float4* o = reinterpret_cast<float4*>(out + (size_t)rows[ch.x] * R + q * 4);
+    float4 x = *o;
+    const float4 p = part[q];
+    x.x += p.x;
+    x.y += p.y;
+    x.z += p.z;
+    x.w += p.w;
+    *o = x;
+  }
+  __syncthreads();
+}
+
+// The long-chain count of dl (every thread of the block gets it); the last
+// block to have read it clears the counters for the next call (they start
+// at zero when the workspace is allocated).
+__device__ __forceinline__ uint32_t det_take_chains(const DetLong& dl, uint32_t* s_nlong) {
+  if (threadIdx.x == 0) *s_nlong = dl.counters[0];
+  __syncthreads();
+  const uint32_t nlong = *s_nlong;
   if (threadIdx.x == 0 && atomicAdd(&dl.counters[2], 1u) == gridDim.x - 1) {
     dl.counters[0] = 0;
     dl.counters[1] = 0;
     dl.counters[2] = 0;
   }
-  for (uint32_t c = blockIdx.x; c < nlong; c += gridDim.x) {
-    const uint4 ch = dl.chains[c];
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (sidx < S)
-      for (uint32_t k = sidx; k < ch.w; k += S) {
-        const float4 v = *reinterpret_cast<const float4*>(dl.segpart + (size_t)(ch.z + k) * R + q * 4);
-        acc.x += v.x;
-        acc.y += v.y;
-        acc.z += v.z;
-        acc.w += v.w;
-      }
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    for (int stride = S / 2; stride >= 1; stride >>= 1) {
-      if (sidx < stride) {
-        const float4 o = part[(sidx + stride) * Q + q];
-        float4& m = part[sidx * Q + q];
-        m.x += o.x;
-        m.y += o.y;
-        m.z += o.z;
-        m.w += o.w;
-      }
-      __syncthreads();
-    }
-    if (sidx == 0) {
-      float4* o = reinterpret_cast<float4*>(out + (size_t)rows[ch.x] * R + q * 4);
-      float4 x = *o;
-      const float4 p = part[q];
-      x.x += p.x;
-      x.y += p.y;
-      x.z += p.z;
-      x.w += p.w;
-      *o = x;
-    }
-    __syncthreads();
+  __syncthreads();
+  return nlong;
+}
+
+__global__ void __launch_bounds__(256)
+    det_fix_final_kernel(const uint32_t* __restrict__ rows, int R, float* __restrict__ out, DetLong dl) {
+  __shared__ float4 part[256];
+  __shared__ uint32_t s_nlong;
+  const uint32_t nlong = det_take_chains(dl, &s_nlong);
+  for (uint32_t c = blockIdx.x; c < nlong; c += gridDim.x) det_chain_final(rows, R, out, dl, c, part);
+}
+
+// ------------------------------------------------ grouped deterministic MTTKRP
+//
+// The same kernels over a table of items (sessions' MTTKRPs, one mode each):
+// a global tile index runs over the items' tiles (prefix sums tile_off), and
+// the fix-ups walk every item's slots, segments and chains in turn.  An
+// item's sums, and their order, are those of its own launch.
+
+__device__ __forceinline__ bool item_live(const int* active) { return !active || *active; }
+
+// The last s in [0, K) with off[s] <= v (items with no blocks are skipped).
+__device__ __forceinline__ int item_of(const uint32_t* __restrict__ off, int K, uint32_t v) {
+  int lo = 0, hi = K;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= v)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) det_zero_group_kernel(Strided<DetItem> items) {
+  const int K = *items.count;
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+  for (int s = 0; s < K; ++s) {
+    const DetItem& it = items[s];
+    if (!item_live(it.active)) continue;
+    float4* o = reinterpret_cast<float4*>(it.a.out);
+    const uint64_t n4 = it.out_floats / 4;
+    for (uint64_t q = tid; q < n4; q += nth) o[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+template <int R, int HW, int NM>
+__global__ void __launch_bounds__(kMttkrpThreads, 3)
+    det_tile_group_kernel(Strided<DetItem> items, const uint32_t* __restrict__ tile_off) {
+  const int K = *items.count;
+  const uint32_t total = K > 0 ? tile_off[K] : 0;
+  const int warp = threadIdx.x >> 5;
+  for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
+    const int s = item_of(tile_off, K, v);
+    const DetItem& it = items[s];
+    if (!item_live(it.active)) continue;
+    const MttkrpArgs& a = it.a;
+    const uint32_t tile = v - tile_off[s];
+    const uint32_t ts = tile * a.tile_nnz;
+    const uint32_t te = min(ts + a.tile_nnz, a.nnz);
+    const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
+    const uint32_t ws = min(ts + warp * chunk, te);
+    const uint32_t we = min(ws + chunk, te);
+    warp_range<R, float, HW, NM, false, true>(a, a.line, ws, we, false, nullptr, 0,
+                                              (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW);
+  }
+}
+
+__global__ void __launch_bounds__(256) det_short_group_kernel(Strided<DetItem> items, int R) {
+  const int K = *items.count;
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = 0; s < K; ++s) {
+    const DetItem& it = items[s];
+    if (!item_live(it.active)) continue;
+    for (uint32_t i = gw; i < it.nslots; i += nw)
+      det_short_chain(it.a.det_rows, it.a.det_vals, it.nslots, R, it.a.out, it.dl, i, lane);
+  }
+}
+
+__global__ void __launch_bounds__(256) det_seg_group_kernel(Strided<DetItem> items, int R) {
+  __shared__ float4 part[256];
+  const int K = *items.count;
+  for (int s = 0; s < K; ++s) {
+    const DetItem& it = items[s];
+    if (!item_live(it.active)) continue;
+    const uint32_t nseg = it.dl.counters[1];
+    for (uint32_t g = blockIdx.x; g < nseg; g += gridDim.x) det_segment(it.a.det_vals, R, it.dl, g, part);
+  }
+}
+
+__global__ void __launch_bounds__(256) det_final_group_kernel(Strided<DetItem> items, int R) {
+  __shared__ float4 part[256];
+  __shared__ uint32_t s_nlong;
+  const int K = *items.count;
+  for (int s = 0; s < K; ++s) {
+    const DetItem& it = items[s];
+    if (!item_live(it.active)) continue;
+    const uint32_t nlong = det_take_chains(it.dl, &s_nlong);
+    for (uint32_t c = blockIdx.x; c < nlong; c += gridDim.x) det_chain_final(it.a.det_rows, R, it.a.out, it.dl, c, part);
   }
 }
 
@@ -1054,13 +1130,20 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   if (!accumulate)
     ALTO_TRY_CUDA(cudaMemsetAsync(out, 0, (size_t)t->dims[mode] * rank * sizeof(float), st));
   if (!t->nnz) return ALTO_OK;
+  if (det) {
+    DetItem it;
+    ALTO_TRY(det_prepare(t, mode, factors, rank, out, &it, st));
+    if (it.hw == 0) return launch_det_rank<0>(it.a, rank, it.dl, st);
+    if (it.hw == 1) return launch_det_rank<1>(it.a, rank, it.dl, st);
+    if (it.hw == kDecoded3) return launch_det_rank<kDecoded3>(it.a, rank, it.dl, st);
+    return launch_det_rank<2>(it.a, rank, it.dl, st);
+  }
   MttkrpArgs a{};
   a.line = t->line.p;
   a.tile_iv = t->tile_iv.as<uint32_t>();
   a.ntiles = t->ntiles;
   int hw = t->dec.hi_words;  // record format of the line walked
-  // (a mode of length 1 is already in row order in the ALTO line)
-  if (variant == ALTO_MTTKRP_SORTED || (det && t->dims[mode] > 1)) {
+  if (variant == ALTO_MTTKRP_SORTED) {
     if (!t->sorted[mode].ready || t->sorted[mode].for_nnz != t->nnz)
       ALTO_TRY(build_sorted_line(t, mode, st));
     const SortedLine& s = t->sorted[mode];
@@ -1089,34 +1172,6 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
-  if (det) {
-    if (!aligned) {
-      set_error("the deterministic MTTKRP needs 16-byte aligned factors and output");
-      return ALTO_ERR_UNSUPPORTED;
-    }
-    const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * groups_per_warp(rank) * 2;
-    ALTO_TRY(t->det_rows.ensure(nslots * 4));
-    ALTO_TRY(t->det_vals.ensure(nslots * rank * 4));
-    // long chains: each has more than kShortChain slots; segments:
-    // sum over chains of ceil(len / kChainSeg)
-    const uint64_t max_chains = nslots / (kShortChain + 1) + 1;
-    const uint64_t max_segs = nslots / kChainSeg + max_chains;
-    auto up = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
-    const uint64_t o_chains = 256, o_segs = o_chains + up(max_chains * sizeof(uint4)),
-                   o_part = o_segs + up(max_segs * sizeof(uint2)), bytes = o_part + max_segs * rank * 4;
-    const size_t before = t->det_long.bytes;  // a new allocation starts with zero counters
-    ALTO_TRY(t->det_long.ensure(bytes));
-    if (t->det_long.bytes != before) ALTO_TRY_CUDA(cudaMemsetAsync(t->det_long.p, 0, 16, st));
-    a.det_rows = t->det_rows.as<uint32_t>();
-    a.det_vals = t->det_vals.as<float>();
-    char* base = t->det_long.as<char>();
-    DetLong dl{reinterpret_cast<uint32_t*>(base), reinterpret_cast<uint4*>(base + o_chains),
-               reinterpret_cast<uint2*>(base + o_segs), reinterpret_cast<float*>(base + o_part)};
-    if (hw == 0) return launch_det_rank<0>(a, rank, dl, st);
-    if (hw == 1) return launch_det_rank<1>(a, rank, dl, st);
-    if (hw == kDecoded3) return launch_det_rank<kDecoded3>(a, rank, dl, st);
-    return launch_det_rank<2>(a, rank, dl, st);
-  }
   const bool bulk = feed == 1;
   if (fdtype == ALTO_BF16) {
     if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
@@ -1128,6 +1183,117 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
   if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, aligned, err, st);
   return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
+}
+
+alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, int rank, float* out, DetItem* item,
+                        cudaStream_t st) {
+  if (!deterministic_supported(rank, ALTO_F32)) {
+    set_error("the deterministic MTTKRP takes float32 factors at rank 8, 16, 32, 64 or 128");
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  MttkrpArgs a{};
+  a.line = t->line.p;
+  a.tile_iv = t->tile_iv.as<uint32_t>();
+  a.ntiles = t->nnz ? t->ntiles : 0;
+  int hw = t->dec.hi_words;
+  // (a mode of length 1 is already in row order in the ALTO line)
+  if (t->dims[mode] > 1 && t->nnz) {
+    if (!t->sorted[mode].ready || t->sorted[mode].for_nnz != t->nnz) ALTO_TRY(build_sorted_line(t, mode, st));
+    const SortedLine& s = t->sorted[mode];
+    a.line = s.line.p;
+    a.tile_iv = s.tile_iv.as<uint32_t>();
+    a.ntiles = s.ntiles;
+    hw = s.hw;
+  }
+  a.nnz = (uint32_t)t->nnz;
+  a.tile_nnz = t->tile_nnz;
+  a.target = mode;
+  a.fiber_mode = -1;
+  a.pf_dist = 0;
+  a.dec = t->dec;
+  a.out = out;
+  bool aligned = (reinterpret_cast<uintptr_t>(out) % 16) == 0;
+  for (int m = 0; m < t->nmodes; ++m) {
+    a.fac.f[m] = factors[m];
+    if (m != mode && (reinterpret_cast<uintptr_t>(factors[m]) % 16) != 0) aligned = false;
+  }
+  if (!aligned) {
+    set_error("the deterministic MTTKRP needs 16-byte aligned factors and output");
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * groups_per_warp(rank) * 2;
+  ALTO_TRY(t->det_rows.ensure(std::max<uint64_t>(nslots, 1) * 4));
+  ALTO_TRY(t->det_vals.ensure(std::max<uint64_t>(nslots, 1) * rank * 4));
+  // long chains: each has more than kShortChain slots; segments:
+  // sum over chains of ceil(len / kChainSeg)
+  const uint64_t max_chains = nslots / (kShortChain + 1) + 1;
+  const uint64_t max_segs = nslots / kChainSeg + max_chains;
+  auto up = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+  const uint64_t o_chains = 256, o_segs = o_chains + up(max_chains * sizeof(uint4)),
+                 o_part = o_segs + up(max_segs * sizeof(uint2)), bytes = o_part + max_segs * rank * 4;
+  const size_t before = t->det_long.bytes;  // a new allocation starts with zero counters
+  ALTO_TRY(t->det_long.ensure(bytes));
+  if (t->det_long.bytes != before) ALTO_TRY_CUDA(cudaMemsetAsync(t->det_long.p, 0, 16, st));
+  a.det_rows = t->det_rows.as<uint32_t>();
+  a.det_vals = t->det_vals.as<float>();
+  char* base = t->det_long.as<char>();
+  item->a = a;
+  item->dl = DetLong{reinterpret_cast<uint32_t*>(base), reinterpret_cast<uint4*>(base + o_chains),
+                     reinterpret_cast<uint2*>(base + o_segs), reinterpret_cast<float*>(base + o_part)};
+  item->nslots = (uint32_t)nslots;
+  item->hw = hw;
+  item->out_floats = t->dims[mode] * (uint64_t)rank;
+  item->active = nullptr;
+  return ALTO_OK;
+}
+
+template <int R, int HW, int NM>
+static alto_status det_group_nm(Strided<DetItem> items, const uint32_t* tile_off, cudaStream_t st) {
+  static int blocks_per_sm = 0;
+  if (!blocks_per_sm) {
+    ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, det_tile_group_kernel<R, HW, NM>,
+                                                                kMttkrpThreads, 0));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const unsigned sm = (unsigned)num_sms();
+  det_zero_group_kernel<<<sm * 4, 256, 0, st>>>(items);
+  ALTO_LAUNCHED();
+  det_tile_group_kernel<R, HW, NM><<<sm * blocks_per_sm, kMttkrpThreads, 0, st>>>(items, tile_off);
+  ALTO_LAUNCHED();
+  det_short_group_kernel<<<sm * 16, 256, 0, st>>>(items, R);
+  ALTO_LAUNCHED();
+  det_seg_group_kernel<<<sm * 4, 256, 0, st>>>(items, R);
+  ALTO_LAUNCHED();
+  det_final_group_kernel<<<sm, 256, 0, st>>>(items, R);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+template <int R>
+static alto_status det_group_rank(Strided<DetItem> items, const uint32_t* tile_off, int hw, int nmodes,
+                                  cudaStream_t st) {
+  if (hw == kDecoded3 && nmodes == 3) return det_group_nm<R, kDecoded3, 3>(items, tile_off, st);
+#define DG_CASE(H, NN) \
+  if (hw == H && nmodes == NN) return det_group_nm<R, H, NN>(items, tile_off, st);
+  DG_CASE(0, 3) DG_CASE(0, 4) DG_CASE(0, 5)
+  DG_CASE(1, 3) DG_CASE(1, 4) DG_CASE(1, 5)
+  DG_CASE(2, 3) DG_CASE(2, 4) DG_CASE(2, 5)
+#undef DG_CASE
+  set_error("grouped MTTKRP: record format %d with %d modes is not supported", hw, nmodes);
+  return ALTO_ERR_UNSUPPORTED;
+}
+
+alto_status det_group_launch(Strided<DetItem> items, const uint32_t* tile_off, int rank, int hw, int nmodes,
+                             cudaStream_t st) {
+  switch (rank) {
+    case 8: return det_group_rank<8>(items, tile_off, hw, nmodes, st);
+    case 16: return det_group_rank<16>(items, tile_off, hw, nmodes, st);
+    case 32: return det_group_rank<32>(items, tile_off, hw, nmodes, st);
+    case 64: return det_group_rank<64>(items, tile_off, hw, nmodes, st);
+    default: break;
+  }
+  set_error("grouped MTTKRP: rank %d is not supported (8, 16, 32 or 64)", rank);
+  return ALTO_ERR_UNSUPPORTED;
 }
 
 // Time every applicable variant once per mode (after one warm run) into a

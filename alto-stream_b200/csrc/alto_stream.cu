@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "alto_dense.cuh"
+#include "alto_group.cuh"
 
 namespace alto {
 
@@ -160,16 +161,18 @@ __device__ __forceinline__ void row_rhs(const float* __restrict__ P32, const flo
 
 // Unconstrained solve of mode j (src/streaming_cpd.cpp:1423-1431):
 // U_j[i] = (prev_U_j[i] A + mttkrp[i]) W, W = (Phi + 1e-12 I)^{-1}.
+// Block `block` of `nblocks` of the solve (rows in warp-sized strides).
 template <int SLOTS, int SEG>
-__global__ void __launch_bounds__(kAdmmThreads)
-    stream_solve_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
-                        const double* __restrict__ W, uint64_t I, int R, float* __restrict__ U32) {
+__device__ __forceinline__ void stream_solve_body(const float* __restrict__ P32, const float* __restrict__ B32,
+                                                  const double* __restrict__ A, const double* __restrict__ W,
+                                                  uint64_t I, int R, float* __restrict__ U32, uint32_t block,
+                                                  uint32_t nblocks) {
   extern __shared__ double sw[];
   for (int p = threadIdx.x; p < R * R; p += blockDim.x) sw[p] = W[p];
   __syncthreads();
   const int lane = threadIdx.x & 31, col = RowMap<SEG>::col(lane), sub = RowMap<SEG>::sub(lane);
-  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t gw = (block * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)nblocks * blockDim.x) >> 5;
   for (uint64_t i0 = gw * RowMap<SEG>::kRows; i0 < I; i0 += nw * RowMap<SEG>::kRows) {
     const uint64_t i = i0 + sub;
     double h[SLOTS], x[SLOTS];
@@ -181,23 +184,34 @@ __global__ void __launch_bounds__(kAdmmThreads)
       if (i < I && c < R) U32[i * R + c] = (float)x[s];
     }
   }
+  __syncthreads();
+}
+
+template <int SLOTS, int SEG>
+__global__ void __launch_bounds__(kAdmmThreads)
+    stream_solve_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                        const double* __restrict__ W, uint64_t I, int R, float* __restrict__ U32) {
+  stream_solve_body<SLOTS, SEG>(P32, B32, A, W, I, R, U32, blockIdx.x, gridDim.x);
 }
 
 // The ADMM rows of mode j: rhs formed on the fly from prev_U_j, the MTTKRP
 // and A; the primal starts from U_j (float32) and ends in U_j; between
 // chunks it is kept in float64 (prim), with aux.
+// Block `block` of `nblocks` of one ADMM pass (see above).
 template <int SLOTS, int SEG, bool PASS1>
-__global__ void __launch_bounds__(kAdmmThreads)
-    admm_rows_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
-                     float* __restrict__ U32, double* __restrict__ primal, double* __restrict__ aux,
-                     double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
-                     uint64_t I, int R, double* __restrict__ partials, AdmmState* __restrict__ state, double tol,
-                     cudaGraphConditionalHandle h, int in_graph) {
+__device__ __forceinline__ void admm_rows_body(const float* __restrict__ P32, const float* __restrict__ B32,
+                                               const double* __restrict__ A, float* __restrict__ U32,
+                                               double* __restrict__ primal, double* __restrict__ aux,
+                                               double* __restrict__ dual, const double* __restrict__ W,
+                                               const double* __restrict__ rho_p, uint64_t I, int R,
+                                               double* __restrict__ partials, AdmmState* __restrict__ state,
+                                               double tol, cudaGraphConditionalHandle h, int in_graph,
+                                               uint32_t block, uint32_t nblocks) {
   constexpr int M = AdmmBatch<SLOTS>::M;
   constexpr int KR = RowMap<SEG>::kRows;
   constexpr int NW = kAdmmThreads / 32;
   if (PASS1 && state->stop) {  // a chunk after the stop (launched directly): nothing stands
-    if (blockIdx.x == 0 && threadIdx.x == 0) state->chunk_sweeps = 0;
+    if (block == 0 && threadIdx.x == 0) state->chunk_sweeps = 0;
     return;
   }
   if (!PASS1 && state->chunk_sweeps == 0) return;
@@ -213,8 +227,8 @@ __global__ void __launch_bounds__(kAdmmThreads)
   const double rho = *rho_p;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int col = RowMap<SEG>::col(lane), sub = RowMap<SEG>::sub(lane);
-  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t gw = (block * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)nblocks * blockDim.x) >> 5;
   for (uint64_t b0 = gw * KR * M; b0 < I; b0 += nw * KR * M) {
     double X[M][SLOTS], Z[M][SLOTS], U[M][SLOTS], H[M][SLOTS], X0[M][SLOTS];
 #pragma unroll
@@ -310,7 +324,7 @@ __global__ void __launch_bounds__(kAdmmThreads)
     for (int p = threadIdx.x; p < kAdmmSums; p += blockDim.x) {
       double t = 0.0;
       for (int w = 0; w < NW; ++w) t += wsum[w][p];
-      partials[(size_t)blockIdx.x * kAdmmSums + p] = t;
+      partials[(size_t)block * kAdmmSums + p] = t;
     }
     // the last block to finish adds the blocks' sums (warp per sum, lanes
     // over blocks in order, fixed butterfly) and takes the chunk's sweep
@@ -318,7 +332,7 @@ __global__ void __launch_bounds__(kAdmmThreads)
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&state->ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = atomicAdd(&state->ticket, 1u) == nblocks - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
@@ -326,7 +340,7 @@ __global__ void __launch_bounds__(kAdmmThreads)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int p = warp; p < kAdmmSums; p += NW) {
       double t = 0.0;
-      for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(partials + (size_t)b * kAdmmSums + p);
+      for (unsigned b = lane; b < nblocks; b += 32) t += __ldcg(partials + (size_t)b * kAdmmSums + p);
       for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
       if (lane == 0) S[p] = t;
     }
@@ -352,15 +366,26 @@ __global__ void __launch_bounds__(kAdmmThreads)
   }
 }
 
+template <int SLOTS, int SEG, bool PASS1>
+__global__ void __launch_bounds__(kAdmmThreads)
+    admm_rows_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                     float* __restrict__ U32, double* __restrict__ primal, double* __restrict__ aux,
+                     double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
+                     uint64_t I, int R, double* __restrict__ partials, AdmmState* __restrict__ state, double tol,
+                     cudaGraphConditionalHandle h, int in_graph) {
+  admm_rows_body<SLOTS, SEG, PASS1>(P32, B32, A, U32, primal, aux, dual, W, rho_p, I, R, partials, state, tol, h,
+                                    in_graph, blockIdx.x, gridDim.x);
+}
+
 // End of an inner iteration (src/streaming_cpd.cpp:1457-1482): delta = sum
 // over the non-stream modes of ||U_j - prev_U_j|| / (||U_j|| + 1e-12) from
 // the per-mode statistics; stop once |prev_delta - delta| < epsilon after
 // the first iteration, when max_inner iterations are done, or when the
 // constrained solve's Cholesky failed.
-__global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, const int* __restrict__ status,
-                                int constrained, double eps, int max_inner, IterState* __restrict__ it,
-                                cudaGraphConditionalHandle h, int in_graph, int sparse) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// The decision itself (one thread); returns whether the batch goes on.
+__device__ __forceinline__ bool converge_step(const double* __restrict__ dstat, int N, int t,
+                                              const int* __restrict__ status, int constrained, double eps,
+                                              int max_inner, IterState* __restrict__ it, int sparse) {
   double delta = 0.0;
   for (int j = 0; j < N; ++j)
     if (j != t)
@@ -378,17 +403,24 @@ __global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, 
   it->delta = delta;
   it->done = k + 1;
   if (stop) it->stop = 1;
-  set_condition(h, in_graph, !stop && k + 1 < max_inner);
+  return !stop && k + 1 < max_inner;
+}
+
+__global__ void converge_kernel(const double* __restrict__ dstat, int N, int t, const int* __restrict__ status,
+                                int constrained, double eps, int max_inner, IterState* __restrict__ it,
+                                cudaGraphConditionalHandle h, int in_graph, int sparse) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  set_condition(h, in_graph, converge_step(dstat, N, t, status, constrained, eps, max_inner, it, sparse));
 }
 
 // The time rows after their solve set-up, one block: s = mttkrp W (float64,
 // k order) into time64 and, rounded, into the float32 factor rows; old =
 // G_t; G_t += sum_rows s s^T (the operations of apply, convert, copy and
 // rank update, in their order).
-__global__ void __launch_bounds__(256)
-    time_update_kernel(const float* __restrict__ B32, const double* __restrict__ W, uint64_t rows, int R,
-                       double* __restrict__ time64, float* __restrict__ U32, double* __restrict__ Gt,
-                       double* __restrict__ old_gram) {
+__device__ __forceinline__ void time_update_body(const float* __restrict__ B32, const double* __restrict__ W,
+                                                 uint64_t rows, int R, double* __restrict__ time64,
+                                                 float* __restrict__ U32, double* __restrict__ Gt,
+                                                 double* __restrict__ old_gram) {
   const int RR = R * R;
   for (uint64_t q = threadIdx.x; q < rows * R; q += blockDim.x) {
     const uint64_t i = q / R;
@@ -406,14 +438,22 @@ __global__ void __launch_bounds__(256)
     for (uint64_t q = 0; q < rows; ++q) sv += time64[q * R + b] * time64[q * R + a];
     Gt[p] = sv;
   }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256)
+    time_update_kernel(const float* __restrict__ B32, const double* __restrict__ W, uint64_t rows, int R,
+                       double* __restrict__ time64, float* __restrict__ U32, double* __restrict__ Gt,
+                       double* __restrict__ old_gram) {
+  time_update_body(B32, W, rows, R, time64, U32, Gt, old_gram);
 }
 
 // Per mode before its solve: the historical product A = base *
 // prod_{m in mask} src[m] (base NULL: 1), and, for a constrained mode, the
 // ADMM state cleared and its chunk loop opened.
-__global__ void mode_prep_kernel(const double* __restrict__ base, const double* __restrict__ src, unsigned mask,
-                                 int N, int RR, double* __restrict__ A, AdmmState* __restrict__ admm,
-                                 cudaGraphConditionalHandle h, int in_graph) {
+__device__ __forceinline__ void mode_prep_body(const double* __restrict__ base, const double* __restrict__ src,
+                                               unsigned mask, int N, int RR, double* __restrict__ A,
+                                               AdmmState* __restrict__ admm) {
   for (int p = threadIdx.x; p < RR; p += blockDim.x) {
     double v = base ? base[p] : 1.0;
     for (int m = 0; m < N; ++m)
@@ -427,8 +467,15 @@ __global__ void mode_prep_kernel(const double* __restrict__ base, const double* 
     admm->chunk_start = 0;
     admm->chunk_sweeps = 0;
     admm->ticket = 0;
-    set_condition(h, in_graph, true);
   }
+  __syncthreads();
+}
+
+__global__ void mode_prep_kernel(const double* __restrict__ base, const double* __restrict__ src, unsigned mask,
+                                 int N, int RR, double* __restrict__ A, AdmmState* __restrict__ admm,
+                                 cudaGraphConditionalHandle h, int in_graph) {
+  mode_prep_body(base, src, mask, N, RR, A, admm);
+  if (admm && threadIdx.x == 0) set_condition(h, in_graph, true);
 }
 
 // Head of the iteration graph: run the loop only if the batch goes on.
@@ -565,6 +612,174 @@ __global__ void __launch_bounds__(kAdmmThreads)
   }
 }
 
+// ------------------------------------------------ grouped inner iterations
+//
+// Many sessions' inner iterations in the same launches: a device table holds
+// one descriptor per session (its state's pointers, sizes and the items of
+// its per-mode MTTKRPs, solve set-ups and Gram passes), and every kernel
+// below runs the single-session kernel's per-block code for each session in
+// turn, over "virtual blocks": session s gets exactly the blocks its own
+// launch would have (the prefix sums in the offset tables map a global block
+// index to (session, block)), so each session's arithmetic, and its order,
+// are those of its own launches -- a session's result does not depend on
+// which other sessions share the launches.  A session whose batch has
+// converged (or ran out of iterations) is skipped (act = 0).
+
+constexpr int kGroupOffKinds = 5;  // tiles, Gram blocks, Gram reduction blocks, ADMM blocks, solve blocks
+enum { kOffTile = 0, kOffGram, kOffGramRed, kOffAdmm, kOffSolve };
+
+struct SlotDesc {
+  DetItem det[ALTO_MAX_MODES];      // MTTKRP of each mode into buf32
+  SetupItem setup[ALTO_MAX_MODES];  // solve set-up of each mode (the stream mode: the time rows)
+  GramItem gram[ALTO_MAX_MODES];    // Gram, cross Gram and statistics of each non-stream mode
+  uint64_t dims[ALTO_MAX_MODES];
+  float* U[ALTO_MAX_MODES];
+  float* P[ALTO_MAX_MODES];
+  double* dual[ALTO_MAX_MODES];
+  uint32_t admm_blocks[ALTO_MAX_MODES];
+  uint32_t solve_blocks[ALTO_MAX_MODES];
+  double *G, *old_gram, *ata, *cross, *W, *rho, *dstat, *aux, *prim, *time64, *admm_part;
+  int* status;
+  float* buf32;
+  AdmmState* admm;
+  IterState* iter;
+  double eps;
+  int con;        // 1: non-negative ADMM solves
+  int max_inner;
+  int act;        // runs the current step (set on the device)
+  int admm_act;   // its ADMM of the current mode still sweeps (set on the device)
+};
+
+// Control block of a group (device): live slots, steps allowed and done in
+// the current launch, and per slot the state after the last step.
+struct GroupCtl {
+  int count;
+  int limit;
+  int steps;
+  int any;
+};
+struct SlotState {
+  int running;  // takes part in further steps
+  int done;     // inner iterations of the batch so far
+  int stop;
+  int info;
+};
+
+__device__ __forceinline__ bool slot_runnable(const SlotDesc& d) {
+  return !d.iter->stop && d.iter->done < d.max_inner;
+}
+
+__device__ __forceinline__ int slot_of(const uint32_t* __restrict__ off, int K, uint32_t v) {
+  int lo = 0, hi = K;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= v)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Before the step loop of a launch: steps = 0; the loop runs if some slot can.
+__global__ void group_begin_kernel(SlotDesc* __restrict__ tab, GroupCtl* __restrict__ ctl,
+                                   cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  bool any = false;
+  for (int s = 0; s < ctl->count; ++s) any = any || slot_runnable(tab[s]);
+  ctl->steps = 0;
+  cudaGraphSetConditional(h, (any && ctl->limit > 0) ? 1u : 0u);
+}
+
+__global__ void group_step_begin_kernel(SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl) {
+  for (int s = threadIdx.x; s < ctl->count; s += blockDim.x) tab[s].act = slot_runnable(tab[s]) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(256) group_time_update_kernel(const SlotDesc* __restrict__ tab,
+                                                                const GroupCtl* __restrict__ ctl, int t, int R) {
+  const size_t RR = (size_t)R * R;
+  for (int s = blockIdx.x; s < ctl->count; s += gridDim.x) {
+    const SlotDesc& d = tab[s];
+    if (!d.act) continue;
+    time_update_body(d.buf32, d.W, d.dims[t], R, d.time64, d.U[t], d.G + t * RR, d.old_gram);
+  }
+}
+
+__global__ void __launch_bounds__(256) group_mode_prep_kernel(SlotDesc* __restrict__ tab,
+                                                              const GroupCtl* __restrict__ ctl, int j, int t,
+                                                              int N, int R) {
+  const int RR = R * R;
+  const unsigned mask = ((1u << N) - 1) & ~(1u << j) & ~(1u << t);
+  for (int s = blockIdx.x; s < ctl->count; s += gridDim.x) {
+    SlotDesc& d = tab[s];
+    if (!d.act) continue;
+    mode_prep_body(d.old_gram, d.cross, mask, N, RR, d.ata, d.con ? d.admm : nullptr);
+    if (threadIdx.x == 0) d.admm_act = d.con;
+  }
+}
+
+template <int SLOTS, int SEG>
+__global__ void __launch_bounds__(kAdmmThreads)
+    group_solve_kernel(const SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
+                       const uint32_t* __restrict__ off, int j, int R) {
+  const int K = ctl->count;
+  const uint32_t total = K > 0 ? off[K] : 0;
+  for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
+    const int s = slot_of(off, K, v);
+    const SlotDesc& d = tab[s];
+    if (!d.act || d.con) continue;
+    stream_solve_body<SLOTS, SEG>(d.P[j], d.buf32, d.ata, d.W, d.dims[j], R, d.U[j], v - off[s], d.solve_blocks[j]);
+  }
+}
+
+// The ADMM chunk loop goes on while some slot's ADMM of mode j sweeps.
+__global__ void group_admm_cond_kernel(SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
+                                       cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  bool any = false;
+  for (int s = 0; s < ctl->count; ++s) {
+    SlotDesc& d = tab[s];
+    if (d.act && d.admm_act && d.admm->stop) d.admm_act = 0;
+    any = any || (d.act && d.admm_act);
+  }
+  cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+template <int SLOTS, int SEG, bool PASS1>
+__global__ void __launch_bounds__(kAdmmThreads)
+    group_admm_kernel(const SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
+                      const uint32_t* __restrict__ off, int j, int R, double tol) {
+  const int K = ctl->count;
+  const uint32_t total = K > 0 ? off[K] : 0;
+  for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
+    const int s = slot_of(off, K, v);
+    const SlotDesc& d = tab[s];
+    if (!d.act || !d.admm_act) continue;
+    admm_rows_body<SLOTS, SEG, PASS1>(d.P[j], d.buf32, d.ata, d.U[j], d.prim, d.aux, d.dual[j], d.W, d.rho,
+                                      d.dims[j], R, d.admm_part, d.admm, tol, cudaGraphConditionalHandle{}, 0,
+                                      v - off[s], d.admm_blocks[j]);
+    __syncthreads();
+  }
+}
+
+// End of a step: each acting slot's convergence decision; the loop goes on
+// while a slot can run and the launch's step allowance lasts.
+__global__ void group_converge_kernel(SlotDesc* __restrict__ tab, GroupCtl* __restrict__ ctl,
+                                      SlotState* __restrict__ out, int N, int t, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  bool any = false;
+  for (int s = 0; s < ctl->count; ++s) {
+    SlotDesc& d = tab[s];
+    if (d.act) converge_step(d.dstat, N, t, d.status, d.con, d.eps, d.max_inner, d.iter, 0);
+    const bool run = slot_runnable(d);
+    out[s] = SlotState{run ? 1 : 0, d.iter->done, d.iter->stop, d.iter->info};
+    any = any || run;
+  }
+  ctl->steps += 1;
+  ctl->any = any ? 1 : 0;
+  cudaGraphSetConditional(h, (any && ctl->steps < ctl->limit) ? 1u : 0u);
+}
+
 }  // namespace alto
 
 using namespace alto;
@@ -592,7 +807,13 @@ struct alto_stream_session {
   DevBuf ridx[ALTO_MAX_MODES], nzl[ALTO_MAX_MODES], Anz[ALTO_MAX_MODES], Aprev[ALTO_MAX_MODES];
   DevBuf spg, coo_idx, coo_val;
   cudaStream_t capst[2] = {nullptr, nullptr};  // capture-only streams (nothing runs on them)
+  // grouped inner iterations: this batch's per-mode MTTKRP items, and the
+  // private group (of this session alone) that runs them when the session
+  // is not served with others
+  DetItem det[ALTO_MAX_MODES];
+  alto::StreamGroup* own_group = nullptr;
   ~alto_stream_session() {
+    alto::group_destroy(own_group);
     delete at;
     for (cudaStream_t c : capst)
       if (c) cudaStreamDestroy(c);
@@ -1081,8 +1302,376 @@ alto_status run_graph(alto_stream_session* s, IterLaunch L) {
   return st;
 }
 
-alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals,
-                       uint64_t n_init, int* inner_out) {
+}  // namespace
+
+// ------------------------------------------------ stream groups (host side)
+
+namespace alto {
+
+struct StreamGroup {
+  int R = 0, N = 0, t = 0, cap = 0, count = 0;
+  int hw[ALTO_MAX_MODES] = {0};
+  cudaStream_t st = nullptr;
+  cudaStream_t capst[2] = {nullptr, nullptr};
+  DevBuf tab, offs, ctl, states;
+  SlotDesc* h_tab = nullptr;  // pinned staging of the table and the offsets
+  uint32_t* h_offs = nullptr;
+  GroupCtl* h_ctl = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace grp {
+
+constexpr uint32_t kSolveGrid = 148 * 8;
+constexpr uint32_t kAdmmGrid = 148 * 4;
+
+template <int SLOTS, int SEG>
+uint32_t admm_blocks_for(uint64_t I) {
+  constexpr uint64_t rpb = (kAdmmThreads / 32) * RowMap<SEG>::kRows * AdmmBatch<SLOTS>::M;
+  uint64_t b = std::min<uint64_t>((I + rpb - 1) / rpb, kAdmmGrid);
+  return (uint32_t)std::max<uint64_t>(b, 1);
+}
+
+template <int SEG>
+uint32_t solve_blocks_for(uint64_t I) {
+  const uint64_t warps = (I + RowMap<SEG>::kRows - 1) / RowMap<SEG>::kRows;
+  uint64_t b = std::min<uint64_t>((warps * 32 + kAdmmThreads - 1) / kAdmmThreads, kSolveGrid);
+  return (uint32_t)std::max<uint64_t>(b, 1);
+}
+
+// (as admm() and rows_solve() dispatch on the rank, ranks <= 32)
+uint32_t admm_blocks(int R, uint64_t I) {
+  return R <= 8 ? admm_blocks_for<1, 8>(I) : (R <= 16 ? admm_blocks_for<1, 16>(I) : admm_blocks_for<1, 32>(I));
+}
+uint32_t solve_blocks(int R, uint64_t I) {
+  return R <= 8 ? solve_blocks_for<8>(I) : (R <= 16 ? solve_blocks_for<16>(I) : solve_blocks_for<32>(I));
+}
+
+uint32_t* off_of(uint32_t* base, int cap, int kind, int mode) {
+  return base + ((size_t)kind * ALTO_MAX_MODES + mode) * (cap + 1);
+}
+
+template <typename T>
+Strided<T> strided(const StreamGroup* g, size_t field_offset) {
+  return Strided<T>{g->tab.as<char>() + field_offset, sizeof(SlotDesc), &g->ctl.as<GroupCtl>()->count};
+}
+
+template <int SLOTS, int SEG>
+alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGraphConditionalHandle h) {
+  const size_t smem = (size_t)g->R * g->R * sizeof(double);
+  SlotDesc* tab = g->tab.as<SlotDesc>();
+  GroupCtl* ctl = g->ctl.as<GroupCtl>();
+  uint32_t* offs = g->offs.as<uint32_t>();
+  group_solve_kernel<SLOTS, SEG><<<kSolveGrid, kAdmmThreads, smem, cs>>>(tab, ctl, off_of(offs, g->cap, kOffSolve, j), j,
+                                                                       g->R);
+  ALTO_LAUNCHED();
+  // while some slot's ADMM of mode j sweeps: one chunk (pass 1, pass 2)
+  group_admm_cond_kernel<<<1, 32, 0, cs>>>(tab, ctl, h);
+  ALTO_LAUNCHED();
+  cudaGraph_t body;
+  ALTO_TRY(capture_while(cs, h, &body));
+  ALTO_TRY_CUDA(cudaStreamBeginCaptureToGraph(g->capst[1], body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+  const double tol = (double)1e-6f;
+  const uint32_t* ao = off_of(offs, g->cap, kOffAdmm, j);
+  group_admm_kernel<SLOTS, SEG, true><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
+  group_admm_kernel<SLOTS, SEG, false><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
+  group_admm_cond_kernel<<<1, 32, 0, g->capst[1]>>>(tab, ctl, h);
+  const cudaError_t le = cudaGetLastError();
+  cudaGraph_t done = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(g->capst[1], &done);
+  ALTO_TRY_CUDA(le);
+  ALTO_TRY_CUDA(ee);
+  return ALTO_OK;
+}
+
+alto_status capture_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGraphConditionalHandle h) {
+  if (g->R <= 8) return capture_mode_solves<1, 8>(g, cs, j, h);
+  if (g->R <= 16) return capture_mode_solves<1, 16>(g, cs, j, h);
+  return capture_mode_solves<1, 32>(g, cs, j, h);
+}
+
+// One inner iteration of every acting slot (the body of the step loop).
+alto_status capture_step(StreamGroup* g, cudaStream_t cs, cudaGraphConditionalHandle outer,
+                         const cudaGraphConditionalHandle* admm_h) {
+  const int N = g->N, t = g->t, R = g->R;
+  SlotDesc* tab = g->tab.as<SlotDesc>();
+  GroupCtl* ctl = g->ctl.as<GroupCtl>();
+  uint32_t* offs = g->offs.as<uint32_t>();
+  const unsigned per_slot = (unsigned)std::min(g->cap, 148);
+  group_step_begin_kernel<<<1, 256, 0, cs>>>(tab, ctl);
+  ALTO_LAUNCHED();
+  // time rows: MTTKRP of the stream mode, solve with the other Grams
+  ALTO_TRY(det_group_launch(strided<DetItem>(g, offsetof(SlotDesc, det) + t * sizeof(DetItem)),
+                            off_of(offs, g->cap, kOffTile, t), R, g->hw[t], N, cs));
+  ALTO_TRY(setup_group_launch(strided<SetupItem>(g, offsetof(SlotDesc, setup) + t * sizeof(SetupItem)), g->cap, R,
+                              cs));
+  group_time_update_kernel<<<per_slot, 256, 0, cs>>>(tab, ctl, t, R);
+  ALTO_LAUNCHED();
+  for (int j = 0; j < N; ++j) {
+    if (j == t) continue;
+    ALTO_TRY(det_group_launch(strided<DetItem>(g, offsetof(SlotDesc, det) + j * sizeof(DetItem)),
+                              off_of(offs, g->cap, kOffTile, j), R, g->hw[j], N, cs));
+    group_mode_prep_kernel<<<per_slot, 256, 0, cs>>>(tab, ctl, j, t, N, R);
+    ALTO_LAUNCHED();
+    ALTO_TRY(setup_group_launch(strided<SetupItem>(g, offsetof(SlotDesc, setup) + j * sizeof(SetupItem)), g->cap,
+                                R, cs));
+    ALTO_TRY(capture_solves(g, cs, j, admm_h[j]));
+    ALTO_TRY(gram_group_launch(strided<GramItem>(g, offsetof(SlotDesc, gram) + j * sizeof(GramItem)),
+                               off_of(offs, g->cap, kOffGram, j), off_of(offs, g->cap, kOffGramRed, j), g->cap, R,
+                               cs));
+  }
+  group_converge_kernel<<<1, 32, 0, cs>>>(tab, ctl, g->states.as<SlotState>(), N, t, outer);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
+// The group's graph: while (a slot runs and steps < limit) { one step }.
+alto_status build_group_graph(StreamGroup* g) {
+  cudaGraph_t graph = nullptr;
+  alto_status st = ALTO_OK;
+  cudaStream_t cs = g->capst[0];
+  do {
+    if ((st = cuda_status(cudaGraphCreate(&graph, 0), "cudaGraphCreate", __FILE__, __LINE__))) break;
+    cudaGraphConditionalHandle outer, admm_h[ALTO_MAX_MODES] = {};
+    if ((st = cuda_status(cudaGraphConditionalHandleCreate(&outer, graph, 0, 0), "conditional handle", __FILE__,
+                          __LINE__)))
+      break;
+    for (int j = 0; j < g->N && st == ALTO_OK; ++j)
+      if (j != g->t)
+        st = cuda_status(cudaGraphConditionalHandleCreate(&admm_h[j], graph, 0, 0), "conditional handle", __FILE__,
+                         __LINE__);
+    if (st) break;
+    if ((st = cuda_status(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0,
+                                                        cudaStreamCaptureModeThreadLocal),
+                          "capture", __FILE__, __LINE__)))
+      break;
+    group_begin_kernel<<<1, 32, 0, cs>>>(g->tab.as<SlotDesc>(), g->ctl.as<GroupCtl>(), outer);
+    if ((st = cuda_status(cudaGetLastError(), "group_begin_kernel", __FILE__, __LINE__))) break;
+    cudaGraph_t body = nullptr, tmp = nullptr;
+    if ((st = capture_while(cs, outer, &body))) break;
+    if ((st = cuda_status(cudaStreamEndCapture(cs, &tmp), "end capture", __FILE__, __LINE__))) break;
+    if ((st = cuda_status(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                                        cudaStreamCaptureModeThreadLocal),
+                          "capture", __FILE__, __LINE__)))
+      break;
+    if ((st = capture_step(g, cs, outer, admm_h))) break;
+    if ((st = cuda_status(cudaStreamEndCapture(cs, &tmp), "end capture", __FILE__, __LINE__))) break;
+    st = cuda_status(cudaGraphInstantiate(&g->exec, graph, 0), "cudaGraphInstantiate", __FILE__, __LINE__);
+  } while (false);
+  if (st) {
+    for (cudaStream_t c : g->capst) {
+      cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(c, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c, &junk);
+      }
+    }
+    cudaGetLastError();
+  }
+  if (graph) cudaGraphDestroy(graph);
+  return st;
+}
+
+}  // namespace grp
+
+using namespace grp;
+
+bool stream_groupable(const alto_stream_session* s) {
+  return !s->sparse && (s->R == 8 || s->R == 16 || s->R == 32) && s->N >= 3 && s->N <= 5 && s->at;
+}
+
+alto_status group_prepare_session(alto_stream_session* s) {
+  const int N = s->N, R = s->R;
+  cudaStream_t st = s->st;
+  const void* fac[ALTO_MAX_MODES] = {};
+  for (int n = 0; n < N; ++n) fac[n] = s->U[n].p;
+  uint64_t admm_part = 1, gram_part = 1;
+  for (int m = 0; m < N; ++m) {
+    ALTO_TRY(det_prepare(s->at, m, fac, R, s->buf32.as<float>(), &s->det[m], st));
+    if (m == s->t) continue;
+    admm_part = std::max<uint64_t>(admm_part, (uint64_t)admm_blocks(R, s->dims[m]) * kAdmmSums);
+    uint32_t nb = 1;
+    uint64_t rpb = 1;
+    gram_split(s->dims[m], &nb, &rpb);
+    gram_part = std::max<uint64_t>(gram_part, (uint64_t)nb * (2 * R * R + 3));
+  }
+  ALTO_TRY(s->admm_part.ensure(admm_part * sizeof(double)));
+  ALTO_TRY(s->gscr.ensure(gram_part * sizeof(double)));
+  ALTO_TRY(s->iter.ensure(sizeof(IterState)));
+  ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
+  return ALTO_OK;
+}
+
+bool group_fits(const StreamGroup* g, const alto_stream_session* s) {
+  if (g->R != s->R || g->N != s->N || g->t != s->t) return false;
+  for (int m = 0; m < s->N; ++m)
+    if (g->hw[m] != s->det[m].hw) return false;
+  return true;
+}
+
+alto_status group_create(const alto_stream_session* like, int capacity, cudaStream_t st, StreamGroup** out) {
+  if (!stream_groupable(like) || capacity < 1) {
+    set_error("the session cannot run in a group");
+    return ALTO_ERR_UNSUPPORTED;
+  }
+  StreamGroup* g = new StreamGroup();
+  g->R = like->R;
+  g->N = like->N;
+  g->t = like->t;
+  g->cap = capacity;
+  g->st = st;
+  for (int m = 0; m < like->N; ++m) g->hw[m] = like->det[m].hw;
+  const size_t offs_n = (size_t)kGroupOffKinds * ALTO_MAX_MODES * (capacity + 1);
+  alto_status r = ALTO_OK;
+  if ((r = g->tab.ensure(sizeof(SlotDesc) * capacity)) || (r = g->offs.ensure(offs_n * 4)) ||
+      (r = g->ctl.ensure(sizeof(GroupCtl))) || (r = g->states.ensure(sizeof(SlotState) * capacity))) {
+    group_destroy(g);
+    return r;
+  }
+  if (cudaMallocHost((void**)&g->h_tab, sizeof(SlotDesc) * capacity) != cudaSuccess ||
+      cudaMallocHost((void**)&g->h_offs, offs_n * 4) != cudaSuccess ||
+      cudaMallocHost((void**)&g->h_ctl, sizeof(GroupCtl)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g->capst[0], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g->capst[1], cudaStreamNonBlocking) != cudaSuccess) {
+    group_destroy(g);
+    set_error("group set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return ALTO_ERR_CUDA;
+  }
+  std::memset(g->h_tab, 0, sizeof(SlotDesc) * capacity);
+  std::memset(g->h_offs, 0, offs_n * 4);
+  *g->h_ctl = GroupCtl{0, 0, 0, 0};
+  ALTO_TRY_CUDA(cudaMemsetAsync(g->tab.p, 0, sizeof(SlotDesc) * capacity, st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(g->offs.p, 0, offs_n * 4, st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(g->ctl.p, 0, sizeof(GroupCtl), st));
+  if ((r = build_group_graph(g))) {
+    group_destroy(g);
+    return r;
+  }
+  *out = g;
+  return ALTO_OK;
+}
+
+void group_destroy(StreamGroup* g) {
+  if (!g) return;
+  if (g->st) cudaStreamSynchronize(g->st);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  for (cudaStream_t c : g->capst)
+    if (c) cudaStreamDestroy(c);
+  if (g->h_tab) cudaFreeHost(g->h_tab);
+  if (g->h_offs) cudaFreeHost(g->h_offs);
+  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  delete g;
+}
+
+// The members' descriptors and offsets, copied to the device on the group's
+// stream (the staging must not be rewritten before the copy has run: the
+// callers synchronise with the group's work between calls).
+alto_status group_set(StreamGroup* g, alto_stream_session* const* members, int k) {
+  if (k < 0 || k > g->cap) {
+    set_error("group of %d slots given %d sessions", g->cap, k);
+    return ALTO_ERR_INVALID;
+  }
+  const int N = g->N, R = g->R;
+  const size_t RR = (size_t)R * R;
+  SlotDesc* dtab = g->tab.as<SlotDesc>();
+  const size_t offs_n = (size_t)kGroupOffKinds * ALTO_MAX_MODES * (g->cap + 1);
+  std::memset(g->h_offs, 0, offs_n * 4);
+  for (int q = 0; q < k; ++q) {
+    alto_stream_session* s = members[q];
+    if (!group_fits(g, s)) {
+      set_error("session does not fit the group (rank, modes or record format)");
+      return ALTO_ERR_INVALID;
+    }
+    SlotDesc& d = g->h_tab[q];
+    std::memset(&d, 0, sizeof(d));
+    const int* act = reinterpret_cast<const int*>(reinterpret_cast<const char*>(dtab + q) + offsetof(SlotDesc, act));
+    double* G = s->G.as<double>();
+    const unsigned all = (1u << N) - 1;
+    for (int m = 0; m < N; ++m) {
+      d.det[m] = s->det[m];
+      d.det[m].active = act;
+      d.dims[m] = s->dims[m];
+      d.U[m] = s->U[m].as<float>();
+      d.P[m] = s->P[m].as<float>();
+      d.dual[m] = s->dual[m].as<double>();
+      const bool admm_mode = m != s->t && s->con != ALTO_UNCONSTRAINED;
+      d.setup[m] = SetupItem{G, all & ~(1u << m), N, admm_mode ? kSolveAdmm : kSolveRidge, admm_mode ? 0.0 : 1e-12,
+                             s->W.as<double>(), s->status.as<int>(), admm_mode ? s->rho.as<double>() : nullptr, act};
+      if (m == s->t) continue;
+      uint32_t nb = 1;
+      uint64_t rpb = 1;
+      gram_split(s->dims[m], &nb, &rpb);
+      d.gram[m] = GramItem{s->P[m].as<float>(), s->U[m].as<float>(), s->dims[m], rpb, nb, G + m * RR,
+                           s->cross.as<double>() + m * RR, s->dstat.as<double>() + 3 * m, s->gscr.as<double>(), act};
+      d.admm_blocks[m] = admm_blocks(R, s->dims[m]);
+      d.solve_blocks[m] = solve_blocks(R, s->dims[m]);
+    }
+    d.G = G;
+    d.old_gram = s->old_gram.as<double>();
+    d.ata = s->ata.as<double>();
+    d.cross = s->cross.as<double>();
+    d.W = s->W.as<double>();
+    d.rho = s->rho.as<double>();
+    d.dstat = s->dstat.as<double>();
+    d.aux = s->aux.as<double>();
+    d.prim = s->prim.as<double>();
+    d.time64 = s->time64.as<double>();
+    d.admm_part = s->admm_part.as<double>();
+    d.status = s->status.as<int>();
+    d.buf32 = s->buf32.as<float>();
+    d.admm = s->admm_state.as<AdmmState>();
+    d.iter = s->iter.as<IterState>();
+    d.eps = s->eps;
+    d.con = s->con != ALTO_UNCONSTRAINED ? 1 : 0;
+    d.max_inner = s->max_inner;
+    for (int m = 0; m < N; ++m) {
+      const uint32_t counts[kGroupOffKinds] = {d.det[m].a.ntiles, m == s->t ? 0u : d.gram[m].nb,
+                                               m == s->t ? 0u : gram_reduce_blocks(R),
+                                               m == s->t ? 0u : d.admm_blocks[m], m == s->t ? 0u : d.solve_blocks[m]};
+      for (int kind = 0; kind < kGroupOffKinds; ++kind) {
+        uint32_t* o = off_of(g->h_offs, g->cap, kind, m);
+        o[q + 1] = o[q] + counts[kind];
+      }
+    }
+  }
+  g->count = k;
+  ALTO_TRY_CUDA(cudaMemcpyAsync(g->tab.p, g->h_tab, sizeof(SlotDesc) * std::max(k, 1), cudaMemcpyHostToDevice, g->st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(g->offs.p, g->h_offs, offs_n * 4, cudaMemcpyHostToDevice, g->st));
+  return ALTO_OK;
+}
+
+// Run up to max_steps inner iterations of every member (stopping early
+// when none can run), as one launch of the group's graph on its stream.
+alto_status group_launch(StreamGroup* g, int max_steps) {
+  *g->h_ctl = GroupCtl{g->count, max_steps, 0, 0};
+  ALTO_TRY_CUDA(cudaMemcpyAsync(g->ctl.p, g->h_ctl, sizeof(GroupCtl), cudaMemcpyHostToDevice, g->st));
+  ALTO_TRY_CUDA(cudaGraphLaunch(g->exec, g->st));
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  return ALTO_OK;
+}
+
+alto_status group_states(StreamGroup* g, int* running, int* done, int* stop, int* info) {
+  std::vector<SlotState> h(std::max(g->count, 1));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(h.data(), g->states.p, sizeof(SlotState) * g->count, cudaMemcpyDeviceToHost, g->st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(g->st));
+  for (int q = 0; q < g->count; ++q) {
+    if (running) running[q] = h[q].running;
+    if (done) done[q] = h[q].done;
+    if (stop) stop[q] = h[q].stop;
+    if (info) info[q] = h[q].info;
+  }
+  return ALTO_OK;
+}
+
+}  // namespace alto
+
+namespace {
+
+// Everything of a batch before its inner iterations (src/streaming_cpd.cpp:
+// 124-186): grow the model, Grams and cross Grams, duals cleared, the
+// batch encoded, the first batch's normalisation, spCP-stream's row maps.
+alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals, uint64_t n_init) {
   const int N = s->N, t = s->t, R = s->R;
   cudaStream_t st = s->st;
   const size_t RR = (size_t)R * R;
@@ -1170,29 +1759,16 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   }
 
   if (s->sparse) ALTO_TRY(sparse_prepare(s, b, first));
+  return ALTO_OK;
+}
 
-  IterLaunch L{};
-  for (int n = 0; n < N; ++n) L.fac[n] = s->sparse ? s->Anz[n].p : s->U[n].p;
-  // the deterministic MTTKRP where it runs, so a stream's results repeat
-  // bit for bit however many other streams share the device
-  L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
-  ALTO_TRY(s->iter.ensure(sizeof(IterState)));
-  ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
-  IterState hs{};
-  // iteration 0 directly: sizes every buffer and builds the sorted lines
-  ALTO_TRY(enqueue_iteration(s, L, st));
-  if (s->use_graph && s->max_inner > 1) {
-    ALTO_TRY(run_graph(s, L));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
-    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  } else {
-    while (true) {
-      ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
-      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-      if (hs.stop || hs.done >= s->max_inner) break;
-      ALTO_TRY(enqueue_iteration(s, L, st));
-    }
-  }
+// After the inner iterations (hs: their state): the failed-solve check,
+// forgetting, prev <- current, the time rows out.
+alto_status finish_batch(alto_stream_session* s, const IterState& hs, int* inner_out) {
+  const int N = s->N, t = s->t, R = s->R;
+  cudaStream_t st = s->st;
+  const size_t RR = (size_t)R * R;
+  double* G = s->G.as<double>();
   if (hs.info) {
     set_error("Cholesky of the ADMM normal equations failed (info %d)", hs.info);
     return ALTO_ERR_NOT_SPD;
@@ -1210,6 +1786,52 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
   s->batches += 1;
   return ALTO_OK;
+}
+
+alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals,
+                       uint64_t n_init, int* inner_out) {
+  const int N = s->N, R = s->R;
+  cudaStream_t st = s->st;
+  ALTO_TRY(prepare_batch(s, b, init_vals, n_init));
+  IterState hs{};
+  if (s->use_graph && stream_groupable(s)) {
+    // the inner iterations as one launch of the session's own group graph,
+    // captured once and relaunched for every batch
+    ALTO_TRY(group_prepare_session(s));
+    if (s->own_group && !group_fits(s->own_group, s)) {
+      group_destroy(s->own_group);
+      s->own_group = nullptr;
+    }
+    if (!s->own_group) ALTO_TRY(group_create(s, 1, st, &s->own_group));
+    alto_stream_session* one = s;
+    ALTO_TRY(group_set(s->own_group, &one, 1));
+    ALTO_TRY(group_launch(s->own_group, s->max_inner));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+    return finish_batch(s, hs, inner_out);
+  }
+  IterLaunch L{};
+  for (int n = 0; n < N; ++n) L.fac[n] = s->sparse ? s->Anz[n].p : s->U[n].p;
+  // the deterministic MTTKRP where it runs, so a stream's results repeat
+  // bit for bit however many other streams share the device
+  L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
+  ALTO_TRY(s->iter.ensure(sizeof(IterState)));
+  ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
+  // iteration 0 directly: sizes every buffer and builds the sorted lines
+  ALTO_TRY(enqueue_iteration(s, L, st));
+  if (s->use_graph && s->max_inner > 1) {
+    ALTO_TRY(run_graph(s, L));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  } else {
+    while (true) {
+      ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+      if (hs.stop || hs.done >= s->max_inner) break;
+      ALTO_TRY(enqueue_iteration(s, L, st));
+    }
+  }
+  return finish_batch(s, hs, inner_out);
 }
 
 // ------------------------------------------------- model error (cpd_error)
