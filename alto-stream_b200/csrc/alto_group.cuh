@@ -163,3 +163,16 @@ alto_status group_launch(StreamGroup* g, int max_steps);
 alto_status group_states(StreamGroup* g, int* running, int* done, int* stop, int* info);
 
 }  // namespace alto
+
+namespace alto {
+// The serving loop's steps of one batch: prepare it (everything before the
+// inner iterations; *grouped tells whether it then runs in a group, else
+// stream_run_ungrouped runs its iterations and finish); after its group
+// has run it to the end, finish it (forgetting, prev <- current, time rows).
+alto_status stream_prepare_grouped(alto_stream_session* s, const alto_coo* b, const double* init_vals,
+                                   uint64_t n_init, bool* grouped);
+alto_status stream_run_ungrouped(alto_stream_session* s, int* inner);
+alto_status stream_finish_grouped(alto_stream_session* s, int* inner);
+bool stream_group_key_equal(const alto_stream_session* a, const alto_stream_session* b);
+void stream_set_cuda_stream(alto_stream_session* s, cudaStream_t st);
+}  // namespace alto

@@ -4,16 +4,27 @@
 // (src/streaming_cpd.cpp:26-366); it has no server.  Here a server accepts
 // slice updates for many streams of different shapes and ranks, keeps each
 // stream's model, Grams and ADMM state resident on the device, admits
-// streams under an HBM budget, and overlaps the streams' work on the device:
+// streams under an HBM budget, and batches their work on the device:
 //
-//   * W worker threads, each with its own non-blocking CUDA stream; a
-//     worker takes the next stream that has queued slices and is not being
-//     processed, runs one slice update on its CUDA stream, and puts the
-//     stream back if it has more work -- so requests that arrive while
-//     others run are picked up as soon as a worker frees up, and the
-//     updates of different streams run concurrently on the GPU;
+//   * W worker threads, each with its own non-blocking CUDA stream, take
+//     the next stream that has a queued slice and is idle and prepare the
+//     slice (grow the model, encode the slice, Grams: everything before the
+//     inner iterations);
+//   * one scheduler thread runs the inner iterations of the prepared slices
+//     in stream groups (one per rank and line format, up to kGroupSlots
+//     slices each): every step is one inner iteration of every slice in the
+//     group, one launch of the group's captured graph, in which each kernel
+//     covers all the group's slices.  Between steps, slices whose batch has
+//     converged leave (a worker then finishes them: forgetting, previous
+//     model, time rows) and newly prepared slices join -- continuous
+//     batching at the granularity of one inner iteration;
+//   * slices of streams that cannot run grouped (the spCP-stream model,
+//     other ranks) run their whole update on the worker;
 //   * a stream's slices run in arrival order, one at a time (its state is
-//     sequential);
+//     sequential); a stream's result is bit-identical alone, in any mix, and
+//     on the plain one-slice-at-a-time path (alto_stream_push runs a
+//     session in a group of one), since each session's arithmetic in a group
+//     is that of its own launches;
 //   * admission: a stream reserves an estimate of its device footprint from
 //     its largest dims and slice size; streams that do not fit the budget
 //     wait (their slices queue) until earlier streams close;
@@ -28,11 +39,7 @@
 #include <unordered_map>
 #include <vector>
 
-#include "alto_internal.cuh"
-
-namespace alto {
-void stream_set_cuda_stream(alto_stream_session* s, cudaStream_t st);
-}
+#include "alto_group.cuh"
 
 using namespace alto;
 
@@ -61,6 +68,21 @@ struct StreamRec {
   std::deque<SliceReq*> q;
   alto_status err = ALTO_OK;
   uint64_t done = 0;
+  SliceReq* cur = nullptr;            // the slice in the group's hands
+  cudaEvent_t ready_ev = nullptr;     // its preparation done (worker stream)
+  cudaEvent_t ran_ev = nullptr;       // its inner iterations done (group stream)
+};
+
+// Slices per stream group.
+constexpr int kGroupSlots = 32;
+// Inner iterations per group launch (one: slices join and leave between
+// every two iterations).
+constexpr int kStepsPerLaunch = 1;
+
+struct GroupRun {
+  StreamGroup* g = nullptr;
+  cudaStream_t st = nullptr;
+  std::vector<StreamRec*> members;
 };
 
 struct TicketInfo {
@@ -86,6 +108,12 @@ struct alto_server {
   bool stop = false;
   // tickets not yet handed back as done by wait/poll (erased then, so the
   // map holds only outstanding work)
+  bool sched_done = false;    // the scheduler has left (set once stopping)
+  std::deque<int> finishing;  // streams whose grouped slice has run (a worker finishes it)
+  std::deque<int> prepared;   // streams whose slice is prepared (the scheduler groups it)
+  std::condition_variable cv_sched;
+  std::thread scheduler;
+  std::vector<GroupRun> groups;  // used by the scheduler thread only
   std::unordered_map<uint64_t, TicketInfo> tickets;
   // latencies of the last kLatencyWindow completed slices (a ring)
   std::vector<double> lat_ms;
@@ -139,6 +167,30 @@ void admit_pending(alto_server* s) {  // caller holds s->mu
   s->cv_work.notify_all();
 }
 
+// Completes a slice: its ticket, the latency record, and the stream's next
+// slice made ready (caller holds s->mu).
+void complete_slice(alto_server* s, StreamRec* r, SliceReq* q, alto_status st, int inner) {
+  const double t_end = now_s();
+  TicketInfo& ti = s->tickets[q->ticket];
+  ti.done = true;
+  ti.inner = inner;
+  ti.status = st;
+  ti.latency_ms = (t_end - q->t_submit) * 1e3;
+  if (st != ALTO_OK) r->err = st;
+  record_latency(s, ti.latency_ms);
+  s->completed++;
+  s->t_last = t_end;
+  r->done++;
+  r->busy = false;
+  if (!r->q.empty()) {
+    r->in_ready = true;
+    s->ready.push_back(r->sid);
+    s->cv_work.notify_one();
+  }
+  delete q;
+  s->cv_done.notify_all();
+}
+
 void worker_main(alto_server* s) {
   cudaSetDevice(s->device);
   cudaStream_t cs = nullptr;
@@ -146,8 +198,28 @@ void worker_main(alto_server* s) {
   tls_alloc_stream = cs;
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
-    s->cv_work.wait(lk, [&] { return s->stop || !s->ready.empty(); });
-    if (s->ready.empty()) break;  // stop requested and nothing left
+    s->cv_work.wait(lk, [&] {
+      return !s->finishing.empty() || !s->ready.empty() || (s->stop && s->sched_done);
+    });
+    if (!s->finishing.empty()) {  // a grouped slice has run: finish it
+      StreamRec* r = s->streams[s->finishing.front()];
+      s->finishing.pop_front();
+      SliceReq* q = r->cur;
+      r->cur = nullptr;
+      s->busy_workers++;
+      lk.unlock();
+      int inner = 0;
+      alto_status st = cuda_status(cudaStreamWaitEvent(cs, r->ran_ev, 0), "cudaStreamWaitEvent", __FILE__, __LINE__);
+      if (st == ALTO_OK) {
+        stream_set_cuda_stream(r->sess, cs);
+        st = stream_finish_grouped(r->sess, &inner);
+      }
+      lk.lock();
+      s->busy_workers--;
+      complete_slice(s, r, q, st, inner);
+      continue;
+    }
+    if (s->ready.empty()) break;  // stopping, and nothing left
     const int sid = s->ready.front();
     s->ready.pop_front();
     StreamRec* r = s->streams[sid];
@@ -160,11 +232,16 @@ void worker_main(alto_server* s) {
 
     alto_status st = r->err;
     int inner = 0;
+    bool grouped = false;
     if (st == ALTO_OK && !r->sess) {
       const alto_stream_config& c = r->cfg;
       st = alto_stream_open(c.nmodes, c.stream_mode, c.rank, c.constraint, c.forgetting, c.max_inner_iters,
                             c.epsilon, cs, &r->sess);
       if (st == ALTO_OK) st = alto_stream_set_model(r->sess, c.model);
+      if (st == ALTO_OK &&
+          (cudaEventCreateWithFlags(&r->ready_ev, cudaEventDisableTiming) != cudaSuccess ||
+           cudaEventCreateWithFlags(&r->ran_ev, cudaEventDisableTiming) != cudaSuccess))
+        st = cuda_status(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__);
     }
     if (st == ALTO_OK) {
       stream_set_cuda_stream(r->sess, cs);
@@ -179,35 +256,127 @@ void worker_main(alto_server* s) {
       coo.vals = q->vals.data();
       coo.val_dtype = ALTO_F64;
       coo.on_device = 0;
-      st = alto_stream_push(r->sess, &coo, q->init.data(), q->init.size(), &inner);
+      st = stream_prepare_grouped(r->sess, &coo, q->init.data(), q->init.size(), &grouped);
+      if (st == ALTO_OK && !grouped) st = stream_run_ungrouped(r->sess, &inner);
+      if (st == ALTO_OK && grouped)
+        st = cuda_status(cudaEventRecord(r->ready_ev, cs), "cudaEventRecord", __FILE__, __LINE__);
     }
-    const double t_end = now_s();
-
     lk.lock();
     s->busy_workers--;
-    TicketInfo& ti = s->tickets[q->ticket];
-    ti.done = true;
-    ti.inner = inner;
-    ti.status = st;
-    ti.latency_ms = (t_end - q->t_submit) * 1e3;
-    if (st != ALTO_OK) r->err = st;
-    record_latency(s, ti.latency_ms);
-    s->completed++;
-    s->t_last = t_end;
-    r->done++;
-    r->busy = false;
-    if (!r->q.empty()) {
-      r->in_ready = true;
-      s->ready.push_back(sid);
-      s->cv_work.notify_one();
+    if (st == ALTO_OK && grouped) {  // to the scheduler
+      r->cur = q;
+      s->prepared.push_back(sid);
+      s->cv_sched.notify_one();
+      continue;
     }
-    delete q;
-    s->cv_done.notify_all();
+    complete_slice(s, r, q, st, inner);
   }
   lk.unlock();
   tls_alloc_stream = nullptr;
   cudaStreamSynchronize(cs);
   cudaStreamDestroy(cs);
+}
+
+// The scheduler: prepared slices join stream groups; every round, one group
+// launch per group with members, then the members whose batch is done
+// leave and go to the workers to be finished.
+void scheduler_main(alto_server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto busy = [&] {
+    for (auto& g : s->groups)
+      if (!g.members.empty()) return true;
+    return false;
+  };
+  while (true) {
+    s->cv_sched.wait(lk, [&] { return s->stop || !s->prepared.empty() || busy(); });
+    if (s->stop && s->prepared.empty() && !busy()) {
+      // stop only once the workers have nothing left that could be prepared
+      bool idle = s->ready.empty() && s->finishing.empty() && s->busy_workers == 0;
+      if (idle) break;
+      s->cv_sched.wait_for(lk, std::chrono::milliseconds(5));
+      continue;
+    }
+    std::vector<StreamRec*> joining;
+    while (!s->prepared.empty()) {
+      joining.push_back(s->streams[s->prepared.front()]);
+      s->prepared.pop_front();
+    }
+    lk.unlock();
+    std::vector<std::pair<StreamRec*, alto_status>> failed;
+    for (StreamRec* r : joining) {
+      GroupRun* gr = nullptr;
+      for (auto& g : s->groups)
+        if ((int)g.members.size() < kGroupSlots && group_fits(g.g, r->sess)) {
+          gr = &g;
+          break;
+        }
+      if (!gr) {
+        GroupRun g;
+        alto_status st = cuda_status(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking), "cudaStreamCreate",
+                                     __FILE__, __LINE__);
+        if (st == ALTO_OK) st = group_create(r->sess, kGroupSlots, g.st, &g.g);
+        if (st != ALTO_OK) {
+          if (g.st) cudaStreamDestroy(g.st);
+          failed.emplace_back(r, st);
+          continue;
+        }
+        s->groups.push_back(g);
+        gr = &s->groups.back();
+      }
+      cudaStreamWaitEvent(gr->st, r->ready_ev, 0);
+      gr->members.push_back(r);
+    }
+    for (auto& g : s->groups) {
+      if (g.members.empty()) continue;
+      std::vector<alto_stream_session*> sess;
+      for (StreamRec* r : g.members) sess.push_back(r->sess);
+      alto_status st = group_set(g.g, sess.data(), (int)sess.size());
+      if (st == ALTO_OK) st = group_launch(g.g, kStepsPerLaunch);
+      if (st != ALTO_OK) {
+        for (StreamRec* r : g.members) failed.emplace_back(r, st);
+        g.members.clear();
+      }
+    }
+    std::vector<StreamRec*> done;
+    for (auto& g : s->groups) {
+      const int k = (int)g.members.size();
+      if (!k) continue;
+      std::vector<int> running(k, 0);
+      alto_status st = group_states(g.g, running.data(), nullptr, nullptr, nullptr);
+      std::vector<StreamRec*> keep;
+      for (int q = 0; q < k; ++q) {
+        StreamRec* r = g.members[q];
+        if (st != ALTO_OK) {
+          failed.emplace_back(r, st);
+        } else if (running[q]) {
+          keep.push_back(r);
+        } else {
+          cudaEventRecord(r->ran_ev, g.st);
+          done.push_back(r);
+        }
+      }
+      g.members.swap(keep);
+    }
+    lk.lock();
+    for (StreamRec* r : done) {
+      s->finishing.push_back(r->sid);
+      s->cv_work.notify_one();
+    }
+    for (auto& f : failed) {
+      SliceReq* q = f.first->cur;
+      f.first->cur = nullptr;
+      complete_slice(s, f.first, q, f.second, 0);
+    }
+  }
+  s->sched_done = true;
+  s->cv_work.notify_all();
+  lk.unlock();
+  for (auto& g : s->groups) {
+    group_destroy(g.g);
+    cudaStreamDestroy(g.st);
+  }
+  s->groups.clear();
 }
 
 double percentile(std::vector<double> v, double p) {
@@ -238,6 +407,7 @@ alto_status alto_server_create(uint64_t hbm_budget_bytes, int workers, alto_serv
     return ALTO_ERR_CUDA;
   }
   for (int w = 0; w < workers; ++w) s->workers.emplace_back(worker_main, s);
+  s->scheduler = std::thread(scheduler_main, s);
   *out = s;
   return ALTO_OK;
 }
@@ -457,6 +627,8 @@ alto_status alto_server_close(alto_server* s, int sid) {
   s->streams.erase(it);
   alto_stream_session* sess = r->sess;
   const alto_status err = r->err;
+  if (r->ready_ev) cudaEventDestroy(r->ready_ev);
+  if (r->ran_ev) cudaEventDestroy(r->ran_ev);
   delete r;
   admit_pending(s);
   if (dropped) s->cv_done.notify_all();
@@ -471,11 +643,15 @@ alto_status alto_server_destroy(alto_server* s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
     s->cv_work.notify_all();
+    s->cv_sched.notify_all();
   }
+  if (s->scheduler.joinable()) s->scheduler.join();
   for (auto& w : s->workers) w.join();
   for (auto& kv : s->streams) {
     for (SliceReq* q : kv.second->q) delete q;
     if (kv.second->sess) alto_stream_close(kv.second->sess);
+    if (kv.second->ready_ev) cudaEventDestroy(kv.second->ready_ev);
+    if (kv.second->ran_ev) cudaEventDestroy(kv.second->ran_ev);
     delete kv.second;
   }
   delete s;

@@ -657,7 +657,14 @@ struct GroupCtl {
   int limit;
   int steps;
   int any;
+  int chunks;  // ADMM chunks of the current mode's loop
+  int error;   // 1: an ADMM loop overran its bound and was stopped
 };
+
+// ADMM sweeps stop after kAdmmMaxIters, so a mode's chunk loop ends within
+// this many chunks; a loop still going past it is stopped with an error
+// (a guard: it cannot happen while every live slot's decision runs).
+constexpr int kAdmmChunkBound = (kAdmmMaxIters + kAdmmChunk - 1) / kAdmmChunk + 2;
 struct SlotState {
   int running;  // takes part in further steps
   int done;     // inner iterations of the batch so far
@@ -732,15 +739,21 @@ __global__ void __launch_bounds__(kAdmmThreads)
   }
 }
 
-// The ADMM chunk loop goes on while some slot's ADMM of mode j sweeps.
-__global__ void group_admm_cond_kernel(SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
-                                       cudaGraphConditionalHandle h) {
+// The ADMM chunk loop goes on while some slot's ADMM of mode j sweeps
+// (first: before the loop, which resets the chunk count).
+__global__ void group_admm_cond_kernel(SlotDesc* __restrict__ tab, GroupCtl* __restrict__ ctl,
+                                       cudaGraphConditionalHandle h, int first) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   bool any = false;
   for (int s = 0; s < ctl->count; ++s) {
     SlotDesc& d = tab[s];
     if (d.act && d.admm_act && d.admm->stop) d.admm_act = 0;
     any = any || (d.act && d.admm_act);
+  }
+  ctl->chunks = first ? 0 : ctl->chunks + 1;
+  if (any && ctl->chunks >= kAdmmChunkBound) {
+    ctl->error = 1;
+    any = false;
   }
   cudaGraphSetConditional(h, any ? 1u : 0u);
 }
@@ -1366,7 +1379,7 @@ alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGrap
                                                                        g->R);
   ALTO_LAUNCHED();
   // while some slot's ADMM of mode j sweeps: one chunk (pass 1, pass 2)
-  group_admm_cond_kernel<<<1, 32, 0, cs>>>(tab, ctl, h);
+  group_admm_cond_kernel<<<1, 32, 0, cs>>>(tab, ctl, h, 1);
   ALTO_LAUNCHED();
   cudaGraph_t body;
   ALTO_TRY(capture_while(cs, h, &body));
@@ -1376,7 +1389,7 @@ alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGrap
   const uint32_t* ao = off_of(offs, g->cap, kOffAdmm, j);
   group_admm_kernel<SLOTS, SEG, true><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
   group_admm_kernel<SLOTS, SEG, false><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
-  group_admm_cond_kernel<<<1, 32, 0, g->capst[1]>>>(tab, ctl, h);
+  group_admm_cond_kernel<<<1, 32, 0, g->capst[1]>>>(tab, ctl, h, 0);
   const cudaError_t le = cudaGetLastError();
   cudaGraph_t done = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(g->capst[1], &done);
@@ -1540,7 +1553,7 @@ alto_status group_create(const alto_stream_session* like, int capacity, cudaStre
   }
   std::memset(g->h_tab, 0, sizeof(SlotDesc) * capacity);
   std::memset(g->h_offs, 0, offs_n * 4);
-  *g->h_ctl = GroupCtl{0, 0, 0, 0};
+  *g->h_ctl = GroupCtl{0, 0, 0, 0, 0, 0};
   ALTO_TRY_CUDA(cudaMemsetAsync(g->tab.p, 0, sizeof(SlotDesc) * capacity, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(g->offs.p, 0, offs_n * 4, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(g->ctl.p, 0, sizeof(GroupCtl), st));
@@ -1644,7 +1657,7 @@ alto_status group_set(StreamGroup* g, alto_stream_session* const* members, int k
 // Run up to max_steps inner iterations of every member (stopping early
 // when none can run), as one launch of the group's graph on its stream.
 alto_status group_launch(StreamGroup* g, int max_steps) {
-  *g->h_ctl = GroupCtl{g->count, max_steps, 0, 0};
+  *g->h_ctl = GroupCtl{g->count, max_steps, 0, 0, 0, 0};
   ALTO_TRY_CUDA(cudaMemcpyAsync(g->ctl.p, g->h_ctl, sizeof(GroupCtl), cudaMemcpyHostToDevice, g->st));
   ALTO_TRY_CUDA(cudaGraphLaunch(g->exec, g->st));
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1654,7 +1667,12 @@ alto_status group_launch(StreamGroup* g, int max_steps) {
 alto_status group_states(StreamGroup* g, int* running, int* done, int* stop, int* info) {
   std::vector<SlotState> h(std::max(g->count, 1));
   ALTO_TRY_CUDA(cudaMemcpyAsync(h.data(), g->states.p, sizeof(SlotState) * g->count, cudaMemcpyDeviceToHost, g->st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(g->h_ctl, g->ctl.p, sizeof(GroupCtl), cudaMemcpyDeviceToHost, g->st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(g->st));
+  if (g->h_ctl->error) {
+    set_error("a grouped ADMM loop overran %d chunks and was stopped", kAdmmChunkBound);
+    return ALTO_ERR_CUDA;
+  }
   for (int q = 0; q < g->count; ++q) {
     if (running) running[q] = h[q].running;
     if (done) done[q] = h[q].done;
@@ -1806,6 +1824,7 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     alto_stream_session* one = s;
     ALTO_TRY(group_set(s->own_group, &one, 1));
     ALTO_TRY(group_launch(s->own_group, s->max_inner));
+    ALTO_TRY(group_states(s->own_group, nullptr, nullptr, nullptr, nullptr));
     ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
     return finish_batch(s, hs, inner_out);
@@ -2009,6 +2028,59 @@ namespace alto {
 void stream_set_cuda_stream(alto_stream_session* s, cudaStream_t st) {
   s->st = st;
   if (s->at) s->at->stream = st;
+}
+
+alto_status stream_prepare_grouped(alto_stream_session* s, const alto_coo* b, const double* init_vals,
+                                   uint64_t n_init, bool* grouped) {
+  *grouped = false;
+  if (b->nmodes != s->N || b->nnz == 0 || (n_init && !init_vals)) {
+    set_error("bad batch (modes %d against %d, nnz %llu)", b->nmodes, s->N, (unsigned long long)b->nnz);
+    return ALTO_ERR_INVALID;
+  }
+  ALTO_TRY(prepare_batch(s, b, init_vals, n_init));
+  if (!s->use_graph || !stream_groupable(s)) return ALTO_OK;
+  ALTO_TRY(group_prepare_session(s));
+  *grouped = true;
+  return ALTO_OK;
+}
+
+alto_status stream_run_ungrouped(alto_stream_session* s, int* inner) {
+  const int N = s->N, R = s->R;
+  cudaStream_t st = s->st;
+  IterLaunch L{};
+  for (int n = 0; n < N; ++n) L.fac[n] = s->sparse ? s->Anz[n].p : s->U[n].p;
+  L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
+  ALTO_TRY(s->iter.ensure(sizeof(IterState)));
+  ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
+  IterState hs{};
+  ALTO_TRY(enqueue_iteration(s, L, st));
+  if (s->use_graph && s->max_inner > 1) {
+    ALTO_TRY(run_graph(s, L));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  } else {
+    while (true) {
+      ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+      ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+      if (hs.stop || hs.done >= s->max_inner) break;
+      ALTO_TRY(enqueue_iteration(s, L, st));
+    }
+  }
+  return finish_batch(s, hs, inner);
+}
+
+alto_status stream_finish_grouped(alto_stream_session* s, int* inner) {
+  IterState hs{};
+  ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, s->st));
+  ALTO_TRY_CUDA(cudaStreamSynchronize(s->st));
+  return finish_batch(s, hs, inner);
+}
+
+bool stream_group_key_equal(const alto_stream_session* a, const alto_stream_session* b) {
+  if (a->R != b->R || a->N != b->N || a->t != b->t) return false;
+  for (int m = 0; m < a->N; ++m)
+    if (a->det[m].hw != b->det[m].hw) return false;
+  return true;
 }
 }  // namespace alto
 

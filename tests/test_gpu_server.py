@@ -70,6 +70,31 @@ def test_each_result_same_alone_and_in_the_mix():
             assert np.array_equal(m, a), (k, normwise(m, a))
 
 
+def test_served_results_equal_the_plain_path():
+    """Slices served in stream groups (every kernel over many streams'
+    slices) give the same factors, bit for bit, as each stream pushed alone
+    through its own session, for several ranks, both constraints and enough
+    streams that groups hold several slices at once."""
+    specs = SPECS + [(15, [120, 80, 30], 32, A.NONNEG), (16, [60, 300, 20], 32, A.UNCONSTRAINED),
+                     (17, [200, 90, 25], 16, A.UNCONSTRAINED), (18, [80, 80, 80], 8, A.NONNEG)]
+    mix, st, _ = run(specs, workers=3)
+    assert st["completed"] == 5 * len(specs)
+    for k, (seed, space, rank, con) in enumerate(specs):
+        b, iv = make_stream(seed, space, 5, rank)
+        s = A.CPStream(4, 0, rank, constraint=con, forgetting=0.99, max_inner=10, epsilon=1e-5)
+        used, prev = 0, np.zeros(4, np.int64)
+        for x in b:
+            d = x["dims"].astype(np.int64)
+            need = int(np.sum(np.maximum(d - prev, 0))) * rank
+            s.push(x["dims"], x["cidx"], x["vals"], iv[used:used + need])
+            used += need
+            prev = np.maximum(prev, d)
+        for m in range(4):
+            rows = len(b) if m == 0 else int(b[-1]["dims"][m])
+            assert np.array_equal(s.factor(m, rows), mix[k][m]), (k, m)
+        s.close()
+
+
 def test_alone_result_matches_oracle():
     seed, space, rank, con = SPECS[0]
     res, _, _ = run([SPECS[0]], workers=1)

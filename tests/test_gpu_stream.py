@@ -79,8 +79,11 @@ def test_stream_repeats_bit_for_bit():
 
 @pytest.mark.parametrize("nonneg", [0, 1])
 def test_graph_and_direct_launches_agree(nonneg):
-    """The batch graph (device-side inner loop and ADMM sweep loop) and the
-    directly launched loop give identical factors and iteration counts."""
+    """The session's stream-group graph (all inner iterations of a batch in
+    one relaunched graph over the session's descriptor: the grouped kernels,
+    device-side inner loop and ADMM chunk loop) and the directly launched
+    per-kernel loop give identical factors and iteration counts, bit for
+    bit."""
     b = load_stream_fixture()[:4]
     iv = synth.init_values(20000, seed=4)
     og, lg, ig = run_gpu(b, 16, 10, 1e-5, nonneg, iv, forgetting=0.95, graph=True)
