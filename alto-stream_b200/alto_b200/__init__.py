@@ -38,6 +38,7 @@ F32, BF16, F64 = 0, 1, 2
 AUTO, ATOMIC, STAGED, STREAM, SORTED, DETERMINISTIC = range(6)
 FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
 FEED_PREFETCH = 0x200  # OR with ATOMIC / SORTED: factor rows prefetched into L2 ahead of the walk
+FEED_WIDE = 0x400  # OR with SORTED (3 modes): four nonzeros per step of the walk
 UNCONSTRAINED, NONNEG, LASSO = range(3)
 CPSTREAM, SPCPSTREAM = range(2)  # streaming models (alto_stream_set_model)
 FIT_REFERENCE, FIT_EXACT = 0, 1
@@ -642,7 +643,8 @@ class alto_stream_config(ctypes.Structure):
 class alto_serving_stats(ctypes.Structure):
     _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("p50_ms", c_double), ("p99_ms", c_double),
                 ("max_ms", c_double), ("slices_per_s", c_double), ("reserved_bytes", c_uint64),
-                ("admitted_streams", c_int), ("pending_streams", c_int)]
+                ("admitted_streams", c_int), ("pending_streams", c_int), ("prepare_ms", c_double),
+                ("step_ms", c_double), ("finish_ms", c_double), ("steps", c_uint64), ("step_slices", c_uint64)]
 
 
 class Server:

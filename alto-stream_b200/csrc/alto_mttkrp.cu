@@ -227,13 +227,15 @@ __device__ __forceinline__ void group_range(uint32_t ws, uint32_t we, int grp, u
   ge = min(gs + sublen, we);
 }
 
-template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool PF = false>
+template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool PF = false, bool WIDE = false>
 __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
                                            bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0,
                                            uint32_t next_ws = 0, uint32_t next_we = 0) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
-  constexpr int U = NM <= 3 ? (DET ? 4 : 2) : 1;  // (4 measured faster for DET only)
+  // nonzeros per step: 2 for 3 modes (4 for DET, and for the wide walk),
+  // 1 beyond
+  constexpr int U = NM <= 3 ? ((DET || WIDE) ? 4 : 2) : 1;
   const int lane = threadIdx.x & 31;
   const int grp = lane / G, sub = lane % G;
   uint32_t sublen, gs, ge;
@@ -420,7 +422,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   }
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, bool PF = false>
+template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, bool PF = false, bool WIDE = false>
 __global__ void __launch_bounds__(kMttkrpThreads, 3)
     mttkrp_tile_kernel(const MttkrpArgs a) {
   extern __shared__ float4 smem4[];
@@ -454,8 +456,8 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
       nws = min(nts + warp * nchunk, nte);
       nwe = min(nws + nchunk, nte);
     }
-    warp_range<R, FT, HW, NM, false, DET, PF>(a, a.line, ws, we, staged, smem, iv_start,
-                                              (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW, nws, nwe);
+    warp_range<R, FT, HW, NM, false, DET, PF, WIDE>(a, a.line, ws, we, staged, smem, iv_start,
+                                                    (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW, nws, nwe);
     if (STAGE && staged) {
       __syncthreads();
       const uint32_t iv_len = a.tile_iv[((size_t)tile * N + a.target) * 2 + 1];
@@ -693,14 +695,29 @@ __global__ void __launch_bounds__(256) det_zero_group_kernel(Strided<DetItem> it
 template <int R, int HW, int NM>
 __global__ void __launch_bounds__(kMttkrpThreads, 3)
     det_tile_group_kernel(Strided<DetItem> items, const uint32_t* __restrict__ tile_off) {
+  // the item's arguments staged in shared memory: the walk reads them per
+  // nonzero (as a launch of its own reads them from the parameter bank)
+  __shared__ MttkrpArgs sa;
+  __shared__ int s_item;
   const int K = *items.count;
   const uint32_t total = K > 0 ? tile_off[K] : 0;
   const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_item = -1;
   for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
     const int s = item_of(tile_off, K, v);
     const DetItem& it = items[s];
     if (!item_live(it.active)) continue;
-    const MttkrpArgs& a = it.a;
+    __syncthreads();  // (everyone is done with the previous item's copy)
+    if (s != s_item) {
+      constexpr int kWords = (int)(sizeof(MttkrpArgs) / 4);
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&it.a);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+      for (int q = threadIdx.x; q < kWords; q += blockDim.x) dst[q] = src[q];
+      __syncthreads();
+      if (threadIdx.x == 0) s_item = s;
+    }
+    __syncthreads();
+    const MttkrpArgs& a = sa;
     const uint32_t tile = v - tile_off[s];
     const uint32_t ts = tile * a.tile_nnz;
     const uint32_t te = min(ts + a.tile_nnz, a.nnz);
@@ -911,7 +928,7 @@ static int num_sms() {
   return g_num_sms;
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool PF = false>
+template <int R, typename FT, int HW, bool STAGE, int NM, bool PF = false, bool WIDE = false>
 static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   MttkrpArgs b = a;
   b.stage_rows = STAGE ? kStageBytes / (R * 4) : 0;
@@ -919,23 +936,26 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     if (STAGE)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF>, kMttkrpThreads, smem));
+        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE>, kMttkrpThreads, smem));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
   if (!grid) return ALTO_OK;
-  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF><<<grid, kMttkrpThreads, smem, st>>>(b);
+  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE><<<grid, kMttkrpThreads, smem, st>>>(b);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
 
 // Direct feed, with the factor-row L2 prefetch when a.pf_dist is set (not
-// for 32-byte records).
+// for 32-byte records), or the wide walk (decoded 3-mode copies).
 template <int R, typename FT, int HW, int NM>
-static alto_status launch_direct(const MttkrpArgs& a, cudaStream_t st) {
+static alto_status launch_direct(const MttkrpArgs& a, bool wide, cudaStream_t st) {
+  if constexpr (HW == kDecoded3) {
+    if (wide) return launch_tile<R, FT, HW, false, NM, false, true>(a, st);
+  }
   if constexpr (HW != 2) {
     if (a.pf_dist) return launch_tile<R, FT, HW, false, NM, true>(a, st);
   }
@@ -1028,15 +1048,15 @@ bool deterministic_supported(int rank, alto_dtype fdtype) {
 }
 
 template <int R, typename FT, int HW>
-static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
+static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, bool wide, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
-    return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_direct<R, FT, HW, 3>(a, st);
+    return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_direct<R, FT, HW, 3>(a, wide, st);
   } else {
 #define NM_CASE(NN)                                                                   \
   case NN:                                                                            \
     if (stage) return launch_tile<R, FT, HW, true, NN>(a, st);                        \
-    return bulk_feed ? launch_tma<R, FT, HW, NN>(a, err, st) : launch_direct<R, FT, HW, NN>(a, st);
+    return bulk_feed ? launch_tma<R, FT, HW, NN>(a, err, st) : launch_direct<R, FT, HW, NN>(a, false, st);
   switch (a.dec.nmodes) {
     NM_CASE(3)
     NM_CASE(4)
@@ -1050,12 +1070,12 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed,
 }
 
 template <typename FT, int HW>
-static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool aligned,
+static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool wide, bool aligned,
                                int* err, cudaStream_t st) {
   if (aligned) {
 #define RANK_CASE(RR) \
   case RR:            \
-    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, err, st);
+    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, wide, err, st);
     switch (rank) {
       RANK_CASE(8)
       RANK_CASE(16)
@@ -1112,8 +1132,9 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
 // directly, 2 loads it directly and prefetches factor rows t->pf_dist
-// nonzeros ahead into L2, -1 uses the autotuned choice (direct when
-// untuned).
+// nonzeros ahead into L2, 3 loads it directly four nonzeros per step (the
+// wide walk of decoded 3-mode copies), -1 uses the autotuned choice (direct
+// when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
@@ -1172,17 +1193,18 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
-  const bool bulk = feed == 1;
+  const bool bulk = feed == 1, wide = feed == 3;
   if (fdtype == ALTO_BF16) {
-    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
-    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, aligned, err, st);
-    if (hw == kDecoded3) return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, aligned, err, st);
-    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == kDecoded3)
+      return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, wide, aligned, err, st);
+    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, false, aligned, err, st);
   }
-  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, aligned, err, st);
-  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
-  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, aligned, err, st);
-  return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, wide, aligned, err, st);
+  return launch_rank<float, 2>(a, rank, stage, bulk, false, aligned, err, st);
 }
 
 alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, int rank, float* out, DetItem* item,
@@ -1320,7 +1342,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
     };
     const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_ATOMIC, 2},
                           {ALTO_MTTKRP_STAGED, 0}, {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1},
-                          {ALTO_MTTKRP_SORTED, 2}};
+                          {ALTO_MTTKRP_SORTED, 2}, {ALTO_MTTKRP_SORTED, 3}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;
@@ -1328,6 +1350,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       const alto_mttkrp_variant v = c.v;
       if (v == ALTO_MTTKRP_STAGED && stageable_fraction(t, m, rank) == 0.0) continue;
       if (v == ALTO_MTTKRP_SORTED && t->nnz / std::max<uint64_t>(t->dims[m], 1) < 2) continue;
+      if (c.feed == 3 && t->nmodes != 3) continue;  // (the wide walk: decoded 3-mode copies only)
       status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);  // warm / build
       if (status != ALTO_OK) break;
       cudaEventRecord(e0, st);

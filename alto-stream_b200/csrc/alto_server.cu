@@ -119,6 +119,8 @@ struct alto_server {
   std::vector<double> lat_ms;
   size_t lat_next = 0;
   uint64_t submitted = 0, completed = 0;
+  double prepare_ms = 0, step_ms = 0, finish_ms = 0;
+  uint64_t steps = 0, step_slices = 0;
   double t_first = 0, t_last = 0;
   int busy_workers = 0;
 };
@@ -209,12 +211,14 @@ void worker_main(alto_server* s) {
       s->busy_workers++;
       lk.unlock();
       int inner = 0;
+      const double t0 = now_s();
       alto_status st = cuda_status(cudaStreamWaitEvent(cs, r->ran_ev, 0), "cudaStreamWaitEvent", __FILE__, __LINE__);
       if (st == ALTO_OK) {
         stream_set_cuda_stream(r->sess, cs);
         st = stream_finish_grouped(r->sess, &inner);
       }
       lk.lock();
+      s->finish_ms += (now_s() - t0) * 1e3;
       s->busy_workers--;
       complete_slice(s, r, q, st, inner);
       continue;
@@ -233,6 +237,7 @@ void worker_main(alto_server* s) {
     alto_status st = r->err;
     int inner = 0;
     bool grouped = false;
+    const double t_prep = now_s();
     if (st == ALTO_OK && !r->sess) {
       const alto_stream_config& c = r->cfg;
       st = alto_stream_open(c.nmodes, c.stream_mode, c.rank, c.constraint, c.forgetting, c.max_inner_iters,
@@ -262,6 +267,7 @@ void worker_main(alto_server* s) {
         st = cuda_status(cudaEventRecord(r->ready_ev, cs), "cudaEventRecord", __FILE__, __LINE__);
     }
     lk.lock();
+    s->prepare_ms += (now_s() - t_prep) * 1e3;
     s->busy_workers--;
     if (st == ALTO_OK && grouped) {  // to the scheduler
       r->cur = q;
@@ -327,8 +333,12 @@ void scheduler_main(alto_server* s) {
       cudaStreamWaitEvent(gr->st, r->ready_ev, 0);
       gr->members.push_back(r);
     }
+    const double t_step = now_s();
+    uint64_t nsteps = 0, nslices = 0;
     for (auto& g : s->groups) {
       if (g.members.empty()) continue;
+      nsteps += 1;
+      nslices += g.members.size();
       std::vector<alto_stream_session*> sess;
       for (StreamRec* r : g.members) sess.push_back(r->sess);
       alto_status st = group_set(g.g, sess.data(), (int)sess.size());
@@ -359,6 +369,9 @@ void scheduler_main(alto_server* s) {
       g.members.swap(keep);
     }
     lk.lock();
+    s->step_ms += (now_s() - t_step) * 1e3;
+    s->steps += nsteps;
+    s->step_slices += nslices;
     for (StreamRec* r : done) {
       s->finishing.push_back(r->sid);
       s->cv_work.notify_one();
@@ -576,6 +589,11 @@ alto_status alto_server_stats(alto_server* s, alto_serving_stats* out) {
   for (auto& kv : s->streams) admitted += kv.second->admitted ? 1 : 0;
   out->admitted_streams = admitted;
   out->pending_streams = (int)s->pending.size();
+  out->prepare_ms = s->prepare_ms;
+  out->step_ms = s->step_ms;
+  out->finish_ms = s->finish_ms;
+  out->steps = s->steps;
+  out->step_slices = s->step_slices;
   return ALTO_OK;
 }
 

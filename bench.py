@@ -949,6 +949,10 @@ def ours_serve(args):
                    "results_identical_to_plain": bool(same), "checked_streams": len(check) * world,
                    "reserved_bytes": st1["reserved_bytes"], "admitted_streams": st1["admitted_streams"],
                    "warmup_completed": st0["completed"],
+                   "server_time_ms": {k: round(st1[k] - st0[k], 1) for k in ("prepare_ms", "step_ms", "finish_ms")},
+                   "group_steps": st1["steps"] - st0["steps"],
+                   "mean_slices_per_step": ((st1["step_slices"] - st0["step_slices"]) /
+                                            max(st1["steps"] - st0["steps"], 1)),
                    "timing": "host clock from the first timed arrival to the drained server",
                    "l2": "per-slice data and factors exceed L2 across streams; no flush"},
         "roofline": None,

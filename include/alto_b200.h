@@ -65,6 +65,10 @@ typedef enum {
  * into L2 the factor rows of the nonzeros a set distance ahead of each lane
  * group's walk (alto_mttkrp_set_prefetch; the autotuner tries it). */
 #define ALTO_MTTKRP_FEED_PREFETCH 0x200
+/* OR-ed into SORTED on a 3-mode tensor: walk the row-sorted copy four
+ * nonzeros per step instead of two (more loads in flight, more registers;
+ * the autotuner tries it). */
+#define ALTO_MTTKRP_FEED_WIDE 0x400
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */
@@ -416,6 +420,12 @@ typedef struct {
   double slices_per_s;            /* completed slices over first submission .. last completion */
   uint64_t reserved_bytes;
   int admitted_streams, pending_streams;
+  /* where the time went (host clock, summed over threads): slice
+   * preparation on the workers, group steps on the scheduler (launch to
+   * states read back), finishing on the workers; group steps run and the
+   * slices they covered (their ratio: the mean slices per step) */
+  double prepare_ms, step_ms, finish_ms;
+  uint64_t steps, step_slices;
 } alto_serving_stats;
 
 alto_status alto_server_create(uint64_t hbm_budget_bytes, int workers, alto_server** out);
