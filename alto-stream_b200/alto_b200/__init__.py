@@ -37,8 +37,6 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_SPD, ERR_UNSUPPORTED, ERR_TIMEOUT 
 F32, BF16, F64 = 0, 1, 2
 AUTO, ATOMIC, STAGED, STREAM, SORTED, DETERMINISTIC = range(6)
 FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
-FEED_PREFETCH = 0x200  # OR with ATOMIC / SORTED: factor rows prefetched into L2 ahead of the walk
-FEED_WIDE = 0x400  # OR with SORTED (3 modes): four nonzeros per step of the walk
 UNCONSTRAINED, NONNEG, LASSO = range(3)
 CPSTREAM, SPCPSTREAM = range(2)  # streaming models (alto_stream_set_model)
 FIT_REFERENCE, FIT_EXACT = 0, 1
@@ -46,7 +44,7 @@ FIT_REFERENCE, FIT_EXACT = 0, 1
 EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
-    "alto_tensor_device_bytes", "alto_tensor_restrict", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run", "alto_mttkrp_set_prefetch",
+    "alto_tensor_device_bytes", "alto_tensor_restrict", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
     "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
     "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph", "alto_stream_error",
@@ -271,10 +269,6 @@ class AltoTensor:
                                             c_void_p(out.data_ptr()), c_int(1 if accumulate else 0),
                                             c_int(variant), _stream_handle(stream)))
         return out
-
-    def set_prefetch(self, distance):
-        """Distance (nonzeros ahead) of FEED_PREFETCH's factor-row L2 prefetch."""
-        check(lib().alto_mttkrp_set_prefetch(self.h, c_uint32(int(distance))))
 
     def choose_variant(self, mode, rank, fdtype=F32):
         v = c_int()

@@ -352,28 +352,14 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
                                     alto_mttkrp_variant variant, alto_cuda_stream stream) {
   ALTO_TRY(check_mttkrp(t, mode, factors, fdtype, rank, out));
   const int bulk = ((int)variant & ALTO_MTTKRP_FEED_BULK) ? 1 : 0;
-  const int pf = ((int)variant & ALTO_MTTKRP_FEED_PREFETCH) ? 1 : 0;
-  const int wide = ((int)variant & ALTO_MTTKRP_FEED_WIDE) ? 1 : 0;
-  const alto_mttkrp_variant v = (alto_mttkrp_variant)((int)variant & ~(ALTO_MTTKRP_FEED_BULK |
-                                                                       ALTO_MTTKRP_FEED_PREFETCH |
-                                                                       ALTO_MTTKRP_FEED_WIDE));
-  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_DETERMINISTIC || bulk + pf + wide > 1 ||
-      ((bulk || pf) && v != ALTO_MTTKRP_ATOMIC && v != ALTO_MTTKRP_SORTED) ||
-      (wide && (v != ALTO_MTTKRP_SORTED || t->nmodes != 3))) {
+  const alto_mttkrp_variant v = (alto_mttkrp_variant)((int)variant & ~ALTO_MTTKRP_FEED_BULK);
+  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_DETERMINISTIC ||
+      (bulk && v != ALTO_MTTKRP_ATOMIC && v != ALTO_MTTKRP_SORTED)) {
     set_error("unknown variant %d", (int)variant);
     return ALTO_ERR_INVALID;
   }
   return run_mttkrp_feed(t, mode, factors, fdtype, rank, out, accumulate, v,
-                         v == ALTO_MTTKRP_AUTO ? -1 : (wide ? 3 : (pf ? 2 : bulk)), (cudaStream_t)stream);
-}
-
-alto_status alto_mttkrp_set_prefetch(alto_tensor* t, uint32_t distance) {
-  if (!t || distance == 0 || distance > (1u << 20)) {
-    set_error("prefetch distance must be 1..2^20 nonzeros");
-    return ALTO_ERR_INVALID;
-  }
-  t->pf_dist = distance;
-  return ALTO_OK;
+                         v == ALTO_MTTKRP_AUTO ? -1 : bulk, (cudaStream_t)stream);
 }
 
 alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,

@@ -755,21 +755,13 @@ alto_status restrict_line(alto_tensor* t, uint64_t begin, uint64_t end, cudaStre
 // ------------------------------------------------ per-mode row-sorted lines
 
 // Row index of every line entry for one mode, and the identity payload.
-// Sort key of each line entry for a row-sorted copy: the row of `mode`,
-// followed (when fiber_mode >= 0) by the row of fiber_mode in the low
-// fiber_bits bits, so that a stable sort groups each output row's nonzeros
-// by their fiber_mode row as well.
-__global__ void mode_rows_kernel(const void* __restrict__ line, LineDecode dec, int mode, int fiber_mode,
-                                 int fiber_bits, uint32_t nnz, uint64_t* __restrict__ rows,
-                                 uint32_t* __restrict__ pos) {
+__global__ void mode_rows_kernel(const void* __restrict__ line, LineDecode dec, int mode, uint32_t nnz,
+                                 uint64_t* __restrict__ rows, uint32_t* __restrict__ pos) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
     uint64_t lo, hi;
     float v;
     rec_read(line, dec.hi_words, i, lo, hi, v);
-    uint64_t k = line_field(lo, hi, dec.pos[mode], dec.mask[mode]);
-    if (fiber_mode >= 0)
-      k = (k << fiber_bits) | line_field(lo, hi, dec.pos[fiber_mode], dec.mask[fiber_mode]);
-    rows[i] = k;
+    rows[i] = line_field(lo, hi, dec.pos[mode], dec.mask[mode]);
     pos[i] = i;
   }
 }
@@ -842,13 +834,6 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   const int hw = t->dec.hi_words;
   // 3-mode copies store the rows decoded (same 16 bytes per record)
   s.hw = t->nmodes == 3 ? kDecoded3 : hw;
-  // (the copy keeps ALTO order among equal rows: a secondary sort on the row
-  // of one other mode -- so that its factor row is gathered once per fiber
-  // -- was measured slower on the power-law tensor, 4.3 against 2.95 ms per
-  // mode: it gives up the interleaved order's locality in the third mode)
-  s.fiber_mode = -1;
-  const int sort_bits =
-      t->mode_bits[mode] + (s.fiber_mode >= 0 ? t->mode_bits[s.fiber_mode] : 0);
   ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(s.hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
   const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
@@ -865,13 +850,11 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   uint32_t* counts = (uint32_t*)(sb + o_cnt);
   const uint32_t n32 = (uint32_t)nnz;
   if (nnz) {
-    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(
-        t->line.p, t->dec, mode, s.fiber_mode, s.fiber_mode >= 0 ? t->mode_bits[s.fiber_mode] : 0, n32, rk[0],
-        pm[0]);
+    mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, mode, n32, rk[0], pm[0]);
     ALTO_LAUNCHED();
     int cur = 0;
     uint64_t* nohi[2] = {nullptr, nullptr};
-    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, sort_bits, counts, t->scan_scratch, st, &cur));
+    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, t->mode_bits[mode], counts, t->scan_scratch, st, &cur));
     if (s.hw == kDecoded3)
       gather_decode3_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, pm[cur], n32,
                                                                  s.line.as<uint4>());

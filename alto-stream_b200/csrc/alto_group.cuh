@@ -24,13 +24,6 @@ struct MttkrpArgs {
   uint32_t ntiles;
   int target;
   int stage_rows;  // rows of the shared staging buffer (0: never stage)
-  // (3-mode row-sorted copies) the mode whose row is the copy's second sort
-  // key: consecutive nonzeros often share it, and its factor row is then
-  // gathered once for the run (-1: no such order)
-  int fiber_mode;
-  // L2 prefetch of the factor rows of nonzeros this far ahead in a lane
-  // group's walk (0: none; 16-byte records only)
-  uint32_t pf_dist;
   LineDecode dec;
   FactorSet fac;
   float* out;

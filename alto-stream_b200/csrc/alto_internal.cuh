@@ -234,9 +234,6 @@ namespace alto {
 struct SortedLine {
   DevBuf line, tile_iv;
   int hw = 0;  // record format: the line's hi_words, or kDecoded3
-  // second sort key (3-mode copies): rows sharing the output row are ordered
-  // by this mode's row; -1 when the copy is ordered by the output row only
-  int fiber_mode = -1;
   uint32_t ntiles = 0;
   uint64_t for_nnz = 0;
   bool ready = false;
@@ -246,7 +243,7 @@ struct SortedLine {
 struct TuneEntry {
   int mode, rank, fdtype;
   alto_mttkrp_variant variant;
-  int feed;  // 0 direct, 1 line streamed through shared memory by bulk copy, 2 direct + L2 prefetch
+  bool bulk_feed;  // line streamed through shared memory by bulk copy
 };
 }  // namespace alto
 
@@ -274,9 +271,6 @@ struct alto_tensor {
   // mode, the first row and the row count of its interval.
   uint32_t tile_nnz = 4096;
   uint32_t ntiles = 0;
-  // distance (nonzeros ahead in a lane group's walk) of the factor-row L2
-  // prefetch of the prefetching feed
-  uint32_t pf_dist = 64;
   alto::DevBuf tile_iv;  // uint32 [ntiles * nmodes * 2]
 
   // The reference's partitions (prtn_ptr / prtn_intervals).

@@ -162,21 +162,6 @@ __device__ __forceinline__ void load_keys(const void* line, uint32_t i0, uint32_
   }
 }
 
-// Prefetch into L2 the factor rows (all lines of each row) of the input
-// modes of one record held as words w.
-template <typename FT, int HW, int NM>
-__device__ __forceinline__ void prefetch_rows(const MttkrpArgs& a, const uint32_t (&w)[4], int R) {
-  constexpr int kLine = 128;
-  const int row_bytes = R * (int)sizeof(FT);
-#pragma unroll
-  for (int j = 0; j < NM - 1; ++j) {
-    const int m = j < a.target ? j : j + 1;
-    if (m >= a.dec.nmodes) continue;
-    const char* p = static_cast<const char*>(a.fac.f[m]) + (size_t)rec_row<HW>(w, a.dec, m) * row_bytes;
-    for (int o = 0; o < row_bytes; o += kLine) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
-  }
-}
-
 // Walk line range [ws, we) with one warp: the range is split into NPW
 // contiguous sub-ranges, one per lane group; a group walks its sub-range in
 // order, U nonzeros per iteration (two for 3 modes, one for more, to stay in
@@ -215,31 +200,23 @@ __device__ __forceinline__ void det_plain(float* out, uint32_t row, int sub, con
   }
 }
 
-// The lane group's sub-range [gs, ge) of warp range [ws, we): NPW
-// contiguous sub-ranges, odd lengths when reading shared memory (so the
-// groups' records fall in different banks).
-template <int NPW, bool SMEM>
-__device__ __forceinline__ void group_range(uint32_t ws, uint32_t we, int grp, uint32_t& sublen, uint32_t& gs,
-                                            uint32_t& ge) {
-  sublen = (we - ws + NPW - 1) / NPW;
-  if (SMEM) sublen |= 1u;
-  gs = min(ws + grp * sublen, we);
-  ge = min(gs + sublen, we);
-}
-
-template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool PF = false, bool WIDE = false>
+template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false>
 __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
-                                           bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0,
-                                           uint32_t next_ws = 0, uint32_t next_we = 0) {
+                                           bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
-  // nonzeros per step: 2 for 3 modes (4 for DET, and for the wide walk),
-  // 1 beyond
-  constexpr int U = NM <= 3 ? ((DET || WIDE) ? 4 : 2) : 1;
+  // nonzeros per step: 2 for 3 modes (4 measured faster for DET only), 2 for
+  // 4 and 5 modes, 1 beyond (the accumulation order is the line order
+  // whatever U is)
+  constexpr int U = NM <= 3 ? (DET ? 4 : 2) : (NM <= 5 ? 2 : 1);
   const int lane = threadIdx.x & 31;
   const int grp = lane / G, sub = lane % G;
-  uint32_t sublen, gs, ge;
-  group_range<NPW, SMEM>(ws, we, grp, sublen, gs, ge);
+  // groups' sub-ranges; odd lengths when reading shared memory, so the
+  // groups' records fall in different banks
+  uint32_t sublen = (we - ws + NPW - 1) / NPW;
+  if (SMEM) sublen |= 1u;
+  const uint32_t gs = min(ws + grp * sublen, we);
+  const uint32_t ge = min(gs + sublen, we);
   float acc[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) acc[q] = 0.f;
@@ -250,78 +227,20 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   uint32_t w[U][4];
   float v[U];
   bool valid[U];
-  // fiber reuse: the last gathered row of the fiber mode and its values
-  // (not in DET, whose four nonzeros per step leave no registers for it)
-  const bool fib = !DET && HW == kDecoded3 && a.fiber_mode >= 0;
-  uint32_t fib_row = kNoRow;
-  float fib_v[V];
-#pragma unroll
-  for (int q = 0; q < V; ++q) fib_v[q] = 0.f;
-  // L2 prefetch (direct feed, 16-byte records): the group's stream is its
-  // sub-range here and then its sub-range of the warp's next range (the
-  // CTA's next tile); every G/U steps each of the G lanes loads the record
-  // pf_dist nonzeros ahead in that stream and, one round later, prefetches
-  // the record's factor rows, so no one waits on the record's load
-  constexpr bool kCanPf = PF && !SMEM && !DET && HW != 2 && G >= U;
-  constexpr uint32_t kPfRound = G;  // nonzeros per group per round
-  uint32_t pw[4] = {0, 0, 0, 0};
-  bool pf_ok = false;
-  uint32_t nsub = 0, ngs = 0, nge = 0;
-  if (kCanPf) group_range<NPW, false>(next_ws, next_we, grp, nsub, ngs, nge);
-  auto pf_load = [&](uint32_t off) {  // record `off` nonzeros into the stream
-    uint32_t i = gs + off;
-    if (i >= ge) i = ngs + (off - (ge - gs));
-    pf_ok = off < (ge - gs) || i < nge;
-    if (pf_ok) {
-      const uint4 q = __ldg(static_cast<const uint4*>(line) + i);
-      pw[0] = q.x, pw[1] = q.y, pw[2] = q.z, pw[3] = q.w;
-    }
-  };
-  if (kCanPf && a.pf_dist) pf_load(a.pf_dist + sub);
   load_keys<HW, U, SMEM>(line, gs, ge, w, v, valid);
   for (uint32_t k = 0; k < sublen; k += U) {
-    if (kCanPf && a.pf_dist && k % kPfRound == 0) {
-      if (pf_ok) prefetch_rows<FT, HW, NM>(a, pw, R);
-      pf_load(k + kPfRound + a.pf_dist + sub);
-    }
     // factor rows of the NM-1 input modes (j-th input mode m = j, or j+1
     // past the target)
     float f[U][NM - 1][V];
-    bool same[U];  // (fiber mode) same row as the nonzero before
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      same[u] = false;
 #pragma unroll
       for (int j = 0; j < NM - 1; ++j) {
         const int m = j < a.target ? j : j + 1;
         if (m < a.dec.nmodes && valid[u]) {
           const uint32_t r = rec_row<HW>(w[u], a.dec, m);
-          if (fib && m == a.fiber_mode) {
-            same[u] = r == (u ? rec_row<HW>(w[u - 1], a.dec, m) : fib_row);
-            if (!same[u]) load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
-          } else {
-            load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
-          }
+          load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
         }
-      }
-    }
-    if (fib) {
-#pragma unroll
-      for (int j = 0; j < NM - 1; ++j) {
-        const int m = j < a.target ? j : j + 1;
-        if (m != a.fiber_mode) continue;
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (same[u])
-#pragma unroll
-            for (int q = 0; q < V; ++q) f[u][j][q] = u ? f[u - 1][j][q] : fib_v[q];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (valid[u]) {
-            fib_row = rec_row<HW>(w[u], a.dec, m);
-#pragma unroll
-            for (int q = 0; q < V; ++q) fib_v[q] = f[u][j][q];
-          }
       }
     }
     uint32_t rows[U];
@@ -422,7 +341,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   }
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, bool PF = false, bool WIDE = false>
+template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false>
 __global__ void __launch_bounds__(kMttkrpThreads, 3)
     mttkrp_tile_kernel(const MttkrpArgs a) {
   extern __shared__ float4 smem4[];
@@ -447,17 +366,8 @@ __global__ void __launch_bounds__(kMttkrpThreads, 3)
     const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
     const uint32_t ws = min(ts + warp * chunk, te);
     const uint32_t we = min(ws + chunk, te);
-    // this warp's range in the CTA's next tile (for the prefetch stream)
-    uint32_t nws = 0, nwe = 0;
-    if (tile + gridDim.x < a.ntiles) {
-      const uint32_t nts = (tile + gridDim.x) * a.tile_nnz;
-      const uint32_t nte = min(nts + a.tile_nnz, a.nnz);
-      const uint32_t nchunk = (nte - nts + kMttkrpWarps - 1) / kMttkrpWarps;
-      nws = min(nts + warp * nchunk, nte);
-      nwe = min(nws + nchunk, nte);
-    }
-    warp_range<R, FT, HW, NM, false, DET, PF, WIDE>(a, a.line, ws, we, staged, smem, iv_start,
-                                                    (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW, nws, nwe);
+    warp_range<R, FT, HW, NM, false, DET>(a, a.line, ws, we, staged, smem, iv_start,
+                                          (tile * kMttkrpWarps + warp) * LaneWidth<R>::NPW);
     if (STAGE && staged) {
       __syncthreads();
       const uint32_t iv_len = a.tile_iv[((size_t)tile * N + a.target) * 2 + 1];
@@ -928,7 +838,7 @@ static int num_sms() {
   return g_num_sms;
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool PF = false, bool WIDE = false>
+template <int R, typename FT, int HW, bool STAGE, int NM>
 static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   MttkrpArgs b = a;
   b.stage_rows = STAGE ? kStageBytes / (R * 4) : 0;
@@ -936,30 +846,17 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     if (STAGE)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE>, kMttkrpThreads, smem));
+        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM>, kMttkrpThreads, smem));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
   if (!grid) return ALTO_OK;
-  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, PF, WIDE><<<grid, kMttkrpThreads, smem, st>>>(b);
+  mttkrp_tile_kernel<R, FT, HW, STAGE, NM><<<grid, kMttkrpThreads, smem, st>>>(b);
   ALTO_LAUNCHED();
   return ALTO_OK;
-}
-
-// Direct feed, with the factor-row L2 prefetch when a.pf_dist is set (not
-// for 32-byte records), or the wide walk (decoded 3-mode copies).
-template <int R, typename FT, int HW, int NM>
-static alto_status launch_direct(const MttkrpArgs& a, bool wide, cudaStream_t st) {
-  if constexpr (HW == kDecoded3) {
-    if (wide) return launch_tile<R, FT, HW, false, NM, false, true>(a, st);
-  }
-  if constexpr (HW != 2) {
-    if (a.pf_dist) return launch_tile<R, FT, HW, false, NM, true>(a, st);
-  }
-  return launch_tile<R, FT, HW, false, NM>(a, st);
 }
 
 template <int R, typename FT, int HW, int NM>
@@ -1048,15 +945,15 @@ bool deterministic_supported(int rank, alto_dtype fdtype) {
 }
 
 template <int R, typename FT, int HW>
-static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, bool wide, int* err,
+static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
-    return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_direct<R, FT, HW, 3>(a, wide, st);
+    return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
   } else {
 #define NM_CASE(NN)                                                                   \
   case NN:                                                                            \
     if (stage) return launch_tile<R, FT, HW, true, NN>(a, st);                        \
-    return bulk_feed ? launch_tma<R, FT, HW, NN>(a, err, st) : launch_direct<R, FT, HW, NN>(a, false, st);
+    return bulk_feed ? launch_tma<R, FT, HW, NN>(a, err, st) : launch_tile<R, FT, HW, false, NN>(a, st);
   switch (a.dec.nmodes) {
     NM_CASE(3)
     NM_CASE(4)
@@ -1070,12 +967,12 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed,
 }
 
 template <typename FT, int HW>
-static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool wide, bool aligned,
+static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool aligned,
                                int* err, cudaStream_t st) {
   if (aligned) {
 #define RANK_CASE(RR) \
   case RR:            \
-    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, wide, err, st);
+    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, err, st);
     switch (rank) {
       RANK_CASE(8)
       RANK_CASE(16)
@@ -1131,16 +1028,13 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 }
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
-// directly, 2 loads it directly and prefetches factor rows t->pf_dist
-// nonzeros ahead into L2, 3 loads it directly four nonzeros per step (the
-// wide walk of decoded 3-mode copies), -1 uses the autotuned choice (direct
-// when untuned).
+// directly, -1 uses the autotuned choice (direct when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
   if (feed < 0) {
     const TuneEntry* e = variant == ALTO_MTTKRP_AUTO ? tuned_entry(t, mode, rank, fdtype) : nullptr;
-    feed = e ? e->feed : 0;
+    feed = e ? (e->bulk_feed ? 1 : 0) : 0;
   }
   if (variant == ALTO_MTTKRP_AUTO) variant = choose_variant(t, mode, rank, fdtype);
   const bool det = variant == ALTO_MTTKRP_DETERMINISTIC;
@@ -1176,9 +1070,6 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   a.nnz = (uint32_t)t->nnz;
   a.tile_nnz = t->tile_nnz;
   a.target = mode;
-  a.fiber_mode = -1;
-  if (hw == kDecoded3) a.fiber_mode = t->sorted[mode].fiber_mode;
-  a.pf_dist = feed == 2 ? t->pf_dist : 0;
   a.dec = t->dec;
   a.out = out;
   bool aligned = (reinterpret_cast<uintptr_t>(out) % 16) == 0;
@@ -1193,18 +1084,17 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
-  const bool bulk = feed == 1, wide = feed == 3;
+  const bool bulk = feed == 1;
   if (fdtype == ALTO_BF16) {
-    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, false, aligned, err, st);
-    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, false, aligned, err, st);
-    if (hw == kDecoded3)
-      return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, wide, aligned, err, st);
-    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == kDecoded3) return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, aligned, err, st);
+    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, aligned, err, st);
   }
-  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, false, aligned, err, st);
-  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, false, aligned, err, st);
-  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, wide, aligned, err, st);
-  return launch_rank<float, 2>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, aligned, err, st);
+  return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
 }
 
 alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, int rank, float* out, DetItem* item,
@@ -1230,8 +1120,6 @@ alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, in
   a.nnz = (uint32_t)t->nnz;
   a.tile_nnz = t->tile_nnz;
   a.target = mode;
-  a.fiber_mode = -1;
-  a.pf_dist = 0;
   a.dec = t->dec;
   a.out = out;
   bool aligned = (reinterpret_cast<uintptr_t>(out) % 16) == 0;
@@ -1340,9 +1228,8 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       alto_mttkrp_variant v;
       int feed;
     };
-    const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_ATOMIC, 2},
-                          {ALTO_MTTKRP_STAGED, 0}, {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1},
-                          {ALTO_MTTKRP_SORTED, 2}, {ALTO_MTTKRP_SORTED, 3}};
+    const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;
@@ -1350,7 +1237,6 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       const alto_mttkrp_variant v = c.v;
       if (v == ALTO_MTTKRP_STAGED && stageable_fraction(t, m, rank) == 0.0) continue;
       if (v == ALTO_MTTKRP_SORTED && t->nnz / std::max<uint64_t>(t->dims[m], 1) < 2) continue;
-      if (c.feed == 3 && t->nmodes != 3) continue;  // (the wide walk: decoded 3-mode copies only)
       status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);  // warm / build
       if (status != ALTO_OK) break;
       cudaEventRecord(e0, st);
@@ -1369,7 +1255,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
         best_feed = c.feed;
       }
     }
-    t->tuned.push_back({m, rank, (int)fdtype, best, best_feed});
+    t->tuned.push_back({m, rank, (int)fdtype, best, best_feed == 1});
     if (chosen) chosen[m] = best;
   }
   cudaEventDestroy(e0);

@@ -61,14 +61,6 @@ typedef enum {
  * SORTED): stream the line through shared memory with bulk copies
  * (cp.async.bulk, double buffered) instead of loading it directly. */
 #define ALTO_MTTKRP_FEED_BULK 0x100
-/* OR-ed into ATOMIC or SORTED likewise: load the line directly and prefetch
- * into L2 the factor rows of the nonzeros a set distance ahead of each lane
- * group's walk (alto_mttkrp_set_prefetch; the autotuner tries it). */
-#define ALTO_MTTKRP_FEED_PREFETCH 0x200
-/* OR-ed into SORTED on a 3-mode tensor: walk the row-sorted copy four
- * nonzeros per step instead of two (more loads in flight, more registers;
- * the autotuner tries it). */
-#define ALTO_MTTKRP_FEED_WIDE 0x400
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */
@@ -180,10 +172,6 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
 alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,
                                  int rank, alto_cuda_stream stream, alto_mttkrp_variant* variants);
 
-/* Distance, in nonzeros ahead of each lane group's walk, of the factor-row
- * L2 prefetch of ALTO_MTTKRP_FEED_PREFETCH (default 64; 1..2^20).  No
- * counterpart in the reference (a tuning knob of the device kernels). */
-alto_status alto_mttkrp_set_prefetch(alto_tensor* t, uint32_t distance);
 /* The variant ALTO_MTTKRP_AUTO resolves to for this tensor, mode and rank. */
 alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dtype fdtype,
                                alto_mttkrp_variant* variant);
