@@ -589,6 +589,8 @@ static alto_status finish_layout(alto_tensor* t, int nprtn, cudaStream_t st) {
     tile_interval_kernel<<<t->ntiles, 256, 0, st>>>(t->line.p, dec, n32, t->tile_nnz,
                                                     t->tile_iv.as<uint32_t>());
     ALTO_LAUNCHED();
+  }
+  if (t->ntiles && t->tile_stats) {
     std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
     ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));

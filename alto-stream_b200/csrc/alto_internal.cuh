@@ -284,6 +284,10 @@ struct alto_tensor {
   std::vector<uint32_t> tile_len_sorted[ALTO_MAX_MODES];
   // Variants chosen by alto_mttkrp_autotune, per (mode, rank, dtype).
   std::vector<alto::TuneEntry> tuned;
+  // Whether encoding collects tile_len_sorted (a host copy and a
+  // synchronisation; only ALTO_MTTKRP_AUTO's rule reads it -- CP-stream
+  // sessions, which always run the deterministic variant, skip it).
+  bool tile_stats = true;
 
   // Device error word of the kernels' bounded waits (0 = none).
   alto::DevBuf err;

@@ -848,6 +848,9 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
     if (STAGE)
       ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
+    else  // no shared memory: all of the unified L1 / shared storage as L1 (factor rows hit it)
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM>, kMttkrpThreads, smem));
     if (blocks_per_sm < 1) blocks_per_sm = 1;

@@ -1749,6 +1749,7 @@ alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const doubl
     for (int n = 0; n < N; ++n) ALTO_TRY_CUDA(cudaMemsetAsync(s->dual[n].p, 0, s->dims[n] * R * 8, st));
   if (!s->at) {
     s->at = new alto_tensor();
+    s->at->tile_stats = false;
     s->at->key_bits = 128;
     s->at->stream_mode = t;
     s->at->stream = st;
