@@ -243,7 +243,7 @@ struct SortedLine {
 struct TuneEntry {
   int mode, rank, fdtype;
   alto_mttkrp_variant variant;
-  bool bulk_feed;  // line streamed through shared memory by bulk copy
+  int feed;  // 0 direct, 1 line streamed through shared memory by bulk copy, 2 direct at five blocks per SM
 };
 }  // namespace alto
 

@@ -341,8 +341,8 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   }
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false>
-__global__ void __launch_bounds__(kMttkrpThreads, 3)
+template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, int MINB = 3>
+__global__ void __launch_bounds__(kMttkrpThreads, MINB)
     mttkrp_tile_kernel(const MttkrpArgs a) {
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
@@ -838,7 +838,7 @@ static int num_sms() {
   return g_num_sms;
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM>
+template <int R, typename FT, int HW, bool STAGE, int NM, int MINB = 3>
 static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   MttkrpArgs b = a;
   b.stage_rows = STAGE ? kStageBytes / (R * 4) : 0;
@@ -846,18 +846,18 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     if (STAGE)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
     else  // no shared memory: all of the unified L1 / shared storage as L1 (factor rows hit it)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>,
                                          cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM>, kMttkrpThreads, smem));
+        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>, kMttkrpThreads, smem));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
   if (!grid) return ALTO_OK;
-  mttkrp_tile_kernel<R, FT, HW, STAGE, NM><<<grid, kMttkrpThreads, smem, st>>>(b);
+  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB><<<grid, kMttkrpThreads, smem, st>>>(b);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -948,9 +948,10 @@ bool deterministic_supported(int rank, alto_dtype fdtype) {
 }
 
 template <int R, typename FT, int HW>
-static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int* err,
+static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, bool dense, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
+    if (dense && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
     return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
   } else {
 #define NM_CASE(NN)                                                                   \
@@ -970,12 +971,12 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed,
 }
 
 template <typename FT, int HW>
-static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool aligned,
-                               int* err, cudaStream_t st) {
+static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool dense,
+                               bool aligned, int* err, cudaStream_t st) {
   if (aligned) {
 #define RANK_CASE(RR) \
   case RR:            \
-    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, err, st);
+    return launch_modes<RR, FT, HW>(a, stage, bulk_feed, dense, err, st);
     switch (rank) {
       RANK_CASE(8)
       RANK_CASE(16)
@@ -1031,13 +1032,15 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 }
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
-// directly, -1 uses the autotuned choice (direct when untuned).
+// directly, 2 loads it directly with five blocks per SM (decoded 3-mode
+// copies: at most 48 registers a thread), -1 uses the autotuned choice
+// (direct when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
   if (feed < 0) {
     const TuneEntry* e = variant == ALTO_MTTKRP_AUTO ? tuned_entry(t, mode, rank, fdtype) : nullptr;
-    feed = e ? (e->bulk_feed ? 1 : 0) : 0;
+    feed = e ? e->feed : 0;
   }
   if (variant == ALTO_MTTKRP_AUTO) variant = choose_variant(t, mode, rank, fdtype);
   const bool det = variant == ALTO_MTTKRP_DETERMINISTIC;
@@ -1087,17 +1090,18 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
-  const bool bulk = feed == 1;
+  const bool bulk = feed == 1, dense = feed == 2;
   if (fdtype == ALTO_BF16) {
-    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, aligned, err, st);
-    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, aligned, err, st);
-    if (hw == kDecoded3) return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, aligned, err, st);
-    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, aligned, err, st);
+    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == kDecoded3)
+      return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, dense, aligned, err, st);
+    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, false, aligned, err, st);
   }
-  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, aligned, err, st);
-  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, aligned, err, st);
-  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, aligned, err, st);
-  return launch_rank<float, 2>(a, rank, stage, bulk, aligned, err, st);
+  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, dense, aligned, err, st);
+  return launch_rank<float, 2>(a, rank, stage, bulk, false, aligned, err, st);
 }
 
 alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, int rank, float* out, DetItem* item,
@@ -1232,7 +1236,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       int feed;
     };
     const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
-                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}};
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;
@@ -1240,6 +1244,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       const alto_mttkrp_variant v = c.v;
       if (v == ALTO_MTTKRP_STAGED && stageable_fraction(t, m, rank) == 0.0) continue;
       if (v == ALTO_MTTKRP_SORTED && t->nnz / std::max<uint64_t>(t->dims[m], 1) < 2) continue;
+      if (c.feed == 2 && t->nmodes != 3) continue;  // (decoded 3-mode copies only)
       status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);  // warm / build
       if (status != ALTO_OK) break;
       cudaEventRecord(e0, st);
@@ -1258,7 +1263,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
         best_feed = c.feed;
       }
     }
-    t->tuned.push_back({m, rank, (int)fdtype, best, best_feed == 1});
+    t->tuned.push_back({m, rank, (int)fdtype, best, best_feed});
     if (chosen) chosen[m] = best;
   }
   cudaEventDestroy(e0);

@@ -61,6 +61,10 @@ typedef enum {
  * SORTED): stream the line through shared memory with bulk copies
  * (cp.async.bulk, double buffered) instead of loading it directly. */
 #define ALTO_MTTKRP_FEED_BULK 0x100
+/* OR-ed into SORTED on a 3-mode tensor: the row-sorted walk compiled for
+ * five resident blocks per SM (at most 48 registers a thread) instead of
+ * four (the autotuner tries it). */
+#define ALTO_MTTKRP_FEED_DENSE 0x200
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */
