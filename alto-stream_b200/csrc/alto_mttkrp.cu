@@ -948,10 +948,11 @@ bool deterministic_supported(int rank, alto_dtype fdtype) {
 }
 
 template <int R, typename FT, int HW>
-static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, bool dense, int* err,
+static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int dense, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
-    if (dense && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
+    if (dense == 1 && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
+    if (dense == 2 && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 6>(a, st);
     return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
   } else {
 #define NM_CASE(NN)                                                                   \
@@ -971,7 +972,7 @@ static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed,
 }
 
 template <typename FT, int HW>
-static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, bool dense,
+static alto_status launch_rank(const MttkrpArgs& a, int rank, bool stage, bool bulk_feed, int dense,
                                bool aligned, int* err, cudaStream_t st) {
   if (aligned) {
 #define RANK_CASE(RR) \
@@ -1032,9 +1033,9 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 }
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
-// directly, 2 loads it directly with five blocks per SM (decoded 3-mode
-// copies: at most 48 registers a thread), -1 uses the autotuned choice
-// (direct when untuned).
+// directly, 2 / 3 load it directly with five / six blocks per SM (decoded
+// 3-mode copies: at most 48 / 40 registers a thread), -1 uses the autotuned
+// choice (direct when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
@@ -1090,18 +1091,19 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
   }
   int* err = t->err.as<int>();
-  const bool bulk = feed == 1, dense = feed == 2;
+  const bool bulk = feed == 1;
+  const int dense = feed == 2 ? 1 : (feed == 3 ? 2 : 0);
   if (fdtype == ALTO_BF16) {
-    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, false, aligned, err, st);
-    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, false, aligned, err, st);
+    if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, 0, aligned, err, st);
+    if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, 0, aligned, err, st);
     if (hw == kDecoded3)
       return launch_rank<__nv_bfloat16, kDecoded3>(a, rank, false, bulk, dense, aligned, err, st);
-    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, false, aligned, err, st);
+    return launch_rank<__nv_bfloat16, 2>(a, rank, stage, bulk, 0, aligned, err, st);
   }
-  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, false, aligned, err, st);
-  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, false, aligned, err, st);
+  if (hw == 0) return launch_rank<float, 0>(a, rank, stage, bulk, 0, aligned, err, st);
+  if (hw == 1) return launch_rank<float, 1>(a, rank, stage, bulk, 0, aligned, err, st);
   if (hw == kDecoded3) return launch_rank<float, kDecoded3>(a, rank, false, bulk, dense, aligned, err, st);
-  return launch_rank<float, 2>(a, rank, stage, bulk, false, aligned, err, st);
+  return launch_rank<float, 2>(a, rank, stage, bulk, 0, aligned, err, st);
 }
 
 alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, int rank, float* out, DetItem* item,
@@ -1236,7 +1238,8 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       int feed;
     };
     const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
-                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2}};
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2},
+                          {ALTO_MTTKRP_SORTED, 3}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;
@@ -1244,7 +1247,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       const alto_mttkrp_variant v = c.v;
       if (v == ALTO_MTTKRP_STAGED && stageable_fraction(t, m, rank) == 0.0) continue;
       if (v == ALTO_MTTKRP_SORTED && t->nnz / std::max<uint64_t>(t->dims[m], 1) < 2) continue;
-      if (c.feed == 2 && t->nmodes != 3) continue;  // (decoded 3-mode copies only)
+      if (c.feed >= 2 && t->nmodes != 3) continue;  // (decoded 3-mode copies only)
       status = run_mttkrp_feed(t, m, factors, fdtype, rank, out.as<float>(), 0, v, c.feed, st);  // warm / build
       if (status != ALTO_OK) break;
       cudaEventRecord(e0, st);

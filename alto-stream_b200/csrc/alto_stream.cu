@@ -377,6 +377,321 @@ __global__ void __launch_bounds__(kAdmmThreads)
                                     in_graph, blockIdx.x, gridDim.x);
 }
 
+// ------------------------------------------------ tiled row solves
+//
+// The row solves of a mode as small matrix products (ranks 8, 16, 32, 64):
+// a block takes a tile of T = 2048 / R rows; thread (rg, cg) holds rows
+// 2rg, 2rg + 1 and columns 4cg .. 4cg + 3 of every per-row quantity in
+// registers, and each row-times-matrix product stages the tile's input rows
+// in shared memory (row stride R + 1 doubles: conflict-free) and forms each
+// output with fused multiply-adds in k order -- the sequence of row_solve,
+// so every row's result is the one row_solve gives, without its shuffles.
+template <int R>
+struct TileMap {
+  static constexpr int CG = R / 4;                 // column groups
+  static constexpr int RGS = kAdmmThreads / CG;    // row groups
+  static constexpr int T = 2 * RGS;                // rows per tile
+  static constexpr int LD = R + 1;                 // padded row stride
+  static constexpr size_t smem_bytes() { return (2 * R * R + (size_t)T * LD) * sizeof(double); }
+};
+
+template <int R>
+uint64_t tile_blocks(uint64_t I, uint64_t cap) {
+  const uint64_t b = std::min<uint64_t>((I + TileMap<R>::T - 1) / TileMap<R>::T, cap);
+  return std::max<uint64_t>(b, 1);
+}
+
+// x[i][j] = sum_k in[r0 + i][k] M[k][c0 + j], k ascending.
+template <int R>
+__device__ __forceinline__ void tile_product(const double* __restrict__ in, const double* __restrict__ M, int r0,
+                                             int c0, double (&x)[2][4]) {
+  constexpr int LD = TileMap<R>::LD;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[i][j] = 0.0;
+#pragma unroll 8
+  for (int k = 0; k < R; ++k) {
+    const double a0 = in[r0 * LD + k], a1 = in[(r0 + 1) * LD + k];
+    const double2 w01 = *reinterpret_cast<const double2*>(M + k * R + c0);
+    const double2 w23 = *reinterpret_cast<const double2*>(M + k * R + c0 + 2);
+    x[0][0] = __fma_rn(a0, w01.x, x[0][0]);
+    x[0][1] = __fma_rn(a0, w01.y, x[0][1]);
+    x[0][2] = __fma_rn(a0, w23.x, x[0][2]);
+    x[0][3] = __fma_rn(a0, w23.y, x[0][3]);
+    x[1][0] = __fma_rn(a1, w01.x, x[1][0]);
+    x[1][1] = __fma_rn(a1, w01.y, x[1][1]);
+    x[1][2] = __fma_rn(a1, w23.x, x[1][2]);
+    x[1][3] = __fma_rn(a1, w23.y, x[1][3]);
+  }
+}
+
+// Stage v (this thread's 2 x 4 block) into the tile's rows, multiply by M,
+// and return the product in x (barriers on both sides).
+template <int R>
+__device__ __forceinline__ void tile_stage_product(double* in, const double* M, int r0, int c0,
+                                                   const double (&v)[2][4], double (&x)[2][4]) {
+  constexpr int LD = TileMap<R>::LD;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) in[(r0 + i) * LD + c0 + j] = v[i][j];
+  __syncthreads();
+  tile_product<R>(in, M, r0, c0, x);
+  __syncthreads();
+}
+
+// Right-hand sides of a tile's rows: h = prev_U_j[i] A + mttkrp[i] (row_rhs).
+template <int R>
+__device__ __forceinline__ void tile_rhs(const float* __restrict__ P32, const float* __restrict__ B32, double* in,
+                                         const double* sA, uint64_t t0, uint64_t I, int r0, int c0,
+                                         double (&h)[2][4]) {
+  double p[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const uint64_t row = t0 + r0 + i;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) p[i][j] = row < I ? (double)P32[row * R + c0 + j] : 0.0;
+  }
+  tile_stage_product<R>(in, sA, r0, c0, p, h);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const uint64_t row = t0 + r0 + i;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) h[i][j] = __dadd_rn(h[i][j], row < I ? (double)B32[row * R + c0 + j] : 0.0);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void tile_load_mats(double* smem, const double* __restrict__ A,
+                                               const double* __restrict__ W) {
+  for (int p = threadIdx.x; p < R * R; p += blockDim.x) {
+    smem[p] = W[p];
+    smem[R * R + p] = A[p];
+  }
+  __syncthreads();
+}
+
+// Unconstrained solve of mode j, tiled: U_j[i] = (prev_U_j[i] A + mttkrp[i]) W.
+template <int R>
+__device__ __forceinline__ void solve_tile_body(const float* __restrict__ P32, const float* __restrict__ B32,
+                                                const double* __restrict__ A, const double* __restrict__ W,
+                                                uint64_t I, float* __restrict__ U32, uint32_t block,
+                                                uint32_t nblocks) {
+  using TM = TileMap<R>;
+  extern __shared__ double smem[];
+  double* sW = smem;
+  double* sA = smem + R * R;
+  double* in = smem + 2 * R * R;
+  tile_load_mats<R>(smem, A, W);
+  const int cg = threadIdx.x % TM::CG, rg = threadIdx.x / TM::CG;
+  const int r0 = 2 * rg, c0 = 4 * cg;
+  for (uint64_t t0 = (uint64_t)block * TM::T; t0 < I; t0 += (uint64_t)nblocks * TM::T) {
+    double h[2][4], x[2][4];
+    tile_rhs<R>(P32, B32, in, sA, t0, I, r0, c0, h);
+    tile_stage_product<R>(in, sW, r0, c0, h, x);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const uint64_t row = t0 + r0 + i;
+      if (row < I)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) U32[row * R + c0 + j] = (float)x[i][j];
+    }
+  }
+  __syncthreads();
+}
+
+template <int R>
+__global__ void __launch_bounds__(kAdmmThreads)
+    solve_tile_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                      const double* __restrict__ W, uint64_t I, float* __restrict__ U32) {
+  solve_tile_body<R>(P32, B32, A, W, I, U32, blockIdx.x, gridDim.x);
+}
+
+// One ADMM pass of mode j, tiled (the passes, the decision and the state
+// are those of admm_rows_kernel; see there).
+template <int R, bool PASS1>
+__device__ __forceinline__ void admm_tile_body(const float* __restrict__ P32, const float* __restrict__ B32,
+                                               const double* __restrict__ A, float* __restrict__ U32,
+                                               double* __restrict__ primal, double* __restrict__ aux,
+                                               double* __restrict__ dual, const double* __restrict__ W,
+                                               const double* __restrict__ rho_p, uint64_t I,
+                                               double* __restrict__ partials, AdmmState* __restrict__ state,
+                                               double tol, cudaGraphConditionalHandle h, int in_graph,
+                                               uint32_t block, uint32_t nblocks) {
+  using TM = TileMap<R>;
+  constexpr int NW = kAdmmThreads / 32;
+  if (PASS1 && state->stop) {  // a chunk after the stop (launched directly): nothing stands
+    if (block == 0 && threadIdx.x == 0) state->chunk_sweeps = 0;
+    return;
+  }
+  if (!PASS1 && state->chunk_sweeps == 0) return;
+  const int start = PASS1 ? state->iters : state->chunk_start;
+  const int nsweeps = PASS1 ? min(kAdmmChunk, kAdmmMaxIters - start) : state->chunk_sweeps;
+  const bool first = start == 0;
+  extern __shared__ double smem[];
+  double* sW = smem;
+  double* sA = smem + R * R;
+  double* in = smem + 2 * R * R;
+  __shared__ double wsum[kAdmmSums];
+  __shared__ double red[NW][4];
+  if (PASS1)
+    for (int p = threadIdx.x; p < kAdmmSums; p += blockDim.x) wsum[p] = 0.0;
+  tile_load_mats<R>(smem, A, W);
+  const double rho = *rho_p;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cg = threadIdx.x % TM::CG, rg = threadIdx.x / TM::CG;
+  const int r0 = 2 * rg, c0 = 4 * cg;
+  for (uint64_t t0 = (uint64_t)block * TM::T; t0 < I; t0 += (uint64_t)nblocks * TM::T) {
+    double H[2][4], X[2][4], Z[2][4], U[2][4], X0[2][4], a[2][4], z[2][4];
+    tile_rhs<R>(P32, B32, in, sA, t0, I, r0, c0, H);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const uint64_t row = t0 + r0 + i;
+      const bool ok = row < I;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint64_t e = row * R + c0 + j;
+        X[i][j] = ok ? (first ? (double)U32[e] : primal[e]) : 0.0;
+        U[i][j] = ok ? dual[e] : 0.0;
+        Z[i][j] = ok && !first ? aux[e] : 0.0;
+        X0[i][j] = X[i][j];
+        // first update (src/admm.cpp:288-327): z = (rhs + rho (x + u)) W
+        a[i][j] = __fma_rn(rho, __dadd_rn(X[i][j], U[i][j]), H[i][j]);
+      }
+    }
+    if (first) {
+      tile_stage_product<R>(in, sW, r0, c0, a, z);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          Z[i][j] = z[i][j];
+          const double v = __dsub_rn(z[i][j], U[i][j]);
+          X[i][j] = v < 0.0 ? 0.0 : v;
+        }
+    }
+    for (int k = 0; k < nsweeps; ++k) {
+      double p_res = 0, d_res = 0, p_norm = 0, d_norm = 0;
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double xv = X[i][j];
+          if (PASS1) {
+            if (first && k == 0) {
+              const double dd = __dsub_rn(xv, X0[i][j]);
+              d_res = __fma_rn(dd, dd, d_res);
+            }
+            p_norm = __fma_rn(xv, xv, p_norm);
+          }
+          const double y = __dsub_rn(xv, Z[i][j]);
+          const double di = __dadd_rn(U[i][j], y);
+          U[i][j] = di;
+          if (PASS1) {
+            d_norm = __fma_rn(di, di, d_norm);
+            p_res = __fma_rn(y, y, p_res);
+          }
+          a[i][j] = __fma_rn(rho, __dadd_rn(xv, di), H[i][j]);
+        }
+      tile_stage_product<R>(in, sW, r0, c0, a, z);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          Z[i][j] = z[i][j];
+          const double v = __dsub_rn(z[i][j], U[i][j]);
+          X[i][j] = v < 0.0 ? 0.0 : v;
+        }
+      if (PASS1) {  // the tile's four sums: lanes, then warps in order, added per tile
+        double v4[4] = {p_res, d_res, p_norm, d_norm};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          for (int o = 16; o; o >>= 1) v4[q] += __shfl_xor_sync(0xffffffffu, v4[q], o);
+          if (lane == 0) red[warp][q] = v4[q];
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+          double t = 0.0;
+          for (int w = 0; w < NW; ++w) t += red[w][threadIdx.x];
+          wsum[k * 4 + threadIdx.x] += t;
+        }
+        __syncthreads();
+      }
+    }
+    if (!PASS1) {
+      const bool final_chunk = state->stop != 0;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const uint64_t row = t0 + r0 + i;
+        if (row >= I) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint64_t e = row * R + c0 + j;
+          dual[e] = U[i][j];
+          if (final_chunk) {
+            U32[e] = (float)X[i][j];
+          } else {
+            primal[e] = X[i][j];
+            aux[e] = Z[i][j];
+          }
+        }
+      }
+    }
+  }
+  if (PASS1) {
+    __syncthreads();
+    for (int p = threadIdx.x; p < kAdmmSums; p += blockDim.x) partials[(size_t)block * kAdmmSums + p] = wsum[p];
+    // the last block to finish adds the blocks' sums (warp per sum, lanes
+    // over blocks in order, fixed butterfly) and takes the chunk's sweep
+    // count: the first sweep whose sums pass the test, else the whole chunk
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&state->ticket, 1u) == nblocks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double S[kAdmmSums];
+    for (int p = warp; p < kAdmmSums; p += NW) {
+      double t = 0.0;
+      for (unsigned b = lane; b < nblocks; b += 32) t += __ldcg(partials + (size_t)b * kAdmmSums + p);
+      for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) S[p] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int n = min(kAdmmChunk, kAdmmMaxIters - start);
+      int kk = n, conv = 0;
+      for (int j = 0; j < n; ++j)
+        if (S[j * 4 + 0] <= tol * S[j * 4 + 2] && S[j * 4 + 1] <= tol * S[j * 4 + 3]) {
+          kk = j + 1;
+          conv = 1;
+          break;
+        }
+      state->ticket = 0;
+      state->chunk_start = start;
+      state->chunk_sweeps = kk;
+      state->iters = start + kk;
+      state->converged = conv;
+      state->stop = conv || start + kk >= kAdmmMaxIters;
+      __threadfence();
+      set_condition(h, in_graph, !state->stop);
+    }
+  }
+}
+
+template <int R, bool PASS1>
+__global__ void __launch_bounds__(kAdmmThreads)
+    admm_tile_kernel(const float* __restrict__ P32, const float* __restrict__ B32, const double* __restrict__ A,
+                     float* __restrict__ U32, double* __restrict__ primal, double* __restrict__ aux,
+                     double* __restrict__ dual, const double* __restrict__ W, const double* __restrict__ rho_p,
+                     uint64_t I, double* __restrict__ partials, AdmmState* __restrict__ state, double tol,
+                     cudaGraphConditionalHandle h, int in_graph) {
+  admm_tile_body<R, PASS1>(P32, B32, A, U32, primal, aux, dual, W, rho_p, I, partials, state, tol, h, in_graph,
+                           blockIdx.x, gridDim.x);
+}
+
 // End of an inner iteration (src/streaming_cpd.cpp:1457-1482): delta = sum
 // over the non-stream modes of ||U_j - prev_U_j|| / (||U_j|| + 1e-12) from
 // the per-mode statistics; stop once |prev_delta - delta| < epsilon after
@@ -725,17 +1040,17 @@ __global__ void __launch_bounds__(256) group_mode_prep_kernel(SlotDesc* __restri
   }
 }
 
-template <int SLOTS, int SEG>
+template <int R>
 __global__ void __launch_bounds__(kAdmmThreads)
     group_solve_kernel(const SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
-                       const uint32_t* __restrict__ off, int j, int R) {
+                       const uint32_t* __restrict__ off, int j) {
   const int K = ctl->count;
   const uint32_t total = K > 0 ? off[K] : 0;
   for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
     const int s = slot_of(off, K, v);
     const SlotDesc& d = tab[s];
     if (!d.act || d.con) continue;
-    stream_solve_body<SLOTS, SEG>(d.P[j], d.buf32, d.ata, d.W, d.dims[j], R, d.U[j], v - off[s], d.solve_blocks[j]);
+    solve_tile_body<R>(d.P[j], d.buf32, d.ata, d.W, d.dims[j], d.U[j], v - off[s], d.solve_blocks[j]);
   }
 }
 
@@ -758,19 +1073,19 @@ __global__ void group_admm_cond_kernel(SlotDesc* __restrict__ tab, GroupCtl* __r
   cudaGraphSetConditional(h, any ? 1u : 0u);
 }
 
-template <int SLOTS, int SEG, bool PASS1>
+template <int R, bool PASS1>
 __global__ void __launch_bounds__(kAdmmThreads)
     group_admm_kernel(const SlotDesc* __restrict__ tab, const GroupCtl* __restrict__ ctl,
-                      const uint32_t* __restrict__ off, int j, int R, double tol) {
+                      const uint32_t* __restrict__ off, int j, double tol) {
   const int K = ctl->count;
   const uint32_t total = K > 0 ? off[K] : 0;
   for (uint32_t v = blockIdx.x; v < total; v += gridDim.x) {
     const int s = slot_of(off, K, v);
     const SlotDesc& d = tab[s];
     if (!d.act || !d.admm_act) continue;
-    admm_rows_body<SLOTS, SEG, PASS1>(d.P[j], d.buf32, d.ata, d.U[j], d.prim, d.aux, d.dual[j], d.W, d.rho,
-                                      d.dims[j], R, d.admm_part, d.admm, tol, cudaGraphConditionalHandle{}, 0,
-                                      v - off[s], d.admm_blocks[j]);
+    admm_tile_body<R, PASS1>(d.P[j], d.buf32, d.ata, d.U[j], d.prim, d.aux, d.dual[j], d.W, d.rho, d.dims[j],
+                             d.admm_part, d.admm, tol, cudaGraphConditionalHandle{}, 0, v - off[s],
+                             d.admm_blocks[j]);
     __syncthreads();
   }
 }
@@ -954,7 +1269,66 @@ alto_status admm_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t 
   return ALTO_OK;
 }
 
+// The tiled ADMM passes (ranks 8, 16, 32, 64): launched as admm_run.
+template <int R>
+alto_status admm_tile_run(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st, const IterLaunch& L) {
+  const size_t smem = TileMap<R>::smem_bytes();
+  const uint64_t blocks = tile_blocks<R>(I, 148ull * 4);
+  ALTO_TRY(s->admm_part.ensure(blocks * kAdmmSums * sizeof(double)));
+  static bool raised = false;  // raised once per kernel, outside any capture
+  if (smem > 48 * 1024 && !raised) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_tile_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(admm_tile_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    raised = true;
+  }
+  double* primal = s->prim.as<double>();
+  double* dual = s->dual[mode].as<double>();
+  const float* P32 = s->P[mode].as<float>();
+  const float* B32 = s->buf32.as<float>();
+  const double* A = s->ata.as<double>();
+  float* U32 = s->U[mode].as<float>();
+  AdmmState* state = s->admm_state.as<AdmmState>();
+  double* part = s->admm_part.as<double>();
+  double* aux = s->aux.as<double>();
+  const double tol = (double)1e-6f;
+  const cudaGraphConditionalHandle h = L.in_graph ? L.admm[mode] : cudaGraphConditionalHandle{};
+  auto chunk = [&](cudaStream_t cs) -> alto_status {
+    admm_tile_kernel<R, true><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, part, state, tol, h,
+        L.in_graph);
+    ALTO_LAUNCHED();
+    admm_tile_kernel<R, false><<<(unsigned)blocks, kAdmmThreads, smem, cs>>>(
+        P32, B32, A, U32, primal, aux, dual, s->W.as<double>(), s->rho.as<double>(), I, part, state, tol, h,
+        L.in_graph);
+    ALTO_LAUNCHED();
+    return ALTO_OK;
+  };
+  if (!L.in_graph) {
+    for (int c = 0; c < (kAdmmMaxIters + kAdmmChunk - 1) / kAdmmChunk; ++c) ALTO_TRY(chunk(st));
+    return ALTO_OK;
+  }
+  cudaGraph_t body;
+  ALTO_TRY(capture_while(st, h, &body));
+  ALTO_TRY_CUDA(cudaStreamBeginCaptureToGraph(L.body_stream, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+  const alto_status cst = chunk(L.body_stream);
+  cudaGraph_t done = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(L.body_stream, &done);
+  ALTO_TRY(cst);
+  ALTO_TRY_CUDA(ee);
+  return ALTO_OK;
+}
+
 alto_status admm(alto_stream_session* s, uint64_t I, int mode, cudaStream_t st, const IterLaunch& L) {
+  switch (s->R) {
+    case 8: return admm_tile_run<8>(s, I, mode, st, L);
+    case 16: return admm_tile_run<16>(s, I, mode, st, L);
+    case 32: return admm_tile_run<32>(s, I, mode, st, L);
+    case 64: return admm_tile_run<64>(s, I, mode, st, L);
+    default: break;
+  }
   if (s->R <= 8) return admm_run<1, 8>(s, I, mode, st, L);
   if (s->R <= 16) return admm_run<1, 16>(s, I, mode, st, L);
   if (s->R <= 32) return admm_run<1, 32>(s, I, mode, st, L);
@@ -981,8 +1355,29 @@ alto_status solve_run(const float* P32, const float* B32, const double* A, const
 }
 
 // U32 = (P32 A + B32) W row by row (float64 arithmetic, float32 in and out).
+template <int R>
+alto_status solve_tile_run(const float* P32, const float* B32, const double* A, const double* W, uint64_t I,
+                           float* U32, cudaStream_t st) {
+  const size_t smem = TileMap<R>::smem_bytes();
+  static bool raised = false;  // raised once per kernel, outside any capture
+  if (smem > 48 * 1024 && !raised) {
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(solve_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raised = true;
+  }
+  solve_tile_kernel<R><<<(unsigned)tile_blocks<R>(I, 148ull * 8), kAdmmThreads, smem, st>>>(P32, B32, A, W, I, U32);
+  ALTO_LAUNCHED();
+  return ALTO_OK;
+}
+
 alto_status rows_solve(const float* P32, const float* B32, const double* A, const double* W, uint64_t I, int R,
                        float* U32, cudaStream_t st) {
+  switch (R) {
+    case 8: return solve_tile_run<8>(P32, B32, A, W, I, U32, st);
+    case 16: return solve_tile_run<16>(P32, B32, A, W, I, U32, st);
+    case 32: return solve_tile_run<32>(P32, B32, A, W, I, U32, st);
+    case 64: return solve_tile_run<64>(P32, B32, A, W, I, U32, st);
+    default: break;
+  }
   if (R <= 8) return solve_run<1, 8>(P32, B32, A, W, I, R, U32, st);
   if (R <= 16) return solve_run<1, 16>(P32, B32, A, W, I, R, U32, st);
   if (R <= 32) return solve_run<1, 32>(P32, B32, A, W, I, R, U32, st);
@@ -1338,26 +1733,14 @@ namespace grp {
 constexpr uint32_t kSolveGrid = 148 * 8;
 constexpr uint32_t kAdmmGrid = 148 * 4;
 
-template <int SLOTS, int SEG>
-uint32_t admm_blocks_for(uint64_t I) {
-  constexpr uint64_t rpb = (kAdmmThreads / 32) * RowMap<SEG>::kRows * AdmmBatch<SLOTS>::M;
-  uint64_t b = std::min<uint64_t>((I + rpb - 1) / rpb, kAdmmGrid);
-  return (uint32_t)std::max<uint64_t>(b, 1);
-}
-
-template <int SEG>
-uint32_t solve_blocks_for(uint64_t I) {
-  const uint64_t warps = (I + RowMap<SEG>::kRows - 1) / RowMap<SEG>::kRows;
-  uint64_t b = std::min<uint64_t>((warps * 32 + kAdmmThreads - 1) / kAdmmThreads, kSolveGrid);
-  return (uint32_t)std::max<uint64_t>(b, 1);
-}
-
-// (as admm() and rows_solve() dispatch on the rank, ranks <= 32)
+// (as admm() and rows_solve() launch the tiled kernels, ranks 8, 16, 32)
 uint32_t admm_blocks(int R, uint64_t I) {
-  return R <= 8 ? admm_blocks_for<1, 8>(I) : (R <= 16 ? admm_blocks_for<1, 16>(I) : admm_blocks_for<1, 32>(I));
+  return (uint32_t)(R == 8 ? tile_blocks<8>(I, kAdmmGrid) : (R == 16 ? tile_blocks<16>(I, kAdmmGrid)
+                                                                     : tile_blocks<32>(I, kAdmmGrid)));
 }
 uint32_t solve_blocks(int R, uint64_t I) {
-  return R <= 8 ? solve_blocks_for<8>(I) : (R <= 16 ? solve_blocks_for<16>(I) : solve_blocks_for<32>(I));
+  return (uint32_t)(R == 8 ? tile_blocks<8>(I, kSolveGrid) : (R == 16 ? tile_blocks<16>(I, kSolveGrid)
+                                                                      : tile_blocks<32>(I, kSolveGrid)));
 }
 
 uint32_t* off_of(uint32_t* base, int cap, int kind, int mode) {
@@ -1369,14 +1752,13 @@ Strided<T> strided(const StreamGroup* g, size_t field_offset) {
   return Strided<T>{g->tab.as<char>() + field_offset, sizeof(SlotDesc), &g->ctl.as<GroupCtl>()->count};
 }
 
-template <int SLOTS, int SEG>
+template <int R>
 alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGraphConditionalHandle h) {
-  const size_t smem = (size_t)g->R * g->R * sizeof(double);
+  const size_t smem = TileMap<R>::smem_bytes();
   SlotDesc* tab = g->tab.as<SlotDesc>();
   GroupCtl* ctl = g->ctl.as<GroupCtl>();
   uint32_t* offs = g->offs.as<uint32_t>();
-  group_solve_kernel<SLOTS, SEG><<<kSolveGrid, kAdmmThreads, smem, cs>>>(tab, ctl, off_of(offs, g->cap, kOffSolve, j), j,
-                                                                       g->R);
+  group_solve_kernel<R><<<kSolveGrid, kAdmmThreads, smem, cs>>>(tab, ctl, off_of(offs, g->cap, kOffSolve, j), j);
   ALTO_LAUNCHED();
   // while some slot's ADMM of mode j sweeps: one chunk (pass 1, pass 2)
   group_admm_cond_kernel<<<1, 32, 0, cs>>>(tab, ctl, h, 1);
@@ -1387,8 +1769,8 @@ alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGrap
                                               cudaStreamCaptureModeThreadLocal));
   const double tol = (double)1e-6f;
   const uint32_t* ao = off_of(offs, g->cap, kOffAdmm, j);
-  group_admm_kernel<SLOTS, SEG, true><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
-  group_admm_kernel<SLOTS, SEG, false><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, g->R, tol);
+  group_admm_kernel<R, true><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, tol);
+  group_admm_kernel<R, false><<<kAdmmGrid, kAdmmThreads, smem, g->capst[1]>>>(tab, ctl, ao, j, tol);
   group_admm_cond_kernel<<<1, 32, 0, g->capst[1]>>>(tab, ctl, h, 0);
   const cudaError_t le = cudaGetLastError();
   cudaGraph_t done = nullptr;
@@ -1399,9 +1781,9 @@ alto_status capture_mode_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGrap
 }
 
 alto_status capture_solves(StreamGroup* g, cudaStream_t cs, int j, cudaGraphConditionalHandle h) {
-  if (g->R <= 8) return capture_mode_solves<1, 8>(g, cs, j, h);
-  if (g->R <= 16) return capture_mode_solves<1, 16>(g, cs, j, h);
-  return capture_mode_solves<1, 32>(g, cs, j, h);
+  if (g->R == 8) return capture_mode_solves<8>(g, cs, j, h);
+  if (g->R == 16) return capture_mode_solves<16>(g, cs, j, h);
+  return capture_mode_solves<32>(g, cs, j, h);
 }
 
 // One inner iteration of every acting slot (the body of the step loop).
