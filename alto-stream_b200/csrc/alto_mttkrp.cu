@@ -951,8 +951,7 @@ template <int R, typename FT, int HW>
 static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int dense, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
-    if (dense == 1 && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
-    if (dense == 2 && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 6>(a, st);
+    if (dense && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
     return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
   } else {
 #define NM_CASE(NN)                                                                   \
@@ -1033,9 +1032,9 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 }
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
-// directly, 2 / 3 load it directly with five / six blocks per SM (decoded
-// 3-mode copies: at most 48 / 40 registers a thread), -1 uses the autotuned
-// choice (direct when untuned).
+// directly, 2 loads it directly with five blocks per SM (decoded 3-mode
+// copies: at most 48 registers a thread; six, at 40, measured slower), -1
+// uses the autotuned choice (direct when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
@@ -1092,7 +1091,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   }
   int* err = t->err.as<int>();
   const bool bulk = feed == 1;
-  const int dense = feed == 2 ? 1 : (feed == 3 ? 2 : 0);
+  const int dense = feed == 2 ? 1 : 0;
   if (fdtype == ALTO_BF16) {
     if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, 0, aligned, err, st);
     if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, 0, aligned, err, st);
@@ -1238,8 +1237,7 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       int feed;
     };
     const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
-                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2},
-                          {ALTO_MTTKRP_SORTED, 3}};
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;

@@ -796,7 +796,8 @@ def serve_setup(args):
 
     from alto_b200 import synth
 
-    streams = synth.serving_streams(args.streams, args.warmup + args.steps, seed=SERVE_SEED)
+    # (each stream's slices: warm-up, the saturated phase, the sustained phase)
+    streams = synth.serving_streams(args.streams, args.warmup + 2 * args.steps, seed=SERVE_SEED)
     rng = np.random.default_rng(SERVE_SEED + 1)
     need = [sum(st["dims"][1:]) * st["rank"] for st in streams]
     pool = rng.uniform(0.0, 3.0, max(need) + 1024) * np.where(rng.random(max(need) + 1024) < 0.5, -1.0, 1.0)
@@ -908,6 +909,25 @@ def ours_serve(args):
     st1 = srv.stats()
     same = all(np.array_equal(srv.factor(sids[k], m), plain_out[k][i]) for k in check
                for i, m in enumerate((1, 2, 3)))
+    # sustained phase: the next slices of every stream at 60% of the rate the
+    # saturated phase sustained (each rank at its share), so latency is the
+    # update's own and not a queue's
+    rate2 = 0.6 * len(order) / served_s
+    rng2 = np.random.default_rng(SERVE_SEED + 2)
+    order2 = np.repeat(np.asarray(mine), K)
+    rng2.shuffle(order2)
+    arrive2 = np.cumsum(rng2.exponential(1.0 / rate2, len(order2)))
+    tickets2 = []
+    t0 = time.perf_counter()
+    for k, ta in zip(order2, arrive2):
+        while time.perf_counter() - t0 < ta:
+            pass
+        b = streams[k]["slices"][nxt[k]]
+        tickets2.append(srv.submit(sids[k], b["dims"], b["cidx"], b["vals"]))
+        nxt[k] += 1
+    srv.drain()
+    sustained_s = time.perf_counter() - t0
+    lat2 = [srv.wait(t)[1] for t in tickets2]
     srv.destroy()
 
     # whole job: every rank's slices over the slowest rank's time
@@ -922,9 +942,12 @@ def ours_serve(args):
         import torch.distributed as dist
 
         parts = [None] * world
-        dist.all_gather_object(parts, (lat, iso))
+        dist.all_gather_object(parts, (lat, iso, lat2, rate2, len(order2), sustained_s))
         lat = [x for p in parts for x in p[0]]
         iso = [x for p in parts for x in p[1]]
+        lat2 = [x for p in parts for x in p[2]]
+        rate2 = sum(p[3] for p in parts)
+        sustained_rate = sum(p[4] for p in parts) / max(p[5] for p in parts)
         dist.barrier()
         dist.destroy_process_group()
         if rank != 0:
@@ -932,6 +955,8 @@ def ours_serve(args):
     value = n / served_s
     plain_rate = n / plain_s
     p99_iso = float(np.percentile(iso, 99))
+    if world == 1:
+        sustained_rate = len(order2) / sustained_s
     line = {
         "metric": SERVE_METRIC + (" [spCP-stream model]" if args.model == "spcpstream" else ""),
         "value": value, "unit": "slices/s", "n_gpus": world, "steps": n, "warmup": W * len(streams),
@@ -946,6 +971,12 @@ def ours_serve(args):
                    "plain_slices_per_s": plain_rate, "speedup_vs_plain": value / plain_rate,
                    "isolated_p50_ms": float(np.percentile(iso, 50)), "isolated_p99_ms": p99_iso,
                    "p99_vs_isolated_p99": float(np.percentile(lat, 99)) / p99_iso,
+                   "sustained": {"arrival_rate": rate2, "slices_per_s": sustained_rate,
+                                 "speedup_vs_plain": sustained_rate / plain_rate,
+                                 "p50_ms": float(np.percentile(lat2, 50)), "p99_ms": float(np.percentile(lat2, 99)),
+                                 "p99_vs_isolated_p99": float(np.percentile(lat2, 99)) / p99_iso,
+                                 "note": "the next slices of every stream arriving at 60% of the saturated "
+                                         "phase's throughput (Poisson)"},
                    "results_identical_to_plain": bool(same), "checked_streams": len(check) * world,
                    "reserved_bytes": st1["reserved_bytes"], "admitted_streams": st1["admitted_streams"],
                    "warmup_completed": st0["completed"],

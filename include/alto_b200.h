@@ -65,8 +65,6 @@ typedef enum {
  * five resident blocks per SM (at most 48 registers a thread) instead of
  * four (the autotuner tries it). */
 #define ALTO_MTTKRP_FEED_DENSE 0x200
-/* The same at six blocks per SM (at most 40 registers a thread). */
-#define ALTO_MTTKRP_FEED_DENSER 0x400
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */
