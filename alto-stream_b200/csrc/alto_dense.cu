@@ -517,25 +517,34 @@ __global__ void solve_setup_kernel(const double* __restrict__ grams, int nmodes,
   }
 }
 
-// The same set-up for R <= RMAX <= 32 in one warp: solve_setup_kernel's
-// steps and operation order (so identical results), with the loops bounded
-// by RMAX and unrolled so the dot products' shared-memory loads overlap.
+// The same set-up with one thread per element of the R x R matrix (R <= 32,
+// blockDim = R * R): a right-looking Cholesky (column j scaled by its
+// diagonal, then the trailing lower triangle updated by the rank-one term),
+// the inverse of L by a right-looking forward substitution of all columns
+// at once, and W = L^-T L^-1.  Every element sees the operations of the
+// column-by-column form in the same order (its subtractions in k order,
+// then its division), as fused multiply-adds; R barriers per phase instead
+// of R^2 dependent steps in one warp.
 template <int RMAX>
-__device__ __forceinline__ void solve_setup_small_body(const double* __restrict__ grams, int nmodes, unsigned mask,
+__device__ __forceinline__ void solve_setup_block_body(const double* __restrict__ grams, int nmodes, unsigned mask,
                                                        int R, int kind, double ridge, double* __restrict__ W,
                                                        int* __restrict__ status, double* __restrict__ rho_out) {
   __shared__ double A[RMAX * RMAX];
+  __shared__ double X[RMAX * RMAX];
   __shared__ double s_rho;
   __shared__ int s_info;
   const int RR = R * R;
   const int tid = threadIdx.x;
-  for (int p = tid; p < RR; p += 32) {
+  const bool mine = tid < RR;
+  const int a = mine ? tid / R : 0, b = mine ? tid % R : 0;  // row, column
+  if (mine) {
     double v = 1.0;
     for (int m = 0; m < nmodes; ++m)
-      if (mask & (1u << m)) v *= grams[(size_t)m * RR + p];
-    A[p] = v;
+      if (mask & (1u << m)) v *= grams[(size_t)m * RR + tid];
+    A[tid] = v;
+    X[tid] = a == b ? 1.0 : 0.0;
   }
-  __syncwarp();
+  __syncthreads();
   if (tid == 0) {
     double add = ridge;
     if (kind == kSolveAdmm) {
@@ -546,114 +555,89 @@ __device__ __forceinline__ void solve_setup_small_body(const double* __restrict_
     s_rho = add;
     s_info = 0;
   }
-  __syncwarp();
-  if (kind == kSolveRidgeDiagFallback && tid < R) W[tid * R + tid] = A[tid * R + tid];
-  if (tid < R) A[tid * R + tid] += s_rho;
-  __syncwarp();
+  __syncthreads();
+  if (kind == kSolveRidgeDiagFallback && mine && a == b) W[tid] = A[tid];
+  if (mine && a == b) A[tid] += s_rho;
+  __syncthreads();
   for (int j = 0; j < R; ++j) {
     if (tid == 0) {
       double d = A[j * R + j];
-#pragma unroll
-      for (int k = 0; k < RMAX; ++k)
-        if (k < j) d -= A[j * R + k] * A[j * R + k];
       if (!(d > 0.0)) {
         if (!s_info) s_info = j + 1;
         d = 1.0;
       }
       A[j * R + j] = sqrt(d);
     }
-    __syncwarp();
-    const double djj = A[j * R + j];
-    const int i = j + 1 + tid;
-    if (i < R) {
-      double sv = A[j * R + i];
-#pragma unroll
-      for (int k = 0; k < RMAX; ++k)
-        if (k < j) sv -= A[i * R + k] * A[j * R + k];
-      A[i * R + j] = sv / djj;
-    }
-    __syncwarp();
+    __syncthreads();
+    if (mine && b == j && a > j) A[tid] = A[tid] / A[j * R + j];
+    __syncthreads();
+    if (mine && b > j && a >= b) A[tid] = __fma_rn(-A[a * R + j], A[b * R + j], A[tid]);
+    __syncthreads();
   }
   const int info = s_info;
   if (info) {
-    for (int p = tid; p < RR; p += 32) {
-      const int a = p / R, b = p % R;
+    if (mine) {
       if (kind == kSolveRidgeDiagFallback) {
-        if (a != b) W[p] = 0.0;
+        if (a != b) W[tid] = 0.0;
       } else {
-        W[p] = (kind == kSolveRidgeKeep && a == b) ? 1.0 : 0.0;
+        W[tid] = (kind == kSolveRidgeKeep && a == b) ? 1.0 : 0.0;
       }
     }
-    __syncwarp();
-    if (kind == kSolveRidgeDiagFallback && tid < R) {
-      const double d = W[tid * R + tid];
-      W[tid * R + tid] = d != 0.0 ? 1.0 / d : 0.0;
+    __syncthreads();
+    if (kind == kSolveRidgeDiagFallback && mine && a == b) {
+      const double d = W[tid];
+      W[tid] = d != 0.0 ? 1.0 / d : 0.0;
     }
   } else {
-    if (tid < R) {
-      const int c = tid;
-      double x[RMAX];
-#pragma unroll
-      for (int i = 0; i < RMAX; ++i) {
-        if (i < c || i >= R) {
-          x[i] = 0.0;
-          continue;
-        }
-        double sv = (i == c) ? 1.0 : 0.0;
-#pragma unroll
-        for (int k = 0; k < RMAX; ++k)
-          if (k >= c && k < i) sv -= A[i * R + k] * x[k];
-        x[i] = sv / A[i * R + i];
-      }
-      __syncwarp(0xffffffffu >> (32 - R));
-      // L^{-1} column c into A's lower triangle
-#pragma unroll
-      for (int i = 0; i < RMAX; ++i)
-        if (i >= c && i < R) A[i * R + c] = x[i];
+    // X = L^-1 (lower): row k divided by L_kk once every earlier row has
+    // been subtracted from it, then subtracted from the rows below
+    for (int k = 0; k < R; ++k) {
+      if (mine && a == k && b <= k) X[tid] = X[tid] / A[k * R + k];
+      __syncthreads();
+      if (mine && a > k && b <= k) X[tid] = __fma_rn(-A[a * R + k], X[k * R + b], X[tid]);
+      __syncthreads();
     }
-    __syncwarp();
-    for (int p = tid; p < RR; p += 32) {
-      const int a = p / R, b = p % R;
+    if (mine) {
       const int k0 = a > b ? a : b;
       double sv = 0.0;
-      for (int k = k0; k < R; ++k) sv += A[k * R + a] * A[k * R + b];
-      W[p] = sv;
+      for (int k = k0; k < R; ++k) sv = __fma_rn(X[k * R + a], X[k * R + b], sv);
+      W[tid] = sv;
     }
   }
   if (tid == 0) {
     status[0] = info;
     if (rho_out) rho_out[0] = s_rho;
   }
-  __syncwarp();
+  __syncthreads();
 }
 
 template <int RMAX>
-__global__ void __launch_bounds__(32)
-    solve_setup_small_kernel(const double* __restrict__ grams, int nmodes, unsigned mask, int R, int kind,
+__global__ void __launch_bounds__(RMAX * RMAX)
+    solve_setup_block_kernel(const double* __restrict__ grams, int nmodes, unsigned mask, int R, int kind,
                              double ridge, double* __restrict__ W, int* __restrict__ status,
                              double* __restrict__ rho_out) {
-  solve_setup_small_body<RMAX>(grams, nmodes, mask, R, kind, ridge, W, status, rho_out);
+  solve_setup_block_body<RMAX>(grams, nmodes, mask, R, kind, ridge, W, status, rho_out);
 }
 
-// One warp-sized CTA per item in turn (R <= 32).
+// One CTA of R * R threads per item in turn (R <= 32).
 template <int RMAX>
-__global__ void __launch_bounds__(32) setup_group_kernel(Strided<SetupItem> items, int R) {
+__global__ void __launch_bounds__(RMAX * RMAX) setup_group_kernel(Strided<SetupItem> items, int R) {
   const int K = *items.count;
   for (int s = blockIdx.x; s < K; s += gridDim.x) {
     const SetupItem& it = items[s];
     if (it.active && !*it.active) continue;
-    solve_setup_small_body<RMAX>(it.grams, it.nmodes, it.mask, R, it.kind, it.ridge, it.W, it.status, it.rho);
+    solve_setup_block_body<RMAX>(it.grams, it.nmodes, it.mask, R, it.kind, it.ridge, it.W, it.status, it.rho);
   }
 }
 
 alto_status setup_group_launch(Strided<SetupItem> items, int max_items, int R, cudaStream_t st) {
   const unsigned grid = (unsigned)std::max(1, std::min(max_items, 1024));
   if (R <= 8)
-    setup_group_kernel<8><<<grid, 32, 0, st>>>(items, R);
+    setup_group_kernel<8><<<grid, R * R, 0, st>>>(items, R);
   else if (R <= 16)
-    setup_group_kernel<16><<<grid, 32, 0, st>>>(items, R);
+    setup_group_kernel<16><<<grid, R * R, 0, st>>>(items, R);
   else if (R <= 32)
-    setup_group_kernel<32><<<grid, 32, 0, st>>>(items, R);
+    setup_group_kernel<32><<<grid, R * R, 0, st>>>(items, R);
   else {
     set_error("grouped solve set-up takes rank <= 32 (got %d)", R);
     return ALTO_ERR_UNSUPPORTED;
@@ -666,11 +650,11 @@ alto_status solve_setup(const double* grams, int nmodes, unsigned mask, int R, i
                         double ridge, double* W, int* status, double* rho, cudaStream_t st) {
   if (R <= 32) {
     if (R <= 8)
-      solve_setup_small_kernel<8><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+      solve_setup_block_kernel<8><<<1, R * R, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
     else if (R <= 16)
-      solve_setup_small_kernel<16><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+      solve_setup_block_kernel<16><<<1, R * R, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
     else
-      solve_setup_small_kernel<32><<<1, 32, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
+      solve_setup_block_kernel<32><<<1, R * R, 0, st>>>(grams, nmodes, mask, R, kind, ridge, W, status, rho);
     ALTO_LAUNCHED();
     return ALTO_OK;
   }
