@@ -183,6 +183,12 @@ class ClockSampler:
             self.th.start()
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver and NVML initialisation) stays out of
+        # the timed region: wait for its first sample, 10 s at most
+        deadline = time.time() + 10
+        while not self.rows and self.proc.poll() is None and time.time() < deadline:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -414,6 +420,7 @@ def ours(args):
     from alto_b200 import shard
 
     sharded = world > 1 and not args.independent
+    encode = None
     seed = 1234 if (sharded or world == 1) else 1234 + rank
     cidx, vals = synth.zipf_coo_device(DIMS, nnz, ZIPF, seed=seed, values="lognormal", device=dev)
     total_nnz = int(cidx.shape[1])
@@ -429,7 +436,20 @@ def ours(args):
         del cidx, vals
         t = tens[0]
     else:
+        # the ALTO encode of the whole tensor (device COO in, line out), timed
+        # after a 1M-nonzero encode has loaded the encoder's kernels
+        A.AltoTensor(DIMS, cidx[:, :1_000_000].contiguous(), vals[:1_000_000].contiguous(), nprtn=1).close()
+        torch.cuda.synchronize()
+        te0 = time.perf_counter()
         t = A.AltoTensor(DIMS, cidx, vals, nprtn=1)
+        torch.cuda.synchronize()
+        encode_s = time.perf_counter() - te0
+        # algorithmic bytes: the COO read once (int64 coordinates, float32
+        # values), the line written once (key words + value)
+        encode_bytes = total_nnz * (8 * N + 4 + line_bytes_per_nnz(t.alto_bits))
+        encode = {"ms": round(encode_s * 1e3, 2), "nnz_per_s": total_nnz / encode_s,
+                  "algorithmic_gbs": encode_bytes / encode_s / 1e9,
+                  "timing": "host clock around the call with device syncs; includes its allocations"}
         tens = [t] * N
     nnz = t.nnz
     torch.cuda.empty_cache()
@@ -602,6 +622,7 @@ def ours(args):
                            "order": "per mode: output row, then the row of the shorter other mode, then "
                                     "ALTO order; built once, outside the timed region"},
                        "alto_line_atomic_ms_per_mode": line_ms,
+                       "alto_encode": encode,
                        "device_bytes": sum(x.device_bytes() for x in set(tens))},
             "error_vs_fp64": err,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -769,8 +790,10 @@ def ours_cpstream(args):
                    "slice_nnz_mean": float(np.mean([len(b["vals"]) for b in batches[W:]])),
                    "inner_iters_mean": float(np.mean(inner)), "inner_iters_max": int(np.max(inner)),
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                   "latency_ms": [round(x, 2) for x in lat],
                    "launch": ("every inner iteration launched directly" if args.no_graph
-                              else "first inner iteration direct, the rest one CUDA graph per slice"),
+                              else "one captured graph per session, relaunched for every slice (a device-side "
+                                   "loop over the inner iterations)"),
                    "l2": "per-slice work streams the slice and the factors (> L2 in total over a slice); no flush"},
         "roofline": {"bound": "hbm", "achieved": nbytes / dev_total / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": nbytes / dev_total / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
