@@ -149,47 +149,99 @@ __device__ __forceinline__ uint32_t digit_of(const uint64_t* klo, const uint64_t
   return (uint32_t)(w >> (shift & 63)) & (kRadix - 1);
 }
 
-// Per-tile digit histogram, written digit-major: counts[d * ntiles + tile].
+// One-sweep LSD radix sort.  The digit counts of every pass come from one
+// read of the keys (radix_all_hist_kernel; radix_offsets_kernel turns them
+// into each digit's start in the array).  A pass is then one kernel: a block
+// takes the next tile in order (a ticket), ranks its pairs by digit,
+// publishes its per-digit counts, and finds each digit's start among the
+// preceding tiles by looking back over their published words (decoupled
+// look-back): an aggregate (that tile's count) or an inclusive prefix (the
+// count of all tiles up to it), so the walk stops at the first prefix.  Each
+// pass reads and writes the pairs once.
+constexpr int kMaxSortPasses = 16;  // 128-bit keys in 8-bit digits
+constexpr unsigned long long kLbAggregate = 1ull << 62;
+constexpr unsigned long long kLbPrefix = 2ull << 62;
+constexpr uint32_t kLookbackSpins = 1u << 22;  // polls of one word before giving up
+
+// Digit counts of every pass, ghist[pass * kRadix + digit] (atomically
+// accumulated; zeroed by the caller).  Equal digits within a warp are counted
+// by their lowest lane: the high digits of keys take few values.
 __global__ void __launch_bounds__(kSortThreads)
-    radix_hist_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
-                      uint32_t n, int shift, uint32_t ntiles, uint32_t* __restrict__ counts) {
-  __shared__ uint32_t hist[kRadix];
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0;
+    radix_all_hist_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi, uint32_t n,
+                          int npass, uint32_t* __restrict__ ghist) {
+  __shared__ uint32_t h[kMaxSortPasses * kRadix];
+  for (int q = threadIdx.x; q < npass * kRadix; q += kSortThreads) h[q] = 0;
   __syncthreads();
-  uint32_t base = blockIdx.x * kSortTile;
-#pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
-    uint32_t i = base + r * kSortThreads + threadIdx.x;
-    if (i < n) atomicAdd(&hist[digit_of(klo, khi, i, shift)], 1u);
+  const int lane = threadIdx.x & 31;
+  for (uint32_t base = blockIdx.x * kSortThreads; base < n; base += gridDim.x * kSortThreads) {
+    const uint32_t i = base + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    const uint64_t lo = valid ? klo[i] : 0, hi = (valid && khi) ? khi[i] : 0;
+    if (valid) {
+      for (int p = 0; p < npass; ++p) {
+        const int shift = p * kRadixBits;
+        const uint32_t d = (uint32_t)((shift >= 64 ? hi : lo) >> (shift & 63)) & (kRadix - 1);
+        const unsigned peers = __match_any_sync(vmask, d);
+        if (lane == __ffs(peers) - 1) atomicAdd(&h[p * kRadix + d], (uint32_t)__popc(peers));
+      }
+    }
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
-    counts[(size_t)d * ntiles + blockIdx.x] = hist[d];
+  for (int q = threadIdx.x; q < npass * kRadix; q += kSortThreads)
+    if (h[q]) atomicAdd(&ghist[q], h[q]);
 }
 
-// Stable scatter of one tile.  Warp w owns the tile's elements
-// [w*256, w*256 + 256) and ranks them in index order, 32 at a time, with its
-// own per-digit counters (the lanes of one digit found with match_any; no
-// block barrier while ranking).  One pass over the digits turns the warps'
-// counts into each warp's start within the digit, and a scan of the tile's
-// digit counts gives each digit's start in the tile.  The ranked tile is
-// then reordered by digit in shared memory and written out in that order,
-// so consecutive threads write consecutive addresses of a digit's run.
+// ghist -> exclusive start of each digit within the array, per pass (one
+// block, a thread per digit).
+static_assert(kRadix == kSortThreads, "one digit per thread");
+__global__ void __launch_bounds__(kSortThreads) radix_offsets_kernel(uint32_t* __restrict__ ghist, int npass) {
+  __shared__ uint32_t wsum[kSortThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int p = 0; p < npass; ++p) {
+    const uint32_t c = ghist[p * kRadix + tid];
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    uint32_t pre = 0;
+    for (int w = 0; w < warp; ++w) pre += wsum[w];
+    ghist[p * kRadix + tid] = pre + x - c;
+    __syncthreads();
+  }
+}
+
+// One pass over the digit at `shift`.  Warp w of the block owns the tile's
+// elements [w*256, w*256 + 256) and ranks them in index order, 32 at a time,
+// with its own per-digit counters (the lanes of one digit found with
+// match_any; no block barrier while ranking).  The tile's digit counts are
+// published and looked back on (thread d for digit d), the tile is
+// reordered by digit in shared memory and written out in that order, so
+// consecutive threads write consecutive addresses of a digit's run.
+// status holds one word per (tile, digit): kind (aggregate / prefix) in bits
+// 62-63, the pass tag in bits 32-61 (words of other passes read as not yet
+// published), the count in bits 0-31.  A look-back that polls one word
+// kLookbackSpins times sets *err and takes the count so far (a lower start,
+// so every write stays inside the array).
 // Dynamic shared memory: the tile's keys (one or two words) and payloads.
-static_assert(kRadix == kSortThreads, "one digit per thread in the tile's digit scan");
 static_assert(kSortTile / (kSortThreads / 32) == kSortItems * 32, "each warp ranks kSortItems rounds of 32");
 __global__ void __launch_bounds__(kSortThreads)
-    radix_scatter_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
-                         const uint32_t* __restrict__ pin, uint32_t n, int shift,
-                         uint32_t ntiles, const uint32_t* __restrict__ offsets,
-                         uint64_t* __restrict__ olo, uint64_t* __restrict__ ohi,
-                         uint32_t* __restrict__ pout) {
+    radix_onesweep_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi,
+                          const uint32_t* __restrict__ pin, uint32_t n, int shift, uint32_t tag,
+                          const uint32_t* __restrict__ goff, uint32_t* __restrict__ ticket,
+                          unsigned long long* __restrict__ status, int* __restrict__ err,
+                          uint64_t* __restrict__ olo, uint64_t* __restrict__ ohi, uint32_t* __restrict__ pout) {
   constexpr int kWarps = kSortThreads / 32;
   constexpr int kPerWarp = kSortTile / kWarps;  // 256 elements, kPerWarp / 32 = kSortItems rounds
   __shared__ uint32_t wrun[kWarps][kRadix];      // per warp: digit counts, then the warp's start in the digit
   __shared__ uint32_t gbase[kRadix];
   __shared__ uint32_t lstart[kRadix];
   __shared__ uint32_t wsum[kWarps];
+  __shared__ uint32_t s_tile;
   extern __shared__ __align__(16) unsigned char dsm[];
   uint64_t* s_lo = reinterpret_cast<uint64_t*>(dsm);
   uint64_t* s_hi = s_lo + kSortTile;
@@ -197,9 +249,10 @@ __global__ void __launch_bounds__(kSortThreads)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) wrun[w][tid] = 0;
-  gbase[tid] = offsets[(size_t)tid * ntiles + blockIdx.x];
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
-  const uint32_t base = blockIdx.x * kSortTile;
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kSortTile;
   uint64_t vlo[kSortItems], vhi[kSortItems];
   uint32_t vp[kSortItems], dg[kSortItems], rk[kSortItems];
 #pragma unroll
@@ -247,6 +300,33 @@ __global__ void __launch_bounds__(kSortThreads)
     }
     cnt = run;
   }
+  {  // digit tid's start among the preceding tiles (decoupled look-back)
+    const unsigned long long tg = (unsigned long long)tag << 32;
+    volatile unsigned long long* mine = status + (size_t)tile * kRadix + tid;
+    uint32_t excl = 0;
+    if (tile == 0) {
+      *mine = kLbPrefix | tg | cnt;
+    } else {
+      *mine = kLbAggregate | tg | cnt;
+      uint32_t j = tile - 1, spins = 0;
+      while (true) {
+        const unsigned long long w = *(volatile unsigned long long*)(status + (size_t)j * kRadix + tid);
+        if ((uint32_t)((w >> 32) & 0x3fffffffu) != tag) {  // not yet published in this pass
+          if (++spins > kLookbackSpins) {
+            atomicOr(err, 1);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += (uint32_t)w;
+        if ((w & kLbPrefix) || j == 0) break;
+        --j;
+      }
+      *mine = kLbPrefix | tg | (excl + cnt);
+    }
+    gbase[tid] = goff[tid] + excl;
+  }
   {  // the tile's digit starts: exclusive scan of its digit counts
     uint32_t x = cnt;
 #pragma unroll
@@ -284,7 +364,7 @@ __global__ void __launch_bounds__(kSortThreads)
   }
 }
 
-// Dynamic shared memory of radix_scatter_kernel for one- or two-word keys.
+// Dynamic shared memory of radix_onesweep_kernel for one- or two-word keys.
 size_t scatter_smem(bool two_words) { return (size_t)kSortTile * ((two_words ? 16 : 8) + 4); }
 
 // Sorted interleaved keys -> line records (mode-contiguous key + value), the
@@ -557,6 +637,20 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Tiles, their intervals and the reference's partitions of the line (the
 // part of encoding after the sort), for t->nnz line entries.
+alto_status ensure_error_words(alto_tensor* t, cudaStream_t st) {
+  if (t->err.p) return ALTO_OK;
+  ALTO_TRY(t->err.ensure(16));
+  ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
+  return ALTO_OK;
+}
+
+alto_status sort_error_status(alto_tensor* t, const int* words, cudaStream_t st) {
+  if (!words[kSortErrorWord]) return ALTO_OK;
+  ALTO_TRY_CUDA(cudaMemsetAsync(t->err.as<int>() + kSortErrorWord, 0, 4, st));
+  set_error("a device radix sort gave up waiting on a preceding tile");
+  return ALTO_ERR_TIMEOUT;
+}
+
 static alto_status finish_layout(alto_tensor* t, int nprtn, cudaStream_t st) {
   const int N = t->nmodes;
   const uint64_t nnz = t->nnz;
@@ -593,7 +687,10 @@ static alto_status finish_layout(alto_tensor* t, int nprtn, cudaStream_t st) {
   if (t->ntiles && t->tile_stats) {
     std::vector<uint32_t> iv((size_t)t->ntiles * N * 2);
     ALTO_TRY_CUDA(cudaMemcpyAsync(iv.data(), t->tile_iv.p, iv.size() * 4, cudaMemcpyDeviceToHost, st));
+    int ew[4] = {0, 0, 0, 0};
+    if (t->err.p) ALTO_TRY_CUDA(cudaMemcpyAsync(ew, t->err.p, sizeof(ew), cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+    ALTO_TRY(sort_error_status(t, ew, st));
     for (int m = 0; m < N; ++m) {
       auto& v = t->tile_len_sorted[m];
       v.resize(t->ntiles);
@@ -667,7 +764,6 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
   // construction scratch: two key/payload buffers, staged COO, counts
   const bool two_words = total > 64;
-  const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
   const int vbytes = coo->val_dtype == ALTO_F64 ? 8 : 4;
   size_t off = 0;
   size_t o_lo0 = off; off = align_up(off + cap * 8, 256);
@@ -676,7 +772,7 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   size_t o_hi1 = off; off = align_up(off + (two_words ? cap * 8 : 0), 256);
   size_t o_p0 = off; off = align_up(off + cap * 4, 256);
   size_t o_p1 = off; off = align_up(off + cap * 4, 256);
-  size_t o_cnt = off; off = align_up(off + (size_t)kRadix * std::max<size_t>(tiles_sort, 1) * 4, 256);
+  size_t o_cnt = off; off = align_up(off + radix_scratch_bytes(nnz), 256);
   size_t o_vals = off; off = align_up(off + (coo->on_device ? 0 : cap * vbytes), 256);
   size_t o_cidx = off; off = align_up(off + (coo->on_device ? 0 : cap * coo->index_bytes * N), 256);
   ALTO_TRY(t->scratch.ensure(off));
@@ -685,7 +781,7 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   uint64_t* khi[2] = {two_words ? (uint64_t*)(sb + o_hi0) : nullptr,
                       two_words ? (uint64_t*)(sb + o_hi1) : nullptr};
   uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
-  uint32_t* counts = (uint32_t*)(sb + o_cnt);
+  void* sort_scratch = sb + o_cnt;
 
   CooPtrs cp{};
   const void* vin = coo->vals;
@@ -721,7 +817,8 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
     // LSD radix sort over the used bits
     int cur = 0;
-    ALTO_TRY(radix_sort_pairs(klo, khi, pm, n32, total, counts, t->scan_scratch, st, &cur));
+    ALTO_TRY(ensure_error_words(t, st));
+    ALTO_TRY(radix_sort_pairs(klo, khi, pm, n32, total, sort_scratch, t->err.as<int>() + kSortErrorWord, st, &cur));
 
     if (coo->val_dtype == ALTO_F64)
       layout_kernel<double><<<grid_for(nnz, 256), 256, 0, st>>>(
@@ -793,28 +890,58 @@ __global__ void gather_decode3_kernel(const void* __restrict__ line, LineDecode 
   }
 }
 
+// Scratch of radix_sort_pairs for n pairs: the look-back words (one per
+// tile and digit), the digit counts / starts of every pass, the per-pass
+// tile tickets.
+static size_t lookback_bytes(uint64_t n) {
+  const size_t tiles = std::max<uint64_t>((n + kSortTile - 1) / kSortTile, 1);
+  return align_up(tiles * kRadix * sizeof(unsigned long long), 256);
+}
+size_t radix_scratch_bytes(uint64_t n) {
+  return lookback_bytes(n) + align_up((size_t)kMaxSortPasses * kRadix * 4 + kMaxSortPasses * 4, 256);
+}
+
 // Stable LSD radix sort of (key, payload) pairs over the low `bits` bits of a
 // 64- or 128-bit key (khi[0] NULL for 64-bit keys), ping-ponging between
 // the two buffers of each array; *cur receives the buffer holding the
-// result.  counts holds kRadix * ceil(n / kSortTile) entries.
+// result.  scratch: radix_scratch_bytes(n) bytes; *err (device) is set if a
+// look-back gave up.
 alto_status radix_sort_pairs(uint64_t* klo[2], uint64_t* khi[2], uint32_t* pm[2], uint32_t n, int bits,
-                             uint32_t* counts, DevBuf& scan_scratch, cudaStream_t st, int* cur_out) {
+                             void* scratch, int* err, cudaStream_t st, int* cur_out) {
   int cur = 0;
+  *cur_out = 0;
+  const int npass = (bits + kRadixBits - 1) / kRadixBits;
+  if (!n || npass <= 0) return ALTO_OK;
+  if (npass > kMaxSortPasses) {
+    set_error("sort key of %d bits (at most %d)", bits, kMaxSortPasses * kRadixBits);
+    return ALTO_ERR_UNSUPPORTED;
+  }
   const uint32_t ntiles = (n + kSortTile - 1) / kSortTile;
   static std::atomic<bool> raised[64];  // per device
   int dev = 0;
   ALTO_TRY_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64 || !raised[dev].load()) {
-    ALTO_TRY_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ALTO_TRY_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)scatter_smem(true)));
     if (dev >= 0 && dev < 64) raised[dev] = true;
   }
-  for (int shift = 0; shift < bits && n; shift += kRadixBits) {
-    radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(klo[cur], khi[cur], n, shift, ntiles, counts);
-    ALTO_LAUNCHED();
-    ALTO_TRY(exclusive_scan_u32(counts, (size_t)kRadix * ntiles, scan_scratch, st));
-    radix_scatter_kernel<<<ntiles, kSortThreads, scatter_smem(khi[cur] != nullptr), st>>>(
-        klo[cur], khi[cur], pm[cur], n, shift, ntiles, counts, klo[cur ^ 1], khi[cur ^ 1], pm[cur ^ 1]);
+  char* sb = static_cast<char*>(scratch);
+  auto* status = reinterpret_cast<unsigned long long*>(sb);
+  auto* ghist = reinterpret_cast<uint32_t*>(sb + lookback_bytes(n));
+  uint32_t* tickets = ghist + kMaxSortPasses * kRadix;
+  ALTO_TRY_CUDA(cudaMemsetAsync(scratch, 0, radix_scratch_bytes(n), st));
+  int sms = 0;
+  ALTO_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned hist_grid =
+      std::min<unsigned>((n + kSortThreads - 1) / kSortThreads, (unsigned)std::max(sms, 1) * 4);
+  radix_all_hist_kernel<<<hist_grid, kSortThreads, 0, st>>>(klo[0], khi[0], n, npass, ghist);
+  ALTO_LAUNCHED();
+  radix_offsets_kernel<<<1, kSortThreads, 0, st>>>(ghist, npass);
+  ALTO_LAUNCHED();
+  for (int p = 0; p < npass; ++p) {
+    radix_onesweep_kernel<<<ntiles, kSortThreads, scatter_smem(khi[cur] != nullptr), st>>>(
+        klo[cur], khi[cur], pm[cur], n, p * kRadixBits, (uint32_t)p + 1, ghist + p * kRadix, tickets + p, status,
+        err, klo[cur ^ 1], khi[cur ^ 1], pm[cur ^ 1]);
     ALTO_LAUNCHED();
     cur ^= 1;
   }
@@ -822,8 +949,6 @@ alto_status radix_sort_pairs(uint64_t* klo[2], uint64_t* khi[2], uint32_t* pm[2]
   return ALTO_OK;
 }
 
-uint32_t sort_tiles(uint64_t n) { return (uint32_t)((n + kSortTile - 1) / kSortTile); }
-int radix_buckets() { return kRadix; }
 
 // A copy of the line ordered by the row of `mode`, ALTO order kept among
 // equal rows (stable LSD sort over the mode's bits).  This is the device
@@ -838,25 +963,26 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   s.hw = t->nmodes == 3 ? kDecoded3 : hw;
   ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(s.hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
-  const size_t tiles_sort = (nnz + kSortTile - 1) / kSortTile;
   size_t off = 0;
   size_t o_r0 = off; off = align_up(off + cap * 8, 256);
   size_t o_r1 = off; off = align_up(off + cap * 8, 256);
   size_t o_p0 = off; off = align_up(off + cap * 4, 256);
   size_t o_p1 = off; off = align_up(off + cap * 4, 256);
-  size_t o_cnt = off; off = align_up(off + (size_t)kRadix * std::max<size_t>(tiles_sort, 1) * 4, 256);
+  size_t o_cnt = off; off = align_up(off + radix_scratch_bytes(nnz), 256);
   ALTO_TRY(t->scratch.ensure(off));
   char* sb = t->scratch.as<char>();
   uint64_t* rk[2] = {(uint64_t*)(sb + o_r0), (uint64_t*)(sb + o_r1)};
   uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
-  uint32_t* counts = (uint32_t*)(sb + o_cnt);
+  void* sort_scratch = sb + o_cnt;
   const uint32_t n32 = (uint32_t)nnz;
   if (nnz) {
+    ALTO_TRY(ensure_error_words(t, st));
     mode_rows_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, mode, n32, rk[0], pm[0]);
     ALTO_LAUNCHED();
     int cur = 0;
     uint64_t* nohi[2] = {nullptr, nullptr};
-    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, t->mode_bits[mode], counts, t->scan_scratch, st, &cur));
+    ALTO_TRY(radix_sort_pairs(rk, nohi, pm, n32, t->mode_bits[mode], sort_scratch,
+                              t->err.as<int>() + kSortErrorWord, st, &cur));
     if (s.hw == kDecoded3)
       gather_decode3_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t->line.p, t->dec, pm[cur], n32,
                                                                  s.line.as<uint4>());

@@ -24,6 +24,9 @@ struct MttkrpArgs {
   uint32_t ntiles;
   int target;
   int stage_rows;  // rows of the shared staging buffer (0: never stage)
+  // walks updating the output with atomics: consecutive tiles per block
+  // chunk, the open run of each lane group carried from tile to tile
+  uint32_t chunk_tiles;
   LineDecode dec;
   FactorSet fac;
   float* out;

@@ -305,11 +305,18 @@ struct alto_tensor {
 namespace alto {
 // Encode (linearise, sort, lay out, partition) a COO tensor into t.
 alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st);
-// Stable LSD radix sort of (key, uint32 payload) pairs (alto_encode.cu).
+// Stable one-sweep LSD radix sort of (key, uint32 payload) pairs
+// (alto_encode.cu); scratch of radix_scratch_bytes(n) bytes; *err (device)
+// is set if a look-back gave up.
 alto_status radix_sort_pairs(uint64_t* klo[2], uint64_t* khi[2], uint32_t* pm[2], uint32_t n, int bits,
-                             uint32_t* counts, DevBuf& scan_scratch, cudaStream_t st, int* cur_out);
-uint32_t sort_tiles(uint64_t n);  // digit-count tiles of radix_sort_pairs for n pairs
-int radix_buckets();              // digit values per pass
+                             void* scratch, int* err, cudaStream_t st, int* cur_out);
+size_t radix_scratch_bytes(uint64_t n);
+// Device error words of a tensor (t->err, four ints): [0] a bulk-feed
+// MTTKRP wait gave up, [kSortErrorWord] a radix-sort look-back gave up.
+constexpr int kSortErrorWord = 3;
+alto_status ensure_error_words(alto_tensor* t, cudaStream_t st);
+// ALTO_ERR_TIMEOUT (and the word cleared) if words[kSortErrorWord] is set.
+alto_status sort_error_status(alto_tensor* t, const int* words, cudaStream_t st);
 // Keep line entries [begin, end) and rebuild tiles, intervals, partitions.
 alto_status restrict_line(alto_tensor* t, uint64_t begin, uint64_t end, cudaStream_t st);
 // Host-side mask setup (setup_packed_alto).

@@ -200,9 +200,18 @@ __device__ __forceinline__ void det_plain(float* out, uint32_t row, int sub, con
   }
 }
 
-template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false>
+// The open run of a lane group (CARRY walks take it in and hand it back
+// instead of updating the output at the end of their sub-range).
+template <int V>
+struct OpenRun {
+  uint32_t row;
+  float acc[V];
+};
+
+template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool CARRY = false>
 __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
-                                           bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0) {
+                                           bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0,
+                                           OpenRun<LaneWidth<R>::V>* carry = nullptr) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
   // nonzeros per step: 2 for 3 modes (4 measured faster for DET only), 2 for
@@ -218,9 +227,15 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   const uint32_t gs = min(ws + grp * sublen, we);
   const uint32_t ge = min(gs + sublen, we);
   float acc[V];
-#pragma unroll
-  for (int q = 0; q < V; ++q) acc[q] = 0.f;
   uint32_t cur = kNoRow;
+  if constexpr (CARRY) {
+    cur = carry->row;
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[q] = carry->acc[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[q] = 0.f;
+  }
   uint32_t nrun = 0;  // runs emitted (DET)
   const uint32_t slot0 = 2 * (sr_base + grp);
 
@@ -321,7 +336,13 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
     }
   }
   if (!DET) {
-    if (cur != kNoRow) flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+    if constexpr (CARRY) {
+      carry->row = cur;
+#pragma unroll
+      for (int q = 0; q < V; ++q) carry->acc[q] = acc[q];
+    } else if (cur != kNoRow) {
+      flush_row<R, V, G>(staged, smem, iv_start, a.out, cur, sub, acc);
+    }
   } else if (cur == kNoRow) {
     // empty sub-range: both slots carry the row of the entry before it (the
     // last run of an earlier sub-range) with zeros, keeping slot rows sorted
@@ -348,6 +369,34 @@ __global__ void __launch_bounds__(kMttkrpThreads, MINB)
   float* smem = reinterpret_cast<float*>(smem4);
   const int warp = threadIdx.x >> 5;
   const int N = a.dec.nmodes;
+  if constexpr (!STAGE && !DET) {
+    // chunks of chunk_tiles consecutive tiles, round robin over the blocks;
+    // within a chunk each lane group walks its sub-range of every tile with
+    // its open run carried along, so a row running through the chunk (a hot
+    // row) is updated once per group and chunk rather than once per tile:
+    // fewer float32 additions in the output, and fewer atomics
+    using LW = LaneWidth<R>;
+    const uint32_t ct = a.chunk_tiles;
+    const uint32_t nchunks = (a.ntiles + ct - 1) / ct;
+    for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+      OpenRun<LW::V> run;
+      run.row = kNoRow;
+#pragma unroll
+      for (int q = 0; q < LW::V; ++q) run.acc[q] = 0.f;
+      const uint32_t t_end = min(c * ct + ct, a.ntiles);
+      for (uint32_t tile = c * ct; tile < t_end; ++tile) {
+        const uint32_t ts = tile * a.tile_nnz;
+        const uint32_t te = min(ts + a.tile_nnz, a.nnz);
+        const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
+        const uint32_t ws = min(ts + warp * chunk, te);
+        const uint32_t we = min(ws + chunk, te);
+        warp_range<R, FT, HW, NM, false, false, true>(a, a.line, ws, we, false, smem, 0, 0, &run);
+      }
+      if (run.row != kNoRow)
+        flush_row<R, LW::V, LW::G>(false, smem, 0, a.out, run.row, (threadIdx.x & 31) % LW::G, run.acc);
+    }
+    return;
+  }
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     const uint32_t ts = tile * a.tile_nnz;
     const uint32_t te = min(ts + a.tile_nnz, a.nnz);
@@ -838,6 +887,17 @@ static int num_sms() {
   return g_num_sms;
 }
 
+// Tiles per chunk of the direct walks: up to kChunkTilesMax, keeping at
+// least kChunksPerBlock chunks per block so the round robin still balances
+// the blocks.
+constexpr uint32_t kChunkTilesMax = 8;
+constexpr uint32_t kChunksPerBlock = 8;
+static uint32_t chunk_tiles_for(uint32_t ntiles, unsigned grid) {
+  uint32_t c = kChunkTilesMax;
+  while (c > 1 && (uint64_t)ntiles < (uint64_t)c * grid * kChunksPerBlock) c >>= 1;
+  return c;
+}
+
 template <int R, typename FT, int HW, bool STAGE, int NM, int MINB = 3>
 static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   MttkrpArgs b = a;
@@ -857,6 +917,7 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   }
   unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
   if (!grid) return ALTO_OK;
+  b.chunk_tiles = chunk_tiles_for(a.ntiles, grid);
   mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB><<<grid, kMttkrpThreads, smem, st>>>(b);
   ALTO_LAUNCHED();
   return ALTO_OK;
@@ -1085,10 +1146,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
     if (m != mode && (reinterpret_cast<uintptr_t>(factors[m]) % (4 * esz)) != 0) aligned = false;
   }
   const bool stage = variant == ALTO_MTTKRP_STAGED || variant == ALTO_MTTKRP_STREAM;
-  if (!t->err.p) {
-    ALTO_TRY(t->err.ensure(16));
-    ALTO_TRY_CUDA(cudaMemsetAsync(t->err.p, 0, 16, st));
-  }
+  ALTO_TRY(ensure_error_words(t, st));
   int* err = t->err.as<int>();
   const bool bulk = feed == 1;
   const int dense = feed == 2 ? 1 : 0;

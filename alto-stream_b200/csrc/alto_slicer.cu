@@ -260,7 +260,6 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   const bool two_words = total > 64;
   const int vbytes = coo->val_dtype == ALTO_F64 ? 8 : 4;
   const size_t cap = std::max<uint64_t>(nnz, 1);
-  const size_t tiles = std::max<uint32_t>(sort_tiles(nnz), 1);
   const size_t nflag = (size_t)N * (nnz + 1);
   ALTO_TRY(s->idx.ensure((size_t)N * cap * 4, st));
   ALTO_TRY(s->gtime.ensure(cap * 4, st));
@@ -276,11 +275,11 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   const size_t o_hi1 = o; o = align256(o + (two_words ? cap * 8 : 0));
   const size_t o_p0 = o; o = align256(o + cap * 4);
   const size_t o_p1 = o; o = align256(o + cap * 4);
-  const size_t o_cnt = o; o = align256(o + (size_t)radix_buckets() * tiles * 4);
+  const size_t o_cnt = o; o = align256(o + radix_scratch_bytes(nnz));
   const size_t o_first = o; o = align256(o + std::max<uint64_t>(nfirst, 1) * 4);
   const size_t o_flag = o; o = align256(o + nflag * 4);
   const size_t o_step = o; o = align256(o + (size_t)(N + 1) * (s->T + 1) * 4);
-  const size_t o_err = o; o = align256(o + 4);
+  const size_t o_err = o; o = align256(o + 8);  // [0] index range, [1] sort look-back
   const size_t o_vin = o; o = align256(o + (coo->on_device ? 0 : cap * vbytes));
   const size_t o_cin = o; o = align256(o + (coo->on_device ? 0 : (size_t)N * cap * coo->index_bytes));
   ALTO_TRY(scratch.ensure(o, st));
@@ -307,7 +306,7 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
     ALTO_TRY_CUDA(cudaMemcpyAsync(sb + o_vin, coo->vals, nnz * vbytes, cudaMemcpyHostToDevice, st));
     vin = sb + o_vin;
   }
-  ALTO_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+  ALTO_TRY_CUDA(cudaMemsetAsync(d_err, 0, 8, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(first, 0xff, std::max<uint64_t>(nfirst, 1) * 4, st));
 
   const dim3 gm(grid_n(nnz + 1, 256), N);
@@ -318,7 +317,7 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
       slice_key_kernel<4><<<grid_n(nnz, 256), 256, 0, st>>>(in, f, n32, klo[0], khi[0], pm[0], d_err);
     ALTO_LAUNCHED();
     int cur = 0;
-    ALTO_TRY(radix_sort_pairs(klo, khi, pm, n32, total, (uint32_t*)(sb + o_cnt), scan_scratch, st, &cur));
+    ALTO_TRY(radix_sort_pairs(klo, khi, pm, n32, total, sb + o_cnt, d_err + 1, st, &cur));
     if (coo->val_dtype == ALTO_F64)
       slice_decode_kernel<double><<<grid_n(nnz, 256), 256, 0, st>>>(
           klo[cur], khi[cur], pm[cur], f, t, n32, (const double*)vin, s->vals.as<double>(), s->gtime.as<uint32_t>(),
@@ -345,16 +344,20 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
                                                             t, d_off, d_cnt);
   ALTO_LAUNCHED();
 
-  int err = 0;
+  int err[2] = {0, 0};
   s->off.assign(s->T + 1, 0);
   s->cnt.assign((size_t)N * (s->T + 1), 0);
   ALTO_TRY_CUDA(cudaMemcpyAsync(s->off.data(), d_off, (s->T + 1) * 4, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaMemcpyAsync(s->cnt.data(), d_cnt, (size_t)N * (s->T + 1) * 4, cudaMemcpyDeviceToHost, st));
-  ALTO_TRY_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st));
+  ALTO_TRY_CUDA(cudaMemcpyAsync(err, d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // (also: host COO outlives its copies; scratch is freed below)
-  if (err) {
+  if (err[0]) {
     set_error("an index of the tensor is outside its mode's dims");
     return ALTO_ERR_INVALID;
+  }
+  if (err[1]) {
+    set_error("the slicer's device sort gave up waiting on a preceding tile");
+    return ALTO_ERR_TIMEOUT;
   }
   return ALTO_OK;
 }

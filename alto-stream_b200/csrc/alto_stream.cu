@@ -2184,7 +2184,11 @@ alto_status finish_batch(alto_stream_session* s, const IterState& hs, int* inner
   s->time_rows.resize(base + s->dims[t] * R);
   ALTO_TRY_CUDA(cudaMemcpyAsync(s->time_rows.data() + base, s->time64.p, s->dims[t] * R * 8,
                                 cudaMemcpyDeviceToHost, st));
+  int ew[4] = {0, 0, 0, 0};  // the slice encoder's error words
+  if (s->at && s->at->err.p)
+    ALTO_TRY_CUDA(cudaMemcpyAsync(ew, s->at->err.p, sizeof(ew), cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  if (s->at) ALTO_TRY(sort_error_status(s->at, ew, st));
   s->batches += 1;
   return ALTO_OK;
 }

@@ -110,6 +110,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed steps before (mttkrp 3; cpstream 3 slices; serve 1 slice per stream)")
     ap.add_argument("--workers", type=int, default=16, help="serve: server worker threads")
+    ap.add_argument("--kernel-share", action="store_true",
+                    help="cpstream/serve: also record every device activity of the timed region with the CUDA "
+                         "profiling interface (torch.profiler) and report kernel time against wall time; the "
+                         "line's throughput is then taken under the profiler and is not a bench number")
     ap.add_argument("--no-graph", action="store_true",
                     help="cpstream: launch every inner iteration directly (no CUDA graph; for per-kernel profiles)")
     ap.add_argument("--model", choices=["cpstream", "spcpstream"], default="cpstream",
@@ -719,6 +723,60 @@ def ref_cpstream_rate(batches, R, iv, model="cpstream"):
     return len(batches) / float(secs.sum()), threads, [round(float(x) * 1e3, 1) for x in secs]
 
 
+class DeviceActivity:
+    """Device activity of a region (kernels, copies, memsets) recorded by
+    torch.profiler (CUPTI), which sees this library's kernels and the kernel
+    nodes of its CUDA graphs as well as torch's own."""
+
+    def __init__(self, enabled):
+        self.prof = None
+        if enabled:
+            from torch.profiler import ProfilerActivity, profile
+
+            self.prof = profile(activities=[ProfilerActivity.CUDA])
+
+    def start(self):
+        if self.prof is not None:
+            self.prof.__enter__()
+
+    def stop(self, wall_s):
+        if self.prof is None:
+            return None
+        import torch
+
+        torch.cuda.synchronize()
+        self.prof.__exit__(None, None, None)
+        try:
+            per = {}
+            busy = []
+            for e in self.prof.events():
+                if e.device_type != torch.autograd.DeviceType.CUDA:
+                    continue
+                t0, t1 = e.time_range.start, e.time_range.end
+                busy.append((t0, t1))
+                k = per.setdefault(e.name, [0.0, 0])
+                k[0] += (t1 - t0) / 1e3
+                k[1] += 1
+            busy.sort()
+            covered, end = 0.0, None  # union of the activity intervals (us)
+            for t0, t1 in busy:
+                if end is None or t0 > end:
+                    covered += t1 - t0
+                    end = t1
+                elif t1 > end:
+                    covered += t1 - end
+                    end = t1
+            top = sorted(per.items(), key=lambda kv: -kv[1][0])[:15]
+            total = sum(v[0] for v in per.values())
+            return {"device_busy_ms": covered / 1e3, "wall_ms": wall_s * 1e3,
+                    "busy_share": covered / 1e3 / (wall_s * 1e3), "activity_ms_sum": total,
+                    "activities": sum(v[1] for v in per.values()),
+                    "top": [{"name": n[:90], "ms": round(v[0], 3), "count": v[1]} for n, v in top],
+                    "note": "recorded with torch.profiler (CUPTI); the throughput of this run is not a bench number"}
+        except Exception as e:  # the profiler's event model differs between torch versions
+            return {"error": f"{type(e).__name__}: {e}"}
+
+
 def ours_cpstream(args):
     import numpy as np
     import torch
@@ -741,6 +799,7 @@ def ours_cpstream(args):
     stream = torch.cuda.current_stream()
     sampler = None
     launches0 = 0
+    activity = DeviceActivity(args.kernel_share)
     for k, b in enumerate(batches):
         if k == W:
             torch.cuda.synchronize()
@@ -748,6 +807,7 @@ def ours_cpstream(args):
             sampler.start()
             time.sleep(0.3)
             launches0 = A.kernel_launches()
+            activity.start()
             t_start = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -764,6 +824,7 @@ def ours_cpstream(args):
             nbytes += cpstream_bytes(b, R, it)
             h2d += b["cidx"].nbytes + b["vals"].nbytes + need[k] * 8
     t_total = time.perf_counter() - t_start
+    share = activity.stop(t_total)
     launches = A.kernel_launches() - launches0
     clocks = sampler.stop()
     s.close()
@@ -791,6 +852,7 @@ def ours_cpstream(args):
                    "inner_iters_mean": float(np.mean(inner)), "inner_iters_max": int(np.max(inner)),
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                    "latency_ms": [round(x, 2) for x in lat],
+                   "inner_iters": [int(x) for x in inner],
                    "launch": ("every inner iteration launched directly" if args.no_graph
                               else "one captured graph per session, relaunched for every slice (a device-side "
                                    "loop over the inner iterations)"),
@@ -804,6 +866,8 @@ def ours_cpstream(args):
         "clocks": clocks,
         "gpu_launches": launches,
     }
+    if share is not None:
+        line["kernel_share"] = share
     return line
 
 
