@@ -14,12 +14,15 @@
 //                           time indices.
 //   stream_prev (:284-327)  the same view over the last `previous` steps.
 //
-// The first-seen relabel needs no second sort: for every index value the
-// smallest sorted position holding it (an atomic minimum, one per run of
-// equal values in a warp), a flag at that position, one exclusive scan of
-// the flags of all modes together, and label = scan[first[value]].  Since
-// labels follow first appearance, the running maximum the reference keeps
-// in _prev_dim is the number of distinct indices before the batch end.
+// The first-seen relabel needs no second pass over the nonzeros before the
+// relabel itself: for every index value the smallest sorted position
+// holding it (an atomic minimum, one per run of equal values in a warp),
+// then a sort of the (mode, first position) -> value pairs -- as many as
+// the modes' lengths, not the nonzeros -- which lists each mode's values in
+// first-appearance order: label = rank in that list.  Since labels follow
+// first appearance, the running maximum the reference keeps in _prev_dim is
+// the number of distinct indices before the batch end, a binary search of
+// the batch end in the sorted first positions.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -121,62 +124,88 @@ __global__ void slice_decode_kernel(const uint64_t* __restrict__ klo, const uint
   }
 }
 
-// flags[m][p] = 1 where sorted position p is the first holding its index
-// (non-stream modes; the stream mode's row and every row's extra entry are 0).
-__global__ void slice_flag_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ first,
-                                  SortFields f, int t, uint32_t nnz, uint32_t* __restrict__ flags) {
-  const int m = blockIdx.y;
-  uint32_t* fl = flags + (size_t)m * (nnz + 1);
-  for (uint64_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= nnz; p += gridDim.x * blockDim.x) {
-    uint32_t b = 0;
-    if (m != t && p < nnz) b = first[f.first_off[m] + idx[(size_t)m * nnz + p]] == p;
-    fl[p] = b;
+// The first-seen relabel.  first[] holds, for every value of every
+// non-stream mode (mode m at first_off[m]), the first sorted position that
+// holds it (kNone if none does).  Sorting the pairs (mode, first position)
+// -> value puts each mode's values in first-appearance order, which is the
+// label order: no pass over the nonzeros beyond the final relabel.
+__device__ __forceinline__ int mode_of(const SortFields& f, int t, uint64_t q) {
+  int m = 0;
+  for (int k = 0; k < f.nmodes; ++k)
+    if (k != t && q >= f.first_off[k] && q < f.first_off[k] + f.dims[k]) m = k;
+  return m;
+}
+
+__global__ void slice_first_pairs_kernel(const uint32_t* __restrict__ first, SortFields f, int t, uint64_t nfirst,
+                                         uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+  for (uint64_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nfirst; q += gridDim.x * blockDim.x) {
+    const int m = mode_of(f, t, q);
+    key[q] = ((uint64_t)m << 32) | first[q];
+    val[q] = (uint32_t)(q - f.first_off[m]);
   }
 }
 
-// idx[m][p] = the label of its index: the exclusive scan at its first position.
-__global__ void slice_label_kernel(uint32_t* __restrict__ idx, const uint32_t* __restrict__ first,
-                                   const uint32_t* __restrict__ scan, SortFields f, int t, uint32_t nnz) {
+// From the sorted pairs: the r-th value of mode m to appear gets label r;
+// label[m][value] = r (in first[]'s storage) and iperm[m][r] = value (the
+// reference's Permutation iperms).
+__global__ void slice_label_table_kernel(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sval,
+                                         SortFields f, uint64_t nfirst, uint32_t* __restrict__ label,
+                                         uint32_t* __restrict__ iperm) {
+  for (uint64_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nfirst; q += gridDim.x * blockDim.x) {
+    const uint64_t k = skey[q];
+    if ((uint32_t)k == kNone) continue;
+    const int m = (int)(k >> 32);
+    const uint32_t r = (uint32_t)(q - f.first_off[m]);
+    label[f.first_off[m] + sval[q]] = r;
+    iperm[f.first_off[m] + r] = sval[q];
+  }
+}
+
+// idx[m][p] = the label of its original index.
+__global__ void slice_relabel_kernel(uint32_t* __restrict__ idx, const uint32_t* __restrict__ label,
+                                     SortFields f, int t, uint32_t nnz) {
   const int m = blockIdx.y;
   if (m == t) return;
-  const uint32_t* sc = scan + (size_t)m * (nnz + 1);
-  const uint32_t base = sc[0];
   uint32_t* ix = idx + (size_t)m * nnz;
+  const uint32_t* lb = label + f.first_off[m];
   for (uint64_t p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)
-    ix[p] = sc[first[f.first_off[m] + ix[p]]] - base;
+    ix[p] = lb[ix[p]];
 }
 
-// iperm[m][label] = original index (the reference's Permutation iperms).
-__global__ void slice_iperm_kernel(const uint32_t* __restrict__ first, const uint32_t* __restrict__ scan,
-                                   SortFields f, int t, uint32_t nnz, uint32_t* __restrict__ iperm) {
-  const int m = blockIdx.y;
-  if (m == t) return;
-  const uint32_t* sc = scan + (size_t)m * (nnz + 1);
-  const uint32_t base = sc[0];
-  const uint32_t* fm = first + f.first_off[m];
-  uint32_t* out = iperm + f.first_off[m];
-  for (uint64_t v = blockIdx.x * blockDim.x + threadIdx.x; v < f.dims[m]; v += gridDim.x * blockDim.x) {
-    const uint32_t q = fm[v];
-    if (q != kNone) out[sc[q] - base] = (uint32_t)v;
-  }
-}
-
-// Step tables: off[b] = first sorted position with time >= b (b = 0..T),
-// cnt[m][b] = distinct indices of mode m before off[b].  Position p owns the
-// steps (time[p-1], time[p]] (p = nnz owns the steps after the last time).
+// off[b] = first sorted position with time >= b (b = 0..T).  Position p
+// owns the steps (time[p-1], time[p]] (p = nnz owns the steps after the
+// last time).
 __global__ void slice_steps_kernel(const uint32_t* __restrict__ gtime, uint32_t nnz, uint32_t T,
-                                   const uint32_t* __restrict__ scan, int N, int t, uint32_t* __restrict__ off,
-                                   uint32_t* __restrict__ cnt) {
+                                   uint32_t* __restrict__ off) {
   for (uint64_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= nnz; p += gridDim.x * blockDim.x) {
     const uint64_t lo = p == 0 ? 0 : (uint64_t)gtime[p - 1] + 1;
     const uint64_t hi = p == nnz ? T : gtime[p];
-    for (uint64_t b = lo; b <= hi; ++b) {
-      off[b] = p;
-      for (int m = 0; m < N; ++m) {
-        const uint32_t* sc = scan + (size_t)m * (nnz + 1);
-        cnt[(size_t)m * (T + 1) + b] = m == t ? 0 : sc[p] - sc[0];
-      }
+    for (uint64_t b = lo; b <= hi; ++b) off[b] = p;
+  }
+}
+
+// cnt[m][b] = distinct indices of mode m before off[b]: the values of m
+// first seen before it, a binary search in m's sorted first positions.
+__global__ void slice_counts_kernel(const uint64_t* __restrict__ skey, SortFields f, int t, uint32_t T,
+                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt) {
+  const uint64_t n = (uint64_t)f.nmodes * (T + 1);
+  for (uint64_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int m = (int)(q / (T + 1));
+    const uint32_t b = (uint32_t)(q % (T + 1));
+    if (m == t) {
+      cnt[q] = 0;
+      continue;
     }
+    const uint64_t target = ((uint64_t)m << 32) | off[b];
+    uint64_t lo = f.first_off[m], hi = lo + f.dims[m];
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (skey[mid] < target)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    cnt[q] = (uint32_t)(lo - f.first_off[m]);
   }
 }
 
@@ -260,24 +289,23 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   const bool two_words = total > 64;
   const int vbytes = coo->val_dtype == ALTO_F64 ? 8 : 4;
   const size_t cap = std::max<uint64_t>(nnz, 1);
-  const size_t nflag = (size_t)N * (nnz + 1);
+  // the sort buffers serve the nonzeros' sort, then the relabel's pair sort
+  const size_t scap = std::max<uint64_t>(cap, nfirst);
   ALTO_TRY(s->idx.ensure((size_t)N * cap * 4, st));
   ALTO_TRY(s->gtime.ensure(cap * 4, st));
   ALTO_TRY(s->vals.ensure(cap * vbytes, st));
   ALTO_TRY(s->iperm.ensure(std::max<uint64_t>(nfirst, 1) * 4, st));
 
   PoolBuf scratch;  // (transient: the library pool keeps it for the next slicer)
-  DevBuf scan_scratch;
   size_t o = 0;
-  const size_t o_lo0 = o; o = align256(o + cap * 8);
-  const size_t o_lo1 = o; o = align256(o + cap * 8);
+  const size_t o_lo0 = o; o = align256(o + scap * 8);
+  const size_t o_lo1 = o; o = align256(o + scap * 8);
   const size_t o_hi0 = o; o = align256(o + (two_words ? cap * 8 : 0));
   const size_t o_hi1 = o; o = align256(o + (two_words ? cap * 8 : 0));
-  const size_t o_p0 = o; o = align256(o + cap * 4);
-  const size_t o_p1 = o; o = align256(o + cap * 4);
-  const size_t o_cnt = o; o = align256(o + radix_scratch_bytes(nnz));
+  const size_t o_p0 = o; o = align256(o + scap * 4);
+  const size_t o_p1 = o; o = align256(o + scap * 4);
+  const size_t o_cnt = o; o = align256(o + radix_scratch_bytes(scap));
   const size_t o_first = o; o = align256(o + std::max<uint64_t>(nfirst, 1) * 4);
-  const size_t o_flag = o; o = align256(o + nflag * 4);
   const size_t o_step = o; o = align256(o + (size_t)(N + 1) * (s->T + 1) * 4);
   const size_t o_err = o; o = align256(o + 8);  // [0] index range, [1] sort look-back
   const size_t o_vin = o; o = align256(o + (coo->on_device ? 0 : cap * vbytes));
@@ -288,7 +316,6 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   uint64_t* khi[2] = {two_words ? (uint64_t*)(sb + o_hi0) : nullptr, two_words ? (uint64_t*)(sb + o_hi1) : nullptr};
   uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
   uint32_t* first = (uint32_t*)(sb + o_first);
-  uint32_t* flags = (uint32_t*)(sb + o_flag);
   uint32_t* d_off = (uint32_t*)(sb + o_step);
   uint32_t* d_cnt = d_off + (s->T + 1);
   int* d_err = (int*)(sb + o_err);
@@ -309,7 +336,7 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
   ALTO_TRY_CUDA(cudaMemsetAsync(d_err, 0, 8, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(first, 0xff, std::max<uint64_t>(nfirst, 1) * 4, st));
 
-  const dim3 gm(grid_n(nnz + 1, 256), N);
+  const dim3 gm(grid_n(nnz, 256), N);
   if (nnz) {
     if (coo->index_bytes == 8)
       slice_key_kernel<8><<<grid_n(nnz, 256), 256, 0, st>>>(in, f, n32, klo[0], khi[0], pm[0], d_err);
@@ -328,21 +355,33 @@ alto_status slicer_build(alto_slicer* s, const alto_coo* coo) {
           s->idx.as<uint32_t>(), first);
     ALTO_LAUNCHED();
   }
-  slice_flag_kernel<<<gm, 256, 0, st>>>(s->idx.as<uint32_t>(), first, f, t, n32, flags);
-  ALTO_LAUNCHED();
-  ALTO_TRY(exclusive_scan_u32(flags, nflag, scan_scratch, st));
-  if (nnz) {
-    slice_label_kernel<<<gm, 256, 0, st>>>(s->idx.as<uint32_t>(), first, flags, f, t, n32);
+  // first-seen labels: the (mode, first position) -> value pairs sorted
+  const uint64_t* skey = nullptr;  // the sorted pairs' keys
+  if (nfirst) {
+    slice_first_pairs_kernel<<<grid_n(nfirst, 256), 256, 0, st>>>(first, f, t, nfirst, klo[0], pm[0]);
     ALTO_LAUNCHED();
+    uint64_t* nohi[2] = {nullptr, nullptr};
+    int pc = 0;
+    const int pair_bits = 32 + (N > 1 ? 32 - __builtin_clz((unsigned)(N - 1)) : 0);
+    ALTO_TRY(radix_sort_pairs(klo, nohi, pm, (uint32_t)nfirst, pair_bits, sb + o_cnt, d_err + 1, st, &pc));
+    slice_label_table_kernel<<<grid_n(nfirst, 256), 256, 0, st>>>(klo[pc], pm[pc], f, nfirst, first,
+                                                                  s->iperm.as<uint32_t>());
+    ALTO_LAUNCHED();
+    if (nnz) {
+      slice_relabel_kernel<<<gm, 256, 0, st>>>(s->idx.as<uint32_t>(), first, f, t, n32);
+      ALTO_LAUNCHED();
+    }
+    skey = klo[pc];
   }
-  uint64_t maxd = 1;
-  for (int m = 0; m < N; ++m)
-    if (m != t) maxd = std::max(maxd, s->dims[m]);
-  slice_iperm_kernel<<<dim3(grid_n(maxd, 256), N), 256, 0, st>>>(first, flags, f, t, n32, s->iperm.as<uint32_t>());
+  slice_steps_kernel<<<grid_n(nnz + 1, 256), 256, 0, st>>>(s->gtime.as<uint32_t>(), n32, (uint32_t)s->T, d_off);
   ALTO_LAUNCHED();
-  slice_steps_kernel<<<grid_n(nnz + 1, 256), 256, 0, st>>>(s->gtime.as<uint32_t>(), n32, (uint32_t)s->T, flags, N,
-                                                            t, d_off, d_cnt);
-  ALTO_LAUNCHED();
+  if (skey) {
+    slice_counts_kernel<<<grid_n((uint64_t)N * (s->T + 1), 256), 256, 0, st>>>(skey, f, t, (uint32_t)s->T, d_off,
+                                                                                 d_cnt);
+    ALTO_LAUNCHED();
+  } else {
+    ALTO_TRY_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)N * (s->T + 1) * 4, st));
+  }
 
   int err[2] = {0, 0};
   s->off.assign(s->T + 1, 0);
