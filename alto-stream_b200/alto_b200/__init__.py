@@ -46,9 +46,9 @@ EXPORTED = [
     "alto_status_string", "alto_last_error", "alto_version", "alto_kernel_launches",
     "alto_compute_masks", "alto_tensor_create", "alto_tensor_update", "alto_tensor_export", "alto_tensor_info",
     "alto_tensor_device_bytes", "alto_tensor_restrict", "alto_tensor_destroy", "alto_mttkrp", "alto_mttkrp_variant_run",
-    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_gram",
+    "alto_mttkrp_choose", "alto_mttkrp_autotune", "alto_mttkrp_host", "alto_mttkrp_host_changed", "alto_gram",
     "alto_gram_noalloc", "alto_cpd_als", "alto_stream_open",
-    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph", "alto_stream_error",
+    "alto_stream_push", "alto_stream_factor", "alto_stream_lambda", "alto_stream_set_model", "alto_stream_set_graph", "alto_stream_stats", "alto_stream_error",
     "alto_stream_close",
     "alto_read_tensor", "alto_dcoo_view", "alto_dcoo_stats", "alto_dcoo_to_host", "alto_dcoo_destroy", "alto_write_tensor",
     "alto_slicer_create", "alto_slicer_next", "alto_slicer_cut_all", "alto_slicer_batch", "alto_slicer_last_batch", "alto_slicer_stream_prev",
@@ -288,15 +288,25 @@ class AltoTensor:
         check(lib().alto_mttkrp_autotune(self.h, ptrs, c_int(dt), c_int(rank), _stream_handle(stream), out))
         return list(out)
 
-    def mttkrp_host(self, mode, factors, rank, stream=None):
+    def mttkrp_host(self, mode, factors, rank, stream=None, changed=None):
         """The reference calling convention on host float64 arrays:
-        factors[mode] is accumulated into, in place."""
+        factors[mode] is accumulated into, in place.  changed: the modes
+        whose arrays the caller modified since this thread's previous
+        host-buffer MTTKRP (alto_mttkrp_host_changed; the others are not
+        copied again), or None to copy every factor."""
         arrs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
         for a, f in zip(arrs, factors):
             if a is not f:
                 raise ValueError("host factors must be C-contiguous float64 arrays")
         ptrs = (POINTER(c_double) * self.nmodes)(*[a.ctypes.data_as(POINTER(c_double)) for a in arrs])
-        check(lib().alto_mttkrp_host(self.h, c_int(mode), ptrs, c_int(rank), _stream_handle(stream)))
+        if changed is None:
+            check(lib().alto_mttkrp_host(self.h, c_int(mode), ptrs, c_int(rank), _stream_handle(stream)))
+        else:
+            mask = 0
+            for m in changed:
+                mask |= 1 << int(m)
+            check(lib().alto_mttkrp_host_changed(self.h, c_int(mode), ptrs, c_int(rank), c_uint32(mask),
+                                                 _stream_handle(stream)))
         return factors
 
     def close(self):
@@ -414,9 +424,18 @@ class CPStream:
         check(lib().alto_stream_set_model(self.h, c_int(model)))
 
     def set_graph(self, enable):
-        """Inner iterations 2.. of each batch as one CUDA graph (default) or
-        launched one by one (alto_stream_set_graph)."""
+        """A batch's inner iterations as one launch of the session's CUDA
+        graph (default) or launched one by one (alto_stream_set_graph)."""
         check(lib().alto_stream_set_graph(self.h, c_int(1 if enable else 0)))
+
+    def stats(self):
+        """Where the pushes spent their time (alto_stream_stats), summed:
+        host ms preparing, from the inner iterations' launch to their
+        outcome, and finishing; device ms of the inner iterations."""
+        out = (c_double * 6)()
+        check(lib().alto_stream_stats(self.h, out))
+        return {"pushes": int(out[0]), "prepare_ms": out[1], "inner_ms": out[2], "inner_device_ms": out[3],
+                "finish_ms": out[4], "inner_iters": int(out[5])}
 
     def error(self, X):
         """cpd_error of the current model against X: a :class:`SliceBatch`

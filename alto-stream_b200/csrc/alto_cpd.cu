@@ -62,15 +62,34 @@ alto_status convert_f32_to_f64(const float* a, uint64_t n, double* b, cudaStream
 
 using namespace alto;
 
-// Device staging owned by one host-buffer MTTKRP call site.
+// Device staging owned by one host-buffer MTTKRP call site (a thread):
+// each factor's float64 copy and its float32 rounding, with the host array
+// they copy (address and length) and whether they still match it.
 struct HostStage {
   DevBuf f64[ALTO_MAX_MODES];
   DevBuf f32[ALTO_MAX_MODES];
   DevBuf out;
+  const double* host[ALTO_MAX_MODES] = {};
+  uint64_t len[ALTO_MAX_MODES] = {};
+  bool f64_ok[ALTO_MAX_MODES] = {};
+  bool f32_ok[ALTO_MAX_MODES] = {};
 };
+
+static alto_status mttkrp_host_impl(alto_tensor* t, int mode, double* const* factors_host, int rank,
+                                    uint32_t changed, alto_cuda_stream stream);
 
 extern "C" alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const* factors_host,
                                         int rank, alto_cuda_stream stream) {
+  return mttkrp_host_impl(t, mode, factors_host, rank, ~0u, stream);
+}
+
+extern "C" alto_status alto_mttkrp_host_changed(alto_tensor* t, int mode, double* const* factors_host,
+                                                int rank, uint32_t changed, alto_cuda_stream stream) {
+  return mttkrp_host_impl(t, mode, factors_host, rank, changed, stream);
+}
+
+static alto_status mttkrp_host_impl(alto_tensor* t, int mode, double* const* factors_host, int rank,
+                                    uint32_t changed, alto_cuda_stream stream) {
   if (!t || !factors_host) {
     set_error("tensor or factors is NULL");
     return ALTO_ERR_INVALID;
@@ -90,14 +109,28 @@ extern "C" alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const*
   const void* dev[ALTO_MAX_MODES] = {nullptr};
   for (int m = 0; m < t->nmodes; ++m) {
     const uint64_t n = t->dims[m] * (uint64_t)rank;
-    ALTO_TRY(stage->f64[m].ensure(n * 8));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(stage->f64[m].p, factors_host[m], n * 8, cudaMemcpyHostToDevice, st));
+    const bool same = stage->f64_ok[m] && !((changed >> m) & 1u) && stage->host[m] == factors_host[m] &&
+                      stage->len[m] == n && stage->f64[m].p;
+    if (!same) {
+      stage->f64_ok[m] = stage->f32_ok[m] = false;
+      ALTO_TRY(stage->f64[m].ensure(n * 8));
+      ALTO_TRY_CUDA(cudaMemcpyAsync(stage->f64[m].p, factors_host[m], n * 8, cudaMemcpyHostToDevice, st));
+      stage->host[m] = factors_host[m];
+      stage->len[m] = n;
+      stage->f64_ok[m] = true;
+    }
     if (m == mode) continue;
-    ALTO_TRY(stage->f32[m].ensure(n * 4));
-    ALTO_TRY(convert_f64_to_f32(stage->f64[m].as<double>(), n, stage->f32[m].as<float>(), st));
+    if (!stage->f32_ok[m]) {
+      ALTO_TRY(stage->f32[m].ensure(n * 4));
+      ALTO_TRY(convert_f64_to_f32(stage->f64[m].as<double>(), n, stage->f32[m].as<float>(), st));
+      stage->f32_ok[m] = true;
+    }
     dev[m] = stage->f32[m].p;
   }
   const uint64_t no = t->dims[mode] * (uint64_t)rank;
+  // until this call completes, the output mode's copies do not match its
+  // host array (an error below leaves them unmatched)
+  stage->f64_ok[mode] = stage->f32_ok[mode] = false;
   ALTO_TRY(stage->out.ensure(no * 4));
   ALTO_TRY(run_mttkrp(t, mode, dev, ALTO_F32, rank, stage->out.as<float>(), 0, ALTO_MTTKRP_AUTO, st));
   if (no) {
@@ -107,6 +140,7 @@ extern "C" alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const*
   }
   ALTO_TRY_CUDA(cudaMemcpyAsync(factors_host[mode], stage->f64[mode].p, no * 8, cudaMemcpyDeviceToHost, st));
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
+  stage->f64_ok[mode] = true;  // the device copy is what the host now holds
   return ALTO_OK;
 }
 

@@ -161,11 +161,13 @@ __device__ __forceinline__ uint32_t digit_of(const uint64_t* klo, const uint64_t
 constexpr int kMaxSortPasses = 16;  // 128-bit keys in 8-bit digits
 constexpr unsigned long long kLbAggregate = 1ull << 62;
 constexpr unsigned long long kLbPrefix = 2ull << 62;
-constexpr uint32_t kLookbackSpins = 1u << 22;  // polls of one word before giving up
+constexpr uint32_t kLookbackSpins = 1u << 22;  // polls of an unpublished word before giving up
+constexpr int kLookbackBatch = 8;               // look-back words loaded together
 
 // Digit counts of every pass, ghist[pass * kRadix + digit] (atomically
-// accumulated; zeroed by the caller).  Equal digits within a warp are counted
-// by their lowest lane: the high digits of keys take few values.
+// accumulated; zeroed by the caller), in shared memory first.  A warp whose
+// lanes all hold one digit (the high digits of keys take few values) adds
+// it once.
 __global__ void __launch_bounds__(kSortThreads)
     radix_all_hist_kernel(const uint64_t* __restrict__ klo, const uint64_t* __restrict__ khi, uint32_t n,
                           int npass, uint32_t* __restrict__ ghist) {
@@ -179,11 +181,16 @@ __global__ void __launch_bounds__(kSortThreads)
     const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     const uint64_t lo = valid ? klo[i] : 0, hi = (valid && khi) ? khi[i] : 0;
     if (valid) {
+      const int leader = __ffs(vmask) - 1;
       for (int p = 0; p < npass; ++p) {
         const int shift = p * kRadixBits;
         const uint32_t d = (uint32_t)((shift >= 64 ? hi : lo) >> (shift & 63)) & (kRadix - 1);
-        const unsigned peers = __match_any_sync(vmask, d);
-        if (lane == __ffs(peers) - 1) atomicAdd(&h[p * kRadix + d], (uint32_t)__popc(peers));
+        const uint32_t d0 = __shfl_sync(vmask, d, leader);
+        if (__all_sync(vmask, d == d0)) {
+          if (lane == leader) atomicAdd(&h[p * kRadix + d], (uint32_t)__popc(vmask));
+        } else {
+          atomicAdd(&h[p * kRadix + d], 1u);
+        }
       }
     }
   }
@@ -300,33 +307,10 @@ __global__ void __launch_bounds__(kSortThreads)
     }
     cnt = run;
   }
-  {  // digit tid's start among the preceding tiles (decoupled look-back)
-    const unsigned long long tg = (unsigned long long)tag << 32;
-    volatile unsigned long long* mine = status + (size_t)tile * kRadix + tid;
-    uint32_t excl = 0;
-    if (tile == 0) {
-      *mine = kLbPrefix | tg | cnt;
-    } else {
-      *mine = kLbAggregate | tg | cnt;
-      uint32_t j = tile - 1, spins = 0;
-      while (true) {
-        const unsigned long long w = *(volatile unsigned long long*)(status + (size_t)j * kRadix + tid);
-        if ((uint32_t)((w >> 32) & 0x3fffffffu) != tag) {  // not yet published in this pass
-          if (++spins > kLookbackSpins) {
-            atomicOr(err, 1);
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        excl += (uint32_t)w;
-        if ((w & kLbPrefix) || j == 0) break;
-        --j;
-      }
-      *mine = kLbPrefix | tg | (excl + cnt);
-    }
-    gbase[tid] = goff[tid] + excl;
-  }
+  // the tile's count of digit tid, published for the tiles after it
+  const unsigned long long tg = (unsigned long long)tag << 32;
+  volatile unsigned long long* mine = status + (size_t)tile * kRadix + tid;
+  *mine = (tile == 0 ? kLbPrefix : kLbAggregate) | tg | cnt;
   {  // the tile's digit starts: exclusive scan of its digit counts
     uint32_t x = cnt;
 #pragma unroll
@@ -343,6 +327,8 @@ __global__ void __launch_bounds__(kSortThreads)
     lstart[tid] = pre + x - cnt;
   }
   __syncthreads();
+  // the tile reordered by digit in shared memory (frees the registers
+  // before the look-back)
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
     if (base + warp * kPerWarp + r * 32 + lane < n) {
@@ -351,6 +337,45 @@ __global__ void __launch_bounds__(kSortThreads)
       if (khi) s_hi[at] = vhi[r];
       s_p[at] = vp[r];
     }
+  }
+  {  // digit tid's start among the preceding tiles (decoupled look-back)
+    uint32_t excl = 0;
+    if (tile > 0) {
+      // the preceding tiles' words, kLookbackBatch at a time (independent
+      // loads in flight together), summed nearest first up to the first
+      // inclusive prefix; an unpublished word is waited on alone
+      uint32_t j = tile;  // tiles [0, j) are still to be looked at
+      uint32_t spins = 0;
+      while (j > 0) {
+        const uint32_t nb = min(j, (uint32_t)kLookbackBatch);
+        unsigned long long w[kLookbackBatch];
+#pragma unroll
+        for (int k = 0; k < kLookbackBatch; ++k)
+          w[k] = (uint32_t)k < nb ? *(volatile unsigned long long*)(status + (size_t)(j - 1 - k) * kRadix + tid)
+                                  : 0ull;
+        bool found = false;
+        uint32_t used = 0;
+#pragma unroll
+        for (int k = 0; k < kLookbackBatch; ++k) {
+          if (found || (uint32_t)k >= nb || used < (uint32_t)k) continue;
+          if ((uint32_t)((w[k] >> 32) & 0x3fffffffu) != tag) continue;  // not yet published in this pass
+          excl += (uint32_t)w[k];
+          used = k + 1;
+          if (w[k] & kLbPrefix) found = true;
+        }
+        if (found) break;
+        j -= used;
+        if (used < nb) {  // word j - 1 is not yet published: wait for it
+          if (++spins > kLookbackSpins) {
+            atomicOr(err, 1);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      *mine = kLbPrefix | tg | (excl + cnt);
+    }
+    gbase[tid] = goff[tid] + excl;
   }
   __syncthreads();
   const uint32_t tile_n = min((uint32_t)kSortTile, n - base);

@@ -33,6 +33,7 @@
 // and one graph launch, with no host synchronisation between inner
 // iterations.  alto_stream_set_graph(s, 0) issues every iteration directly
 // instead (the same kernels in the same order: identical results).
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -1140,11 +1141,18 @@ struct alto_stream_session {
   // is not served with others
   DetItem det[ALTO_MAX_MODES];
   alto::StreamGroup* own_group = nullptr;
+  // alto_stream_stats: host seconds per phase of the pushes, device ms of
+  // their inner iterations (between the two events), pushes, iterations
+  double t_prepare = 0, t_inner = 0, t_finish = 0, dev_inner_ms = 0;
+  uint64_t pushes = 0, inner_total = 0;
+  cudaEvent_t inner_ev[2] = {nullptr, nullptr};
   ~alto_stream_session() {
     alto::group_destroy(own_group);
     delete at;
     for (cudaStream_t c : capst)
       if (c) cudaStreamDestroy(c);
+    for (cudaEvent_t e : inner_ev)
+      if (e) cudaEventDestroy(e);
   }
 };
 
@@ -2193,10 +2201,33 @@ alto_status finish_batch(alto_stream_session* s, const IterState& hs, int* inner
   return ALTO_OK;
 }
 
+static double host_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// The push's inner iterations are done: their device time (the events) and
+// the finish, into the session's timing.
+static alto_status timed_finish(alto_stream_session* s, const IterState& hs, int* inner_out, double t_launch) {
+  const double t_ran = host_seconds();
+  s->t_inner += t_ran - t_launch;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, s->inner_ev[0], s->inner_ev[1]) == cudaSuccess) s->dev_inner_ms += ms;
+  int inner = 0;
+  ALTO_TRY(finish_batch(s, hs, &inner));
+  if (inner_out) *inner_out = inner;
+  s->t_finish += host_seconds() - t_ran;
+  s->pushes += 1;
+  s->inner_total += (uint64_t)inner;
+  return ALTO_OK;
+}
+
 alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals,
                        uint64_t n_init, int* inner_out) {
   const int N = s->N, R = s->R;
   cudaStream_t st = s->st;
+  const double t0 = host_seconds();
+  for (cudaEvent_t& e : s->inner_ev)
+    if (!e) ALTO_TRY_CUDA(cudaEventCreate(&e));
   ALTO_TRY(prepare_batch(s, b, init_vals, n_init));
   IterState hs{};
   if (s->use_graph && stream_groupable(s)) {
@@ -2210,11 +2241,15 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
     if (!s->own_group) ALTO_TRY(group_create(s, 1, st, &s->own_group));
     alto_stream_session* one = s;
     ALTO_TRY(group_set(s->own_group, &one, 1));
+    const double t_launch = host_seconds();
+    s->t_prepare += t_launch - t0;
+    ALTO_TRY_CUDA(cudaEventRecord(s->inner_ev[0], st));
     ALTO_TRY(group_launch(s->own_group, s->max_inner));
+    ALTO_TRY_CUDA(cudaEventRecord(s->inner_ev[1], st));
     ALTO_TRY(group_states(s->own_group, nullptr, nullptr, nullptr, nullptr));
     ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-    return finish_batch(s, hs, inner_out);
+    return timed_finish(s, hs, inner_out, t_launch);
   }
   IterLaunch L{};
   for (int n = 0; n < N; ++n) L.fac[n] = s->sparse ? s->Anz[n].p : s->U[n].p;
@@ -2223,21 +2258,26 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   L.mv = deterministic_supported(R, ALTO_F32) ? ALTO_MTTKRP_DETERMINISTIC : ALTO_MTTKRP_AUTO;
   ALTO_TRY(s->iter.ensure(sizeof(IterState)));
   ALTO_TRY_CUDA(cudaMemsetAsync(s->iter.p, 0, sizeof(IterState), st));
+  const double t_launch = host_seconds();
+  s->t_prepare += t_launch - t0;
+  ALTO_TRY_CUDA(cudaEventRecord(s->inner_ev[0], st));
   // iteration 0 directly: sizes every buffer and builds the sorted lines
   ALTO_TRY(enqueue_iteration(s, L, st));
   if (s->use_graph && s->max_inner > 1) {
     ALTO_TRY(run_graph(s, L));
+    ALTO_TRY_CUDA(cudaEventRecord(s->inner_ev[1], st));
     ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
     ALTO_TRY_CUDA(cudaStreamSynchronize(st));
   } else {
     while (true) {
+      ALTO_TRY_CUDA(cudaEventRecord(s->inner_ev[1], st));
       ALTO_TRY_CUDA(cudaMemcpyAsync(&hs, s->iter.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
       ALTO_TRY_CUDA(cudaStreamSynchronize(st));
       if (hs.stop || hs.done >= s->max_inner) break;
       ALTO_TRY(enqueue_iteration(s, L, st));
     }
   }
-  return finish_batch(s, hs, inner_out);
+  return timed_finish(s, hs, inner_out, t_launch);
 }
 
 // ------------------------------------------------- model error (cpd_error)
@@ -2547,6 +2587,20 @@ alto_status alto_stream_push(alto_stream_session* s, const alto_coo* batch, cons
     return ALTO_ERR_INVALID;
   }
   return push_batch(s, batch, init_vals, n_init, inner_iters);
+}
+
+alto_status alto_stream_stats(const alto_stream_session* s, double out[6]) {
+  if (!s || !out) {
+    set_error("session or out is NULL");
+    return ALTO_ERR_INVALID;
+  }
+  out[0] = (double)s->pushes;
+  out[1] = s->t_prepare * 1e3;
+  out[2] = s->t_inner * 1e3;
+  out[3] = s->dev_inner_ms;
+  out[4] = s->t_finish * 1e3;
+  out[5] = (double)s->inner_total;
+  return ALTO_OK;
 }
 
 alto_status alto_stream_factor(alto_stream_session* s, int mode, double* host_out, uint64_t* rows) {

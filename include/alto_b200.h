@@ -187,6 +187,17 @@ alto_status alto_mttkrp_choose(const alto_tensor* t, int mode, int rank, alto_dt
 alto_status alto_mttkrp_host(alto_tensor* t, int mode, double* const* factors_host, int rank,
                              alto_cuda_stream stream);
 
+/* alto_mttkrp_host for callers that change few factors between calls (a
+ * CP-ALS loop rewrites one factor per mode step): bit m of `changed` says
+ * factors_host[m] was modified on the host since this thread's previous
+ * host-buffer MTTKRP.  A factor with its bit clear, at the same host
+ * address and size as in that call, is not copied again (the device keeps
+ * the copy it last sent or returned); factors_host[mode] is still
+ * accumulated into and copied back.  The first call copies everything.
+ * Same results as alto_mttkrp_host. */
+alto_status alto_mttkrp_host_changed(alto_tensor* t, int mode, double* const* factors_host, int rank,
+                                     uint32_t changed, alto_cuda_stream stream);
+
 /* ------------------------------------------------------ dense helpers */
 
 /* G = U^T U in float64 (rank x rank, full symmetric, row-major, device) of a
@@ -264,13 +275,22 @@ typedef enum { ALTO_MODEL_CPSTREAM = 0, ALTO_MODEL_SPCPSTREAM = 1 } alto_stream_
 alto_status alto_stream_set_model(alto_stream_session* s, alto_stream_model model);
 
 /* How alto_stream_push issues a batch's inner iterations (the reference's
- * loop, src/streaming_cpd.cpp:1240-1482).  enable = 1 (the default): the
- * first directly, the rest as one CUDA graph per batch whose while nodes
- * run the inner loop and the ADMM sweeps, with the stopping tests on the
- * device.  enable = 0: every launch directly, one host synchronisation per
- * inner iteration.  Both issue the same kernels in the same order and give
- * identical results. */
+ * loop, src/streaming_cpd.cpp:1240-1482).  enable = 1 (the default): all
+ * of them as one launch of a CUDA graph captured once per session and
+ * relaunched for every batch, whose while nodes run the inner loop and the
+ * ADMM sweeps with the stopping tests on the device (sizes and pointers
+ * read from device memory).  enable = 0: every launch directly, one host
+ * synchronisation per inner iteration.  Both give identical results. */
 alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
+
+/* Where a session's pushes spent their time, summed over its pushes:
+ * out[0] pushes; out[1] host ms preparing batches (model growth, the
+ * batch's encoding and row-sorted copies, Grams); out[2] host ms from the
+ * inner iterations' launch until their outcome is on the host; out[3]
+ * device ms of the inner iterations (CUDA events around their launch);
+ * out[4] host ms finishing (forgetting, copies, the time row out); out[5]
+ * inner iterations. */
+alto_status alto_stream_stats(const alto_stream_session* s, double out[6]);
 /* cpd_error(X, M), src/streaming_cpd.cpp:368-464: the relative residual
  * ||X - M|| / ||X|| of the session's current model (unit weights, as
  * cpd_error sets them) against a COO tensor X in the session's indexing

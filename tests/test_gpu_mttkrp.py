@@ -138,6 +138,33 @@ def test_host_buffer_entry_point():
         assert rel_err(fs[m] - start, ref) <= TOL
 
 
+def test_host_buffer_changed_mask_matches_full_copies():
+    """A CP-ALS-like sequence of host-buffer MTTKRPs in which the caller
+    rewrites the factor it just received (here: halves it) before the next
+    call and declares only that factor changed (alto_mttkrp_host_changed):
+    every call still matches the oracle on the caller's current arrays
+    (a stale device copy would be off by the halving)."""
+    dims = np.array([400, 500, 600], np.uint64)
+    cidx, vals = synth.uniform_coo(dims, 50000, seed=12)
+    R = 16
+    rng = np.random.default_rng(4)
+    G = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+    t = A.create_alto(dims, cidx, vals)
+    enc = O.build(dims, cidx, vals.astype(np.float32).astype(np.float64))
+    prev = None
+    for it in range(2):
+        for m in range(3):
+            start = G[m].copy()
+            fo = [g.astype(np.float32).astype(np.float64) for g in G]
+            fo[m][:] = 0
+            ref = O.mttkrp(enc, m, fo, R)[m]
+            t.mttkrp_host(m, G, R, changed=range(3) if prev is None else [prev])
+            assert rel_err(G[m] - start, ref) <= TOL, (it, m)
+            G[m] *= 0.5
+            prev = m
+    t.close()
+
+
 def test_launch_counter_advances():
     import torch
 
