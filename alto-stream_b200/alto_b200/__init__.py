@@ -432,10 +432,11 @@ class CPStream:
         """Where the pushes spent their time (alto_stream_stats), summed:
         host ms preparing, from the inner iterations' launch to their
         outcome, and finishing; device ms of the inner iterations."""
-        out = (c_double * 6)()
+        out = (c_double * 9)()
         check(lib().alto_stream_stats(self.h, out))
         return {"pushes": int(out[0]), "prepare_ms": out[1], "inner_ms": out[2], "inner_device_ms": out[3],
-                "finish_ms": out[4], "inner_iters": int(out[5])}
+                "finish_ms": out[4], "inner_iters": int(out[5]), "grow_ms": out[6], "encode_ms": out[7],
+                "sorted_copies_ms": out[8]}
 
     def error(self, X):
         """cpd_error of the current model against X: a :class:`SliceBatch`

@@ -120,6 +120,7 @@ void gram_split(uint64_t I, uint32_t* nb, uint64_t* rpb);
 alto_status setup_group_launch(Strided<SetupItem> items, int max_items, int R, cudaStream_t st);
 // Grouped gram_cross_stats: block_off (device, [count + 1]) holds the prefix
 // sums of the items' nb; red_off likewise for their reduction blocks.
+alto_status gram_group_ready(int R);  // before capturing gram_group_launch at rank R
 alto_status gram_group_launch(Strided<GramItem> items, const uint32_t* block_off, const uint32_t* red_off,
                               int max_items, int R, cudaStream_t st);
 // Reduction blocks of one GramItem's pass at rank R.

@@ -214,10 +214,11 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
                                            OpenRun<LaneWidth<R>::V>* carry = nullptr) {
   using LW = LaneWidth<R>;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
-  // nonzeros per step: 2 for 3 modes (4 measured faster for DET only), 2 for
-  // 4 and 5 modes, 1 beyond (the accumulation order is the line order
-  // whatever U is)
-  constexpr int U = NM <= 3 ? (DET ? 4 : 2) : (NM <= 5 ? 2 : 1);
+  // nonzeros per step: 2 for 3 modes (4 measured faster for DET only), 1
+  // beyond (two measured 30% slower on the rank-64 5-mode tensor: its four
+  // gathered rows per nonzero already fill the registers); the accumulation
+  // order is the line order whatever U is
+  constexpr int U = NM <= 3 ? (DET ? 4 : 2) : 1;
   const int lane = threadIdx.x & 31;
   const int grp = lane / G, sub = lane % G;
   // groups' sub-ranges; odd lengths when reading shared memory, so the

@@ -1144,8 +1144,13 @@ struct alto_stream_session {
   // alto_stream_stats: host seconds per phase of the pushes, device ms of
   // their inner iterations (between the two events), pushes, iterations
   double t_prepare = 0, t_inner = 0, t_finish = 0, dev_inner_ms = 0;
+  double t_grow = 0, t_encode = 0, t_sorted = 0;  // parts of t_prepare
   uint64_t pushes = 0, inner_total = 0;
   cudaEvent_t inner_ev[2] = {nullptr, nullptr};
+  // pinned staging of the new model rows (grown geometrically; the
+  // previous push's copies out of it are complete when a push starts)
+  float* pin_rows = nullptr;
+  size_t pin_cap = 0;
   ~alto_stream_session() {
     alto::group_destroy(own_group);
     delete at;
@@ -1153,17 +1158,25 @@ struct alto_stream_session {
       if (c) cudaStreamDestroy(c);
     for (cudaEvent_t e : inner_ev)
       if (e) cudaEventDestroy(e);
+    if (pin_rows) cudaFreeHost(pin_rows);
   }
 };
 
 namespace {
+
+// At least n bytes, growing by half again past the request, so a buffer
+// that grows slice by slice is reallocated a logarithmic number of times.
+alto_status ensure_headroom(DevBuf& b, size_t n) {
+  if (n <= b.bytes && b.p) return ALTO_OK;
+  return b.ensure(std::max(n, b.bytes + b.bytes / 2));
+}
 
 alto_status grow_rows(DevBuf& b, uint64_t old_rows, uint64_t new_cap, size_t row_bytes, DevBuf& tmp,
                       cudaStream_t st) {
   if (b.bytes >= new_cap * row_bytes && b.p) return ALTO_OK;
   const size_t keep = old_rows * row_bytes;
   if (keep) {
-    ALTO_TRY(tmp.ensure(keep));
+    ALTO_TRY(ensure_headroom(tmp, keep));
     ALTO_TRY_CUDA(cudaMemcpyAsync(tmp.p, b.p, keep, cudaMemcpyDeviceToDevice, st));
   }
   ALTO_TRY_CUDA(cudaStreamSynchronize(st));
@@ -1947,7 +1960,7 @@ alto_status group_create(const alto_stream_session* like, int capacity, cudaStre
   ALTO_TRY_CUDA(cudaMemsetAsync(g->tab.p, 0, sizeof(SlotDesc) * capacity, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(g->offs.p, 0, offs_n * 4, st));
   ALTO_TRY_CUDA(cudaMemsetAsync(g->ctl.p, 0, sizeof(GroupCtl), st));
-  if ((r = build_group_graph(g))) {
+  if ((r = gram_group_ready(g->R)) || (r = build_group_graph(g))) {
     group_destroy(g);
     return r;
   }
@@ -2079,16 +2092,29 @@ namespace {
 // Everything of a batch before its inner iterations (src/streaming_cpd.cpp:
 // 124-186): grow the model, Grams and cross Grams, duals cleared, the
 // batch encoded, the first batch's normalisation, spCP-stream's row maps.
+static double host_seconds();
+
 alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const double* init_vals, uint64_t n_init) {
   const int N = s->N, t = s->t, R = s->R;
   cudaStream_t st = s->st;
   const size_t RR = (size_t)R * R;
   const bool first = s->batches == 0;
+  const double t_grow0 = host_seconds();
 
-  // grow the model: new rows of U from init_vals (mode order), prev rows zero
+  // grow the model: new rows of U from init_vals (mode order), prev rows
+  // zero; every mode's new rows staged in the session's pinned buffer
   uint64_t old[ALTO_MAX_MODES];
+  uint64_t new_vals = 0;
+  for (int n = 0; n < N; ++n) new_vals += (std::max<uint64_t>(b->dims[n], s->dims[n]) - s->dims[n]) * R;
+  if (new_vals > s->pin_cap) {
+    const size_t want = std::max<size_t>(new_vals, s->pin_cap + s->pin_cap / 2);
+    if (s->pin_rows) cudaFreeHost(s->pin_rows);
+    s->pin_rows = nullptr;
+    s->pin_cap = 0;
+    ALTO_TRY_CUDA(cudaMallocHost((void**)&s->pin_rows, want * sizeof(float)));
+    s->pin_cap = want;
+  }
   uint64_t consumed = 0;
-  std::vector<float> host_rows;
   for (int n = 0; n < N; ++n) {
     old[n] = s->dims[n];
     const uint64_t nd = std::max<uint64_t>(b->dims[n], old[n]);
@@ -2102,25 +2128,24 @@ alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const doubl
     }
     if (nd > old[n]) {
       const uint64_t cnt = (nd - old[n]) * R;
-      host_rows.assign(cnt, 0.0f);
+      float* rows = s->pin_rows + consumed;
       for (uint64_t q = 0; q < cnt; ++q)
-        host_rows[q] = consumed + q < n_init ? (float)init_vals[consumed + q] : 0.0f;
+        rows[q] = consumed + q < n_init ? (float)init_vals[consumed + q] : 0.0f;
       consumed += cnt;
-      ALTO_TRY_CUDA(cudaMemcpyAsync(s->U[n].as<float>() + old[n] * R, host_rows.data(), cnt * 4,
-                                    cudaMemcpyHostToDevice, st));
+      ALTO_TRY_CUDA(cudaMemcpyAsync(s->U[n].as<float>() + old[n] * R, rows, cnt * 4, cudaMemcpyHostToDevice, st));
       ALTO_TRY_CUDA(cudaMemsetAsync(s->P[n].as<float>() + old[n] * R, 0, cnt * 4, st));
-      ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // host_rows is reused
     }
     s->dims[n] = nd;
   }
   uint64_t max_dim = 0;
   for (int n = 0; n < N; ++n) max_dim = std::max(max_dim, s->dims[n]);
-  ALTO_TRY(s->buf32.ensure(max_dim * R * 4));
+  ALTO_TRY(ensure_headroom(s->buf32, max_dim * R * 4));
   if (s->con != ALTO_UNCONSTRAINED) {  // the ADMM primal and aux between chunks
-    ALTO_TRY(s->aux.ensure(max_dim * R * 8));
-    ALTO_TRY(s->prim.ensure(max_dim * R * 8));
+    ALTO_TRY(ensure_headroom(s->aux, max_dim * R * 8));
+    ALTO_TRY(ensure_headroom(s->prim, max_dim * R * 8));
   }
-  ALTO_TRY(s->time64.ensure(s->dims[t] * R * 8));
+  ALTO_TRY(ensure_headroom(s->time64, s->dims[t] * R * 8));
+  s->t_grow += host_seconds() - t_grow0;
   double* G = s->G.as<double>();
   if (first) {
     ALTO_TRY(rr_op(s->lam.as<double>(), nullptr, R, 3, 0.0, st));
@@ -2149,7 +2174,9 @@ alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const doubl
     uint64_t bd[ALTO_MAX_MODES];
     for (int n = 0; n < N; ++n) bd[n] = s->dims[n];
     c.dims = bd;
+    const double t_enc0 = host_seconds();
     ALTO_TRY(encode_tensor(s->at, &c, 1, st));
+    s->t_encode += host_seconds() - t_enc0;
   }
 
   // first batch: 2-norm normalise the non-stream factors, lambda = 1
@@ -2233,7 +2260,9 @@ alto_status push_batch(alto_stream_session* s, const alto_coo* b, const double* 
   if (s->use_graph && stream_groupable(s)) {
     // the inner iterations as one launch of the session's own group graph,
     // captured once and relaunched for every batch
+    const double t_sort0 = host_seconds();
     ALTO_TRY(group_prepare_session(s));
+    s->t_sorted += host_seconds() - t_sort0;
     if (s->own_group && !group_fits(s->own_group, s)) {
       group_destroy(s->own_group);
       s->own_group = nullptr;
@@ -2589,7 +2618,7 @@ alto_status alto_stream_push(alto_stream_session* s, const alto_coo* batch, cons
   return push_batch(s, batch, init_vals, n_init, inner_iters);
 }
 
-alto_status alto_stream_stats(const alto_stream_session* s, double out[6]) {
+alto_status alto_stream_stats(const alto_stream_session* s, double out[9]) {
   if (!s || !out) {
     set_error("session or out is NULL");
     return ALTO_ERR_INVALID;
@@ -2600,6 +2629,9 @@ alto_status alto_stream_stats(const alto_stream_session* s, double out[6]) {
   out[3] = s->dev_inner_ms;
   out[4] = s->t_finish * 1e3;
   out[5] = (double)s->inner_total;
+  out[6] = s->t_grow * 1e3;
+  out[7] = s->t_encode * 1e3;
+  out[8] = s->t_sorted * 1e3;
   return ALTO_OK;
 }
 

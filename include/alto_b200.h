@@ -289,8 +289,10 @@ alto_status alto_stream_set_graph(alto_stream_session* s, int enable);
  * inner iterations' launch until their outcome is on the host; out[3]
  * device ms of the inner iterations (CUDA events around their launch);
  * out[4] host ms finishing (forgetting, copies, the time row out); out[5]
- * inner iterations. */
-alto_status alto_stream_stats(const alto_stream_session* s, double out[6]);
+ * inner iterations; parts of out[1]: out[6] host ms growing the model
+ * (reallocations, new rows), out[7] encoding the batch, out[8] building its
+ * row-sorted copies. */
+alto_status alto_stream_stats(const alto_stream_session* s, double out[9]);
 /* cpd_error(X, M), src/streaming_cpd.cpp:368-464: the relative residual
  * ||X - M|| / ||X|| of the session's current model (unit weights, as
  * cpd_error sets them) against a COO tensor X in the session's indexing
