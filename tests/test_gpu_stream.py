@@ -93,6 +93,31 @@ def test_graph_and_direct_launches_agree(nonneg):
         assert np.array_equal(a, c)
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_session_stats_account_for_every_push(graph):
+    """alto_stream_stats: the pushes and inner iterations it counts are those
+    the pushes returned, the preparation's parts fit inside the preparation,
+    and the inner iterations took device time."""
+    b = load_stream_fixture()[:4]
+    R = 8
+    iv = synth.init_values(20000, seed=6)
+    N = len(b[0]["dims"])
+    s = A.CPStream(N, 0, R, constraint=A.NONNEG, forgetting=0.95, max_inner=10, epsilon=1e-5)
+    s.set_graph(graph)
+    used, prev, inner = 0, np.zeros(N, np.int64), []
+    for x in b:
+        d = x["dims"].astype(np.int64)
+        need = int(np.sum(np.maximum(d - prev, 0))) * R
+        inner.append(s.push(x["dims"], x["cidx"], x["vals"], iv[used:used + need]))
+        used += need
+        prev = np.maximum(prev, d)
+    st = s.stats()
+    s.close()
+    assert st["pushes"] == len(b) and st["inner_iters"] == sum(inner)
+    assert st["inner_device_ms"] > 0 and st["inner_ms"] > 0 and st["finish_ms"] >= 0
+    assert st["grow_ms"] + st["encode_ms"] + st["sorted_copies_ms"] <= st["prepare_ms"] + 1e-6
+
+
 # ------------------------------------------------------------ spCP-stream
 
 def run_sparse(batches, R, max_iters, eps, iv, graph=True, constraint=A.UNCONSTRAINED):
