@@ -698,7 +698,7 @@ static alto_status finish_layout(alto_tensor* t, int nprtn, cudaStream_t st) {
     t->tile_nnz = tile;
   }
   t->ntiles = (uint32_t)((nnz + t->tile_nnz - 1) / t->tile_nnz);
-  ALTO_TRY(t->tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
+  ALTO_TRY(tensor_ensure(t, t->tile_iv, (size_t)std::max<uint32_t>(t->ntiles, 1) * N * 2 * 4));
   for (int m = 0; m < ALTO_MAX_MODES; ++m) {
     t->sorted[m].ready = false;
     t->tile_len_sorted[m].clear();
@@ -781,9 +781,9 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
 
   // capacity of the per-nonzero arrays
   uint64_t cap = std::max<uint64_t>(nnz, 1);
-  ALTO_TRY(t->line.ensure((cap + kLinePad) * rec_bytes(dec.hi_words)));
+  ALTO_TRY(tensor_ensure(t, t->line, (cap + kLinePad) * rec_bytes(dec.hi_words)));
   if (cap > t->cap || !t->perm.p) {
-    ALTO_TRY(t->perm.ensure(cap * 4));
+    ALTO_TRY(tensor_ensure(t, t->perm, cap * 4));
     t->cap = cap;
   }
 
@@ -800,7 +800,7 @@ alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaSt
   size_t o_cnt = off; off = align_up(off + radix_scratch_bytes(nnz), 256);
   size_t o_vals = off; off = align_up(off + (coo->on_device ? 0 : cap * vbytes), 256);
   size_t o_cidx = off; off = align_up(off + (coo->on_device ? 0 : cap * coo->index_bytes * N), 256);
-  ALTO_TRY(t->scratch.ensure(off));
+  ALTO_TRY(tensor_ensure(t, t->scratch, off));
   char* sb = t->scratch.as<char>();
   uint64_t* klo[2] = {(uint64_t*)(sb + o_lo0), (uint64_t*)(sb + o_lo1)};
   uint64_t* khi[2] = {two_words ? (uint64_t*)(sb + o_hi0) : nullptr,
@@ -986,7 +986,7 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   const int hw = t->dec.hi_words;
   // 3-mode copies store the rows decoded (same 16 bytes per record)
   s.hw = t->nmodes == 3 ? kDecoded3 : hw;
-  ALTO_TRY(s.line.ensure((nnz + kLinePad) * rec_bytes(s.hw)));
+  ALTO_TRY(tensor_ensure(t, s.line, (nnz + kLinePad) * rec_bytes(s.hw)));
   const size_t cap = std::max<uint64_t>(nnz, 1);
   size_t off = 0;
   size_t o_r0 = off; off = align_up(off + cap * 8, 256);
@@ -994,7 +994,7 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
   size_t o_p0 = off; off = align_up(off + cap * 4, 256);
   size_t o_p1 = off; off = align_up(off + cap * 4, 256);
   size_t o_cnt = off; off = align_up(off + radix_scratch_bytes(nnz), 256);
-  ALTO_TRY(t->scratch.ensure(off));
+  ALTO_TRY(tensor_ensure(t, t->scratch, off));
   char* sb = t->scratch.as<char>();
   uint64_t* rk[2] = {(uint64_t*)(sb + o_r0), (uint64_t*)(sb + o_r1)};
   uint32_t* pm[2] = {(uint32_t*)(sb + o_p0), (uint32_t*)(sb + o_p1)};
@@ -1017,7 +1017,7 @@ alto_status build_sorted_line(alto_tensor* t, int mode, cudaStream_t st) {
     ALTO_LAUNCHED();
   }
   s.ntiles = t->ntiles;
-  ALTO_TRY(s.tile_iv.ensure((size_t)std::max<uint32_t>(t->ntiles, 1) * t->nmodes * 2 * 4));
+  ALTO_TRY(tensor_ensure(t, s.tile_iv, (size_t)std::max<uint32_t>(t->ntiles, 1) * t->nmodes * 2 * 4));
   // (tile intervals are read only by shared-memory staging, which never
   // walks a sorted copy; the decoded copies carry none)
   if (t->ntiles && s.hw != kDecoded3) {

@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -288,6 +289,10 @@ struct alto_tensor {
   // synchronisation; only ALTO_MTTKRP_AUTO's rule reads it -- CP-stream
   // sessions, which always run the deterministic variant, skip it).
   bool tile_stats = true;
+  // Whether the per-nonzero buffers grow by half again past a request (a
+  // session's tensor, re-encoded slice after slice: slices of varying
+  // sizes then reallocate rarely).
+  bool grow = false;
 
   // Device error word of the kernels' bounded waits (0 = none).
   alto::DevBuf err;
@@ -303,6 +308,12 @@ struct alto_tensor {
 };
 
 namespace alto {
+// At least n bytes in b, with t->grow's headroom.
+inline alto_status tensor_ensure(const alto_tensor* t, DevBuf& b, size_t n) {
+  if (n <= b.bytes && b.p) return ALTO_OK;
+  return b.ensure(t->grow ? std::max(n, b.bytes + b.bytes / 2) : n);
+}
+
 // Encode (linearise, sort, lay out, partition) a COO tensor into t.
 alto_status encode_tensor(alto_tensor* t, const alto_coo* coo, int nprtn, cudaStream_t st);
 // Stable one-sweep LSD radix sort of (key, uint32 payload) pairs

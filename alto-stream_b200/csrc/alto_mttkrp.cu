@@ -1199,8 +1199,8 @@ alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, in
     return ALTO_ERR_UNSUPPORTED;
   }
   const uint64_t nslots = (uint64_t)a.ntiles * kMttkrpWarps * groups_per_warp(rank) * 2;
-  ALTO_TRY(t->det_rows.ensure(std::max<uint64_t>(nslots, 1) * 4));
-  ALTO_TRY(t->det_vals.ensure(std::max<uint64_t>(nslots, 1) * rank * 4));
+  ALTO_TRY(tensor_ensure(t, t->det_rows, std::max<uint64_t>(nslots, 1) * 4));
+  ALTO_TRY(tensor_ensure(t, t->det_vals, std::max<uint64_t>(nslots, 1) * rank * 4));
   // long chains: each has more than kShortChain slots; segments:
   // sum over chains of ceil(len / kChainSeg)
   const uint64_t max_chains = nslots / (kShortChain + 1) + 1;
@@ -1209,7 +1209,7 @@ alto_status det_prepare(alto_tensor* t, int mode, const void* const* factors, in
   const uint64_t o_chains = 256, o_segs = o_chains + up(max_chains * sizeof(uint4)),
                  o_part = o_segs + up(max_segs * sizeof(uint2)), bytes = o_part + max_segs * rank * 4;
   const size_t before = t->det_long.bytes;  // a new allocation starts with zero counters
-  ALTO_TRY(t->det_long.ensure(bytes));
+  ALTO_TRY(tensor_ensure(t, t->det_long, bytes));
   if (t->det_long.bytes != before) ALTO_TRY_CUDA(cudaMemsetAsync(t->det_long.p, 0, 16, st));
   a.det_rows = t->det_rows.as<uint32_t>();
   a.det_vals = t->det_vals.as<float>();

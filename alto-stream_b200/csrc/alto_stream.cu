@@ -2165,6 +2165,7 @@ alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const doubl
   if (!s->at) {
     s->at = new alto_tensor();
     s->at->tile_stats = false;
+    s->at->grow = true;
     s->at->key_bits = 128;
     s->at->stream_mode = t;
     s->at->stream = st;
