@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kMttkrpThreads, MINB)
     // row) is updated once per group and chunk rather than once per tile:
     // fewer float32 additions in the output, and fewer atomics
     using LW = LaneWidth<R>;
-    const uint32_t ct = a.chunk_tiles;
+    const uint32_t ct = a.chunk_tiles ? a.chunk_tiles : 1;
     const uint32_t nchunks = (a.ntiles + ct - 1) / ct;
     for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
       OpenRun<LW::V> run;

@@ -1171,19 +1171,21 @@ alto_status ensure_headroom(DevBuf& b, size_t n) {
   return b.ensure(std::max(n, b.bytes + b.bytes / 2));
 }
 
-alto_status grow_rows(DevBuf& b, uint64_t old_rows, uint64_t new_cap, size_t row_bytes, DevBuf& tmp,
-                      cudaStream_t st) {
+// b grown to new_cap rows keeping its first old_rows: the new buffer is
+// allocated first and the kept rows copied into it directly; the old one is
+// freed once the copy is done.
+alto_status grow_rows(DevBuf& b, uint64_t old_rows, uint64_t new_cap, size_t row_bytes, cudaStream_t st) {
   if (b.bytes >= new_cap * row_bytes && b.p) return ALTO_OK;
-  const size_t keep = old_rows * row_bytes;
+  const size_t keep = std::min<size_t>(old_rows * row_bytes, b.p ? b.bytes : 0);
+  DevBuf nb;
+  ALTO_TRY(nb.ensure(new_cap * row_bytes));
   if (keep) {
-    ALTO_TRY(ensure_headroom(tmp, keep));
-    ALTO_TRY_CUDA(cudaMemcpyAsync(tmp.p, b.p, keep, cudaMemcpyDeviceToDevice, st));
+    ALTO_TRY_CUDA(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, st));
+    ALTO_TRY_CUDA(cudaStreamSynchronize(st));  // (the old buffer is freed below)
   }
-  ALTO_TRY_CUDA(cudaStreamSynchronize(st));
-  b.release();
-  ALTO_TRY(b.ensure(new_cap * row_bytes));
-  if (keep) ALTO_TRY_CUDA(cudaMemcpyAsync(b.p, tmp.p, keep, cudaMemcpyDeviceToDevice, st));
-  return ALTO_OK;
+  std::swap(b.p, nb.p);
+  std::swap(b.bytes, nb.bytes);
+  return ALTO_OK;  // nb, now the old buffer, is released here
 }
 
 __global__ void lambda_from_gram_kernel(const double* __restrict__ G, int R, double* __restrict__ lam) {
@@ -2120,8 +2122,8 @@ alto_status prepare_batch(alto_stream_session* s, const alto_coo* b, const doubl
     const uint64_t nd = std::max<uint64_t>(b->dims[n], old[n]);
     if (nd > s->cap[n]) {
       const uint64_t nc = std::max<uint64_t>(nd, s->cap[n] + s->cap[n] / 2);
-      ALTO_TRY(grow_rows(s->U[n], old[n], nc, R * 4, s->copy_tmp, st));
-      ALTO_TRY(grow_rows(s->P[n], old[n], nc, R * 4, s->copy_tmp, st));
+      ALTO_TRY(grow_rows(s->U[n], old[n], nc, R * 4, st));
+      ALTO_TRY(grow_rows(s->P[n], old[n], nc, R * 4, st));
       s->dual[n].release();
       ALTO_TRY(s->dual[n].ensure(nc * R * 8));
       s->cap[n] = nc;
