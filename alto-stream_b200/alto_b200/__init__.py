@@ -38,6 +38,7 @@ F32, BF16, F64 = 0, 1, 2
 AUTO, ATOMIC, STAGED, STREAM, SORTED, DETERMINISTIC = range(6)
 FEED_BULK = 0x100  # OR with ATOMIC / SORTED: line streamed through shared memory by bulk copy
 FEED_DENSE = 0x200  # OR with SORTED (3 modes): the walk compiled for five blocks per SM
+FEED_FIXED_TARGET = 0x400  # OR with SORTED (3 modes): as FEED_DENSE, compiled once per target mode
 UNCONSTRAINED, NONNEG, LASSO = range(3)
 CPSTREAM, SPCPSTREAM = range(2)  # streaming models (alto_stream_set_model)
 FIT_REFERENCE, FIT_EXACT = 0, 1

@@ -353,16 +353,17 @@ alto_status alto_mttkrp_variant_run(alto_tensor* t, int mode, const void* const*
   ALTO_TRY(check_mttkrp(t, mode, factors, fdtype, rank, out));
   const int bulk = ((int)variant & ALTO_MTTKRP_FEED_BULK) ? 1 : 0;
   const int dense = ((int)variant & ALTO_MTTKRP_FEED_DENSE) ? 1 : 0;
-  const alto_mttkrp_variant v =
-      (alto_mttkrp_variant)((int)variant & ~(ALTO_MTTKRP_FEED_BULK | ALTO_MTTKRP_FEED_DENSE));
-  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_DETERMINISTIC || (bulk && dense) ||
+  const int fixed = ((int)variant & ALTO_MTTKRP_FEED_FIXED_TARGET) ? 1 : 0;
+  const alto_mttkrp_variant v = (alto_mttkrp_variant)(
+      (int)variant & ~(ALTO_MTTKRP_FEED_BULK | ALTO_MTTKRP_FEED_DENSE | ALTO_MTTKRP_FEED_FIXED_TARGET));
+  if (v < ALTO_MTTKRP_AUTO || v > ALTO_MTTKRP_DETERMINISTIC || bulk + dense + fixed > 1 ||
       (bulk && v != ALTO_MTTKRP_ATOMIC && v != ALTO_MTTKRP_SORTED) ||
-      (dense && (v != ALTO_MTTKRP_SORTED || t->nmodes != 3))) {
+      ((dense || fixed) && (v != ALTO_MTTKRP_SORTED || t->nmodes != 3))) {
     set_error("unknown variant %d", (int)variant);
     return ALTO_ERR_INVALID;
   }
   return run_mttkrp_feed(t, mode, factors, fdtype, rank, out, accumulate, v,
-                         v == ALTO_MTTKRP_AUTO ? -1 : (dense ? 2 : bulk), (cudaStream_t)stream);
+                         v == ALTO_MTTKRP_AUTO ? -1 : (fixed ? 3 : dense ? 2 : bulk), (cudaStream_t)stream);
 }
 
 alto_status alto_mttkrp_autotune(alto_tensor* t, const void* const* factors, alto_dtype fdtype,

@@ -244,7 +244,8 @@ struct SortedLine {
 struct TuneEntry {
   int mode, rank, fdtype;
   alto_mttkrp_variant variant;
-  int feed;  // 0 direct, 1 line streamed through shared memory by bulk copy, 2 direct at five blocks per SM
+  int feed;  // 0 direct, 1 line streamed through shared memory by bulk copy, 2 direct at five blocks per SM,
+             // 3 as 2 with the target mode fixed at compile time
 };
 }  // namespace alto
 

@@ -208,11 +208,16 @@ struct OpenRun {
   float acc[V];
 };
 
-template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool CARRY = false>
+// TGT >= 0 (decoded 3-mode records only) fixes the target mode at compile
+// time: the target and input rows are then fixed words of the record and the
+// input factors fixed arguments, with no per-nonzero selects or mode checks.
+template <int R, typename FT, int HW, int NM, bool SMEM, bool DET = false, bool CARRY = false, int TGT = -1>
 __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line, uint32_t ws, uint32_t we,
                                            bool staged, float* smem, uint32_t iv_start, uint32_t sr_base = 0,
                                            OpenRun<LaneWidth<R>::V>* carry = nullptr) {
+  static_assert(TGT < 0 || (HW == kDecoded3 && NM == 3), "a compile-time target needs decoded 3-mode records");
   using LW = LaneWidth<R>;
+  const int target = TGT >= 0 ? TGT : a.target;
   constexpr int V = LW::V, G = LW::G, NPW = LW::NPW;
   // nonzeros per step: 2 for 3 modes (4 measured faster for DET only), 1
   // beyond (two measured 30% slower on the rank-64 5-mode tensor: its four
@@ -252,8 +257,8 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
     for (int u = 0; u < U; ++u) {
 #pragma unroll
       for (int j = 0; j < NM - 1; ++j) {
-        const int m = j < a.target ? j : j + 1;
-        if (m < a.dec.nmodes && valid[u]) {
+        const int m = j < target ? j : j + 1;
+        if ((TGT >= 0 || m < a.dec.nmodes) && valid[u]) {
           const uint32_t r = rec_row<HW>(w[u], a.dec, m);
           load_row<FT, V, G>(a.fac.f[m], (size_t)r * R, sub, f[u][j]);
         }
@@ -264,7 +269,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
     bool ok[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      rows[u] = rec_row<HW>(w[u], a.dec, a.target);
+      rows[u] = rec_row<HW>(w[u], a.dec, target);
       vals[u] = v[u];
       ok[u] = valid[u];
     }
@@ -363,7 +368,7 @@ __device__ __forceinline__ void warp_range(const MttkrpArgs& a, const void* line
   }
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, int MINB = 3>
+template <int R, typename FT, int HW, bool STAGE, int NM, bool DET = false, int MINB = 3, int TGT = -1>
 __global__ void __launch_bounds__(kMttkrpThreads, MINB)
     mttkrp_tile_kernel(const MttkrpArgs a) {
   extern __shared__ float4 smem4[];
@@ -391,7 +396,7 @@ __global__ void __launch_bounds__(kMttkrpThreads, MINB)
         const uint32_t chunk = (te - ts + kMttkrpWarps - 1) / kMttkrpWarps;
         const uint32_t ws = min(ts + warp * chunk, te);
         const uint32_t we = min(ws + chunk, te);
-        warp_range<R, FT, HW, NM, false, false, true>(a, a.line, ws, we, false, smem, 0, 0, &run);
+        warp_range<R, FT, HW, NM, false, false, true, TGT>(a, a.line, ws, we, false, smem, 0, 0, &run);
       }
       if (run.row != kNoRow)
         flush_row<R, LW::V, LW::G>(false, smem, 0, a.out, run.row, (threadIdx.x & 31) % LW::G, run.acc);
@@ -899,7 +904,7 @@ static uint32_t chunk_tiles_for(uint32_t ntiles, unsigned grid) {
   return c;
 }
 
-template <int R, typename FT, int HW, bool STAGE, int NM, int MINB = 3>
+template <int R, typename FT, int HW, bool STAGE, int NM, int MINB = 3, int TGT = -1>
 static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   MttkrpArgs b = a;
   b.stage_rows = STAGE ? kStageBytes / (R * 4) : 0;
@@ -907,19 +912,19 @@ static alto_status launch_tile(const MttkrpArgs& a, cudaStream_t st) {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     if (STAGE)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB, TGT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
     else  // no shared memory: all of the unified L1 / shared storage as L1 (factor rows hit it)
-      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>,
+      ALTO_TRY_CUDA(cudaFuncSetAttribute(mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB, TGT>,
                                          cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     ALTO_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB>, kMttkrpThreads, smem));
+        &blocks_per_sm, mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB, TGT>, kMttkrpThreads, smem));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   unsigned grid = std::min<unsigned>(a.ntiles, (unsigned)(num_sms() * blocks_per_sm));
   if (!grid) return ALTO_OK;
   b.chunk_tiles = chunk_tiles_for(a.ntiles, grid);
-  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB><<<grid, kMttkrpThreads, smem, st>>>(b);
+  mttkrp_tile_kernel<R, FT, HW, STAGE, NM, false, MINB, TGT><<<grid, kMttkrpThreads, smem, st>>>(b);
   ALTO_LAUNCHED();
   return ALTO_OK;
 }
@@ -1013,6 +1018,13 @@ template <int R, typename FT, int HW>
 static alto_status launch_modes(const MttkrpArgs& a, bool stage, bool bulk_feed, int dense, int* err,
                                 cudaStream_t st) {
   if constexpr (HW == kDecoded3) {  // sorted 3-mode copies: no staging
+    if (dense == 2 && !bulk_feed) {  // the target mode fixed at compile time
+      switch (a.target) {
+        case 0: return launch_tile<R, FT, HW, false, 3, 5, 0>(a, st);
+        case 1: return launch_tile<R, FT, HW, false, 3, 5, 1>(a, st);
+        default: return launch_tile<R, FT, HW, false, 3, 5, 2>(a, st);
+      }
+    }
     if (dense && !bulk_feed) return launch_tile<R, FT, HW, false, 3, 5>(a, st);
     return bulk_feed ? launch_tma<R, FT, HW, 3>(a, err, st) : launch_tile<R, FT, HW, false, 3>(a, st);
   } else {
@@ -1095,8 +1107,9 @@ alto_status run_mttkrp(alto_tensor* t, int mode, const void* const* factors, alt
 
 // feed: 1 streams the line through shared memory by bulk copy, 0 loads it
 // directly, 2 loads it directly with five blocks per SM (decoded 3-mode
-// copies: at most 48 registers a thread; six, at 40, measured slower), -1
-// uses the autotuned choice (direct when untuned).
+// copies: at most 48 registers a thread; six, at 40, measured slower), 3 as
+// 2 with the target mode fixed at compile time, -1 uses the autotuned choice
+// (direct when untuned).
 alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors, alto_dtype fdtype,
                             int rank, float* out, int accumulate, alto_mttkrp_variant variant, int feed,
                             cudaStream_t st) {
@@ -1150,7 +1163,7 @@ alto_status run_mttkrp_feed(alto_tensor* t, int mode, const void* const* factors
   ALTO_TRY(ensure_error_words(t, st));
   int* err = t->err.as<int>();
   const bool bulk = feed == 1;
-  const int dense = feed == 2 ? 1 : 0;
+  const int dense = feed == 2 ? 1 : feed == 3 ? 2 : 0;
   if (fdtype == ALTO_BF16) {
     if (hw == 0) return launch_rank<__nv_bfloat16, 0>(a, rank, stage, bulk, 0, aligned, err, st);
     if (hw == 1) return launch_rank<__nv_bfloat16, 1>(a, rank, stage, bulk, 0, aligned, err, st);
@@ -1296,7 +1309,8 @@ alto_status autotune(alto_tensor* t, const void* const* factors, alto_dtype fdty
       int feed;
     };
     const Cand cands[] = {{ALTO_MTTKRP_ATOMIC, 0}, {ALTO_MTTKRP_ATOMIC, 1}, {ALTO_MTTKRP_STAGED, 0},
-                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2}};
+                          {ALTO_MTTKRP_SORTED, 0}, {ALTO_MTTKRP_SORTED, 1}, {ALTO_MTTKRP_SORTED, 2},
+                          {ALTO_MTTKRP_SORTED, 3}};
     alto_mttkrp_variant best = ALTO_MTTKRP_ATOMIC;
     int best_feed = 0;
     float best_ms = 1e30f;

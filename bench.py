@@ -547,6 +547,13 @@ def ours(args):
     # the ALTO line itself (vector atomics, no row-sorted copy), per mode
     line_ms = [round(timed(lambda: tens[m].mttkrp(m, factors, R, out=outs[m], variant=A.ATOMIC, stream=stream), 3),
                      4) for m in range(N)]
+    # the row-sorted walks the autotuner chooses among, per mode (3-mode tensors)
+    feed_ms = None
+    if N == 3:
+        feed_ms = {name: [round(timed(lambda: tens[m].mttkrp(m, factors, R, out=outs[m], variant=A.SORTED | f,
+                                                               stream=stream), 3), 4) for m in range(N)]
+                   for name, f in (("four_blocks", 0), ("five_blocks", A.FEED_DENSE),
+                                   ("five_blocks_fixed_target", A.FEED_FIXED_TARGET))}
     # error against float64 sums from the generated COO, on the last timed step's outputs
     err = None
     if not sharded:
@@ -630,9 +637,10 @@ def ours(args):
                        "variants": [vnames.get(v, str(v)) for v in variants],
                        "row_sorted_copies": {
                            "bytes": sorted_bytes, "build_ms_per_mode": sorted_build_ms,
-                           "order": "per mode: output row, then the row of the shorter other mode, then "
-                                    "ALTO order; built once, outside the timed region"},
+                           "order": "per mode: output row, ALTO order kept among equal rows (stable LSD "
+                                    "sort on the row); built once, outside the timed region"},
                        "alto_line_atomic_ms_per_mode": line_ms,
+                       "row_sorted_walks_ms_per_mode": feed_ms,
                        "alto_encode": encode,
                        "device_bytes": sum(x.device_bytes() for x in set(tens))},
             "error_vs_fp64": err,

@@ -65,6 +65,10 @@ typedef enum {
  * five resident blocks per SM (at most 48 registers a thread) instead of
  * four (the autotuner tries it). */
 #define ALTO_MTTKRP_FEED_DENSE 0x200
+/* OR-ed into SORTED on a 3-mode tensor: the five-blocks walk compiled once
+ * per target mode, so the rows of the decoded records need no per-nonzero
+ * mode selection (the autotuner tries it). */
+#define ALTO_MTTKRP_FEED_FIXED_TARGET 0x400
 
 /* Constraint of the CP-stream factor solves (src/constraints.cpp:39-66; the
  * reference projects LASSO onto the non-negative orthant too). */

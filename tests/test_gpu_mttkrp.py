@@ -15,6 +15,8 @@ from conftest import FIXTURE_NAMES, load_fixture
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
 ALL_VARIANTS = (A.AUTO, A.ATOMIC, A.STAGED, A.SORTED, A.ATOMIC | A.FEED_BULK, A.SORTED | A.FEED_BULK)
+# the row-sorted walks that exist for 3-mode tensors only
+THREE_MODE_FEEDS = (A.SORTED | A.FEED_DENSE, A.SORTED | A.FEED_FIXED_TARGET)
 
 
 def to_dev(F, dtype):
@@ -46,7 +48,8 @@ def check_modes(dims, cidx, vals, R, variants=(A.AUTO,), dtype=None, seed=0):
         fs = [f.copy() for f in Fo]
         fs[m][:] = 0
         ref = O.mttkrp(enc, m, fs, R)[m]
-        for v in variants:
+        extra = THREE_MODE_FEEDS if len(dims) == 3 and A.SORTED in variants else ()
+        for v in tuple(variants) + extra:
             out = t.mttkrp(m, Fd, R, variant=v).cpu().numpy()
             assert rel_err(out, ref) <= TOL, (m, v, rel_err(out, ref))
 
