@@ -647,6 +647,7 @@ def ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                         "traffic_captured_on": traffic.get("kernel") if traffic else None,
                          "per_mode_ms": [round(dt * 1e3, 4) for _, dt, _ in per_mode],
                          "algorithmic_bytes_per_mode": [b for _, _, b in per_mode]},
             "cpu_baseline": cpu,
