@@ -34,6 +34,19 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, name), name
 
 
+def test_mirror_constants_match_the_header():
+    """The Python mirror's variant, feed, dtype and constraint values are
+    the header's (a mismatch would run a different kernel than asked for)."""
+    text = open(HEADER).read()
+    defines = {k: int(v, 0) for k, v in re.findall(r"#define\s+(ALTO_[A-Z0-9_]+)\s+(0x[0-9a-fA-F]+|\d+)", text)}
+    for name in ("FEED_BULK", "FEED_DENSE", "FEED_FIXED_TARGET"):
+        assert getattr(A, name) == defines["ALTO_MTTKRP_" + name], name
+    enums = {k: int(v) for k, v in re.findall(r"\b(ALTO_[A-Z0-9_]+)\s*=\s*(\d+)", text)}
+    for name in ("AUTO", "ATOMIC", "STAGED", "STREAM", "SORTED", "DETERMINISTIC"):
+        assert getattr(A, name) == enums["ALTO_MTTKRP_" + name], name
+    assert A.F32 == enums["ALTO_F32"] and A.BF16 == enums["ALTO_BF16"]
+
+
 def test_status_strings_and_version():
     L = A.lib()
     assert L.alto_version() == 100
