@@ -148,6 +148,33 @@ class TestAgainstCompiledReference:
                 assert np.array_equal(e["intervals"], o["intervals"])
                 t.close()
 
+    def test_mttkrp_random_power_law_and_five_modes(self):
+        """The oracle's MTTKRP (float64) against the reference's
+        mttkrp_alto_par (include/alto.hpp:826-908 and the variant it picks)
+        on a Zipf 3-mode tensor with a 65-bit key (the 128-bit build) and a
+        5-mode tensor, every mode, at several partition counts.  The
+        reference sums in a thread-dependent order, so the bound is
+        normwise 1e-12."""
+        cases = [(np.array([4800000, 1800000, 1800000], np.uint64), 40000, [1.2, 1.2, 1.2], 32),
+                 (np.array([100000, 100000, 10000, 1000, 100], np.uint64), 30000, [1.1, 1.1, None, None, None], 16)]
+        for k, (dims, nnz, zipf, R) in enumerate(cases):
+            cidx, vals = synth.powerlaw_coo(dims, nnz, zipf, seed=11 + k)
+            rng = np.random.default_rng(k)
+            F = [rng.uniform(-1, 1, (int(d), R)) for d in dims]
+            enc = O.build(dims, cidx, vals)
+            for P in (1, 7):
+                t = O.RefTensor(dims, cidx, vals, P)
+                for m in range(len(dims)):
+                    fs = [f.copy() for f in F]
+                    fs[m][:] = 0
+                    ref = t.mttkrp(m, fs, R)[m]
+                    fo = [f.copy() for f in F]
+                    fo[m][:] = 0
+                    out = O.mttkrp(enc, m, fo, R)[m]
+                    err = np.abs(out - ref).max() / np.abs(ref).max()
+                    assert err <= 1e-12, (k, P, m, err)
+                t.close()
+
     def test_cpd_als_random(self):
         dims = np.array([30, 40, 50], np.uint64)
         cidx, vals = synth.uniform_coo(dims, 3000, seed=1)
