@@ -337,7 +337,7 @@ def reference_arm(args):
         n, seed, same = args.cpu_sample, 2024, False
     try:
         sec, threads, nnz, avail = time_reference_cpu(n, args.rank, max(args.steps, 1), seed=seed)
-    except Exception as e:  # the checker library is missing or failed to load
+    except Exception as e:  # the compiled reference (oracle/_ref) is missing or failed to load
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref could not run: {e}"}))
         return 0
     units = nnz * args.rank * len(DIMS)

@@ -1,7 +1,7 @@
 /* ALTO oracle: a plain-C, single-threaded, FP64 restatement of the reference
  * algorithm for the hot path (jeewhanchoi/ALTO-stream).
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA path is
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is
  * compared against; only tests/, __graft_entry__.smoke() and bench.py's
  * cpu_baseline leg load it (through oracle/oracle.py).  The product library
  * never links it and has no CPU fallback.

@@ -1,9 +1,9 @@
 """ctypes wrappers for the ALTO oracle (test infrastructure only).
 
-Two checkers live here:
+Two test libraries are wrapped here:
 
 * ``liboracle.so`` -- the single-threaded FP64 C restatement of the reference
-  algorithm (``oracle/alto_oracle.c``), the checker the CUDA path's parity
+  algorithm (``oracle/alto_oracle.c``), the oracle the CUDA path's parity
   tests compare against;
 * ``_ref/libaltoref{64,128}.so`` -- the reference implementation itself,
   compiled from its own sources by ``oracle/ref/Makefile`` and driven by

@@ -1,7 +1,7 @@
 // Test infrastructure only: a thin C-callable harness around the reference
 // implementation of ALTO (jeewhanchoi/ALTO-stream), compiled from the
 // reference's own, unmodified sources by oracle/ref/Makefile into
-// oracle/_ref/libaltoref{64,128}.so.  It is the checker that pins the C
+// oracle/_ref/libaltoref{64,128}.so.  It is the compiled reference that pins the C
 // restatement in oracle/alto_oracle.c and the timed CPU baseline of bench.py;
 // nothing in the product links or loads it.
 //

@@ -1,1 +1,1 @@
-/* Empty stand-in: the checker build never calls libnuma. */
+/* Empty stand-in: the compiled-reference build never calls libnuma. */

@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run here, where the reference sources exist (the GPU box has no copy):
+Run where the reference sources exist (the machines that run the GPU tests
+have no copy):
 
     make -C oracle ref REF=<reference dir>   # oracle/_ref/libaltoref{64,128}.so
     python tests/golden/make_golden.py [path-to-reference]

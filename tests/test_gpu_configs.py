@@ -5,11 +5,11 @@ holds -- so each bound below is the end-to-end error of the device path, not
 only of its accumulation.
 
   * CP-ALS on 1000^3 with 1,000,000 uniform nonzeros, rank 16, 20
-    iterations, plus 100 standalone mode-0 MTTKRPs (the configuration at its
+    iterations, plus 100 standalone mode-0 MTTKRPs (that workload at its
     full size).
   * CP-ALS at rank 64 on the 5-mode shape 100k x 100k x 10k x 1k x 100 with
     Zipf(1.1) on modes 0-1 and uniform values, with float32 and with bfloat16
-    factor storage (2,000,000 nonzeros against the configuration's 50M: the
+    factor storage (2,000,000 nonzeros against the workload's 50M: the
     oracle is single-threaded).
   * The bfloat16 MTTKRP's error against the oracle given the original
     float32 factors (what halving the gather bytes costs).
