@@ -2,6 +2,7 @@
 vectors that the compiled reference produced (tests/golden/make_golden.py),
 and against the compiled reference itself when oracle/_ref is built."""
 import hashlib
+import os
 
 import numpy as np
 import pytest
@@ -174,6 +175,35 @@ class TestAgainstCompiledReference:
                     err = np.abs(out - ref).max() / np.abs(ref).max()
                     assert err <= 1e-12, (k, P, m, err)
                 t.close()
+
+    @pytest.mark.parametrize("nonneg", [0, 1])
+    def test_cpstream_random_slices(self, nonneg):
+        """The oracle's CP-stream against the reference's cpstream
+        (src/streaming_cpd.cpp:26-366, 1198-1519) on four random slices
+        drawn like the CP-stream workload (Zipf 1.1 coordinates with
+        first-seen labels, Poisson(3) values) at a reduced size, rank 8, ten
+        inner iterations at most, forgetting 0.99 (the reference's fixed
+        value); the reference single-threaded.  Bound: 1e-10 normwise per
+        factor, identical lambda."""
+        space = [3000, 3000, 500]
+        b = synth.stream_batches(space, 4, lambda rng, s: int(np.clip(rng.lognormal(np.log(4000), 0.5), 1500, 12000)),
+                                 [1.1, 1.1, 1.1], seed=5, values="poisson3")
+        R, need, prev = 8, 0, np.zeros(4, np.int64)
+        for x in b:
+            d = x["dims"].astype(np.int64)
+            need += int(np.sum(np.maximum(d - prev, 0))) * R
+            prev = np.maximum(prev, d)
+        iv = synth.init_values(need, seed=9)
+        L = O.ref_lib(64)
+        L.ref_set_threads(1)
+        try:
+            outs, lam, inner = O.cpstream(b, 0, R, 10, 1e-5, nonneg, iv)
+            routs, rlam, _ = O.ref_cpstream(b, 0, R, 10, 1e-5, nonneg, iv)
+        finally:
+            L.ref_set_threads(os.cpu_count() or 1)
+        for o, r in zip(outs, routs):
+            assert np.abs(o - r).max() <= 1e-10 * np.abs(r).max()
+        np.testing.assert_allclose(lam, rlam, rtol=1e-12)
 
     def test_cpd_als_random(self):
         dims = np.array([30, 40, 50], np.uint64)
