@@ -205,6 +205,32 @@ class TestAgainstCompiledReference:
             assert np.abs(o - r).max() <= 1e-10 * np.abs(r).max()
         np.testing.assert_allclose(lam, rlam, rtol=1e-12)
 
+    def test_spcpstream_random_slices(self):
+        """The oracle's spCP-stream against the reference's
+        spcpstream_alto_iter (src/streaming_cpd.cpp:466-1085) on four random
+        slices of the CP-stream workload's distribution at a reduced size,
+        rank 8, the reference single-threaded.  Bound: 1e-10 normwise per
+        factor, identical lambda."""
+        space = [3000, 3000, 500]
+        b = synth.stream_batches(space, 4, lambda rng, s: int(np.clip(rng.lognormal(np.log(4000), 0.5), 1500, 12000)),
+                                 [1.1, 1.1, 1.1], seed=6, values="poisson3")
+        R, need, prev = 8, 0, np.zeros(4, np.int64)
+        for x in b:
+            d = x["dims"].astype(np.int64)
+            need += int(np.sum(np.maximum(d - prev, 0))) * R
+            prev = np.maximum(prev, d)
+        iv = synth.init_values(need, seed=10)
+        L = O.ref_lib(64)
+        L.ref_set_threads(1)
+        try:
+            outs, lam, inner = O.spcpstream(b, 0, R, 10, 1e-5, iv)
+            routs, rlam, _ = O.ref_spcpstream(b, 0, R, 10, 1e-5, iv)
+        finally:
+            L.ref_set_threads(os.cpu_count() or 1)
+        for o, r in zip(outs, routs):
+            assert np.abs(o - r).max() <= 1e-10 * np.abs(r).max()
+        np.testing.assert_allclose(lam, rlam, rtol=1e-12)
+
     def test_cpd_als_random(self):
         dims = np.array([30, 40, 50], np.uint64)
         cidx, vals = synth.uniform_coo(dims, 3000, seed=1)
