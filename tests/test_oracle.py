@@ -231,6 +231,36 @@ class TestAgainstCompiledReference:
             assert np.abs(o - r).max() <= 1e-10 * np.abs(r).max()
         np.testing.assert_allclose(lam, rlam, rtol=1e-12)
 
+    @pytest.mark.parametrize("dims,zipf,R", [([65537, 65539, 65541, 70000], [1.2, 1.2, 1.2, None], 16),
+                                             ([2000, 2000, 300, 50, 10], [1.1, 1.1, None, None, None], 10)],
+                             ids=["128bit-4mode-r16", "5mode-r10"])
+    def test_cpd_als_wide_keys_and_runtime_rank(self, dims, zipf, R):
+        """The oracle's CP-ALS against the reference's cpd_alto
+        (include/cpd.hpp:47-191) on a 4-mode tensor with a 68-bit key (the
+        128-bit build) at a specialised rank and a 5-mode tensor at a
+        runtime rank (10, outside the reference's 8/16/100 specialisers);
+        six iterations, the reference single-threaded."""
+        dims = np.array(dims, np.uint64)
+        cidx, vals = synth.powerlaw_coo(dims, 20000, zipf, seed=3)
+        init = synth.init_values(int(dims.sum()) * R, seed=4)
+        U0, off = [], 0
+        for d in dims:
+            U0.append(init[off:off + int(d) * R].reshape(int(d), R))
+            off += int(d) * R
+        t = O.RefTensor(dims, cidx, vals, 4)
+        L = O.ref_lib(t.bits)
+        L.ref_set_threads(1)
+        try:
+            Ur, lr, fr, itr = t.cpd_als(U0, np.ones(R), R, 6, 1e-12)
+        finally:
+            L.ref_set_threads(os.cpu_count() or 1)
+            t.close()
+        Uo, lo, fo, ito = O.cpd_als(O.build(dims, cidx, vals), U0, np.ones(R), R, 6, 1e-12)
+        assert itr == ito
+        np.testing.assert_allclose(fo, fr, rtol=1e-12)
+        for a, b in zip(Ur, Uo):
+            assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
     def test_cpd_als_random(self):
         dims = np.array([30, 40, 50], np.uint64)
         cidx, vals = synth.uniform_coo(dims, 3000, seed=1)
