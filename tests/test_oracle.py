@@ -261,6 +261,26 @@ class TestAgainstCompiledReference:
         for a, b in zip(Ur, Uo):
             assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
 
+    def test_slicer_random_power_law(self):
+        """The slicer restatement against the reference's
+        StreamingSparseTensor (src/streaming_sptensor.cpp:69-327) on a
+        tensor shaped like the CP-stream workload (a uniform time mode of 60
+        steps, Zipf 1.1 on the other three, Poisson(3) values), whole
+        batches compared: dims, every index and value.  The time mode is
+        uniform so that no step is empty: the reference asserts on an empty
+        step."""
+        dims = np.array([60, 3000, 3000, 500], np.uint64)
+        cidx, vals = synth.powerlaw_coo(dims, 30000, [None, 1.1, 1.1, 1.1], seed=8, values="poisson3")
+        assert len(np.unique(cidx[0])) == 60
+        for thr, lim in [(1, 1), (2000, 5), (1, 7)]:
+            a = O.slice_stream(dims, cidx, vals, 0, thr, lim)
+            b = O.ref_slice_stream(dims, cidx, vals, 0, thr, lim)
+            assert len(a) == len(b)
+            for x, y in zip(a, b):
+                assert np.array_equal(x["dims"], y["dims"])
+                assert np.array_equal(x["cidx"], y["cidx"])
+                assert np.array_equal(x["vals"], y["vals"])
+
     def test_cpd_als_random(self):
         dims = np.array([30, 40, 50], np.uint64)
         cidx, vals = synth.uniform_coo(dims, 3000, seed=1)
